@@ -1,0 +1,490 @@
+// Krylov drivers on the device (FP64): preconditioned CG and restarted,
+// right-preconditioned GMRES(m).  They stand in for Krylov.jl's CG/GMRES,
+// which the reference reaches through LinearSolve.jl (Pl = P,
+// test/test_preconditioners.jl:65,93) and which calls ldiv!(y, P, x) once per
+// iteration.
+//
+// PCG keeps every scalar on the device.  One iteration (SpMV + fused dot,
+// alpha, x/r update + fused norm, convergence test, M^-1 r, r.z, beta, p
+// update) is captured once as a CUDA graph and replayed in batches; the
+// convergence test freezes x and r on the iteration that meets
+// ||r|| <= rtol ||b||, so replaying past convergence changes nothing and the
+// reported iteration count is the first one that met the test.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "reduce.cuh"
+
+namespace hs {
+int matrix_spmv(const hs_matrix* M, const void* x, void* y, double alpha, double beta, cudaStream_t st);
+int matrix_n(const hs_matrix* M);
+int cheb_apply(hs_cheb* S, const void* r, void* z, int io, cudaStream_t st);
+}  // namespace hs
+
+namespace {
+
+constexpr int kT = 256;
+
+struct PcgScalars {
+    double bb, rr, rz, pq, alpha, beta, tol2;
+    int done, it, conv_it, pad;
+};
+
+inline int grid_elems(int64_t n) {
+    const int64_t b = (n + kT - 1) / kT;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(b, (int64_t)hs::num_sms() * 8));
+}
+
+__global__ void copy_kernel(int64_t n, const double* __restrict__ a, double* __restrict__ b) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        b[i] = a[i];
+}
+
+__global__ void zero_kernel(int64_t n, double* __restrict__ a) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        a[i] = 0.0;
+}
+
+// partial sums of a.b
+__global__ void dot_kernel(int64_t n, const double* __restrict__ a, const double* __restrict__ b,
+                           double* __restrict__ partials) {
+    double v = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        v += a[i] * b[i];
+    v = hsdev::block_sum(v);
+    if (threadIdx.x == 0) partials[blockIdx.x] = v;
+}
+
+__device__ __forceinline__ double sum_partials(const double* __restrict__ partials, int nb) {
+    double v = 0.0;
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) v += partials[i];
+    return hsdev::block_sum(v);
+}
+
+__global__ void pcg_init_scalars(const double* __restrict__ partials_bb, const double* __restrict__ partials_rz,
+                                 int nb, PcgScalars* s, double rtol) {
+    const double bb = sum_partials(partials_bb, nb);
+    __syncthreads();
+    const double rz = sum_partials(partials_rz, nb);
+    if (threadIdx.x == 0) {
+        s->bb = bb;
+        s->rr = bb;
+        s->rz = rz;
+        s->tol2 = rtol * rtol * bb;
+        s->done = (bb == 0.0);
+        s->it = 0;
+        s->conv_it = s->done ? 0 : -1;
+    }
+}
+
+__global__ void pcg_alpha(const double* __restrict__ partials, int nb, PcgScalars* s) {
+    const double pq = sum_partials(partials, nb);
+    if (threadIdx.x == 0) {
+        s->pq = pq;
+        s->alpha = s->rz / pq;
+    }
+}
+
+// x += alpha p; r -= alpha q; partial r.r   (skipped once converged)
+__global__ void pcg_update(int64_t n, const PcgScalars* __restrict__ s, const double* __restrict__ p,
+                           const double* __restrict__ q, double* __restrict__ x, double* __restrict__ r,
+                           double* __restrict__ partials) {
+    const bool done = s->done;
+    const double alpha = s->alpha;
+    double v = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double ri = r[i];
+        if (!done) {
+            x[i] += alpha * p[i];
+            ri -= alpha * q[i];
+            r[i] = ri;
+        }
+        v += ri * ri;
+    }
+    v = hsdev::block_sum(v);
+    if (threadIdx.x == 0) partials[blockIdx.x] = v;
+}
+
+__global__ void pcg_check(const double* __restrict__ partials, int nb, PcgScalars* s) {
+    const double rr = sum_partials(partials, nb);
+    if (threadIdx.x == 0) {
+        if (!s->done) {
+            s->it += 1;
+            s->rr = rr;
+            if (rr <= s->tol2) {
+                s->done = 1;
+                s->conv_it = s->it;
+            }
+        }
+    }
+}
+
+__global__ void pcg_beta(const double* __restrict__ partials, int nb, PcgScalars* s) {
+    const double rz = sum_partials(partials, nb);
+    if (threadIdx.x == 0 && !s->done) {
+        s->beta = rz / s->rz;
+        s->rz = rz;
+    }
+}
+
+__global__ void pcg_p(int64_t n, const PcgScalars* __restrict__ s, const double* __restrict__ z, double* __restrict__ p) {
+    if (s->done) return;
+    const double beta = s->beta;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        p[i] = z[i] + beta * p[i];
+}
+
+// q = A p fused with p.q partials (CSR scalar row loop; FP64)
+struct MatView {
+    int32_t n;
+    const int32_t* rp;
+    const int32_t* ci;
+    const double* v;
+};
+
+int prec_apply(int type, void* prec, const double* r, double* z, int64_t n, cudaStream_t st) {
+    if (type == HS_PREC_L1GS) return hs_l1gs_apply(static_cast<hs_l1gs*>(prec), r, z, HS_F64, st);
+    if (type == HS_PREC_CHEB) return hs::cheb_apply(static_cast<hs_cheb*>(prec), r, z, HS_F64, st);
+    copy_kernel<<<grid_elems(n), kT, 0, st>>>(n, r, z);
+    HS_LAUNCH_CHECK("copy_kernel");
+    return HS_OK;
+}
+
+struct DevBuf {
+    std::vector<void*> ptrs;
+    ~DevBuf() {
+        for (void* p : ptrs) cudaFree(p);
+    }
+    template <typename T>
+    int alloc(T** p, size_t bytes) {
+        cudaError_t e = cudaMalloc((void**)p, bytes ? bytes : 8);
+        if (e != cudaSuccess) return hs::cuda_error(e, "cudaMalloc (krylov)");
+        ptrs.push_back(*p);
+        return HS_OK;
+    }
+};
+
+double true_relres(hs_matrix* A, const double* b, const double* x, double* work, double* partials, double* scal,
+                   int64_t n, cudaStream_t st, double bnorm) {
+    copy_kernel<<<grid_elems(n), kT, 0, st>>>(n, b, work);
+    hs::matrix_spmv(A, x, work, -1.0, 1.0, st);
+    const int nb = hsdev::red_blocks(n);
+    dot_kernel<<<nb, kT, 0, st>>>(n, work, work, partials);
+    hsdev::finalize_sum_kernel<<<1, hsdev::kRedThreads, 0, st>>>(partials, nb, scal, 1);
+    hs::count_launch(3);
+    double v = 0;
+    cudaMemcpyAsync(&v, scal, 8, cudaMemcpyDeviceToHost, st);
+    cudaStreamSynchronize(st);
+    return bnorm > 0 ? v / bnorm : 0.0;
+}
+
+// ---- GMRES helpers ---------------------------------------------------------
+// partials[i*nb + block] = V_i . w  for i < jc
+__global__ void mdot_kernel(int64_t n, const double* __restrict__ V, int64_t ldv, int jc, const double* __restrict__ w,
+                            double* __restrict__ partials, int nb) {
+    for (int i = 0; i < jc; ++i) {
+        const double* Vi = V + (size_t)i * ldv;
+        double v = 0.0;
+        for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x)
+            v += Vi[r] * w[r];
+        v = hsdev::block_sum(v);
+        if (threadIdx.x == 0) partials[(size_t)i * nb + blockIdx.x] = v;
+        __syncthreads();
+    }
+}
+
+// hcol[i] = sum of partials row i; H[i][j] += hcol[i]   (grid = jc blocks)
+__global__ void mdot_finalize(const double* __restrict__ partials, int nb, double* __restrict__ hcol,
+                              double* __restrict__ H, int m, int j) {
+    const int i = blockIdx.x;
+    const double v = sum_partials(partials + (size_t)i * nb, nb);
+    if (threadIdx.x == 0) {
+        hcol[i] = v;
+        H[(size_t)i * m + j] += v;
+    }
+}
+
+// w -= sum_i hcol[i] V_i
+__global__ void gs_update(int64_t n, const double* __restrict__ V, int64_t ldv, int jc, const double* __restrict__ hcol,
+                          double* __restrict__ w) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+        double s = w[r];
+        for (int i = 0; i < jc; ++i) s -= hcol[i] * V[(size_t)i * ldv + r];
+        w[r] = s;
+    }
+}
+
+// H[j+1][j] = ||w||, V_{j+1} = w / ||w||, Givens update; flag = converged/breakdown
+__global__ void arnoldi_close(const double* __restrict__ partials, int nb, double* __restrict__ H, int m, int j,
+                              double* __restrict__ cs, double* __restrict__ sn, double* __restrict__ g,
+                              double* __restrict__ hn_out, int* __restrict__ flag, double tol) {
+    const double ss = sum_partials(partials, nb);
+    if (threadIdx.x != 0) return;
+    const double hn = sqrt(ss);
+    *hn_out = hn;
+    H[(size_t)(j + 1) * m + j] = hn;
+    for (int i = 0; i < j; ++i) {
+        const double a0 = H[(size_t)i * m + j], a1 = H[(size_t)(i + 1) * m + j];
+        H[(size_t)i * m + j] = cs[i] * a0 + sn[i] * a1;
+        H[(size_t)(i + 1) * m + j] = -sn[i] * a0 + cs[i] * a1;
+    }
+    const double a0 = H[(size_t)j * m + j], a1 = H[(size_t)(j + 1) * m + j];
+    const double den = sqrt(a0 * a0 + a1 * a1);
+    const double c = den == 0.0 ? 1.0 : a0 / den, s = den == 0.0 ? 0.0 : a1 / den;
+    cs[j] = c;
+    sn[j] = s;
+    H[(size_t)j * m + j] = c * a0 + s * a1;
+    H[(size_t)(j + 1) * m + j] = 0.0;
+    g[j + 1] = -s * g[j];
+    g[j] = c * g[j];
+    *flag = (fabs(g[j + 1]) <= tol || hn == 0.0) ? 1 : 0;
+}
+
+__global__ void scale_from(int64_t n, const double* __restrict__ w, const double* __restrict__ hn, double* __restrict__ out) {
+    const double h = *hn;
+    if (h == 0.0) return;
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x)
+        out[r] = w[r] / h;
+}
+
+__global__ void back_solve(const double* __restrict__ H, int m, int jend, const double* __restrict__ g, double* __restrict__ y) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    for (int i = jend - 1; i >= 0; --i) {
+        double s = g[i];
+        for (int t = i + 1; t < jend; ++t) s -= H[(size_t)i * m + t] * y[t];
+        y[i] = s / H[(size_t)i * m + i];
+    }
+}
+
+// t = sum_i y_i V_i
+__global__ void combine(int64_t n, const double* __restrict__ V, int64_t ldv, int jc, const double* __restrict__ y,
+                        double* __restrict__ t) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int i = 0; i < jc; ++i) s += y[i] * V[(size_t)i * ldv + r];
+        t[r] = s;
+    }
+}
+
+__global__ void add_to(int64_t n, const double* __restrict__ u, double* __restrict__ x) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x)
+        x[r] += u[r];
+}
+
+__global__ void set_g(double* g, int m, double beta) {
+    for (int i = threadIdx.x; i <= m; i += blockDim.x) g[i] = (i == 0) ? beta : 0.0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hs_pcg_solve(hs_matrix* A, int32_t prec_type, void* prec, const double* b, double* x, double rtol, int32_t maxit,
+                 void* stream, hs_solve_info* info) {
+    if (!A || !b || !x || !info) return hs::set_error(HS_ERR_ARG, "hs_pcg_solve: NULL argument");
+    if (prec_type != HS_PREC_NONE && !prec) return hs::set_error(HS_ERR_ARG, "preconditioner handle is NULL");
+    if (maxit < 1) return hs::set_error(HS_ERR_ARG, "maxit must be positive");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int64_t n = hs::matrix_n(A);
+    DevBuf buf;
+    double *r, *z, *p, *q, *pa, *pb, *scal;
+    PcgScalars* s;
+    int rc;
+    if ((rc = buf.alloc(&r, 8 * n)) || (rc = buf.alloc(&z, 8 * n)) || (rc = buf.alloc(&p, 8 * n)) ||
+        (rc = buf.alloc(&q, 8 * n)) || (rc = buf.alloc(&pa, 8 * hsdev::kRedMaxBlocks)) ||
+        (rc = buf.alloc(&pb, 8 * hsdev::kRedMaxBlocks)) || (rc = buf.alloc(&scal, 16)) ||
+        (rc = buf.alloc(&s, sizeof(PcgScalars))))
+        return rc;
+    const int ge = grid_elems(n), nb = hsdev::red_blocks(n);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, st);
+    // x = 0, r = b, z = M^-1 r, p = z
+    zero_kernel<<<ge, kT, 0, st>>>(n, x);
+    copy_kernel<<<ge, kT, 0, st>>>(n, b, r);
+    hs::count_launch(2);
+    if ((rc = prec_apply(prec_type, prec, r, z, n, st))) return rc;
+    copy_kernel<<<ge, kT, 0, st>>>(n, z, p);
+    dot_kernel<<<nb, kT, 0, st>>>(n, b, b, pa);
+    dot_kernel<<<nb, kT, 0, st>>>(n, r, z, pb);
+    pcg_init_scalars<<<1, kT, 0, st>>>(pa, pb, nb, s, rtol);
+    hs::count_launch(4);
+    HS_LAUNCH_CHECK("pcg init");
+
+    // One iteration as a graph.
+    auto iteration = [&](cudaStream_t cs) -> int {
+        int r2;
+        if ((r2 = hs::matrix_spmv(A, p, q, 1.0, 0.0, cs))) return r2;
+        dot_kernel<<<nb, kT, 0, cs>>>(n, p, q, pa);
+        pcg_alpha<<<1, kT, 0, cs>>>(pa, nb, s);
+        pcg_update<<<nb, kT, 0, cs>>>(n, s, p, q, x, r, pa);
+        pcg_check<<<1, kT, 0, cs>>>(pa, nb, s);
+        hs::count_launch(4);
+        if ((r2 = prec_apply(prec_type, prec, r, z, n, cs))) return r2;
+        dot_kernel<<<nb, kT, 0, cs>>>(n, r, z, pb);
+        pcg_beta<<<1, kT, 0, cs>>>(pb, nb, s);
+        pcg_p<<<ge, kT, 0, cs>>>(n, s, z, p);
+        hs::count_launch(3);
+        return HS_OK;
+    };
+    // warm launch outside capture (sets kernel attributes), then capture
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    bool use_graph = true;
+    if ((rc = iteration(st))) return rc;
+    int launches_per_iter = 0;
+    {
+        const int64_t before = hs_kernel_launches();
+        if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            use_graph = false;
+        } else {
+            rc = iteration(st);
+            cudaError_t ce = cudaStreamEndCapture(st, &graph);
+            if (rc || ce != cudaSuccess || cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) {
+                use_graph = false;
+                cudaGetLastError();
+            }
+        }
+        launches_per_iter = (int)(hs_kernel_launches() - before);
+        hs::count_launch(-launches_per_iter);  // counted per replay below
+    }
+    PcgScalars hsc{};
+    int iters_run = 1;
+    const int batch = 8;
+    while (true) {
+        HS_CUDA(cudaMemcpyAsync(&hsc, s, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
+        HS_CUDA(cudaStreamSynchronize(st));
+        if (hsc.done || iters_run >= maxit) break;
+        const int todo = std::min(batch, maxit - iters_run);
+        for (int k = 0; k < todo; ++k) {
+            if (use_graph) {
+                HS_CUDA(cudaGraphLaunch(exec, st));
+                hs::count_launch(launches_per_iter);
+            } else if ((rc = iteration(st))) {
+                return rc;
+            }
+        }
+        iters_run += todo;
+    }
+    cudaEventRecord(e1, st);
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    const double bnorm = std::sqrt(hsc.bb);
+    info->iterations = hsc.done ? hsc.conv_it : hsc.it;
+    info->converged = hsc.done ? 1 : 0;
+    info->ms = ms;
+    info->relres = true_relres(A, b, x, q, pa, scal, n, st, bnorm);
+    HS_CUDA(cudaGetLastError());
+    if (!hsc.done) return hs::set_error(HS_ERR_NOT_CONVERGED, "PCG did not converge in %d iterations", maxit);
+    return HS_OK;
+}
+
+int hs_gmres_solve(hs_matrix* A, int32_t prec_type, void* prec, int32_t restart, const double* b, double* x, double rtol,
+                   int32_t maxit, void* stream, hs_solve_info* info) {
+    if (!A || !b || !x || !info) return hs::set_error(HS_ERR_ARG, "hs_gmres_solve: NULL argument");
+    if (prec_type != HS_PREC_NONE && !prec) return hs::set_error(HS_ERR_ARG, "preconditioner handle is NULL");
+    if (restart < 1 || restart > 256 || maxit < 1) return hs::set_error(HS_ERR_ARG, "bad restart/maxit");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int64_t n = hs::matrix_n(A);
+    const int m = restart;
+    DevBuf buf;
+    double *V, *u, *w, *r, *partials, *H, *cs, *sn, *g, *y, *hcol, *scal;
+    int* flag;
+    int rc;
+    if ((rc = buf.alloc(&V, 8 * (size_t)n * (m + 1))) || (rc = buf.alloc(&u, 8 * n)) || (rc = buf.alloc(&w, 8 * n)) ||
+        (rc = buf.alloc(&r, 8 * n)) || (rc = buf.alloc(&partials, 8 * (size_t)hsdev::kRedMaxBlocks * (m + 1))) ||
+        (rc = buf.alloc(&H, 8 * (size_t)(m + 1) * m)) || (rc = buf.alloc(&cs, 8 * m)) || (rc = buf.alloc(&sn, 8 * m)) ||
+        (rc = buf.alloc(&g, 8 * (m + 1))) || (rc = buf.alloc(&y, 8 * m)) || (rc = buf.alloc(&hcol, 8 * (m + 1))) ||
+        (rc = buf.alloc(&scal, 16)) || (rc = buf.alloc(&flag, sizeof(int))))
+        return rc;
+    const int ge = grid_elems(n), nb = hsdev::red_blocks(n);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, st);
+    auto norm = [&](const double* a) -> double {
+        dot_kernel<<<nb, kT, 0, st>>>(n, a, a, partials);
+        hsdev::finalize_sum_kernel<<<1, hsdev::kRedThreads, 0, st>>>(partials, nb, scal, 1);
+        hs::count_launch(2);
+        double v = 0;
+        cudaMemcpyAsync(&v, scal, 8, cudaMemcpyDeviceToHost, st);
+        cudaStreamSynchronize(st);
+        return v;
+    };
+    zero_kernel<<<ge, kT, 0, st>>>(n, x);
+    copy_kernel<<<ge, kT, 0, st>>>(n, b, r);
+    hs::count_launch(2);
+    const double bnorm = norm(b);
+    double beta = bnorm;
+    int total = 0;
+    bool conv = bnorm == 0.0;
+    const double tol = rtol * bnorm;
+    while (!conv && total < maxit) {
+        const double invb = 1.0 / beta;
+        // V0 = r / beta
+        {
+            double* vb = scal + 1;
+            cudaMemcpyAsync(vb, &beta, 8, cudaMemcpyHostToDevice, st);
+            scale_from<<<ge, kT, 0, st>>>(n, r, vb, V);
+            hs::count_launch();
+            (void)invb;
+        }
+        HS_CUDA(cudaMemsetAsync(H, 0, 8 * (size_t)(m + 1) * m, st));
+        set_g<<<1, 64, 0, st>>>(g, m, beta);
+        hs::count_launch();
+        int jend = 0;
+        for (int j = 0; j < m; ++j) {
+            double* Vj = V + (size_t)j * n;
+            if ((rc = prec_apply(prec_type, prec, Vj, u, n, st))) return rc;
+            if ((rc = hs::matrix_spmv(A, u, w, 1.0, 0.0, st))) return rc;
+            for (int pass = 0; pass < 2; ++pass) {  // classical Gram-Schmidt, twice
+                mdot_kernel<<<nb, kT, 0, st>>>(n, V, n, j + 1, w, partials, nb);
+                mdot_finalize<<<j + 1, kT, 0, st>>>(partials, nb, hcol, H, m, j);
+                gs_update<<<ge, kT, 0, st>>>(n, V, n, j + 1, hcol, w);
+                hs::count_launch(3);
+            }
+            dot_kernel<<<nb, kT, 0, st>>>(n, w, w, partials);
+            arnoldi_close<<<1, kT, 0, st>>>(partials, nb, H, m, j, cs, sn, g, scal, flag, tol);
+            scale_from<<<ge, kT, 0, st>>>(n, w, scal, V + (size_t)(j + 1) * n);
+            hs::count_launch(3);
+            int hflag = 0;
+            HS_CUDA(cudaMemcpyAsync(&hflag, flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+            HS_CUDA(cudaStreamSynchronize(st));
+            ++total;
+            jend = j + 1;
+            if (hflag || total >= maxit) break;
+        }
+        back_solve<<<1, 32, 0, st>>>(H, m, jend, g, y);
+        combine<<<ge, kT, 0, st>>>(n, V, n, jend, y, w);
+        hs::count_launch(2);
+        if ((rc = prec_apply(prec_type, prec, w, u, n, st))) return rc;
+        add_to<<<ge, kT, 0, st>>>(n, u, x);
+        copy_kernel<<<ge, kT, 0, st>>>(n, b, r);
+        hs::count_launch(2);
+        if ((rc = hs::matrix_spmv(A, x, r, -1.0, 1.0, st))) return rc;
+        beta = norm(r);
+        if (beta <= tol) conv = true;
+    }
+    cudaEventRecord(e1, st);
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    HS_CUDA(cudaGetLastError());
+    info->iterations = total;
+    info->converged = conv ? 1 : 0;
+    info->relres = bnorm > 0 ? beta / bnorm : 0.0;
+    info->ms = ms;
+    if (!conv) return hs::set_error(HS_ERR_NOT_CONVERGED, "GMRES did not converge in %d iterations", maxit);
+    return HS_OK;
+}
+
+}  // extern "C"

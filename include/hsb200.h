@@ -1,0 +1,197 @@
+/*
+ * hsb200.h — C ABI of libhsb200.so, the B200 (sm_100a) implementation of
+ * HybridSmoothers.jl's preconditioner/smoother apply path.
+ *
+ * Plain C types only.  Every function returns an hs_status; the message for
+ * the last non-zero status of the calling thread is hs_last_error().
+ * Handles are not thread-safe: a caller serialises the calls on one handle.
+ * `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
+ *
+ * Each entry point names the reference interface it replaces, as
+ * `file:line` inside HybridSmoothers.jl v0.1.4.
+ */
+#ifndef HSB200_H
+#define HSB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------------- */
+/* Status codes.  The reference raises Julia exceptions instead:          */
+/*   error("... must be greater than 0")  src/l1_gauss_seidel.jl:201,217-218,327 -> HS_ERR_ARG */
+/*   SingularException(col)               src/l1_gauss_seidel.jl:430            -> HS_ERR_SINGULAR */
+/* ---------------------------------------------------------------------- */
+typedef enum {
+    HS_OK = 0,
+    HS_ERR_ARG = 1,           /* invalid argument */
+    HS_ERR_OOM = 2,           /* device allocation failed */
+    HS_ERR_CUDA = 3,          /* CUDA runtime/driver error */
+    HS_ERR_SINGULAR = 4,      /* missing or zero diagonal (non-symmetric CSC path) */
+    HS_ERR_NONFINITE = 5,     /* NaN/Inf met where a finite value is required */
+    HS_ERR_NOT_CONVERGED = 6, /* Krylov solver hit its iteration cap */
+    HS_ERR_TIMEOUT = 7,       /* a bounded device-side wait gave up */
+    HS_ERR_UNSUPPORTED = 8,   /* valid but not provided (e.g. a CPU backend) */
+    HS_ERR_BUDGET = 9         /* request does not fit the configured HBM budget */
+} hs_status;
+
+enum { HS_F64 = 0, HS_F32 = 1 };
+enum { HS_CSC = 0, HS_CSR = 1 };
+/* ForwardSweep, BackwardSweep, SymmetricSweep: src/l1_gauss_seidel.jl:18,25,83 */
+enum { HS_SWEEP_FORWARD = 0, HS_SWEEP_BACKWARD = 1, HS_SWEEP_SYMMETRIC = 2 };
+/* PackedBufferCache, MatrixViewCache: src/l1_gauss_seidel.jl:93,100 */
+enum { HS_CACHE_PACKED = 0, HS_CACHE_VIEW = 1 };
+/* Chebyshev spectral estimate: the reference's 50-step power iteration
+ * (src/chebyshev.jl:40-54) or Lanczos bounds (this library's addition). */
+enum { HS_EIG_POWER = 0, HS_EIG_LANCZOS = 1 };
+
+/* A square sparse matrix in HOST memory, 0-based int32 indices, sorted
+ * indices within each column (CSC) or row (CSR) — SparseMatrixCSC /
+ * SparseMatrixCSR at the reference boundary (src/HybridSmoothers.jl:31-36). */
+typedef struct {
+    int32_t n;
+    int64_t nnz;
+    int32_t format;       /* HS_CSC or HS_CSR */
+    int32_t dtype;        /* HS_F64 or HS_F32 (value type) */
+    const int32_t* ptr;   /* n+1: colptr (CSC) or rowptr (CSR) */
+    const int32_t* idx;   /* nnz: rowval (CSC) or colval (CSR) */
+    const void* val;      /* nnz values */
+} hs_sparse;
+
+typedef struct hs_l1gs_s hs_l1gs;
+typedef struct hs_cheb_s hs_cheb;
+typedef struct hs_matrix_s hs_matrix;
+
+/* BlockPartitioning (src/l1_gauss_seidel.jl:118-124) plus storage facts. */
+typedef struct {
+    int32_t n, partsize, nparts, nchunks, chunksize;
+    int32_t sweep, cache, is_sym, format;
+    int32_t matrix_dtype, smoother_dtype;
+    int64_t packed_len;        /* S: length of SLbuffer/SUbuffer in the reference layout */
+    int64_t device_bytes;      /* device memory held by the preconditioner */
+    double eta;
+} hs_l1gs_info;
+
+/* ---------------------------------------------------------------------- */
+/* L1 Gauss-Seidel                                                        */
+/* ---------------------------------------------------------------------- */
+
+/*
+ * Replaces L1GSPrecBuilder(backend::KA.GPU; threads, blocks)
+ * (src/l1_gauss_seidel.jl:251-262) called on (A, partsize; isSymA, η, sweep,
+ * cache_strategy) (src/l1_gauss_seidel.jl:287-313) -> build_l1prec (:317-338).
+ * A is host memory and is copied to the device.  threads/blocks are recorded as
+ * the reference's BlockPartitioning; results do not depend on them.
+ * smoother_dtype: HS_F64, or HS_F32 for an FP32 smoother built from an FP64
+ * matrix (D_Dl1 computed in FP64, then rounded).
+ */
+int hs_l1gs_create(const hs_sparse* A, int32_t partsize, int32_t is_sym, double eta,
+                   int32_t sweep, int32_t cache, int32_t smoother_dtype, int32_t threads,
+                   int32_t blocks, void* stream, hs_l1gs** out);
+
+/*
+ * LinearSolve.ldiv!(y, P, x) on device vectors (src/l1_gauss_seidel.jl:367-384
+ * without the adapt/copyto!): y = M^-1 x.  x and y are device pointers of
+ * length n in io_dtype (HS_F64 or HS_F32); x == y (in place) is allowed, any
+ * other overlap is not.  Asynchronous on `stream`.
+ */
+int hs_l1gs_apply(hs_l1gs* P, const void* x, void* y, int32_t io_dtype, void* stream);
+
+/*
+ * The generic LinearSolve.ldiv!(y, P, x) with HOST vectors
+ * (src/l1_gauss_seidel.jl:367-384): y .= x, adapt to the device, sweep,
+ * copyto! back.  Synchronous; uses pinned staging owned by P.
+ */
+int hs_l1gs_apply_host(hs_l1gs* P, const void* x_host, void* y_host, int32_t io_dtype, void* stream);
+
+int hs_l1gs_info_get(const hs_l1gs* P, hs_l1gs_info* info);
+
+/* P.sweep.op.D_DL1 (src/l1_gauss_seidel.jl:509,516): n values in smoother dtype. */
+int hs_l1gs_get_diag(const hs_l1gs* P, void* out_host);
+
+/* P.sweep.op.L.SLbuffer (which=0) / .U.SUbuffer (which=1) in the reference's
+ * packed layout (src/l1_gauss_seidel.jl:480-502), packed cache only.
+ * capacity = number of elements available at out_host. */
+int hs_l1gs_get_packed(const hs_l1gs* P, int32_t which, void* out_host, int64_t capacity);
+
+/* DiagonalIndices (src/l1_gauss_seidel.jl:417-436), 0-based; non-symmetric CSC only. */
+int hs_l1gs_get_diag_indices(const hs_l1gs* P, int32_t* out_host);
+
+int hs_l1gs_destroy(hs_l1gs* P);
+
+/* ---------------------------------------------------------------------- */
+/* Sparse matrix on the device: mul!(y, A, x[, α, β]) as SparseMatricesCSR  */
+/* (called at src/chebyshev.jl:47,165,179,287,305 and by Krylov drivers).  */
+/* ---------------------------------------------------------------------- */
+int hs_matrix_create(const hs_sparse* A, int32_t dtype, void* stream, hs_matrix** out);
+/* y = alpha*A*x + beta*y, device vectors in the matrix dtype.  (alpha,beta) =
+ * (1,0) is the three-argument mul!; (-1,1) the five-argument form of
+ * src/chebyshev.jl:179.  Other pairs compute y[i] = beta*y[i] + sum alpha*(a*x). */
+int hs_matrix_spmv(hs_matrix* A, const void* x, void* y, double alpha, double beta, void* stream);
+int hs_matrix_destroy(hs_matrix* A);
+
+/* ---------------------------------------------------------------------- */
+/* Chebyshev smoothers                                                    */
+/* ---------------------------------------------------------------------- */
+typedef struct {
+    int32_t n, kind, degree, eig, smoother_dtype;
+    double rho;            /* spectral estimate used by the recurrence */
+    double rho_power;      /* 50-step power iteration (reference) */
+    double lanczos_min, lanczos_max; /* Lanczos bounds on spec(M^-1 A), if computed */
+    double astar;          /* a* (1st kind), else 0 */
+} hs_cheb_info;
+
+/*
+ * Replaces ChebyshevFourth/ChebyshevFirst(; degree, backend) + _build_smoother
+ * (src/chebyshev.jl:115-156, :218-276).  kind = 4 or 1.  A is a host CSC
+ * matrix (FP64); l1 row sums and the spectral estimate are FP64 on the device;
+ * smoother_dtype selects FP64 or FP32 smoothing arithmetic.
+ */
+int hs_cheb_create(const hs_sparse* A, int32_t kind, int32_t degree, int32_t eig,
+                   int32_t smoother_dtype, void* stream, hs_cheb** out);
+/* smooth!(x, s, b) (src/chebyshev.jl:158-183, :278-322), device vectors in smoother dtype. */
+int hs_cheb_smooth(hs_cheb* S, void* x, const void* b, void* stream);
+/* z = M^-1 r := smooth!(0, s, r); r and z in io_dtype (FP64 or the smoother dtype). */
+int hs_cheb_apply(hs_cheb* S, const void* r, void* z, int32_t io_dtype, void* stream);
+int hs_cheb_info_get(const hs_cheb* S, hs_cheb_info* info);
+/* Override the spectral estimate (parity runs at a fixed rho). */
+int hs_cheb_set_rho(hs_cheb* S, double rho);
+int hs_cheb_destroy(hs_cheb* S);
+
+/* ---------------------------------------------------------------------- */
+/* Krylov drivers (stand-ins for Krylov.jl's CG/GMRES reached through      */
+/* LinearSolve: test/test_preconditioners.jl:65,93).  FP64, device vectors. */
+/* ---------------------------------------------------------------------- */
+enum { HS_PREC_NONE = 0, HS_PREC_L1GS = 1, HS_PREC_CHEB = 2 };
+typedef struct {
+    int32_t iterations;
+    int32_t converged;
+    double relres;      /* true ||b - A x|| / ||b|| at exit */
+    double ms;          /* device time of the solve */
+} hs_solve_info;
+
+int hs_pcg_solve(hs_matrix* A, int32_t prec_type, void* prec, const double* b, double* x,
+                 double rtol, int32_t maxit, void* stream, hs_solve_info* info);
+int hs_gmres_solve(hs_matrix* A, int32_t prec_type, void* prec, int32_t restart, const double* b,
+                   double* x, double rtol, int32_t maxit, void* stream, hs_solve_info* info);
+
+/* ---------------------------------------------------------------------- */
+/* Diagnostics                                                            */
+/* ---------------------------------------------------------------------- */
+const char* hs_last_error(void);
+/* Column (1-based, like SingularException) of the last HS_ERR_SINGULAR. */
+int32_t hs_last_singular_col(void);
+/* Reads and clears the device-side error word that bounded waits set
+ * (0 = none).  Synchronises `stream`. */
+int hs_device_error(void* stream, int32_t* code);
+/* Number of kernels this library has launched in this process. */
+int64_t hs_kernel_launches(void);
+const char* hs_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HSB200_H */
