@@ -135,14 +135,6 @@ __global__ void pcg_p(int64_t n, const PcgScalars* __restrict__ s, const double*
         p[i] = z[i] + beta * p[i];
 }
 
-// q = A p fused with p.q partials (CSR scalar row loop; FP64)
-struct MatView {
-    int32_t n;
-    const int32_t* rp;
-    const int32_t* ci;
-    const double* v;
-};
-
 int prec_apply(int type, void* prec, const double* r, double* z, int64_t n, cudaStream_t st) {
     if (type == HS_PREC_L1GS) return hs_l1gs_apply(static_cast<hs_l1gs*>(prec), r, z, HS_F64, st);
     if (type == HS_PREC_CHEB) return hs::cheb_apply(static_cast<hs_cheb*>(prec), r, z, HS_F64, st);
@@ -285,7 +277,27 @@ int hs_pcg_solve(hs_matrix* A, int32_t prec_type, void* prec, const double* b, d
     if (!A || !b || !x || !info) return hs::set_error(HS_ERR_ARG, "hs_pcg_solve: NULL argument");
     if (prec_type != HS_PREC_NONE && !prec) return hs::set_error(HS_ERR_ARG, "preconditioner handle is NULL");
     if (maxit < 1) return hs::set_error(HS_ERR_ARG, "maxit must be positive");
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // The solve runs on a private non-blocking stream (graph capture is not
+    // allowed on the legacy default stream), ordered after and before the
+    // caller's stream by events.
+    cudaStream_t caller = static_cast<cudaStream_t>(stream);
+    static thread_local cudaStream_t own = nullptr;
+    static thread_local cudaEvent_t join = nullptr;
+    if (!own) {
+        HS_CUDA(cudaStreamCreateWithFlags(&own, cudaStreamNonBlocking));
+        HS_CUDA(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+    }
+    HS_CUDA(cudaEventRecord(join, caller));
+    HS_CUDA(cudaStreamWaitEvent(own, join, 0));
+    cudaStream_t st = own;
+    struct Rejoin {
+        cudaStream_t a, b;
+        cudaEvent_t e;
+        ~Rejoin() {
+            cudaEventRecord(e, a);
+            cudaStreamWaitEvent(b, e, 0);
+        }
+    } rejoin{own, caller, join};
     const int64_t n = hs::matrix_n(A);
     DevBuf buf;
     double *r, *z, *p, *q, *pa, *pb, *scal;
@@ -339,6 +351,7 @@ int hs_pcg_solve(hs_matrix* A, int32_t prec_type, void* prec, const double* b, d
         const int64_t before = hs_kernel_launches();
         if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
             use_graph = false;
+            cudaGetLastError();
         } else {
             rc = iteration(st);
             cudaError_t ce = cudaStreamEndCapture(st, &graph);

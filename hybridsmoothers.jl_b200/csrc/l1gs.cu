@@ -23,6 +23,8 @@
 // the reference's sequence (:1090-1092, :1547-1585), so results are bitwise
 // equal to the reference order of operations.
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -90,152 +92,307 @@ __global__ void convert_kernel(const TA* __restrict__ a, TB* __restrict__ b, int
 
 // ---------------------------------------------------------------------------
 // Packed apply: thread per partition, warp per 32 partitions, TMA ring.
+//
+// Each warp walks its groups g = g0, g0+gstride, ... (32 partitions each) and
+// consumes, per group, the lower stream then/or the upper stream as tiles of
+// E rows x 32 lanes.  Tile t of the warp's whole sequence lives in ring stage
+// t % STAGES; lane 0 refills a stage with tile t+STAGES as soon as the warp has
+// read tile t, so STAGES-1 tiles are always in flight, across group
+// boundaries too.  Every wait is bounded; on a timeout the warp records
+// kErrWaitTimeout, lets its in-flight copies land (bounded) and returns.
 // ---------------------------------------------------------------------------
 struct PackedParams {
     int32_t n, ps, nparts;
     int64_t npad;
     int32_t ngroups;
-    int64_t tlen;      // ps(ps-1)/2 stream elements per direction
+    int32_t tlen;      // ps(ps-1)/2 stream elements per direction
     int32_t ntiles;    // ceil(tlen / E) tiles per direction
     const void* Di;
     const void* x;
     void* y;
     int32_t* err;
-    int32_t ys_stride; // 33
     uint32_t warp_bytes;
     uint32_t ring_bytes;
 };
 
-// Issue tile c of this warp's tile sequence.
 template <typename T, int E, int STAGES, int SWEEP>
-__device__ __forceinline__ void issue_tile(const CUtensorMap* tmL, const CUtensorMap* tmU, T* buf, uint64_t* bars,
-                                           int64_t c, int32_t g0, int32_t gstride, int32_t ntiles) {
-    const int32_t ntpg = (SWEEP == 2) ? 2 * ntiles : ntiles;
-    const int64_t gi = c / ntpg;
-    int32_t ti = (int32_t)(c - gi * ntpg);
-    const int32_t g = g0 + (int32_t)gi * gstride;
-    const CUtensorMap* map = (SWEEP == 1) ? tmU : tmL;
-    if (SWEEP == 2 && ti >= ntiles) {
-        map = tmU;
-        ti -= ntiles;
-    }
-    const int stage = (int)(c % STAGES);
-    uint64_t* bar = bars + stage;
-    hsdev::mbar_arrive_expect_tx(bar, (uint32_t)(E * 32 * sizeof(T)));
-    hsdev::tma_load_2d(buf + (size_t)stage * E * 32, map, g * 32, ti * E, bar);
-}
+struct TileRing {
+    const CUtensorMap* tmL;
+    const CUtensorMap* tmU;
+    T* buf;
+    uint64_t* bars;
+    int32_t g0, gstride, ntiles, total;
+    int lane;
 
-template <typename T, typename IO, int SWEEP, int E, int STAGES>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32)
-    l1gs_packed_kernel(const __grid_constant__ CUtensorMap tmL, const __grid_constant__ CUtensorMap tmU,
-                       const PackedParams p) {
+    __device__ __forceinline__ void issue(int32_t c) const {
+        const int32_t ntpg = (SWEEP == 2) ? 2 * ntiles : ntiles;
+        const int32_t gi = c / ntpg;
+        int32_t ti = c - gi * ntpg;
+        const CUtensorMap* map = (SWEEP == 1) ? tmU : tmL;
+        if (SWEEP == 2 && ti >= ntiles) {
+            map = tmU;
+            ti -= ntiles;
+        }
+        const int stage = c & (STAGES - 1);
+        hsdev::mbar_arrive_expect_tx(bars + stage, (uint32_t)(E * 32 * sizeof(T)));
+        hsdev::tma_load_2d(buf + stage * (E * 32), map, (g0 + gi * gstride) * 32, ti * E, bars + stage);
+    }
+    __device__ __forceinline__ void prologue() const {
+        if (lane == 0) {
+            for (int s = 0; s < STAGES; ++s) hsdev::mbar_init(bars + s, 1);
+            hsdev::fence_barrier_init();
+            const int32_t pro = total < STAGES ? total : STAGES;
+            for (int32_t c = 0; c < pro; ++c) issue(c);
+        }
+        __syncwarp();
+    }
+    // Wait for tile c; false (on every lane) if a bounded wait ran out.
+    __device__ __forceinline__ bool wait(int32_t c) const {
+        const bool ok = hsdev::mbar_wait_bounded(bars + (c & (STAGES - 1)), (uint32_t)((c / STAGES) & 1));
+        return __all_sync(0xffffffffu, ok);
+    }
+    __device__ __forceinline__ const T* tile(int32_t c) const { return buf + (c & (STAGES - 1)) * (E * 32); }
+    // The warp has read tile c: refill its stage with tile c+STAGES.
+    __device__ __forceinline__ void release(int32_t c) const {
+        __syncwarp();
+        if (lane == 0 && c + STAGES < total) {
+            hsdev::fence_proxy_async_smem();
+            issue(c + STAGES);
+        }
+    }
+    // After a timeout at tile c: let copies already issued land, then return.
+    __device__ void drain(int32_t c, int32_t* err) const {
+        if (lane == 0) hsdev::report_error(err, hsdev::kErrWaitTimeout);
+        const int32_t end = (c + STAGES < total) ? c + STAGES : total;
+        for (int32_t cc = c; cc < end; ++cc)
+            (void)hsdev::mbar_wait_bounded(bars + (cc & (STAGES - 1)), (uint32_t)((cc / STAGES) & 1));
+    }
+};
+
+// ---- compile-time partsize: y and D_Dl1 in registers, fully unrolled -------
+template <typename T, typename IO, int SWEEP, int PS, int E, int STAGES, int MINB>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, MINB)
+    l1gs_packed_small_kernel(const __grid_constant__ CUtensorMap tmL, const __grid_constant__ CUtensorMap tmU,
+                             const PackedParams p) {
+    constexpr int TLEN = PS * (PS - 1) / 2;
+    constexpr int NT = (TLEN + E - 1) / E;
+    constexpr int XS = (PS % 2 == 0) ? PS + 1 : PS;  // odd stride: conflict-free transposes
     extern __shared__ __align__(128) unsigned char smem[];
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     unsigned char* wbase = smem + (size_t)warp * p.warp_bytes;
-    T* ring = reinterpret_cast<T*>(wbase);
-    uint64_t* bars = reinterpret_cast<uint64_t*>(wbase + p.ring_bytes);
-    T* ys = reinterpret_cast<T*>(wbase + p.ring_bytes + 8 * STAGES);
-    const int S = p.ys_stride;
+    T* xs = reinterpret_cast<T*>(wbase + p.ring_bytes + 8 * STAGES);
     const T* __restrict__ Di = static_cast<const T*>(p.Di);
     const IO* __restrict__ x = static_cast<const IO*>(p.x);
     IO* __restrict__ y = static_cast<IO*>(p.y);
 
     const int wpb = blockDim.x >> 5;
-    const int32_t g0 = blockIdx.x * wpb + warp;
-    const int32_t gstride = gridDim.x * wpb;
-    const int64_t my_groups = g0 < p.ngroups ? (int64_t)(p.ngroups - 1 - g0) / gstride + 1 : 0;
-    const int32_t ntpg = (SWEEP == 2) ? 2 * p.ntiles : p.ntiles;
-    const int64_t total = my_groups * ntpg;
+    TileRing<T, E, STAGES, SWEEP> ring;
+    ring.tmL = &tmL;
+    ring.tmU = &tmU;
+    ring.buf = reinterpret_cast<T*>(wbase);
+    ring.bars = reinterpret_cast<uint64_t*>(wbase + p.ring_bytes);
+    ring.g0 = blockIdx.x * wpb + warp;
+    ring.gstride = gridDim.x * wpb;
+    ring.ntiles = NT;
+    ring.lane = lane;
+    const int32_t my_groups = ring.g0 < p.ngroups ? (p.ngroups - 1 - ring.g0) / ring.gstride + 1 : 0;
+    ring.total = my_groups * ((SWEEP == 2) ? 2 * NT : NT);
+    if (NT > 0) ring.prologue();
 
-    if (lane == 0) {
-        if (total > 0) {
-            hsdev::prefetch_tensormap(&tmL);
-            if (SWEEP != 0) hsdev::prefetch_tensormap(&tmU);
+    int32_t c = 0;  // first tile of the current direction
+    for (int32_t gi = 0; gi < my_groups; ++gi) {
+        const int64_t g = ring.g0 + (int64_t)gi * ring.gstride;
+        const int64_t k = g * 32 + lane;
+        const int64_t rowbase = g * 32 * PS;
+        T d[PS];
+#pragma unroll
+        for (int li = 0; li < PS; ++li) d[li] = Di[(int64_t)li * p.npad + k];
+#pragma unroll
+        for (int m = 0; m < PS; ++m) {
+            const int t = lane + 32 * m;
+            const int64_t row = rowbase + t;
+            xs[(t / PS) * XS + (t % PS)] = row < p.n ? (T)x[row] : T(0);
         }
-        for (int s = 0; s < STAGES; ++s) hsdev::mbar_init(bars + s, 1);
-        hsdev::fence_barrier_init();
-        const int64_t pro = total < STAGES ? total : STAGES;
-        for (int64_t c = 0; c < pro; ++c)
-            issue_tile<T, E, STAGES, SWEEP>(&tmL, &tmU, ring, bars, c, g0, gstride, p.ntiles);
-    }
-    __syncwarp();
-
-    int64_t c = 0;       // tile being consumed
-    int32_t r = 0;       // row inside it
-    const T* cur = nullptr;
-    bool abort = false;
-
-    // Wait for tile c; false if the bounded wait ran out on any lane.
-    auto wait_tile = [&]() -> bool {
-        const int stage = (int)(c % STAGES);
-        const uint32_t parity = (uint32_t)((c / STAGES) & 1);
-        const bool ok = hsdev::mbar_wait_bounded(bars + stage, parity);
-        cur = ring + (size_t)stage * E * 32;
-        return __all_sync(0xffffffffu, ok);
-    };
-    // All lanes are done with tile c: refill its stage with tile c+STAGES.
-    auto finish_tile = [&]() {
         __syncwarp();
-        if (lane == 0) {
-            hsdev::fence_proxy_async_smem();
-            if (c + STAGES < total)
-                issue_tile<T, E, STAGES, SWEEP>(&tmL, &tmU, ring, bars, c + STAGES, g0, gstride, p.ntiles);
-        }
-        ++c;
-        r = 0;
-    };
+        T yv[PS];
+#pragma unroll
+        for (int li = 0; li < PS; ++li) yv[li] = xs[lane * XS + li];
 
+        if (SWEEP != 1) {  // forward: rows ascending, lower stream e = li(li-1)/2 + lj
+#pragma unroll
+            for (int li = 0; li < PS; ++li) {
+                T acc = T(0);
+#pragma unroll
+                for (int lj = 0; lj < li; ++lj) {
+                    const int e = li * (li - 1) / 2 + lj;
+                    if (e % E == 0 && !ring.wait(c + e / E)) goto timeout;
+                    acc = add_rn(acc, mul_rn(ring.tile(c + e / E)[(e % E) * 32 + lane], yv[lj]));
+                    if (e % E == E - 1 || e == TLEN - 1) ring.release(c + e / E);
+                }
+                yv[li] = div_rn(sub_rn(yv[li], acc), d[li]);
+            }
+            c += NT;
+        }
+        if (SWEEP == 2) {  // y .= D_Dl1 .* y  (:897)
+#pragma unroll
+            for (int li = 0; li < PS; ++li) yv[li] = mul_rn(d[li], yv[li]);
+        }
+        if (SWEEP != 0) {  // backward: rows descending, upper stream e = q(q-1)/2 + (lj-li-1)
+#pragma unroll
+            for (int li = PS - 1; li >= 0; --li) {
+                T acc = T(0);
+#pragma unroll
+                for (int lj = li + 1; lj < PS; ++lj) {
+                    const int q = PS - 1 - li;
+                    const int e = q * (q - 1) / 2 + (lj - li - 1);
+                    if (e % E == 0 && !ring.wait(c + e / E)) goto timeout;
+                    acc = add_rn(acc, mul_rn(ring.tile(c + e / E)[(e % E) * 32 + lane], yv[lj]));
+                    if (e % E == E - 1 || e == TLEN - 1) ring.release(c + e / E);
+                }
+                yv[li] = div_rn(sub_rn(yv[li], acc), d[li]);
+            }
+            c += NT;
+        }
+        __syncwarp();
+#pragma unroll
+        for (int li = 0; li < PS; ++li) xs[lane * XS + li] = yv[li];
+        __syncwarp();
+#pragma unroll
+        for (int m = 0; m < PS; ++m) {
+            const int t = lane + 32 * m;
+            const int64_t row = rowbase + t;
+            if (row < p.n) y[row] = (IO)xs[(t / PS) * XS + (t % PS)];
+        }
+        __syncwarp();
+    }
+    return;
+timeout:
+    ring.drain(c, p.err);
+}
+
+// ---- runtime partsize: y in shared memory, tile-major stream walk ---------
+template <typename T, typename IO, int SWEEP, int E, int STAGES>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+    l1gs_packed_kernel(const __grid_constant__ CUtensorMap tmL, const __grid_constant__ CUtensorMap tmU,
+                       const PackedParams p) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    constexpr int S = 33;
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    unsigned char* wbase = smem + (size_t)warp * p.warp_bytes;
+    T* ys = reinterpret_cast<T*>(wbase + p.ring_bytes + 8 * STAGES);
+    const T* __restrict__ Di = static_cast<const T*>(p.Di);
+    const IO* __restrict__ x = static_cast<const IO*>(p.x);
+    IO* __restrict__ y = static_cast<IO*>(p.y);
     const int ps = p.ps;
-    for (int64_t gi = 0; gi < my_groups && !abort; ++gi) {
-        const int64_t g = g0 + gi * gstride;
+
+    const int wpb = blockDim.x >> 5;
+    TileRing<T, E, STAGES, SWEEP> ring;
+    ring.tmL = &tmL;
+    ring.tmU = &tmU;
+    ring.buf = reinterpret_cast<T*>(wbase);
+    ring.bars = reinterpret_cast<uint64_t*>(wbase + p.ring_bytes);
+    ring.g0 = blockIdx.x * wpb + warp;
+    ring.gstride = gridDim.x * wpb;
+    ring.ntiles = p.ntiles;
+    ring.lane = lane;
+    const int32_t my_groups = ring.g0 < p.ngroups ? (p.ngroups - 1 - ring.g0) / ring.gstride + 1 : 0;
+    ring.total = my_groups * ((SWEEP == 2) ? 2 * p.ntiles : p.ntiles);
+    if (p.ntiles > 0) ring.prologue();
+
+    int32_t c = 0;
+    for (int32_t gi = 0; gi < my_groups; ++gi) {
+        const int64_t g = ring.g0 + (int64_t)gi * ring.gstride;
         const int64_t k = g * 32 + lane;
         const int64_t rowbase = g * 32 * (int64_t)ps;
-        // x -> ys (transpose through shared memory, coalesced global reads)
+        const T* __restrict__ dk = Di + k;   // D_Dl1 of row li at dk[li * npad]
+        T* yk = ys + lane;                   // y of row li at yk[li * S]
         for (int t = lane; t < 32 * ps; t += 32) {
             const int64_t row = rowbase + t;
-            const T v = row < p.n ? (T)x[row] : T(0);
-            ys[(t % ps) * S + t / ps] = v;
+            ys[(t % ps) * S + t / ps] = row < p.n ? (T)x[row] : T(0);
         }
         __syncwarp();
 
-        if (SWEEP != 1) {  // forward, lower stream
-            for (int li = 0; li < ps && !abort; ++li) {
+        if (SWEEP != 1) {  // forward: rows ascending over the lower stream
+            T dnext = dk[(ps > 1 ? 1 : 0) * p.npad];
+            yk[0] = div_rn(sub_rn(yk[0], T(0)), dk[0]);
+            int32_t t = 0, r = 0;
+            for (int li = 1; li < ps; ++li) {
+                const T dcur = dnext;
+                if (li + 1 < ps) dnext = dk[(int64_t)(li + 1) * p.npad];
                 T acc = T(0);
-                for (int lj = 0; lj < li; ++lj) {
-                    if (r == 0) {
-                        if (!wait_tile()) { abort = true; break; }
+                int lj = 0;
+                while (lj < li) {
+                    if (r == 0 && !ring.wait(c + t)) goto timeout;
+                    const T* tl = ring.tile(c + t) + r * 32 + lane;
+                    const int cnt = min(li - lj, E - r);
+                    for (int b0 = 0; b0 < cnt; b0 += 8) {
+                        T av[8], yv[8];
+#pragma unroll
+                        for (int m = 0; m < 8; ++m)
+                            if (b0 + m < cnt) {
+                                av[m] = tl[(b0 + m) * 32];
+                                yv[m] = yk[(lj + b0 + m) * S];
+                            }
+#pragma unroll
+                        for (int m = 0; m < 8; ++m)
+                            if (b0 + m < cnt) acc = add_rn(acc, mul_rn(av[m], yv[m]));
                     }
-                    acc = add_rn(acc, mul_rn(cur[r * 32 + lane], ys[lj * S + lane]));
-                    if (++r == E) finish_tile();
+                    lj += cnt;
+                    r += cnt;
+                    if (r == E) {
+                        ring.release(c + t);
+                        ++t;
+                        r = 0;
+                    }
                 }
-                if (abort) break;
-                const T d = Di[(int64_t)li * p.npad + k];
-                ys[li * S + lane] = div_rn(sub_rn(ys[li * S + lane], acc), d);
+                yk[li * S] = div_rn(sub_rn(yk[li * S], acc), dcur);
             }
-            if (!abort && r != 0) finish_tile();
+            if (r != 0) ring.release(c + t);
+            c += p.ntiles;
         }
-        if (SWEEP == 2 && !abort) {  // y .= D_Dl1 .* y  (:897)
-            for (int li = 0; li < ps; ++li)
-                ys[li * S + lane] = mul_rn(Di[(int64_t)li * p.npad + k], ys[li * S + lane]);
+        if (SWEEP == 2) {
+            for (int li = 0; li < ps; ++li) yk[li * S] = mul_rn(dk[(int64_t)li * p.npad], yk[li * S]);
         }
-        if (SWEEP != 0 && !abort) {  // backward, upper stream
-            for (int li = ps - 1; li >= 0 && !abort; --li) {
+        if (SWEEP != 0) {  // backward: rows descending over the upper stream
+            T dnext = dk[(int64_t)(ps > 1 ? ps - 2 : 0) * p.npad];
+            yk[(ps - 1) * S] = div_rn(sub_rn(yk[(ps - 1) * S], T(0)), dk[(int64_t)(ps - 1) * p.npad]);
+            int32_t t = 0, r = 0;
+            for (int li = ps - 2; li >= 0; --li) {
+                const T dcur = dnext;
+                if (li > 0) dnext = dk[(int64_t)(li - 1) * p.npad];
                 T acc = T(0);
-                for (int lj = li + 1; lj < ps; ++lj) {
-                    if (r == 0) {
-                        if (!wait_tile()) { abort = true; break; }
+                int lj = li + 1;
+                while (lj < ps) {
+                    if (r == 0 && !ring.wait(c + t)) goto timeout;
+                    const T* tl = ring.tile(c + t) + r * 32 + lane;
+                    const int cnt = min(ps - lj, E - r);
+                    for (int b0 = 0; b0 < cnt; b0 += 8) {
+                        T av[8], yv[8];
+#pragma unroll
+                        for (int m = 0; m < 8; ++m)
+                            if (b0 + m < cnt) {
+                                av[m] = tl[(b0 + m) * 32];
+                                yv[m] = yk[(lj + b0 + m) * S];
+                            }
+#pragma unroll
+                        for (int m = 0; m < 8; ++m)
+                            if (b0 + m < cnt) acc = add_rn(acc, mul_rn(av[m], yv[m]));
                     }
-                    acc = add_rn(acc, mul_rn(cur[r * 32 + lane], ys[lj * S + lane]));
-                    if (++r == E) finish_tile();
+                    lj += cnt;
+                    r += cnt;
+                    if (r == E) {
+                        ring.release(c + t);
+                        ++t;
+                        r = 0;
+                    }
                 }
-                if (abort) break;
-                const T d = Di[(int64_t)li * p.npad + k];
-                ys[li * S + lane] = div_rn(sub_rn(ys[li * S + lane], acc), d);
+                yk[li * S] = div_rn(sub_rn(yk[li * S], acc), dcur);
             }
-            if (!abort && r != 0) finish_tile();
+            if (r != 0) ring.release(c + t);
+            c += p.ntiles;
         }
-        if (abort) break;
         __syncwarp();
         for (int t = lane; t < 32 * ps; t += 32) {
             const int64_t row = rowbase + t;
@@ -243,15 +400,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
         }
         __syncwarp();
     }
-
-    if (abort) {
-        // Record the timeout, then let every copy already in flight land
-        // (bounded) before the CTA's shared memory goes away.
-        if (lane == 0) hsdev::report_error(p.err, hsdev::kErrWaitTimeout);
-        const int64_t issued_end = (c + STAGES < total) ? c + STAGES : total;
-        for (int64_t cc = c; cc < issued_end; ++cc)
-            (void)hsdev::mbar_wait_bounded(bars + (int)(cc % STAGES), (uint32_t)((cc / STAGES) & 1));
-    }
+    return;
+timeout:
+    ring.drain(c, p.err);
 }
 
 // ---------------------------------------------------------------------------
@@ -423,7 +574,10 @@ struct hs_l1gs_s {
     void* dev_x = nullptr;
     void* dev_y = nullptr;
     int64_t bytes = 0;
-    int E = 8, stages = 4;
+    int E = 8, stages = 4, minb = 3;
+    int launch_key = -1, launch_grid = 1;
+    const void* launch_kernel = nullptr;
+    int32_t* err_word = nullptr;
 };
 
 namespace {
@@ -593,6 +747,57 @@ int setup_device(hs_l1gs* P, const int32_t* rp_h, const int32_t* ci_h, const TM*
     return HS_OK;
 }
 
+// Tile geometry of the packed stream: E rows x 32 lanes per TMA tile, STAGES
+// tiles in the per-warp ring.  Large partsizes keep fewer warps per SM (the
+// y slice lives in shared memory), so they get bigger tiles and a deeper ring.
+inline void pick_tile(int ps, int sdt, int* E, int* stages, int* minb) {
+    const bool big = ps >= 128;
+    if (sdt == HS_F64) { *E = big ? 16 : 8; }
+    else { *E = big ? 32 : 16; }
+    *stages = big ? 8 : 4;
+    *minb = 3;
+    // Tuning override: HSB200_L1GS_TILE="big,minb" selects the large-tile ring
+    // (1) or the small one (0), and the blocks-per-SM register cap of the
+    // partsize-16 kernel (3 or 4).
+    if (const char* env = getenv("HSB200_L1GS_TILE")) {
+        int b = -1, mb = -1;
+        if (sscanf(env, "%d,%d", &b, &mb) >= 1) {
+            if (b == 0 || b == 1) {
+                *E = sdt == HS_F64 ? (b ? 16 : 8) : (b ? 32 : 16);
+                *stages = b ? 8 : 4;
+            }
+            if (mb == 3 || mb == 4) *minb = mb;
+        }
+    }
+}
+
+
+template <typename KERN>
+int launch_packed_kernel(KERN kern, hs_l1gs* P, PackedParams& p, uint32_t extra_bytes, cudaStream_t st,
+                         int* configured_smem) {
+    p.warp_bytes = (p.ring_bytes + 8 * 8 + extra_bytes + 127) / 128 * 128;
+    const int wpb = (int)std::max<int64_t>(1, std::min<int64_t>(kWarpsPerBlock, (200 * 1024) / p.warp_bytes));
+    const size_t smem = (size_t)p.warp_bytes * wpb;
+    // The launch shape depends only on the handle and the io type: compute it once.
+    const int key = (int)sizeof(p) ^ (int)p.warp_bytes ^ (wpb << 20);
+    if (P->launch_key != key || P->launch_kernel != (const void*)kern) {
+        if ((int)smem > *configured_smem) {
+            HS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            *configured_smem = (int)smem;
+        }
+        int per_sm = 0;
+        HS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, wpb * 32, smem));
+        if (per_sm < 1) return hs::set_error(HS_ERR_UNSUPPORTED, "partsize %d needs too much shared memory", P->ps);
+        const int64_t want = (P->ngroups + wpb - 1) / wpb;
+        P->launch_grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)per_sm * hs::num_sms()));
+        P->launch_key = key;
+        P->launch_kernel = (const void*)kern;
+    }
+    kern<<<P->launch_grid, wpb * 32, smem, st>>>(P->tmL, P->tmU, p);
+    HS_LAUNCH_CHECK("l1gs_packed_kernel");
+    return HS_OK;
+}
+
 template <typename T, typename IO, int SWEEP, int E, int STAGES>
 int launch_packed_t(hs_l1gs* P, const void* x, void* y, cudaStream_t st) {
     PackedParams p;
@@ -601,38 +806,45 @@ int launch_packed_t(hs_l1gs* P, const void* x, void* y, cudaStream_t st) {
     p.nparts = P->nparts;
     p.npad = P->npad;
     p.ngroups = P->ngroups;
-    p.tlen = P->tlen;
+    p.tlen = (int32_t)P->tlen;
     p.ntiles = (int32_t)((P->tlen + E - 1) / E);
     p.Di = P->Di;
     p.x = x;
     p.y = y;
-    p.err = hs::device_error_word();
-    p.ys_stride = 33;
+    if (!P->err_word) P->err_word = hs::device_error_word();
+    p.err = P->err_word;
     p.ring_bytes = (uint32_t)(E * 32 * sizeof(T) * STAGES);
-    const uint32_t ys_bytes = (uint32_t)(P->ps * 33 * sizeof(T));
-    p.warp_bytes = (p.ring_bytes + 8 * STAGES + ys_bytes + 127) / 128 * 128;
-    const int wpb = (int)std::max<int64_t>(1, std::min<int64_t>(kWarpsPerBlock, (200 * 1024) / p.warp_bytes));
-    const size_t smem = (size_t)p.warp_bytes * wpb;
-    auto kern = l1gs_packed_kernel<T, IO, SWEEP, E, STAGES>;
-    static thread_local int configured_smem = -1;
-    if ((int)smem > configured_smem) {
-        HS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        configured_smem = (int)smem;
+#define HS_SMALL(PSV, MB)                                                                                \
+    {                                                                                                    \
+        static thread_local int cfg = -1;                                                                \
+        constexpr int XS = (PSV % 2 == 0) ? PSV + 1 : PSV;                                               \
+        return launch_packed_kernel(l1gs_packed_small_kernel<T, IO, SWEEP, PSV, E, STAGES, MB>, P, p,    \
+                                    (uint32_t)(32 * XS * sizeof(T)), st, &cfg);                          \
     }
-    int per_sm = 0;
-    HS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, wpb * 32, smem));
-    if (per_sm < 1) return hs::set_error(HS_ERR_UNSUPPORTED, "partsize %d needs too much shared memory", P->ps);
-    const int64_t want = (P->ngroups + wpb - 1) / wpb;
-    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)per_sm * hs::num_sms()));
-    kern<<<grid, wpb * 32, smem, st>>>(P->tmL, P->tmU, p);
-    HS_LAUNCH_CHECK("l1gs_packed_kernel");
-    return HS_OK;
+    if constexpr (STAGES == 4) {
+        switch (P->ps) {
+            case 2: HS_SMALL(2, 4)
+            case 4: HS_SMALL(4, 4)
+            case 8: HS_SMALL(8, 4)
+            case 16:
+                if (P->minb == 4) HS_SMALL(16, 4)
+                HS_SMALL(16, 3)
+            case 32: HS_SMALL(32, 3)
+            default: break;
+        }
+    }
+#undef HS_SMALL
+    static thread_local int cfg = -1;
+    return launch_packed_kernel(l1gs_packed_kernel<T, IO, SWEEP, E, STAGES>, P, p,
+                                (uint32_t)(P->ps * 33 * sizeof(T)), st, &cfg);
 }
 
 template <typename T, typename IO, int SWEEP>
 int launch_packed_cfg(hs_l1gs* P, const void* x, void* y, cudaStream_t st) {
-    constexpr int E = sizeof(T) == 8 ? 8 : 16;
-    return launch_packed_t<T, IO, SWEEP, E, 4>(P, x, y, st);
+    constexpr int EA = sizeof(T) == 8 ? 8 : 16;
+    constexpr int EB = sizeof(T) == 8 ? 16 : 32;
+    if (P->E == EA && P->stages == 4) return launch_packed_t<T, IO, SWEEP, EA, 4>(P, x, y, st);
+    return launch_packed_t<T, IO, SWEEP, EB, 8>(P, x, y, st);
 }
 
 template <typename T, typename IO, int SWEEP>
@@ -786,7 +998,8 @@ int hs_l1gs_create(const hs_sparse* A, int32_t partsize, int32_t is_sym, double 
         return rc;
     }
     if (cache == HS_CACHE_PACKED) {
-        const uint32_t E = smoother_dtype == HS_F64 ? 8 : 16;
+        pick_tile(partsize, smoother_dtype, &P->E, &P->stages, &P->minb);
+        const uint32_t E = (uint32_t)P->E;
         const void* l = P->SLi ? P->SLi : P->SUi;
         const void* u = P->SUi ? P->SUi : P->SLi;
         if (l) {

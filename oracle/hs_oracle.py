@@ -189,6 +189,14 @@ def spmv(rp, ci, v, x):
     return y
 
 
+def spmv_sub(rp, ci, v, z, r):
+    """r = r - A z term by term (five-argument mul!, alpha=-1, beta=1); r updated in place."""
+    n = len(rp) - 1
+    getattr(lib(), "hso_spmv_sub" + _sfx(v.dtype))(C.c_int32(n), _p(_i32(rp)), _p(_i32(ci)), _p(v),
+                                                  _p(np.ascontiguousarray(z, dtype=v.dtype)), _p(r))
+    return r
+
+
 def power_rho(rp, ci, v, l1inv, iters=50):
     n = len(rp) - 1
     wv = np.empty(n, dtype=v.dtype)

@@ -54,10 +54,7 @@ def test_spmv_modes_bitwise(mat):
         np.testing.assert_array_equal(yd.cpu().numpy(), O.spmv(R.indptr, R.indices, v, x.astype(dt)))
         yd = dev(y0, tdt)
         hsb200.mul_(yd, M, xd, -1.0, 1.0)
-        ref = y0.astype(dt).copy()
-        O.lib().__getattribute__("hso_spmv_sub" + ("_f64" if dt == np.float64 else "_f32"))(
-            O.C.c_int32(n), O._p(O._i32(R.indptr)), O._p(O._i32(R.indices)), O._p(v),
-            O._p(x.astype(dt)), O._p(ref))
+        ref = O.spmv_sub(R.indptr, R.indices, v, x.astype(dt), y0.astype(dt).copy())
         np.testing.assert_array_equal(yd.cpu().numpy(), ref)
     # general alpha, beta against numpy
     M = hsb200.DeviceSparseMatrix(A)
