@@ -546,6 +546,143 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) l1gs_view_kernel(const Vi
     }
 }
 
+// View apply, thread per partition: warp per 32 consecutive partitions (the
+// packed kernel's mapping).  The warp first gathers every row's in-block
+// strict-lower / strict-upper entries into per-partition lists in shared
+// memory, laid out [entry][lane] so each lane's reads are conflict-free and in
+// the reference's order (rows ascending, columns ascending within a row); then
+// each lane runs the serial row recurrence of its own partition.
+struct ViewLanesParams {
+    int32_t n, ps, nparts, ngroups;
+    const int32_t* rp;
+    const int32_t* ci;
+    const void* v;
+    const void* D;
+    const void* x;
+    void* y;
+    int32_t cap_lo, cap_up;
+    uint32_t warp_bytes;
+};
+
+template <typename T, typename IO, int SWEEP>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) l1gs_view_lanes_kernel(const ViewLanesParams p) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    constexpr int S = 33;
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int ps = p.ps;
+    const bool want_lo = SWEEP != 1, want_up = SWEEP != 0;
+    unsigned char* w = smem + (size_t)warp * p.warp_bytes;
+    T* ys = reinterpret_cast<T*>(w);
+    T* ds = ys + ps * S;
+    T* lval = ds + ps * S;
+    T* uval = lval + p.cap_lo * 32;
+    uint16_t* loff = reinterpret_cast<uint16_t*>(uval + p.cap_up * 32);
+    uint16_t* uoff = loff + (ps + 1) * 32;
+    uint16_t* lcol = uoff + (ps + 1) * 32;
+    uint16_t* ucol = lcol + p.cap_lo * 32;
+    const int32_t* __restrict__ rp = p.rp;
+    const int32_t* __restrict__ ci = p.ci;
+    const T* __restrict__ v = static_cast<const T*>(p.v);
+    const T* __restrict__ D = static_cast<const T*>(p.D);
+    const IO* __restrict__ x = static_cast<const IO*>(p.x);
+    IO* __restrict__ y = static_cast<IO*>(p.y);
+
+    const int wpb = blockDim.x >> 5;
+    for (int64_t g = (int64_t)blockIdx.x * wpb + warp; g < p.ngroups; g += (int64_t)gridDim.x * wpb) {
+        const int64_t rowbase = g * 32 * (int64_t)ps;
+        // pass 1: stage x and D_Dl1, count in-block entries per row
+        for (int t = lane; t < 32 * ps; t += 32) {
+            const int pp = t / ps, li = t % ps;
+            const int64_t i = rowbase + t;
+            const bool valid = i < p.n;
+            ys[li * S + pp] = valid ? (T)x[i] : T(0);
+            ds[li * S + pp] = valid ? D[i] : T(1);
+            int cl = 0, cu = 0;
+            if (valid) {
+                const int64_t s0 = rowbase + (int64_t)pp * ps;
+                const int64_t e0 = min(s0 + ps - 1, (int64_t)p.n - 1);
+                const int32_t q1 = rp[i + 1];
+                for (int32_t q = rp[i]; q < q1; ++q) {
+                    const int64_t j = ci[q];
+                    cl += (want_lo && j >= s0 && j < i);
+                    cu += (want_up && j > i && j <= e0);
+                }
+            }
+            loff[(li + 1) * 32 + pp] = (uint16_t)cl;
+            uoff[(li + 1) * 32 + pp] = (uint16_t)cu;
+        }
+        __syncwarp();
+        {   // per-partition exclusive prefix over its rows
+            uint16_t al = 0, au = 0;
+            loff[lane] = 0;
+            uoff[lane] = 0;
+            for (int li = 1; li <= ps; ++li) {
+                al = (uint16_t)(al + loff[li * 32 + lane]);
+                au = (uint16_t)(au + uoff[li * 32 + lane]);
+                loff[li * 32 + lane] = al;
+                uoff[li * 32 + lane] = au;
+            }
+        }
+        __syncwarp();
+        // pass 2: write the entries
+        for (int t = lane; t < 32 * ps; t += 32) {
+            const int pp = t / ps, li = t % ps;
+            const int64_t i = rowbase + t;
+            if (i < p.n) {
+                const int64_t s0 = rowbase + (int64_t)pp * ps;
+                const int64_t e0 = min(s0 + ps - 1, (int64_t)p.n - 1);
+                int wl = loff[li * 32 + pp], wu = uoff[li * 32 + pp];
+                const int32_t q1 = rp[i + 1];
+                for (int32_t q = rp[i]; q < q1; ++q) {
+                    const int64_t j = ci[q];
+                    if (want_lo && j >= s0 && j < i) {
+                        lval[wl * 32 + pp] = v[q];
+                        lcol[wl * 32 + pp] = (uint16_t)(j - s0);
+                        ++wl;
+                    } else if (want_up && j > i && j <= e0) {
+                        uval[wu * 32 + pp] = v[q];
+                        ucol[wu * 32 + pp] = (uint16_t)(j - s0);
+                        ++wu;
+                    }
+                }
+            }
+        }
+        __syncwarp();
+        // serial recurrence per lane (partition g*32 + lane)
+        const int64_t k = g * 32 + lane;
+        const int aps = k < p.nparts ? (int)min((int64_t)ps, (int64_t)p.n - k * ps) : 0;
+        T* yk = ys + lane;
+        const T* dk = ds + lane;
+        if (want_lo) {
+            for (int li = 0; li < aps; ++li) {
+                T acc = T(0);
+                const int q1 = loff[(li + 1) * 32 + lane];
+                for (int q = loff[li * 32 + lane]; q < q1; ++q)
+                    acc = add_rn(acc, mul_rn(lval[q * 32 + lane], yk[lcol[q * 32 + lane] * S]));
+                yk[li * S] = div_rn(sub_rn(yk[li * S], acc), dk[li * S]);
+            }
+        }
+        if (SWEEP == 2)
+            for (int li = 0; li < aps; ++li) yk[li * S] = mul_rn(dk[li * S], yk[li * S]);
+        if (want_up) {
+            for (int li = aps - 1; li >= 0; --li) {
+                T acc = T(0);
+                const int q1 = uoff[(li + 1) * 32 + lane];
+                for (int q = uoff[li * 32 + lane]; q < q1; ++q)
+                    acc = add_rn(acc, mul_rn(uval[q * 32 + lane], yk[ucol[q * 32 + lane] * S]));
+                yk[li * S] = div_rn(sub_rn(yk[li * S], acc), dk[li * S]);
+            }
+        }
+        __syncwarp();
+        for (int t = lane; t < 32 * ps; t += 32) {
+            const int64_t i = rowbase + t;
+            if (i < p.n) y[i] = (IO)ys[(t % ps) * S + t / ps];
+        }
+        __syncwarp();
+    }
+}
+
 template <typename T>
 inline int dt_size() { return (int)sizeof(T); }
 inline size_t dsize(int dt) { return dt == HS_F64 ? 8 : 4; }
@@ -848,7 +985,52 @@ int launch_packed_cfg(hs_l1gs* P, const void* x, void* y, cudaStream_t st) {
 }
 
 template <typename T, typename IO, int SWEEP>
+int launch_view_lanes(hs_l1gs* P, const void* x, void* y, cudaStream_t st, size_t warp_bytes) {
+    ViewLanesParams p;
+    p.n = P->n;
+    p.ps = P->ps;
+    p.nparts = P->nparts;
+    p.ngroups = P->ngroups;
+    p.rp = P->rp;
+    p.ci = P->ci;
+    p.v = P->vs;
+    p.D = P->D;
+    p.x = x;
+    p.y = y;
+    p.cap_lo = P->cap_lo;
+    p.cap_up = P->cap_up;
+    p.warp_bytes = (uint32_t)warp_bytes;
+    const int wpb = (int)std::max<int64_t>(1, std::min<int64_t>(kWarpsPerBlock, (200 * 1024) / p.warp_bytes));
+    const size_t smem = (size_t)p.warp_bytes * wpb;
+    auto kern = l1gs_view_lanes_kernel<T, IO, SWEEP>;
+    if (P->launch_kernel != (const void*)kern) {
+        static thread_local int configured_smem = -1;
+        if ((int)smem > configured_smem) {
+            HS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            configured_smem = (int)smem;
+        }
+        int per_sm = 0;
+        HS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, wpb * 32, smem));
+        if (per_sm < 1) return hs::set_error(HS_ERR_UNSUPPORTED, "view partition needs too much shared memory");
+        const int64_t want = (P->ngroups + wpb - 1) / wpb;
+        P->launch_grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)per_sm * hs::num_sms()));
+        P->launch_kernel = (const void*)kern;
+    }
+    kern<<<P->launch_grid, wpb * 32, smem, st>>>(p);
+    HS_LAUNCH_CHECK("l1gs_view_lanes_kernel");
+    return HS_OK;
+}
+
+template <typename T, typename IO, int SWEEP>
 int launch_view_t(hs_l1gs* P, const void* x, void* y, cudaStream_t st) {
+    {
+        const size_t ps = (size_t)P->ps;
+        const size_t lanes_bytes = (sizeof(T) * (2 * ps * 33 + 32 * (size_t)(P->cap_lo + P->cap_up)) +
+                                    sizeof(uint16_t) * (2 * (ps + 1) * 32 + 32 * (size_t)(P->cap_lo + P->cap_up)) +
+                                    127) / 128 * 128;
+        if (lanes_bytes <= 100 * 1024 && P->cap_lo < 65535 && P->cap_up < 65535)
+            return launch_view_lanes<T, IO, SWEEP>(P, x, y, st, lanes_bytes);
+    }
     ViewParams p;
     p.n = P->n;
     p.ps = P->ps;
