@@ -19,6 +19,7 @@
 // norm is a fixed-order parallel sum (the reference's BLAS nrm2 order is
 // library-specific), so rho matches the reference to rounding.
 #include <algorithm>
+#include <mutex>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -836,3 +837,80 @@ int cheb_apply(hs_cheb* S, const void* r, void* z, int io, cudaStream_t st) {
     return HS_OK;
 }
 }  // namespace hs
+
+// ---------------------------------------------------------------------------
+// Chebyshev smoothing without device allocation.
+//
+// For callers that cannot call cudaMalloc at the point where they smooth: a
+// runtime that owns the whole device pool (an XLA/JAX or Julia CUDA.jl
+// allocator), code running under an allocator lock, or a serving loop that
+// forbids allocation on its hot path.  The caller passes every operand as a
+// device buffer it already owns; the smoother's work vectors (r and z, each
+// double-buffered) live in one file-scope device array instead of memory from
+// cudaMalloc.
+//
+// The array holds 4 * kNoAllocMaxN doubles (8 MiB) on every GPU that loads
+// this library, until the process exits.  All calls on a device share it and
+// it keeps the previous call's contents; every element a call reads has been
+// written earlier in the same call, so nothing needs clearing.  Calls whose
+// GPU work overlaps (two streams, or two host threads) race on the array.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int32_t kNoAllocMaxN = 262144;
+static __device__ __align__(256) double g_cheb_noalloc_scratch[4 * (size_t)kNoAllocMaxN];
+double* g_cheb_noalloc_addr[64] = {nullptr};
+std::mutex g_cheb_noalloc_mu;
+}  // namespace
+
+extern "C" int hs_cheb_smooth_noalloc(int32_t n, int64_t nnz, const int32_t* rp, const int32_t* ci, const double* v,
+                                      const double* l1inv, int32_t kind, int32_t degree, double rho, double astar,
+                                      double* x, const double* b, void* stream) {
+    if (n <= 0 || n > kNoAllocMaxN)
+        return hs::set_error(HS_ERR_ARG, "hs_cheb_smooth_noalloc: n = %d outside 1..%d (static scratch limit)", n,
+                             kNoAllocMaxN);
+    if (nnz < 0 || !rp || !ci || !v || !l1inv || !x || !b)
+        return hs::set_error(HS_ERR_ARG, "hs_cheb_smooth_noalloc: NULL operand or negative nnz");
+    if (kind != 1 && kind != 4) return hs::set_error(HS_ERR_ARG, "kind must be 1 or 4");
+    if (degree < 1) return hs::set_error(HS_ERR_ARG, "degree must be at least 1");
+    if (!(rho > 0)) return hs::set_error(HS_ERR_ARG, "rho must be positive");
+    if (kind == 1 && !(astar > 0 && astar < 1)) return hs::set_error(HS_ERR_ARG, "astar must lie in (0, 1)");
+    int dev = 0;
+    HS_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return hs::set_error(HS_ERR_ARG, "device index out of range");
+    double* scratch = nullptr;
+    {
+        // First call on this device (the device current here): resolve the
+        // device address of the array.  The host-side symbol is only a
+        // stand-in, never a device pointer.
+        std::lock_guard<std::mutex> lk(g_cheb_noalloc_mu);
+        if (!g_cheb_noalloc_addr[dev]) {
+            void* p = nullptr;
+            HS_CUDA(cudaGetSymbolAddress(&p, g_cheb_noalloc_scratch));
+            g_cheb_noalloc_addr[dev] = static_cast<double*>(p);
+        }
+        scratch = g_cheb_noalloc_addr[dev];
+    }
+    hs_matrix M;
+    M.n = n;
+    M.nnz = nnz;
+    M.dtype = HS_F64;
+    M.rp = const_cast<int32_t*>(rp);
+    M.ci = const_cast<int32_t*>(ci);
+    M.v = const_cast<double*>(v);
+    M.lpr = hsm::pick_lpr(nnz, n);
+    hs_cheb S;
+    S.n = n;
+    S.kind = kind;
+    S.degree = degree;
+    S.sdt = HS_F64;
+    S.rho = rho;
+    S.astar = kind == 1 ? astar : 0.0;
+    S.A = &M;
+    S.l1inv = const_cast<double*>(l1inv);
+    for (int i = 0; i < 4; ++i) S.w[i] = scratch + (size_t)i * n;
+    const int rc = hsm::cheb_smooth_t<double>(&S, x, b, HS_F64, false, static_cast<cudaStream_t>(stream));
+    S.A = nullptr;      // stack descriptors own nothing
+    S.l1inv = nullptr;
+    for (int i = 0; i < 4; ++i) S.w[i] = nullptr;
+    return rc;
+}

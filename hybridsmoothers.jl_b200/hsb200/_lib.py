@@ -82,6 +82,7 @@ PROTOTYPES = {
     "hs_cheb_info_get": (C.c_int, [_vp, C.POINTER(hs_cheb_info)]),
     "hs_cheb_set_rho": (C.c_int, [_vp, _d]),
     "hs_cheb_destroy": (C.c_int, [_vp]),
+    "hs_cheb_smooth_noalloc": (C.c_int, [_i32, _i64, _vp, _vp, _vp, _vp, _i32, _i32, _d, _d, _vp, _vp, _vp]),
     "hs_pcg_solve": (C.c_int, [_vp, _i32, _vp, _vp, _vp, _d, _i32, _vp, C.POINTER(hs_solve_info)]),
     "hs_gmres_solve": (C.c_int, [_vp, _i32, _vp, _i32, _vp, _vp, _d, _i32, _vp, C.POINTER(hs_solve_info)]),
     "hs_last_error": (C.c_char_p, []),
