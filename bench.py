@@ -45,6 +45,11 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--soak-s", type=float, default=1.0, help="untimed load before timing, for clock samples")
+    ap.add_argument("--suite", default=None,
+                    help="secondary measurements instead of the headline line: pcg1d, pcg128, gmres96, mixed160, "
+                         "serving (comma-separated; prints one JSON line each)")
+    ap.add_argument("--serving-count", type=int, default=512)
+    ap.add_argument("--serving-max", type=float, default=2e6)
     return ap.parse_args()
 
 
@@ -187,8 +192,186 @@ def cpu_apply_rate(A, wl, x, budget_s=10.0, max_reps=None):
     return reps, el, threads
 
 
+# ---------------------------------------------------------------------------
+# Secondary measurements (the other workloads; not the driver's headline line)
+# ---------------------------------------------------------------------------
+def _pcg_runs(M, b, P, reps, rtol=1e-8):
+    import torch
+    import hsb200
+    bd = torch.from_numpy(np.ascontiguousarray(b)).cuda()
+    x = torch.zeros_like(bd)
+    hsb200.pcg(M, bd, x, P, rtol=rtol)   # warm (kernel attributes, workspace)
+    ms, it, rel = [], None, None
+    for _ in range(reps):
+        info = hsb200.pcg(M, bd, x, P, rtol=rtol)
+        ms.append(info.ms)
+        it, rel = info.iterations, info.relres
+    return x, it, rel, ms
+
+
+def _pct(v, q):
+    return float(np.percentile(np.asarray(v), q))
+
+
+def suite_pcg1d(args):
+    """Workload 1: 1D Laplacian N=2048, b = ones, L1GS ps16 symmetric packed, PCG to 1e-8."""
+    import hsb200
+    from hsb200 import workloads as W
+    from oracle import hs_oracle as O
+    A = W.poisson_test_matrix(2048)
+    b = np.ones(2048)
+    P = hsb200.L1GSPrecBuilder(hsb200.CUDABackend(), threads=256, blocks=148)(A, 16, isSymA=True)
+    M = hsb200.DeviceSparseMatrix(A)
+    _, it, rel, ms = _pcg_runs(M, b, P, 50)
+    ref = O.OracleL1GS(A, 16, isSymA=True, sweep="symmetric", cache="packed", nchunks=4, chunksize=2)
+    t0 = time.perf_counter()
+    reps = 0
+    while time.perf_counter() - t0 < 3.0:
+        _, it_cpu, _ = O.pcg(A, b, ref)
+        reps += 1
+    cpu_s = (time.perf_counter() - t0) / reps
+    return {"suite": "pcg1d", "workload": "1D Laplacian N=2048, L1GS symmetric packed ps16, PCG 1e-8",
+            "iterations": it, "iterations_oracle": it_cpu, "relres": rel, "solves_per_s": 1e3 / float(np.median(ms)),
+            "p50_ms": _pct(ms, 50), "p99_ms": _pct(ms, 99),
+            "cpu_port_solves_per_s": 1.0 / cpu_s, "cpu_port_threads": O.omp_threads()}
+
+
+def suite_pcg128(args):
+    """Workload 2: 128^3 Poisson inside PCG: L1GS sweeps at partsize 16/64/256 and Chebyshev-4."""
+    import hsb200
+    from hsb200 import workloads as W
+    A = W.poisson3d_7pt(128)
+    b = W.rhs_uniform(A.shape[0])
+    M = hsb200.DeviceSparseMatrix(A)
+    out = []
+    for ps in (16, 64, 256):
+        for prec in (None, np.float32):
+            P = hsb200.L1GSPrecBuilder(hsb200.CUDABackend(), threads=256, blocks=148)(A, ps, isSymA=True,
+                                                                                     precision=prec)
+            _, it, rel, ms = _pcg_runs(M, b, P, 3)
+            out.append({"preconditioner": f"L1GS symmetric packed ps{ps}" + (" fp32" if prec else " fp64"),
+                        "iterations": it, "relres": rel, "ms": float(np.median(ms))})
+            del P
+    for eig in ("power", "lanczos"):
+        S = hsb200.build_smoother(hsb200.ChebyshevFourth(degree=4, eig=eig), A)
+        _, it, rel, ms = _pcg_runs(M, b, S, 3)
+        info = S.info
+        out.append({"preconditioner": f"Chebyshev-4 degree 4 ({eig})", "rho": info.rho,
+                    "lanczos": [info.lanczos_min, info.lanczos_max], "iterations": it, "relres": rel,
+                    "ms": float(np.median(ms))})
+    _, it, rel, ms = _pcg_runs(M, b, None, 2)
+    out.append({"preconditioner": "none", "iterations": it, "relres": rel, "ms": float(np.median(ms))})
+    return {"suite": "pcg128", "workload": "128^3 7-point Poisson, b~U[-1,1], PCG 1e-8", "runs": out}
+
+
+def suite_gmres96(args):
+    """Workload 3: 96^3 upwind convection-diffusion, ForwardSweep L1GS ps16, packed vs view, GMRES(30)."""
+    import torch
+    import hsb200
+    from hsb200 import workloads as W
+    A = W.convdiff3d_upwind(96)
+    b = W.rhs_uniform(A.shape[0])
+    M = hsb200.DeviceSparseMatrix(A)
+    bd = torch.from_numpy(b).cuda()
+    out = []
+    for cache in ("packed", "view"):
+        P = hsb200.L1GSPrecBuilder(hsb200.CUDABackend(), threads=256, blocks=148)(
+            A, 16, sweep=hsb200.ForwardSweep(),
+            cache_strategy=hsb200.PackedBufferCache() if cache == "packed" else hsb200.MatrixViewCache())
+        x = torch.zeros_like(bd)
+        hsb200.gmres(M, bd, x, P, restart=30)
+        info = hsb200.gmres(M, bd, x, P, restart=30)
+        out.append({"cache": cache, "iterations": info.iterations, "relres": info.relres, "ms": info.ms})
+    return {"suite": "gmres96", "workload": "96^3 upwind convection-diffusion (Pe=10), FWD L1GS ps16, GMRES(30) 1e-8",
+            "runs": out}
+
+
+def suite_mixed160(args):
+    """Workload 4: 160^3 27-point lognormal anisotropic diffusion, FP32 smoothers inside FP64 PCG."""
+    import torch
+    import hsb200
+    from hsb200 import workloads as W
+    t0 = time.perf_counter()
+    A = W.aniso27_lognormal(160)
+    gen_s = time.perf_counter() - t0
+    b = W.rhs_uniform(A.shape[0])
+    M = hsb200.DeviceSparseMatrix(A)
+    runs, sols = [], {}
+    for name, mk in (
+        ("L1GS symmetric packed ps16 fp64", lambda: hsb200.L1GSPrecBuilder(hsb200.CUDABackend(), threads=256,
+                                                                            blocks=148)(A, 16, isSymA=True)),
+        ("L1GS symmetric packed ps16 fp32", lambda: hsb200.L1GSPrecBuilder(hsb200.CUDABackend(), threads=256,
+                                                                            blocks=148)(A, 16, isSymA=True,
+                                                                                        precision=np.float32)),
+        ("Chebyshev-1 degree 6 fp64", lambda: hsb200.build_smoother(hsb200.ChebyshevFirst(degree=6), A)),
+        ("Chebyshev-1 degree 6 fp32", lambda: hsb200.build_smoother(hsb200.ChebyshevFirst(degree=6,
+                                                                                      precision=np.float32), A)),
+    ):
+        P = mk()
+        x, it, rel, ms = _pcg_runs(M, b, P, 2)
+        sols[name] = x.cpu().numpy()
+        runs.append({"preconditioner": name, "iterations": it, "relres": rel, "ms": float(np.median(ms))})
+        del P
+    for r in runs:
+        ref = sols[r["preconditioner"].replace("fp32", "fp64")]
+        x = sols[r["preconditioner"]]
+        r["error_vs_fp64_smoother_solve"] = float(np.linalg.norm(x - ref) / np.linalg.norm(ref))
+    return {"suite": "mixed160", "workload": "160^3 27-point lognormal(1) anisotropic diffusion, PCG 1e-8",
+            "n": A.shape[0], "nnz": A.nnz, "generate_s": gen_s, "runs": runs}
+
+
+def suite_serving(args):
+    """Workload 5: stream of SPD systems, served + batched FP32-smoother PCG vs the plain FP64 drop-in."""
+    from hsb200 import serving
+    from hsb200 import workloads as W
+    from hsb200.autotune import Autotuner
+    t0 = time.perf_counter()
+    reqs = W.serving_stream(count=args.serving_count, lo=1e3, hi=args.serving_max)
+    gen_s = time.perf_counter() - t0
+    rows = sum(A.shape[0] for _, A, _ in reqs)
+    seq = serving.solve_sequential(reqs, partsize=16)
+    tuner = Autotuner(trial_iters=20)
+    t1 = time.perf_counter()
+    for _, A, _ in reqs:
+        tuner.choose(A)
+    tune_s = time.perf_counter() - t1
+    # closed loop (all requests waiting at t=0): throughput
+    closed = serving.serve([(0.0, A, b) for _, A, b in reqs], max_slots=64, iters_per_step=8,
+                           partsize_of=tuner.partsize_of)
+    # open loop: Poisson arrivals at 80% of the served throughput
+    rate = 0.8 * closed["solves_per_s"]
+    rng = np.random.default_rng(1)
+    t = np.cumsum(rng.exponential(1.0 / rate, size=len(reqs)))
+    opened = serving.serve([(float(t[i]), A, b) for i, (_, A, b) in enumerate(reqs)], max_slots=64,
+                           iters_per_step=8, partsize_of=tuner.partsize_of)
+    return {"suite": "serving", "workload": f"{len(reqs)} 2D-5pt/3D-7pt variable-coefficient SPD systems, "
+                                             f"n log-uniform [1e3, {args.serving_max:.0e}], PCG 1e-8",
+            "total_rows": rows, "generate_s": gen_s,
+            "plain_fp64_dropin": {"solves_per_s": seq["solves_per_s"], "p50_s": seq["p50_s"], "p99_s": seq["p99_s"]},
+            "served_fp32_batched_closed_loop": {"solves_per_s": closed["solves_per_s"], "p50_s": closed["p50_s"],
+                                                "p99_s": closed["p99_s"]},
+            "served_fp32_batched_poisson": {"rate_per_s": rate, "solves_per_s": opened["solves_per_s"],
+                                            "p50_s": opened["p50_s"], "p99_s": opened["p99_s"]},
+            "speedup_closed_loop": closed["solves_per_s"] / seq["solves_per_s"],
+            "autotune": {"classes": len(tuner.cache), "seconds": tune_s,
+                         "choices": {str(k): v[0] for k, v in tuner.cache.items()}}}
+
+
+SUITES = {"pcg1d": suite_pcg1d, "pcg128": suite_pcg128, "gmres96": suite_gmres96, "mixed160": suite_mixed160,
+          "serving": suite_serving}
+
+
 def main():
     args = parse_args()
+    if args.suite:
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        for name in args.suite.split(","):
+            t0 = time.perf_counter()
+            res = SUITES[name](args)
+            res["seconds"] = round(time.perf_counter() - t0, 1)
+            print(json.dumps(res), flush=True)
+        return
     wl = parse_workload(args.workload)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -1,0 +1,787 @@
+// Batched, served PCG for many independent systems on one B200.
+//
+// Every admitted system ("slot") keeps its FP64 CSR matrix, its FP32 L1GS
+// symmetric packed preconditioner and its Krylov state (x, r, z, p, q and the
+// scalars) resident in HBM until it converges.  One batched PCG iteration
+// advances all active slots with a fixed number of launches, independent of
+// how many slots are active:
+//   seg_spmv_dot  q = A p and per-block partials of p.q      (all slots)
+//   seg_alpha     alpha = rz / pq                            (one block per slot)
+//   seg_update    x += alpha p, r -= alpha q, partials of r.r
+//   seg_check     convergence test, iteration count
+//   l1gs_batched  z = M^-1 r, one launch per partsize class (FP32 smoother, FP64 in/out)
+//   seg_dot       partials of r.z
+//   seg_beta      beta = rz_new / rz
+//   seg_p         p = z + beta p
+// The iteration is captured once as a CUDA graph per active set and replayed.
+// A slot's reductions always use the same blocks over its own rows and a
+// fixed-order finalize, so a slot's iterates are bitwise the same whether it
+// runs alone or among others.
+//
+// Admission (hs_batch_submit) builds the slot on a setup stream while the
+// solve stream keeps iterating, so new requests overlap running ones; a
+// request is refused with HS_ERR_BUDGET until a slot and enough of the HBM
+// budget are free.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "internal.cuh"
+#include "reduce.cuh"
+
+namespace {
+
+constexpr int kRPB = 256;     // rows per block of the segmented kernels
+constexpr int kT = 256;
+constexpr int kLPR = 8;       // lanes per row in the segmented SpMV
+
+struct Scalars {
+    double bb, rr, rz, pq, alpha, beta, tol2;
+    int done, it, conv_it, active;
+};
+
+struct SlotDev {
+    int32_t n, blk0, nblk, pad;
+    const int32_t* rp;
+    const int32_t* ci;
+    const double* v;
+    double *x, *r, *z, *p, *q;
+    Scalars* s;
+};
+
+struct BlockMap {
+    int32_t slot, row0;
+};
+
+// One work item of the batched L1GS apply: 32 partitions (a group) of a slot.
+struct PrecItem {
+    int32_t slot, group;
+};
+
+struct PrecDev {
+    int32_t n, ngroups, tlen, pad;
+    int64_t npad;
+    const float* Di;
+    const float* SLi;
+    const float* SUi;
+    const double* x;   // r
+    double* y;         // z
+    const Scalars* s;
+};
+
+__device__ __forceinline__ double block_partial(double v) { return hsdev::block_sum(v); }
+
+// ---- segmented PCG kernels --------------------------------------------------
+__global__ void __launch_bounds__(kT) seg_spmv_dot(const BlockMap* __restrict__ map, const SlotDev* __restrict__ slots,
+                                                   double* __restrict__ partials) {
+    const BlockMap m = map[blockIdx.x];
+    const SlotDev sd = slots[m.slot];
+    double part = 0.0;
+    if (!sd.s->done) {
+        const int lane = threadIdx.x & 31;
+        const int sub = lane & (kLPR - 1), base = lane - sub;
+        for (int r0 = m.row0 + (threadIdx.x >> 3); r0 < m.row0 + kRPB; r0 += kT / kLPR) {
+            // rows of one warp are 4 consecutive r0 values; the loop trip count is uniform
+            const bool valid = r0 < sd.n;
+            int32_t p0 = 0, p1 = 0;
+            if (valid) {
+                p0 = sd.rp[r0];
+                p1 = sd.rp[r0 + 1];
+            }
+            int chunks = valid ? (p1 - p0 + kLPR - 1) / kLPR : 0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) chunks = max(chunks, __shfl_xor_sync(0xffffffffu, chunks, o));
+            double acc = 0.0;
+            for (int c = 0; c < chunks; ++c) {
+                const int32_t q = p0 + c * kLPR + sub;
+                double prod = 0.0;
+                const int cnt = valid ? min(kLPR, p1 - (p0 + c * kLPR)) : 0;
+                if (sub < cnt) prod = __dmul_rn(sd.v[q], sd.p[sd.ci[q]]);
+#pragma unroll
+                for (int k = 0; k < kLPR; ++k) {
+                    const double pk = __shfl_sync(0xffffffffu, prod, base + k);
+                    if (sub == 0 && k < cnt) acc = __dadd_rn(acc, pk);
+                }
+            }
+            if (valid && sub == 0) {
+                sd.q[r0] = acc;
+                part += sd.p[r0] * acc;
+            }
+        }
+    }
+    part = block_partial(part);
+    if (threadIdx.x == 0) partials[blockIdx.x] = part;
+}
+
+__device__ __forceinline__ double slot_sum(const double* __restrict__ partials, const SlotDev& sd) {
+    double v = 0.0;
+    for (int i = threadIdx.x; i < sd.nblk; i += blockDim.x) v += partials[sd.blk0 + i];
+    return hsdev::block_sum(v);
+}
+
+__global__ void seg_alpha(const SlotDev* __restrict__ slots, const int32_t* __restrict__ active,
+                          const double* __restrict__ partials) {
+    const SlotDev sd = slots[active[blockIdx.x]];
+    const double pq = slot_sum(partials, sd);
+    if (threadIdx.x == 0 && !sd.s->done) {
+        sd.s->pq = pq;
+        sd.s->alpha = sd.s->rz / pq;
+    }
+}
+
+__global__ void __launch_bounds__(kT) seg_update(const BlockMap* __restrict__ map, const SlotDev* __restrict__ slots,
+                                                 double* __restrict__ partials) {
+    const BlockMap m = map[blockIdx.x];
+    const SlotDev sd = slots[m.slot];
+    double part = 0.0;
+    if (!sd.s->done) {
+        const double alpha = sd.s->alpha;
+        const int i = m.row0 + threadIdx.x;
+        if (i < sd.n) {
+            sd.x[i] += alpha * sd.p[i];
+            const double ri = sd.r[i] - alpha * sd.q[i];
+            sd.r[i] = ri;
+            part = ri * ri;
+        }
+    }
+    part = block_partial(part);
+    if (threadIdx.x == 0) partials[blockIdx.x] = part;
+}
+
+__global__ void seg_check(const SlotDev* __restrict__ slots, const int32_t* __restrict__ active,
+                          const double* __restrict__ partials, int32_t maxit) {
+    const SlotDev sd = slots[active[blockIdx.x]];
+    const double rr = slot_sum(partials, sd);
+    if (threadIdx.x == 0 && !sd.s->done) {
+        Scalars* s = sd.s;
+        s->it += 1;
+        s->rr = rr;
+        if (rr <= s->tol2) {
+            s->done = 1;
+            s->conv_it = s->it;
+        } else if (s->it >= maxit) {
+            s->done = 2;   // gave up
+            s->conv_it = s->it;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kT) seg_dot(const BlockMap* __restrict__ map, const SlotDev* __restrict__ slots,
+                                              double* __restrict__ partials) {
+    const BlockMap m = map[blockIdx.x];
+    const SlotDev sd = slots[m.slot];
+    double part = 0.0;
+    if (!sd.s->done) {
+        const int i = m.row0 + threadIdx.x;
+        if (i < sd.n) part = sd.r[i] * sd.z[i];
+    }
+    part = block_partial(part);
+    if (threadIdx.x == 0) partials[blockIdx.x] = part;
+}
+
+__global__ void seg_beta(const SlotDev* __restrict__ slots, const int32_t* __restrict__ active,
+                         const double* __restrict__ partials) {
+    const SlotDev sd = slots[active[blockIdx.x]];
+    const double rz = slot_sum(partials, sd);
+    if (threadIdx.x == 0 && !sd.s->done) {
+        sd.s->beta = rz / sd.s->rz;
+        sd.s->rz = rz;
+    }
+}
+
+__global__ void __launch_bounds__(kT) seg_p(const BlockMap* __restrict__ map, const SlotDev* __restrict__ slots) {
+    const BlockMap m = map[blockIdx.x];
+    const SlotDev sd = slots[m.slot];
+    if (sd.s->done) return;
+    const double beta = sd.s->beta;
+    const int i = m.row0 + threadIdx.x;
+    if (i < sd.n) sd.p[i] = sd.z[i] + beta * sd.p[i];
+}
+
+// Slot initialisation after admission: x = 0, r = b, bb = b.b (z, p, rz after the first apply)
+__global__ void init_vectors(int32_t n, const double* __restrict__ b, double* __restrict__ x, double* __restrict__ r) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        x[i] = 0.0;
+        r[i] = b[i];
+    }
+}
+
+__global__ void init_p_partials(int32_t n, const double* __restrict__ z, double* __restrict__ p,
+                                const double* __restrict__ r, const double* __restrict__ b,
+                                double* __restrict__ pbb, double* __restrict__ prz) {
+    double bb = 0.0, rz = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        p[i] = z[i];
+        bb += b[i] * b[i];
+        rz += r[i] * z[i];
+    }
+    bb = hsdev::block_sum(bb);
+    __syncthreads();
+    rz = hsdev::block_sum(rz);
+    if (threadIdx.x == 0) {
+        pbb[blockIdx.x] = bb;
+        prz[blockIdx.x] = rz;
+    }
+}
+
+__global__ void init_scalars(const double* __restrict__ pbb, const double* __restrict__ prz, int nb, Scalars* s,
+                             double rtol) {
+    double bb = 0.0, rz = 0.0;
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+        bb += pbb[i];
+        rz += prz[i];
+    }
+    bb = hsdev::block_sum(bb);
+    __syncthreads();
+    rz = hsdev::block_sum(rz);
+    if (threadIdx.x == 0) {
+        s->bb = bb;
+        s->rr = bb;
+        s->rz = rz;
+        s->tol2 = rtol * rtol * bb;
+        s->done = bb == 0.0 ? 1 : 0;
+        s->it = 0;
+        s->conv_it = s->done ? 0 : -1;
+        s->active = 1;
+    }
+}
+
+// ---- batched L1GS symmetric apply (FP32 smoother, FP64 vectors) -----------
+// Work item w -> (slot, group): 32 partitions of one slot, one lane each.
+// The packed streams of the slot are read tile by tile with 1D bulk copies
+// (one per stream row, 128 bytes) into a per-warp ring; y and D_Dl1 live in
+// registers, exactly like the single-system partsize<=32 kernel.
+template <int PS, int E, int STAGES>
+__global__ void __launch_bounds__(128, 3)
+    l1gs_batched_kernel(const PrecItem* __restrict__ items, int32_t nitems, const PrecDev* __restrict__ precs,
+                        int32_t* err) {
+    constexpr int TLEN = PS * (PS - 1) / 2;
+    constexpr int NT = (TLEN + E - 1) / E;
+    constexpr int NTPG = 2 * NT;
+    constexpr int XS = PS + 1;
+    static_assert(PS % 2 == 0, "even partsize");
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    constexpr uint32_t kRing = E * 32 * 4 * STAGES;
+    constexpr uint32_t kWarpBytes = (kRing + 8 * STAGES + 32 * XS * 4 + 127) / 128 * 128;
+    unsigned char* wbase = smem + (size_t)warp * kWarpBytes;
+    float* ring = reinterpret_cast<float*>(wbase);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(wbase + kRing);
+    float* xs = reinterpret_cast<float*>(wbase + kRing + 8 * STAGES);
+    const int wpb = blockDim.x >> 5;
+    const int32_t w0 = blockIdx.x * wpb + warp, wstride = gridDim.x * wpb;
+    const int32_t my_items = w0 < nitems ? (nitems - 1 - w0) / wstride + 1 : 0;
+    const int32_t total = my_items * NTPG;
+
+    auto issue = [&](int32_t c) {
+        const int32_t ii = c / NTPG;
+        int32_t ti = c - ii * NTPG;
+        const PrecItem it = items[w0 + ii * wstride];
+        const PrecDev& pd = precs[it.slot];
+        const float* base = ti < NT ? pd.SLi : pd.SUi;
+        if (ti >= NT) ti -= NT;
+        const int stage = c & (STAGES - 1);
+        const int rows = pd.s->done ? 0 : min(E, pd.tlen - ti * E);   // converged slot: empty tile
+        uint64_t* bar = bars + stage;
+        hsdev::mbar_arrive_expect_tx(bar, (uint32_t)(rows * 128));
+        for (int r = 0; r < rows; ++r) {
+            const float* src = base + ((int64_t)(ti * E + r)) * pd.npad + (int64_t)it.group * 32;
+            float* dst = ring + stage * (E * 32) + r * 32;
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], 128, [%2];" ::"r"(
+                    hsdev::smem_u32(dst)),
+                "l"(src), "r"(hsdev::smem_u32(bar))
+                : "memory");
+        }
+    };
+    auto wait = [&](int32_t c) -> bool {
+        const bool ok = hsdev::mbar_wait_bounded(bars + (c & (STAGES - 1)), (uint32_t)((c / STAGES) & 1));
+        return __all_sync(0xffffffffu, ok);
+    };
+    auto release = [&](int32_t c) {
+        __syncwarp();
+        if (lane == 0 && c + STAGES < total) {
+            hsdev::fence_proxy_async_smem();
+            issue(c + STAGES);
+        }
+    };
+    if (lane == 0) {
+        for (int s = 0; s < STAGES; ++s) hsdev::mbar_init(bars + s, 1);
+        hsdev::fence_barrier_init();
+        for (int32_t c = 0; c < min(total, STAGES); ++c) issue(c);
+    }
+    __syncwarp();
+
+    int32_t c = 0;
+    for (int32_t ii = 0; ii < my_items; ++ii) {
+        const PrecItem it = items[w0 + ii * wstride];
+        const PrecDev& pd = precs[it.slot];
+        if (pd.s->done) {   // converged: walk the (empty) tiles, leave z alone
+            for (int32_t t = 0; t < NTPG; ++t) {
+                if (!wait(c + t)) goto timeout;
+                release(c + t);
+            }
+            c += NTPG;
+            continue;
+        }
+        const int64_t k = (int64_t)it.group * 32 + lane;
+        const int64_t rowbase = (int64_t)it.group * 32 * PS;
+        float d[PS];
+#pragma unroll
+        for (int li = 0; li < PS; ++li) d[li] = pd.Di[(int64_t)li * pd.npad + k];
+#pragma unroll
+        for (int m = 0; m < PS; ++m) {
+            const int t = lane + 32 * m;
+            const int64_t row = rowbase + t;
+            xs[(t / PS) * XS + (t % PS)] = row < pd.n ? (float)pd.x[row] : 0.0f;
+        }
+        __syncwarp();
+        float yv[PS];
+#pragma unroll
+        for (int li = 0; li < PS; ++li) yv[li] = xs[lane * XS + li];
+#pragma unroll
+        for (int li = 0; li < PS; ++li) {
+            float acc = 0.0f;
+#pragma unroll
+            for (int lj = 0; lj < li; ++lj) {
+                const int e = li * (li - 1) / 2 + lj;
+                if (e % E == 0 && !wait(c + e / E)) goto timeout;
+                acc = __fadd_rn(acc, __fmul_rn(ring[((c + e / E) & (STAGES - 1)) * (E * 32) + (e % E) * 32 + lane],
+                                               yv[lj]));
+                if (e % E == E - 1 || e == TLEN - 1) release(c + e / E);
+            }
+            yv[li] = __fdiv_rn(__fsub_rn(yv[li], acc), d[li]);
+        }
+        c += NT;
+#pragma unroll
+        for (int li = 0; li < PS; ++li) yv[li] = __fmul_rn(d[li], yv[li]);
+#pragma unroll
+        for (int li = PS - 1; li >= 0; --li) {
+            float acc = 0.0f;
+#pragma unroll
+            for (int lj = li + 1; lj < PS; ++lj) {
+                const int q = PS - 1 - li;
+                const int e = q * (q - 1) / 2 + (lj - li - 1);
+                if (e % E == 0 && !wait(c + e / E)) goto timeout;
+                acc = __fadd_rn(acc, __fmul_rn(ring[((c + e / E) & (STAGES - 1)) * (E * 32) + (e % E) * 32 + lane],
+                                               yv[lj]));
+                if (e % E == E - 1 || e == TLEN - 1) release(c + e / E);
+            }
+            yv[li] = __fdiv_rn(__fsub_rn(yv[li], acc), d[li]);
+        }
+        c += NT;
+        __syncwarp();
+#pragma unroll
+        for (int li = 0; li < PS; ++li) xs[lane * XS + li] = yv[li];
+        __syncwarp();
+#pragma unroll
+        for (int m = 0; m < PS; ++m) {
+            const int t = lane + 32 * m;
+            const int64_t row = rowbase + t;
+            if (row < pd.n) pd.y[row] = (double)xs[(t / PS) * XS + (t % PS)];
+        }
+        __syncwarp();
+    }
+    return;
+timeout:
+    if (lane == 0) hsdev::report_error(err, hsdev::kErrWaitTimeout);
+    {
+        const int32_t end = min(total, c + STAGES);
+        for (int32_t cc = c; cc < end; ++cc)
+            (void)hsdev::mbar_wait_bounded(bars + (cc & (STAGES - 1)), (uint32_t)((cc / STAGES) & 1));
+    }
+}
+
+template <int PS>
+constexpr uint32_t batched_warp_bytes() {
+    return ((16 * 32 * 4 * 4) + 8 * 4 + 32 * (PS + 1) * 4 + 127) / 128 * 128;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Host engine
+// ---------------------------------------------------------------------------
+struct hs_batch_slot {
+    int state = 0;           // 0 free, 1 active, 2 finished (waiting for poll)
+    int64_t tag = 0;
+    hs_matrix* A = nullptr;
+    hs_l1gs* P = nullptr;
+    int32_t n = 0, ps = 0;
+    double* vec = nullptr;   // x r z p q b (6n doubles)
+    double* x_out = nullptr; // host destination
+    int64_t bytes = 0;
+    int32_t blk0 = 0, nblk = 0;
+};
+
+struct hs_batch_s {
+    hs_batch_config cfg;
+    cudaStream_t solve = nullptr, setup = nullptr;
+    std::vector<hs_batch_slot> slots;
+    SlotDev* d_slots = nullptr;
+    PrecDev* d_precs = nullptr;
+    Scalars* d_scal = nullptr;
+    std::vector<Scalars> h_scal;
+    BlockMap* d_map = nullptr;
+    int32_t* d_active = nullptr;
+    PrecItem* d_items = nullptr;
+    double* d_partials = nullptr;
+    double* d_init = nullptr;    // init partials (2 x kRedMaxBlocks)
+    int32_t max_blocks = 0, max_items = 0;
+    int64_t used = 0;
+    // current launch geometry
+    int32_t nblocks = 0, nactive = 0;
+    struct Cls {
+        int ps;
+        int32_t item0, nitems;
+    };
+    std::vector<Cls> classes;
+    bool dirty = true;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int32_t* err = nullptr;
+    int64_t iterations_run = 0;
+};
+
+namespace {
+
+int64_t slot_estimate(int32_t n, int64_t nnz, int ps) {
+    const int64_t nparts = (n + ps - 1) / ps;
+    const int64_t npad = (nparts + 31) / 32 * 32;
+    const int64_t tlen = (int64_t)ps * (ps - 1) / 2;
+    const int64_t prec = 4 * (2 * tlen * npad + (int64_t)ps * npad + n);
+    const int64_t mat = 4 * (n + 1) + 12 * nnz;
+    return prec + mat + 6 * 8 * (int64_t)n + 64 * 1024;
+}
+
+template <int PS>
+int launch_batched(hs_batch* B, const hs_batch_s::Cls& cl, cudaStream_t st) {
+    constexpr uint32_t wb = batched_warp_bytes<PS>();
+    const int wpb = 4;
+    const size_t smem = (size_t)wb * wpb;
+    auto kern = l1gs_batched_kernel<PS, 16, 4>;
+    static int configured = 0;
+    if (!configured) {
+        HS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        configured = 1;
+    }
+    int per_sm = 0;
+    HS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, wpb * 32, smem));
+    const int64_t want = (cl.nitems + wpb - 1) / wpb;
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)std::max(1, per_sm) * hs::num_sms()));
+    kern<<<grid, wpb * 32, smem, st>>>(B->d_items + cl.item0, cl.nitems, B->d_precs, B->err);
+    HS_LAUNCH_CHECK("l1gs_batched_kernel");
+    return HS_OK;
+}
+
+int launch_prec_class(hs_batch* B, const hs_batch_s::Cls& cl, cudaStream_t st) {
+    switch (cl.ps) {
+        case 8: return launch_batched<8>(B, cl, st);
+        case 16: return launch_batched<16>(B, cl, st);
+        case 32: return launch_batched<32>(B, cl, st);
+        default: return hs::set_error(HS_ERR_UNSUPPORTED, "batched partsize %d", cl.ps);
+    }
+}
+
+// Rebuild the device tables for the current active set.
+int rebuild(hs_batch* B) {
+    std::vector<BlockMap> map;
+    std::vector<int32_t> active;
+    std::vector<PrecItem> items;
+    B->classes.clear();
+    for (int ps : {8, 16, 32}) {
+        hs_batch_s::Cls cl{ps, (int32_t)items.size(), 0};
+        for (size_t s = 0; s < B->slots.size(); ++s) {
+            const hs_batch_slot& sl = B->slots[s];
+            if (sl.state != 1 || sl.ps != ps) continue;
+            hs::L1gsView lv;
+            hs::l1gs_view_of(sl.P, &lv);
+            for (int32_t g = 0; g < lv.ngroups; ++g) items.push_back({(int32_t)s, g});
+        }
+        cl.nitems = (int32_t)items.size() - cl.item0;
+        if (cl.nitems) B->classes.push_back(cl);
+    }
+    for (size_t s = 0; s < B->slots.size(); ++s) {
+        hs_batch_slot& sl = B->slots[s];
+        if (sl.state != 1) continue;
+        active.push_back((int32_t)s);
+        sl.blk0 = (int32_t)map.size();
+        sl.nblk = (sl.n + kRPB - 1) / kRPB;
+        for (int32_t b = 0; b < sl.nblk; ++b) map.push_back({(int32_t)s, b * kRPB});
+    }
+    if ((int32_t)map.size() > B->max_blocks || (int32_t)items.size() > B->max_items) {
+        cudaFree(B->d_map);
+        cudaFree(B->d_partials);
+        cudaFree(B->d_items);
+        B->max_blocks = std::max<int32_t>((int32_t)map.size() * 2, 1024);
+        B->max_items = std::max<int32_t>((int32_t)items.size() * 2, 1024);
+        HS_CUDA(cudaMalloc(&B->d_map, sizeof(BlockMap) * B->max_blocks));
+        HS_CUDA(cudaMalloc(&B->d_partials, sizeof(double) * B->max_blocks));
+        HS_CUDA(cudaMalloc(&B->d_items, sizeof(PrecItem) * B->max_items));
+    }
+    // slot tables
+    std::vector<SlotDev> sd(B->slots.size());
+    std::vector<PrecDev> pd(B->slots.size());
+    for (size_t s = 0; s < B->slots.size(); ++s) {
+        const hs_batch_slot& sl = B->slots[s];
+        if (sl.state == 0) continue;
+        SlotDev d{};
+        d.n = sl.n;
+        d.blk0 = sl.blk0;
+        d.nblk = sl.nblk;
+        const void* mv = nullptr;
+        int mdt = 0;
+        hs::matrix_arrays(sl.A, &d.rp, &d.ci, &mv, &mdt);
+        d.v = static_cast<const double*>(mv);
+        d.x = sl.vec;
+        d.r = sl.vec + sl.n;
+        d.z = sl.vec + 2 * (size_t)sl.n;
+        d.p = sl.vec + 3 * (size_t)sl.n;
+        d.q = sl.vec + 4 * (size_t)sl.n;
+        d.s = B->d_scal + s;
+        sd[s] = d;
+        hs::L1gsView lv;
+        hs::l1gs_view_of(sl.P, &lv);
+        PrecDev p{};
+        p.n = lv.n;
+        p.ngroups = lv.ngroups;
+        p.tlen = lv.tlen;
+        p.npad = lv.npad;
+        p.Di = static_cast<const float*>(lv.Di);
+        p.SLi = static_cast<const float*>(lv.SLi);
+        p.SUi = static_cast<const float*>(lv.SUi);
+        p.x = d.r;
+        p.y = d.z;
+        p.s = d.s;
+        pd[s] = p;
+    }
+    cudaStream_t st = B->solve;
+    if (!sd.empty()) {
+        HS_CUDA(cudaMemcpyAsync(B->d_slots, sd.data(), sizeof(SlotDev) * sd.size(), cudaMemcpyHostToDevice, st));
+        HS_CUDA(cudaMemcpyAsync(B->d_precs, pd.data(), sizeof(PrecDev) * pd.size(), cudaMemcpyHostToDevice, st));
+    }
+    if (!map.empty()) HS_CUDA(cudaMemcpyAsync(B->d_map, map.data(), sizeof(BlockMap) * map.size(), cudaMemcpyHostToDevice, st));
+    if (!active.empty())
+        HS_CUDA(cudaMemcpyAsync(B->d_active, active.data(), sizeof(int32_t) * active.size(), cudaMemcpyHostToDevice, st));
+    if (!items.empty())
+        HS_CUDA(cudaMemcpyAsync(B->d_items, items.data(), sizeof(PrecItem) * items.size(), cudaMemcpyHostToDevice, st));
+    HS_CUDA(cudaStreamSynchronize(st));   // host vectors above go out of scope
+    B->nblocks = (int32_t)map.size();
+    B->nactive = (int32_t)active.size();
+    if (B->exec) {
+        cudaGraphExecDestroy(B->exec);
+        B->exec = nullptr;
+    }
+    if (B->graph) {
+        cudaGraphDestroy(B->graph);
+        B->graph = nullptr;
+    }
+    B->dirty = false;
+    return HS_OK;
+}
+
+int enqueue_iteration(hs_batch* B, cudaStream_t st) {
+    if (B->nactive == 0) return HS_OK;
+    seg_spmv_dot<<<B->nblocks, kT, 0, st>>>(B->d_map, B->d_slots, B->d_partials);
+    seg_alpha<<<B->nactive, kT, 0, st>>>(B->d_slots, B->d_active, B->d_partials);
+    seg_update<<<B->nblocks, kT, 0, st>>>(B->d_map, B->d_slots, B->d_partials);
+    seg_check<<<B->nactive, kT, 0, st>>>(B->d_slots, B->d_active, B->d_partials, B->cfg.maxit);
+    hs::count_launch(4);
+    for (const auto& cl : B->classes) {
+        int rc = launch_prec_class(B, cl, st);
+        if (rc) return rc;
+    }
+    seg_dot<<<B->nblocks, kT, 0, st>>>(B->d_map, B->d_slots, B->d_partials);
+    seg_beta<<<B->nactive, kT, 0, st>>>(B->d_slots, B->d_active, B->d_partials);
+    seg_p<<<B->nblocks, kT, 0, st>>>(B->d_map, B->d_slots);
+    hs::count_launch(3);
+    HS_CUDA(cudaGetLastError());
+    return HS_OK;
+}
+
+void free_slot(hs_batch* B, hs_batch_slot& sl) {
+    if (sl.P) hs_l1gs_destroy(sl.P);
+    if (sl.A) hs_matrix_destroy(sl.A);
+    if (sl.vec) cudaFree(sl.vec);
+    B->used -= sl.bytes;
+    sl = hs_batch_slot();
+}
+
+}  // namespace
+
+extern "C" {
+
+int hs_batch_create(const hs_batch_config* cfg, void* stream, hs_batch** out) {
+    (void)stream;
+    if (!cfg || !out) return hs::set_error(HS_ERR_ARG, "hs_batch_create: NULL argument");
+    *out = nullptr;
+    if (cfg->max_slots < 1 || cfg->max_slots > 4096) return hs::set_error(HS_ERR_ARG, "max_slots out of range");
+    if (cfg->hbm_budget <= 0) return hs::set_error(HS_ERR_ARG, "hbm_budget must be positive");
+    if (cfg->maxit < 1) return hs::set_error(HS_ERR_ARG, "maxit must be positive");
+    hs_batch* B = new hs_batch();
+    B->cfg = *cfg;
+    B->slots.resize(cfg->max_slots);
+    B->h_scal.resize(cfg->max_slots);
+    cudaError_t e;
+    if ((e = cudaStreamCreateWithFlags(&B->solve, cudaStreamNonBlocking)) ||
+        (e = cudaStreamCreateWithFlags(&B->setup, cudaStreamNonBlocking)) ||
+        (e = cudaMalloc(&B->d_slots, sizeof(SlotDev) * cfg->max_slots)) ||
+        (e = cudaMalloc(&B->d_precs, sizeof(PrecDev) * cfg->max_slots)) ||
+        (e = cudaMalloc(&B->d_scal, sizeof(Scalars) * cfg->max_slots)) ||
+        (e = cudaMalloc(&B->d_active, sizeof(int32_t) * cfg->max_slots)) ||
+        (e = cudaMalloc(&B->d_init, sizeof(double) * 2 * hsdev::kRedMaxBlocks))) {
+        delete B;
+        return hs::cuda_error(e, "hs_batch_create");
+    }
+    cudaMemset(B->d_scal, 0, sizeof(Scalars) * cfg->max_slots);
+    B->err = hs::device_error_word();
+    *out = B;
+    return HS_OK;
+}
+
+int hs_batch_submit(hs_batch* B, const hs_sparse* A, const double* b_host, double* x_host, int64_t tag,
+                    int32_t partsize, int32_t* slot_out) {
+    if (!B || !A || !b_host || !x_host) return hs::set_error(HS_ERR_ARG, "hs_batch_submit: NULL argument");
+    const int ps = partsize > 0 ? partsize : B->cfg.partsize;
+    if (ps != 8 && ps != 16 && ps != 32) return hs::set_error(HS_ERR_ARG, "batched partsize must be 8, 16 or 32");
+    int32_t free_idx = -1;
+    for (size_t s = 0; s < B->slots.size(); ++s)
+        if (B->slots[s].state == 0) {
+            free_idx = (int32_t)s;
+            break;
+        }
+    const int64_t est = slot_estimate(A->n, A->nnz, ps);
+    if (free_idx < 0 || B->used + est > B->cfg.hbm_budget)
+        return hs::set_error(HS_ERR_BUDGET, "no free slot or HBM budget (%lld + %lld > %lld)", (long long)B->used,
+                             (long long)est, (long long)B->cfg.hbm_budget);
+    hs_batch_slot sl;
+    sl.tag = tag;
+    sl.n = A->n;
+    sl.ps = ps;
+    sl.x_out = x_host;
+    int rc = hs_matrix_create(A, HS_F64, B->setup, &sl.A);
+    if (!rc) rc = hs_l1gs_create(A, ps, 1, 1.5, HS_SWEEP_SYMMETRIC, HS_CACHE_PACKED, HS_F32, 256, 148, B->setup, &sl.P);
+    if (!rc) {
+        cudaError_t e = cudaMalloc(&sl.vec, sizeof(double) * 6 * (size_t)A->n);
+        if (e) rc = hs::cuda_error(e, "cudaMalloc (slot vectors)");
+    }
+    if (rc) {
+        if (sl.P) hs_l1gs_destroy(sl.P);
+        if (sl.A) hs_matrix_destroy(sl.A);
+        return rc;
+    }
+    sl.bytes = est;
+    const int32_t n = A->n;
+    double* x = sl.vec;
+    double* r = x + n;
+    double* z = r + n;
+    double* p = z + n;
+    double* b = p + 2 * (size_t)n;
+    cudaStream_t st = B->setup;
+    HS_CUDA(cudaMemcpyAsync(b, b_host, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+    const int g = (int)std::min<int64_t>((n + kT - 1) / kT, hsdev::kRedMaxBlocks);
+    init_vectors<<<g, kT, 0, st>>>(n, b, x, r);
+    hs::count_launch();
+    if ((rc = hs_l1gs_apply(sl.P, r, z, HS_F64, st))) return rc;
+    init_p_partials<<<g, kT, 0, st>>>(n, z, p, r, b, B->d_init, B->d_init + hsdev::kRedMaxBlocks);
+    init_scalars<<<1, kT, 0, st>>>(B->d_init, B->d_init + hsdev::kRedMaxBlocks, g, B->d_scal + free_idx, B->cfg.rtol);
+    hs::count_launch(2);
+    HS_CUDA(cudaGetLastError());
+    HS_CUDA(cudaStreamSynchronize(st));
+    sl.state = 1;
+    B->slots[free_idx] = sl;
+    B->used += est;
+    B->dirty = true;
+    if (slot_out) *slot_out = free_idx;
+    return HS_OK;
+}
+
+int hs_batch_step(hs_batch* B, int32_t iters, int32_t* finished) {
+    if (!B || iters < 1) return hs::set_error(HS_ERR_ARG, "hs_batch_step: bad argument");
+    int rc;
+    if (B->dirty && (rc = rebuild(B))) return rc;
+    if (B->nactive > 0) {
+        if (!B->exec) {
+            // warm launch (kernel attributes), then capture one iteration
+            cudaStream_t st = B->solve;
+            if ((rc = enqueue_iteration(B, st))) return rc;
+            HS_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            rc = enqueue_iteration(B, st);
+            cudaError_t ce = cudaStreamEndCapture(st, &B->graph);
+            if (rc) return rc;
+            HS_CUDA(ce);
+            HS_CUDA(cudaGraphInstantiate(&B->exec, B->graph, 0));
+            B->iterations_run += 1;
+            iters -= 1;
+        }
+        for (int k = 0; k < iters; ++k) HS_CUDA(cudaGraphLaunch(B->exec, B->solve));
+        B->iterations_run += iters;
+    }
+    HS_CUDA(cudaMemcpyAsync(B->h_scal.data(), B->d_scal, sizeof(Scalars) * B->slots.size(), cudaMemcpyDeviceToHost,
+                            B->solve));
+    HS_CUDA(cudaStreamSynchronize(B->solve));
+    int32_t nf = 0;
+    for (size_t s = 0; s < B->slots.size(); ++s) {
+        hs_batch_slot& sl = B->slots[s];
+        if (sl.state == 1 && B->h_scal[s].done) {
+            sl.state = 2;
+            B->dirty = true;
+            // copy the solution out now (the solve stream is idle)
+            HS_CUDA(cudaMemcpy(sl.x_out, sl.vec, sizeof(double) * sl.n, cudaMemcpyDeviceToHost));
+            ++nf;
+        }
+    }
+    if (finished) *finished = nf;
+    return HS_OK;
+}
+
+int hs_batch_poll(hs_batch* B, hs_batch_result* results, int32_t max_results, int32_t* count) {
+    if (!B || !count || (max_results > 0 && !results)) return hs::set_error(HS_ERR_ARG, "hs_batch_poll: bad argument");
+    int32_t c = 0;
+    for (size_t s = 0; s < B->slots.size() && c < max_results; ++s) {
+        hs_batch_slot& sl = B->slots[s];
+        if (sl.state != 2) continue;
+        const Scalars& sc = B->h_scal[s];
+        results[c].tag = sl.tag;
+        results[c].iterations = sc.conv_it;
+        results[c].converged = sc.done == 1;
+        results[c].relres = sc.bb > 0 ? std::sqrt(sc.rr / sc.bb) : 0.0;
+        ++c;
+        free_slot(B, sl);
+    }
+    *count = c;
+    return HS_OK;
+}
+
+int hs_batch_info_get(const hs_batch* B, hs_batch_info* info) {
+    if (!B || !info) return hs::set_error(HS_ERR_ARG, "hs_batch_info_get: NULL argument");
+    int32_t a = 0, f = 0;
+    for (const auto& s : B->slots) {
+        a += s.state == 1;
+        f += s.state == 2;
+    }
+    info->active = a;
+    info->finished = f;
+    info->hbm_used = B->used;
+    info->hbm_budget = B->cfg.hbm_budget;
+    info->iterations_run = B->iterations_run;
+    return HS_OK;
+}
+
+int hs_batch_destroy(hs_batch* B) {
+    if (!B) return HS_OK;
+    cudaDeviceSynchronize();
+    for (auto& s : B->slots)
+        if (s.state) free_slot(B, s);
+    if (B->exec) cudaGraphExecDestroy(B->exec);
+    if (B->graph) cudaGraphDestroy(B->graph);
+    void* ptrs[] = {B->d_slots, B->d_precs, B->d_scal, B->d_map, B->d_active, B->d_items, B->d_partials, B->d_init};
+    for (void* p : ptrs) cudaFree(p);
+    cudaStreamDestroy(B->solve);
+    cudaStreamDestroy(B->setup);
+    delete B;
+    return HS_OK;
+}
+
+}  // extern "C"

@@ -24,6 +24,7 @@
 #include <cstring>
 #include <vector>
 
+#include "internal.cuh"
 #include "reduce.cuh"
 #include "spmv.cuh"
 
@@ -466,6 +467,12 @@ int matrix_spmv(const hs_matrix* M, const void* x, void* y, double alpha, double
                               : hsm::spmv_t<float>(M, x, y, alpha, beta, st);
 }
 int matrix_n(const hs_matrix* M) { return M->n; }
+void matrix_arrays(const hs_matrix* M, const int32_t** rp, const int32_t** ci, const void** v, int* dtype) {
+    *rp = M->rp;
+    *ci = M->ci;
+    *v = M->v;
+    *dtype = M->dtype;
+}
 }  // namespace hs
 
 // ---------------------------------------------------------------------------
@@ -614,10 +621,6 @@ int cheb_smooth_t(hs_cheb* S, T* x, const void* b, int io, bool x_is_zero, cudaS
 
 }  // namespace hsm
 
-namespace hs {
-// z = M^-1 r for the Krylov drivers and hs_cheb_apply.
-int cheb_apply(hs_cheb* S, const void* r, void* z, int io, cudaStream_t st);
-}
 
 extern "C" {
 

@@ -14,13 +14,8 @@
 #include <cmath>
 #include <vector>
 
+#include "internal.cuh"
 #include "reduce.cuh"
-
-namespace hs {
-int matrix_spmv(const hs_matrix* M, const void* x, void* y, double alpha, double beta, cudaStream_t st);
-int matrix_n(const hs_matrix* M);
-int cheb_apply(hs_cheb* S, const void* r, void* z, int io, cudaStream_t st);
-}  // namespace hs
 
 namespace {
 
@@ -299,15 +294,34 @@ int hs_pcg_solve(hs_matrix* A, int32_t prec_type, void* prec, const double* b, d
         }
     } rejoin{own, caller, join};
     const int64_t n = hs::matrix_n(A);
-    DevBuf buf;
-    double *r, *z, *p, *q, *pa, *pb, *scal;
-    PcgScalars* s;
+    // Workspace kept per thread and device, grown on demand: repeated solves
+    // (a Krylov loop inside a time stepper, a served stream) do not pay
+    // cudaMalloc/cudaFree (and the device synchronisation of cudaFree) per solve.
+    static thread_local struct Ws {
+        int dev = -1;
+        int64_t cap = 0;
+        double* base = nullptr;
+    } ws;
+    int dev = 0;
+    HS_CUDA(cudaGetDevice(&dev));
+    const int64_t need = 4 * n + 2 * hsdev::kRedMaxBlocks + 2 + (int64_t)(sizeof(PcgScalars) / 8 + 1);
+    if (ws.dev != dev || ws.cap < need) {
+        if (ws.base && ws.dev == dev) cudaFree(ws.base);
+        ws.base = nullptr;
+        ws.cap = 0;
+        HS_CUDA(cudaMalloc(&ws.base, sizeof(double) * need));
+        ws.dev = dev;
+        ws.cap = need;
+    }
+    double* r = ws.base;
+    double* z = r + n;
+    double* p = z + n;
+    double* q = p + n;
+    double* pa = q + n;
+    double* pb = pa + hsdev::kRedMaxBlocks;
+    double* scal = pb + hsdev::kRedMaxBlocks;
+    PcgScalars* s = reinterpret_cast<PcgScalars*>(scal + 2);
     int rc;
-    if ((rc = buf.alloc(&r, 8 * n)) || (rc = buf.alloc(&z, 8 * n)) || (rc = buf.alloc(&p, 8 * n)) ||
-        (rc = buf.alloc(&q, 8 * n)) || (rc = buf.alloc(&pa, 8 * hsdev::kRedMaxBlocks)) ||
-        (rc = buf.alloc(&pb, 8 * hsdev::kRedMaxBlocks)) || (rc = buf.alloc(&scal, 16)) ||
-        (rc = buf.alloc(&s, sizeof(PcgScalars))))
-        return rc;
     const int ge = grid_elems(n), nb = hsdev::red_blocks(n);
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);

@@ -28,7 +28,7 @@
 #include <cstring>
 #include <vector>
 
-#include "hs_common.cuh"
+#include "internal.cuh"
 
 namespace {
 
@@ -1100,6 +1100,23 @@ void unpack_reference(const hs_l1gs* P, const TS* inter, TS* out, bool lower) {
 }
 
 }  // namespace
+
+namespace hs {
+int l1gs_view_of(const hs_l1gs* P, L1gsView* v) {
+    v->n = P->n;
+    v->ps = P->ps;
+    v->ngroups = P->ngroups;
+    v->tlen = (int32_t)P->tlen;
+    v->npad = P->npad;
+    v->Di = P->Di;
+    v->SLi = P->SLi;
+    v->SUi = P->SUi;
+    v->sdt = P->sdt;
+    v->sweep = P->sweep;
+    v->cache = P->cache;
+    return HS_OK;
+}
+}  // namespace hs
 
 // ---------------------------------------------------------------------------
 // C ABI

@@ -57,6 +57,20 @@ class hs_solve_info(C.Structure):
     _fields_ = [("iterations", C.c_int32), ("converged", C.c_int32), ("relres", C.c_double), ("ms", C.c_double)]
 
 
+class hs_batch_config(C.Structure):
+    _fields_ = [("max_slots", C.c_int32), ("hbm_budget", C.c_int64), ("partsize", C.c_int32), ("rtol", C.c_double),
+                ("maxit", C.c_int32)]
+
+
+class hs_batch_result(C.Structure):
+    _fields_ = [("tag", C.c_int64), ("iterations", C.c_int32), ("converged", C.c_int32), ("relres", C.c_double)]
+
+
+class hs_batch_info(C.Structure):
+    _fields_ = [("active", C.c_int32), ("finished", C.c_int32), ("hbm_used", C.c_int64), ("hbm_budget", C.c_int64),
+                ("iterations_run", C.c_int64)]
+
+
 _vp = C.c_void_p
 _i32 = C.c_int32
 _i64 = C.c_int64
@@ -85,6 +99,12 @@ PROTOTYPES = {
     "hs_cheb_smooth_noalloc": (C.c_int, [_i32, _i64, _vp, _vp, _vp, _vp, _i32, _i32, _d, _d, _vp, _vp, _vp]),
     "hs_pcg_solve": (C.c_int, [_vp, _i32, _vp, _vp, _vp, _d, _i32, _vp, C.POINTER(hs_solve_info)]),
     "hs_gmres_solve": (C.c_int, [_vp, _i32, _vp, _i32, _vp, _vp, _d, _i32, _vp, C.POINTER(hs_solve_info)]),
+    "hs_batch_create": (C.c_int, [C.POINTER(hs_batch_config), _vp, C.POINTER(_vp)]),
+    "hs_batch_submit": (C.c_int, [_vp, C.POINTER(hs_sparse), _vp, _vp, _i64, _i32, C.POINTER(_i32)]),
+    "hs_batch_step": (C.c_int, [_vp, _i32, C.POINTER(_i32)]),
+    "hs_batch_poll": (C.c_int, [_vp, C.POINTER(hs_batch_result), _i32, C.POINTER(_i32)]),
+    "hs_batch_info_get": (C.c_int, [_vp, C.POINTER(hs_batch_info)]),
+    "hs_batch_destroy": (C.c_int, [_vp]),
     "hs_last_error": (C.c_char_p, []),
     "hs_last_singular_col": (C.c_int32, []),
     "hs_device_error": (C.c_int, [_vp, C.POINTER(_i32)]),

@@ -1,0 +1,164 @@
+"""Serving and batching around the smoother path (no counterpart in the
+reference, whose callers solve one system at a time through LinearSolve).
+
+* ``BatchEngine`` wraps the C engine (``hs_batch_*``): each admitted system
+  keeps its FP64 matrix, an FP32 L1GS SymmetricSweep packed preconditioner and
+  its PCG state in HBM; one ``step`` advances every active system with one set
+  of graph-captured launches.  Admission is refused while no slot or not enough
+  of the HBM budget is free.
+* ``serve`` replays a timed request stream with continuous batching: requests
+  that arrive while others are on the GPU are admitted as slots and memory free
+  up, their setup overlaps the running iterations, and finished systems leave
+  at the next step.  It reports solves/s and p50/p99 latency
+  (arrival -> solution on the host).
+* ``solve_sequential`` is the plain drop-in: one FP64 L1GS-preconditioned PCG
+  solve after another, no batching.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import time
+from collections import deque
+
+import numpy as np
+
+from . import _lib as _L
+from ._lib import check, lib
+
+
+from ._lib import hs_batch_config, hs_batch_info, hs_batch_result  # noqa: E402
+
+
+class BatchEngine:
+    def __init__(self, max_slots=64, hbm_budget=64 << 30, partsize=16, rtol=1e-8, maxit=5000):
+        import torch
+        torch.cuda.init()
+        cfg = hs_batch_config(max_slots, int(hbm_budget), partsize, rtol, maxit)
+        self._h = C.c_void_p()
+        check(lib().hs_batch_create(C.byref(cfg), None, C.byref(self._h)))
+        self._keep = {}      # tag -> (host sparse, b, x)
+
+    def submit(self, A, b, tag, partsize=0):
+        """Admit a system; returns False (nothing changed) when it does not fit now."""
+        from . import _HostSparse
+        hA = _HostSparse(A, dtype=np.float64)
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros_like(b)
+        slot = C.c_int32()
+        st = lib().hs_batch_submit(self._h, C.byref(hA.desc), b.ctypes.data_as(C.c_void_p),
+                                   x.ctypes.data_as(C.c_void_p), int(tag), int(partsize), C.byref(slot))
+        if st == _L.HS_ERR_BUDGET:
+            return False
+        check(st)
+        self._keep[int(tag)] = (hA, b, x)
+        return True
+
+    def step(self, iters=4):
+        nf = C.c_int32()
+        check(lib().hs_batch_step(self._h, int(iters), C.byref(nf)))
+        return nf.value
+
+    def poll(self):
+        """[(tag, x, iterations, converged, relres)] of finished systems."""
+        out = []
+        buf = (hs_batch_result * 256)()
+        while True:
+            cnt = C.c_int32()
+            check(lib().hs_batch_poll(self._h, buf, 256, C.byref(cnt)))
+            for i in range(cnt.value):
+                r = buf[i]
+                _, _, x = self._keep.pop(int(r.tag))
+                out.append((int(r.tag), x, int(r.iterations), bool(r.converged), float(r.relres)))
+            if cnt.value < 256:
+                break
+        return out
+
+    def info(self):
+        i = hs_batch_info()
+        check(lib().hs_batch_info_get(self._h, C.byref(i)))
+        return i
+
+    def close(self):
+        if self._h:
+            lib().hs_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def percentile(v, q):
+    return float(np.percentile(np.asarray(v, dtype=np.float64), q)) if len(v) else float("nan")
+
+
+def serve(requests, max_slots=64, hbm_budget=64 << 30, iters_per_step=4, rtol=1e-8, partsize_of=None,
+          realtime=True, maxit=5000):
+    """Continuous-batching replay of [(arrival_s, A, b)].
+
+    partsize_of(A) -> 8/16/32 (the autotuner); default 16.
+    Returns dict with per-request latency, iterations, results and totals.
+    """
+    eng = BatchEngine(max_slots=max_slots, hbm_budget=hbm_budget, rtol=rtol, maxit=maxit)
+    order = sorted(range(len(requests)), key=lambda i: requests[i][0])
+    pending = deque(order)
+    waiting = deque()
+    arrival = {}
+    done_at, iters, conv, xs = {}, {}, {}, {}
+    t0 = time.perf_counter()
+    active = 0
+    while pending or waiting or active:
+        now = time.perf_counter() - t0
+        while pending and (not realtime or requests[pending[0]][0] <= now):
+            i = pending.popleft()
+            arrival[i] = requests[i][0] if realtime else now
+            waiting.append(i)
+        while waiting:
+            i = waiting[0]
+            _, A, b = requests[i]
+            ps = partsize_of(A) if partsize_of else 16
+            if not eng.submit(A, b, i, ps):
+                break
+            waiting.popleft()
+            active += 1
+        if active:
+            eng.step(iters_per_step)
+            for tag, x, it, ok, rel in eng.poll():
+                done_at[tag] = time.perf_counter() - t0
+                iters[tag], conv[tag], xs[tag] = it, ok, x
+                active -= 1
+        elif pending:
+            wait = requests[pending[0]][0] - (time.perf_counter() - t0)
+            if wait > 0:
+                time.sleep(min(wait, 0.01))
+    total = time.perf_counter() - t0
+    eng.close()
+    lat = [done_at[i] - arrival[i] for i in done_at]
+    return {"latency_s": lat, "iterations": iters, "converged": conv, "x": xs, "wall_s": total,
+            "solves_per_s": len(done_at) / total, "p50_s": percentile(lat, 50), "p99_s": percentile(lat, 99)}
+
+
+def solve_sequential(requests, partsize=16, rtol=1e-8, precision=None, maxit=5000):
+    """The plain FP64 drop-in: build + PCG per request, one after the other."""
+    import torch
+    import hsb200
+    t0 = time.perf_counter()
+    lat, iters = [], []
+    for arr, A, b in sorted(requests, key=lambda r: r[0]):
+        ts = time.perf_counter()
+        P = hsb200.L1GSPrecBuilder(hsb200.CUDABackend(), threads=256, blocks=148)(
+            A, partsize, isSymA=True, sweep=hsb200.SymmetricSweep(), cache_strategy=hsb200.PackedBufferCache(),
+            precision=precision)
+        M = hsb200.DeviceSparseMatrix(A)
+        bd = torch.from_numpy(np.ascontiguousarray(b)).cuda()
+        x = torch.zeros_like(bd)
+        info = hsb200.pcg(M, bd, x, P, rtol=rtol, maxit=maxit)
+        x.cpu()
+        lat.append(time.perf_counter() - ts)
+        iters.append(info.iterations)
+        del P, M
+    total = time.perf_counter() - t0
+    return {"wall_s": total, "solves_per_s": len(requests) / total, "latency_s": lat, "iterations": iters,
+            "p50_s": percentile(lat, 50), "p99_s": percentile(lat, 99)}

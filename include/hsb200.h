@@ -197,6 +197,45 @@ int hs_gmres_solve(hs_matrix* A, int32_t prec_type, void* prec, int32_t restart,
                    double* x, double rtol, int32_t maxit, void* stream, hs_solve_info* info);
 
 /* ---------------------------------------------------------------------- */
+/* Batched, served PCG (no counterpart in the reference: the serving and   */
+/* batching patterns around ldiv!).  Each admitted system keeps its FP64    */
+/* matrix, an FP32 L1GS SymmetricSweep packed preconditioner and its PCG    */
+/* state in HBM; hs_batch_step advances all of them with one set of        */
+/* launches.  Requests are refused with HS_ERR_BUDGET until a slot and      */
+/* enough of the HBM budget are free.                                      */
+/* ---------------------------------------------------------------------- */
+typedef struct hs_batch_s hs_batch;
+typedef struct {
+    int32_t max_slots;     /* systems resident at once */
+    int64_t hbm_budget;    /* bytes the batch may hold on the device */
+    int32_t partsize;      /* default partsize (8, 16 or 32) */
+    double rtol;           /* ||r|| <= rtol ||b|| */
+    int32_t maxit;         /* per-system iteration cap */
+} hs_batch_config;
+typedef struct {
+    int64_t tag;
+    int32_t iterations, converged;
+    double relres;         /* recursive residual ||r_k|| / ||b|| at exit */
+} hs_batch_result;
+typedef struct {
+    int32_t active, finished;
+    int64_t hbm_used, hbm_budget, iterations_run;
+} hs_batch_info;
+
+int hs_batch_create(const hs_batch_config* cfg, void* stream, hs_batch** out);
+/* Admit one system (host matrix, host b); x_host receives the solution when
+ * it converges.  partsize 0 = the batch default. */
+int hs_batch_submit(hs_batch* B, const hs_sparse* A, const double* b_host, double* x_host, int64_t tag,
+                    int32_t partsize, int32_t* slot);
+/* Run `iters` batched PCG iterations over every active system; *finished =
+ * systems that converged (or hit maxit) during this call. */
+int hs_batch_step(hs_batch* B, int32_t iters, int32_t* finished);
+/* Collect finished systems and release their device memory. */
+int hs_batch_poll(hs_batch* B, hs_batch_result* results, int32_t max_results, int32_t* count);
+int hs_batch_info_get(const hs_batch* B, hs_batch_info* info);
+int hs_batch_destroy(hs_batch* B);
+
+/* ---------------------------------------------------------------------- */
 /* Diagnostics                                                            */
 /* ---------------------------------------------------------------------- */
 const char* hs_last_error(void);

@@ -1,0 +1,137 @@
+"""Batched / served PCG (hs_batch_*): correctness, isolation and admission.
+
+* Every batched solve reaches ||b - A x|| <= ~1e-8 ||b|| and matches the
+  single-system device PCG with the same FP32 smoother within +-1 iteration.
+* A system's result is the same alone and in a mix of other systems — the
+  stated tolerance is exact equality (per-slot reductions use fixed blocks and
+  a fixed-order finalize).
+* Admission is refused beyond the HBM budget / slot count and succeeds once
+  memory frees up.
+"""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+import hsb200
+from hsb200 import serving
+from hsb200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def small_stream(count, seed, lo=800, hi=40000):
+    return W.serving_stream(count=count, lo=lo, hi=hi, seed=seed)
+
+
+def true_relres(A, x, b):
+    return np.linalg.norm(b - A @ x) / np.linalg.norm(b)
+
+
+def single_pcg_iters(A, b, ps):
+    P = hsb200.L1GSPrecBuilder(hsb200.CUDABackend(), threads=256, blocks=148)(A, ps, isSymA=True,
+                                                                             precision=np.float32)
+    M = hsb200.DeviceSparseMatrix(A)
+    bd = torch.from_numpy(b).cuda()
+    x = torch.zeros_like(bd)
+    info = hsb200.pcg(M, bd, x, P, rtol=1e-8)
+    return info.iterations
+
+
+@pytest.mark.parametrize("ps", [8, 16, 32])
+def test_batch_solves_match_single(ps):
+    reqs = small_stream(6, seed=ps)
+    eng = serving.BatchEngine(max_slots=16)
+    for i, (_, A, b) in enumerate(reqs):
+        assert eng.submit(A, b, i, ps)
+    results = {}
+    for _ in range(2000):
+        eng.step(8)
+        for tag, x, it, ok, rel in eng.poll():
+            results[tag] = (x, it, ok, rel)
+        if len(results) == len(reqs):
+            break
+    assert len(results) == len(reqs)
+    for i, (_, A, b) in enumerate(reqs):
+        x, it, ok, rel = results[i]
+        assert ok and rel <= 1e-8
+        assert true_relres(A, x, b) <= 5e-8
+        assert abs(it - single_pcg_iters(A, b, ps)) <= 1
+    eng.close()
+
+
+def test_same_result_alone_and_in_mix():
+    reqs = small_stream(8, seed=11)
+    target = reqs[3]
+    # alone
+    eng = serving.BatchEngine(max_slots=8)
+    eng.submit(target[1], target[2], 0, 16)
+    alone = None
+    while alone is None:
+        eng.step(4)
+        for tag, x, it, ok, rel in eng.poll():
+            alone = (x.copy(), it)
+    eng.close()
+    # in a mix, admitted after others are already iterating
+    eng = serving.BatchEngine(max_slots=8)
+    for i in (0, 1, 2):
+        eng.submit(reqs[i][1], reqs[i][2], 100 + i, (8, 16, 32)[i % 3])
+    eng.step(3)
+    eng.submit(target[1], target[2], 0, 16)
+    for i in (4, 5):
+        eng.submit(reqs[i][1], reqs[i][2], 100 + i, 32)
+    mixed = None
+    for _ in range(5000):
+        eng.step(5)
+        for tag, x, it, ok, rel in eng.poll():
+            if tag == 0:
+                mixed = (x.copy(), it)
+        if mixed is not None:
+            break
+    eng.close()
+    assert mixed is not None
+    assert mixed[1] == alone[1]
+    np.testing.assert_array_equal(mixed[0], alone[0])
+
+
+def test_budget_admission():
+    reqs = small_stream(4, seed=5, lo=20000, hi=30000)
+    eng = serving.BatchEngine(max_slots=8, hbm_budget=7_000_000)   # one ~20-30k-row system at a time
+    admitted = [eng.submit(A, b, i, 16) for i, (_, A, b) in enumerate(reqs)]
+    assert admitted[0] and not all(admitted)
+    done = set()
+    for _ in range(5000):
+        eng.step(8)
+        for tag, *_ in eng.poll():
+            done.add(tag)
+        for i, ok in enumerate(admitted):
+            if not ok and eng.submit(reqs[i][1], reqs[i][2], i, 16):
+                admitted[i] = True
+        if len(done) == len(reqs):
+            break
+    assert len(done) == len(reqs)
+    info = eng.info()
+    assert info.active == 0 and info.hbm_used == 0
+    eng.close()
+
+
+def test_serve_stream_reports_latency():
+    reqs = small_stream(24, seed=3)
+    # arrivals spread over 0.2 s
+    rng = np.random.default_rng(0)
+    t = np.cumsum(rng.exponential(0.2 / 24, size=24))
+    reqs = [(float(t[i]), A, b) for i, (_, A, b) in enumerate(reqs)]
+    out = serving.serve(reqs, max_slots=8, iters_per_step=4)
+    assert len(out["latency_s"]) == 24 and all(out["converged"].values())
+    assert out["p99_s"] >= out["p50_s"] > 0
+    for i, (_, A, b) in enumerate(reqs):
+        assert true_relres(A, out["x"][i], b) <= 5e-8
+
+
+def test_autotuner_picks_a_candidate():
+    from hsb200.autotune import Autotuner
+    A = W.variable_diffusion((24, 24, 24), np.random.default_rng(1))
+    tuner = Autotuner(trial_iters=10)
+    ps, cache = tuner.choose(A)
+    assert ps in (8, 16, 32) and cache == "packed"
+    assert tuner.choose(A) == (ps, cache)   # cached by matrix class
