@@ -18,10 +18,11 @@
 // fixed-order finalize, so a slot's iterates are bitwise the same whether it
 // runs alone or among others.
 //
-// Admission (hs_batch_submit) builds the slot on a setup stream while the
-// solve stream keeps iterating, so new requests overlap running ones; a
-// request is refused with HS_ERR_BUDGET until a slot and enough of the HBM
-// budget are free.
+// Admission (hs_batch_submit) builds the slot on a setup stream; called
+// between hs_batch_launch and hs_batch_wait it overlaps the running
+// iterations, and the new system joins at the next launch.  A request is
+// refused with HS_ERR_BUDGET until a slot and enough of the HBM budget are
+// free.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -29,17 +30,27 @@
 
 #include "internal.cuh"
 #include "reduce.cuh"
+#include "spmv.cuh"
 
 namespace {
 
 constexpr int kRPB = 256;     // rows per block of the segmented kernels
 constexpr int kT = 256;
-constexpr int kLPR = 8;       // lanes per row in the segmented SpMV
 
 struct Scalars {
-    double bb, rr, rz, pq, alpha, beta, tol2;
+    double bb, rr, rz, pq, alpha, beta, rtol;
     int done, it, conv_it, active;
 };
+
+using hsdev::DD;
+
+__device__ __forceinline__ void store_dd(double* partials, DD v) {
+    v = hsdev::block_dd(v);
+    if (threadIdx.x == 0) {
+        partials[2 * blockIdx.x] = v.s;
+        partials[2 * blockIdx.x + 1] = v.c;
+    }
+}
 
 struct SlotDev {
     int32_t n, blk0, nblk, pad;
@@ -70,54 +81,43 @@ struct PrecDev {
     const Scalars* s;
 };
 
-__device__ __forceinline__ double block_partial(double v) { return hsdev::block_sum(v); }
-
 // ---- segmented PCG kernels --------------------------------------------------
+// Same arithmetic as the single-system driver: compensated (Dot2) dots,
+// separately rounded updates, storage-order SpMV rows.
 __global__ void __launch_bounds__(kT) seg_spmv_dot(const BlockMap* __restrict__ map, const SlotDev* __restrict__ slots,
                                                    double* __restrict__ partials) {
+    __shared__ hsdev::CsrStream<double, kRPB, hsdev::stream_cap<kRPB>()> sh;
     const BlockMap m = map[blockIdx.x];
     const SlotDev sd = slots[m.slot];
-    double part = 0.0;
-    if (!sd.s->done) {
-        const int lane = threadIdx.x & 31;
-        const int sub = lane & (kLPR - 1), base = lane - sub;
-        for (int r0 = m.row0 + (threadIdx.x >> 3); r0 < m.row0 + kRPB; r0 += kT / kLPR) {
-            // rows of one warp are 4 consecutive r0 values; the loop trip count is uniform
-            const bool valid = r0 < sd.n;
-            int32_t p0 = 0, p1 = 0;
-            if (valid) {
-                p0 = sd.rp[r0];
-                p1 = sd.rp[r0 + 1];
-            }
-            int chunks = valid ? (p1 - p0 + kLPR - 1) / kLPR : 0;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) chunks = max(chunks, __shfl_xor_sync(0xffffffffu, chunks, o));
-            double acc = 0.0;
-            for (int c = 0; c < chunks; ++c) {
-                const int32_t q = p0 + c * kLPR + sub;
-                double prod = 0.0;
-                const int cnt = valid ? min(kLPR, p1 - (p0 + c * kLPR)) : 0;
-                if (sub < cnt) prod = __dmul_rn(sd.v[q], sd.p[sd.ci[q]]);
-#pragma unroll
-                for (int k = 0; k < kLPR; ++k) {
-                    const double pk = __shfl_sync(0xffffffffu, prod, base + k);
-                    if (sub == 0 && k < cnt) acc = __dadd_rn(acc, pk);
-                }
-            }
-            if (valid && sub == 0) {
-                sd.q[r0] = acc;
-                part += sd.p[r0] * acc;
-            }
+    DD part{0.0, 0.0};
+    if (!sd.s->done) {   // uniform over the block (one slot per block)
+        auto fp = [&](int32_t j) { return __ldg(sd.p + j); };
+        const double acc = hsdev::csr_stream_fold<double, kRPB, hsdev::stream_cap<kRPB>()>(
+            sh, sd.n, sd.rp, sd.ci, sd.v, m.row0, 0.0, fp, hsdev::AddOp<double>());
+        const int64_t r = m.row0 + threadIdx.x;
+        if (r < sd.n) {
+            sd.q[r] = acc;
+            hsdev::dd_add_prod(part, sd.p[r], acc);
         }
     }
-    part = block_partial(part);
-    if (threadIdx.x == 0) partials[blockIdx.x] = part;
+    store_dd(partials, part);
 }
 
+// Sum of a slot's block partials (valid on thread 0).  A large slot has
+// thousands of blocks: each thread loads 8 partials before adding any.
 __device__ __forceinline__ double slot_sum(const double* __restrict__ partials, const SlotDev& sd) {
-    double v = 0.0;
-    for (int i = threadIdx.x; i < sd.nblk; i += blockDim.x) v += partials[sd.blk0 + i];
-    return hsdev::block_sum(v);
+    DD v{0.0, 0.0};
+    const double2* p2 = reinterpret_cast<const double2*>(partials) + sd.blk0;
+    for (int base = threadIdx.x; base < sd.nblk; base += 8 * blockDim.x) {
+        double2 w[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            if (base + k * (int)blockDim.x < sd.nblk) w[k] = p2[base + k * blockDim.x];
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            if (base + k * (int)blockDim.x < sd.nblk) v = hsdev::dd_add(v, DD{w[k].x, w[k].y});
+    }
+    return hsdev::dd_value(hsdev::block_dd(v));
 }
 
 __global__ void seg_alpha(const SlotDev* __restrict__ slots, const int32_t* __restrict__ active,
@@ -126,7 +126,7 @@ __global__ void seg_alpha(const SlotDev* __restrict__ slots, const int32_t* __re
     const double pq = slot_sum(partials, sd);
     if (threadIdx.x == 0 && !sd.s->done) {
         sd.s->pq = pq;
-        sd.s->alpha = sd.s->rz / pq;
+        sd.s->alpha = __ddiv_rn(sd.s->rz, pq);
     }
 }
 
@@ -134,19 +134,18 @@ __global__ void __launch_bounds__(kT) seg_update(const BlockMap* __restrict__ ma
                                                  double* __restrict__ partials) {
     const BlockMap m = map[blockIdx.x];
     const SlotDev sd = slots[m.slot];
-    double part = 0.0;
+    DD part{0.0, 0.0};
     if (!sd.s->done) {
         const double alpha = sd.s->alpha;
         const int i = m.row0 + threadIdx.x;
         if (i < sd.n) {
-            sd.x[i] += alpha * sd.p[i];
-            const double ri = sd.r[i] - alpha * sd.q[i];
+            sd.x[i] = __dadd_rn(sd.x[i], __dmul_rn(alpha, sd.p[i]));
+            const double ri = __dsub_rn(sd.r[i], __dmul_rn(alpha, sd.q[i]));
             sd.r[i] = ri;
-            part = ri * ri;
+            hsdev::dd_add_prod(part, ri, ri);
         }
     }
-    part = block_partial(part);
-    if (threadIdx.x == 0) partials[blockIdx.x] = part;
+    store_dd(partials, part);
 }
 
 __global__ void seg_check(const SlotDev* __restrict__ slots, const int32_t* __restrict__ active,
@@ -157,7 +156,7 @@ __global__ void seg_check(const SlotDev* __restrict__ slots, const int32_t* __re
         Scalars* s = sd.s;
         s->it += 1;
         s->rr = rr;
-        if (rr <= s->tol2) {
+        if (sqrt(rr) <= __dmul_rn(s->rtol, sqrt(s->bb))) {
             s->done = 1;
             s->conv_it = s->it;
         } else if (s->it >= maxit) {
@@ -171,13 +170,12 @@ __global__ void __launch_bounds__(kT) seg_dot(const BlockMap* __restrict__ map, 
                                               double* __restrict__ partials) {
     const BlockMap m = map[blockIdx.x];
     const SlotDev sd = slots[m.slot];
-    double part = 0.0;
+    DD part{0.0, 0.0};
     if (!sd.s->done) {
         const int i = m.row0 + threadIdx.x;
-        if (i < sd.n) part = sd.r[i] * sd.z[i];
+        if (i < sd.n) hsdev::dd_add_prod(part, sd.r[i], sd.z[i]);
     }
-    part = block_partial(part);
-    if (threadIdx.x == 0) partials[blockIdx.x] = part;
+    store_dd(partials, part);
 }
 
 __global__ void seg_beta(const SlotDev* __restrict__ slots, const int32_t* __restrict__ active,
@@ -185,7 +183,7 @@ __global__ void seg_beta(const SlotDev* __restrict__ slots, const int32_t* __res
     const SlotDev sd = slots[active[blockIdx.x]];
     const double rz = slot_sum(partials, sd);
     if (threadIdx.x == 0 && !sd.s->done) {
-        sd.s->beta = rz / sd.s->rz;
+        sd.s->beta = __ddiv_rn(rz, sd.s->rz);
         sd.s->rz = rz;
     }
 }
@@ -196,7 +194,7 @@ __global__ void __launch_bounds__(kT) seg_p(const BlockMap* __restrict__ map, co
     if (sd.s->done) return;
     const double beta = sd.s->beta;
     const int i = m.row0 + threadIdx.x;
-    if (i < sd.n) sd.p[i] = sd.z[i] + beta * sd.p[i];
+    if (i < sd.n) sd.p[i] = __dadd_rn(sd.z[i], __dmul_rn(beta, sd.p[i]));
 }
 
 // Slot initialisation after admission: x = 0, r = b, bb = b.b (z, p, rz after the first apply)
@@ -210,36 +208,32 @@ __global__ void init_vectors(int32_t n, const double* __restrict__ b, double* __
 __global__ void init_p_partials(int32_t n, const double* __restrict__ z, double* __restrict__ p,
                                 const double* __restrict__ r, const double* __restrict__ b,
                                 double* __restrict__ pbb, double* __restrict__ prz) {
-    double bb = 0.0, rz = 0.0;
+    DD bb{0.0, 0.0}, rz{0.0, 0.0};
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         p[i] = z[i];
-        bb += b[i] * b[i];
-        rz += r[i] * z[i];
+        hsdev::dd_add_prod(bb, b[i], b[i]);
+        hsdev::dd_add_prod(rz, r[i], z[i]);
     }
-    bb = hsdev::block_sum(bb);
+    store_dd(pbb, bb);
     __syncthreads();
-    rz = hsdev::block_sum(rz);
-    if (threadIdx.x == 0) {
-        pbb[blockIdx.x] = bb;
-        prz[blockIdx.x] = rz;
-    }
+    store_dd(prz, rz);
 }
 
 __global__ void init_scalars(const double* __restrict__ pbb, const double* __restrict__ prz, int nb, Scalars* s,
                              double rtol) {
-    double bb = 0.0, rz = 0.0;
+    DD vb{0.0, 0.0}, vr{0.0, 0.0};
     for (int i = threadIdx.x; i < nb; i += blockDim.x) {
-        bb += pbb[i];
-        rz += prz[i];
+        vb = hsdev::dd_add(vb, DD{pbb[2 * i], pbb[2 * i + 1]});
+        vr = hsdev::dd_add(vr, DD{prz[2 * i], prz[2 * i + 1]});
     }
-    bb = hsdev::block_sum(bb);
+    const double bb = hsdev::dd_value(hsdev::block_dd(vb));
     __syncthreads();
-    rz = hsdev::block_sum(rz);
+    const double rz = hsdev::dd_value(hsdev::block_dd(vr));
     if (threadIdx.x == 0) {
         s->bb = bb;
         s->rr = bb;
         s->rz = rz;
-        s->tol2 = rtol * rtol * bb;
+        s->rtol = rtol;
         s->done = bb == 0.0 ? 1 : 0;
         s->it = 0;
         s->conv_it = s->done ? 0 : -1;
@@ -413,6 +407,7 @@ struct hs_batch_slot {
     double* x_out = nullptr; // host destination
     int64_t bytes = 0;
     int32_t blk0 = 0, nblk = 0;
+    bool launched = false;   // part of the active set of the launch in flight
 };
 
 struct hs_batch_s {
@@ -422,12 +417,14 @@ struct hs_batch_s {
     SlotDev* d_slots = nullptr;
     PrecDev* d_precs = nullptr;
     Scalars* d_scal = nullptr;
-    std::vector<Scalars> h_scal;
+    Scalars* h_scal = nullptr;          // pinned mirror of d_scal
+    cudaEvent_t launched = nullptr;     // end of the last hs_batch_launch
+    bool inflight = false;
     BlockMap* d_map = nullptr;
     int32_t* d_active = nullptr;
     PrecItem* d_items = nullptr;
     double* d_partials = nullptr;
-    double* d_init = nullptr;    // init partials (2 x kRedMaxBlocks)
+    double* d_init = nullptr;    // init partials (2 x 2 x kRedMaxBlocks)
     int32_t max_blocks = 0, max_items = 0;
     int64_t used = 0;
     // current launch geometry
@@ -517,7 +514,7 @@ int rebuild(hs_batch* B) {
         B->max_blocks = std::max<int32_t>((int32_t)map.size() * 2, 1024);
         B->max_items = std::max<int32_t>((int32_t)items.size() * 2, 1024);
         HS_CUDA(cudaMalloc(&B->d_map, sizeof(BlockMap) * B->max_blocks));
-        HS_CUDA(cudaMalloc(&B->d_partials, sizeof(double) * B->max_blocks));
+        HS_CUDA(cudaMalloc(&B->d_partials, 2 * sizeof(double) * B->max_blocks));
         HS_CUDA(cudaMalloc(&B->d_items, sizeof(PrecItem) * B->max_items));
     }
     // slot tables
@@ -622,15 +619,16 @@ int hs_batch_create(const hs_batch_config* cfg, void* stream, hs_batch** out) {
     hs_batch* B = new hs_batch();
     B->cfg = *cfg;
     B->slots.resize(cfg->max_slots);
-    B->h_scal.resize(cfg->max_slots);
     cudaError_t e;
     if ((e = cudaStreamCreateWithFlags(&B->solve, cudaStreamNonBlocking)) ||
+        (e = cudaEventCreateWithFlags(&B->launched, cudaEventDisableTiming)) ||
+        (e = cudaMallocHost(&B->h_scal, sizeof(Scalars) * cfg->max_slots)) ||
         (e = cudaStreamCreateWithFlags(&B->setup, cudaStreamNonBlocking)) ||
         (e = cudaMalloc(&B->d_slots, sizeof(SlotDev) * cfg->max_slots)) ||
         (e = cudaMalloc(&B->d_precs, sizeof(PrecDev) * cfg->max_slots)) ||
         (e = cudaMalloc(&B->d_scal, sizeof(Scalars) * cfg->max_slots)) ||
         (e = cudaMalloc(&B->d_active, sizeof(int32_t) * cfg->max_slots)) ||
-        (e = cudaMalloc(&B->d_init, sizeof(double) * 2 * hsdev::kRedMaxBlocks))) {
+        (e = cudaMalloc(&B->d_init, sizeof(double) * 4 * hsdev::kRedMaxBlocks))) {
         delete B;
         return hs::cuda_error(e, "hs_batch_create");
     }
@@ -660,8 +658,13 @@ int hs_batch_submit(hs_batch* B, const hs_sparse* A, const double* b_host, doubl
     sl.n = A->n;
     sl.ps = ps;
     sl.x_out = x_host;
-    int rc = hs_matrix_create(A, HS_F64, B->setup, &sl.A);
-    if (!rc) rc = hs_l1gs_create(A, ps, 1, 1.5, HS_SWEEP_SYMMETRIC, HS_CACHE_PACKED, HS_F32, 256, 148, B->setup, &sl.P);
+    // The engine solves SPD systems (CG): a symmetric CSC's columns are its
+    // rows, so the arrays are uploaded once, as CSR, and the FP32 smoother is
+    // packed from that device copy (isSymA reads column i as row i).
+    hs_sparse rows = *A;
+    rows.format = HS_CSR;
+    int rc = hs_matrix_create(&rows, HS_F64, B->setup, &sl.A);
+    if (!rc) rc = hs::l1gs_create_from_matrix(sl.A, ps, 1.5, HS_SWEEP_SYMMETRIC, HS_F32, B->setup, &sl.P);
     if (!rc) {
         cudaError_t e = cudaMalloc(&sl.vec, sizeof(double) * 6 * (size_t)A->n);
         if (e) rc = hs::cuda_error(e, "cudaMalloc (slot vectors)");
@@ -684,8 +687,9 @@ int hs_batch_submit(hs_batch* B, const hs_sparse* A, const double* b_host, doubl
     init_vectors<<<g, kT, 0, st>>>(n, b, x, r);
     hs::count_launch();
     if ((rc = hs_l1gs_apply(sl.P, r, z, HS_F64, st))) return rc;
-    init_p_partials<<<g, kT, 0, st>>>(n, z, p, r, b, B->d_init, B->d_init + hsdev::kRedMaxBlocks);
-    init_scalars<<<1, kT, 0, st>>>(B->d_init, B->d_init + hsdev::kRedMaxBlocks, g, B->d_scal + free_idx, B->cfg.rtol);
+    init_p_partials<<<g, kT, 0, st>>>(n, z, p, r, b, B->d_init, B->d_init + 2 * hsdev::kRedMaxBlocks);
+    init_scalars<<<1, kT, 0, st>>>(B->d_init, B->d_init + 2 * hsdev::kRedMaxBlocks, g, B->d_scal + free_idx,
+                                   B->cfg.rtol);
     hs::count_launch(2);
     HS_CUDA(cudaGetLastError());
     HS_CUDA(cudaStreamSynchronize(st));
@@ -697,8 +701,9 @@ int hs_batch_submit(hs_batch* B, const hs_sparse* A, const double* b_host, doubl
     return HS_OK;
 }
 
-int hs_batch_step(hs_batch* B, int32_t iters, int32_t* finished) {
-    if (!B || iters < 1) return hs::set_error(HS_ERR_ARG, "hs_batch_step: bad argument");
+int hs_batch_launch(hs_batch* B, int32_t iters) {
+    if (!B || iters < 1) return hs::set_error(HS_ERR_ARG, "hs_batch_launch: bad argument");
+    if (B->inflight) return hs::set_error(HS_ERR_ARG, "hs_batch_launch: the previous launch was not waited for");
     int rc;
     if (B->dirty && (rc = rebuild(B))) return rc;
     if (B->nactive > 0) {
@@ -718,22 +723,41 @@ int hs_batch_step(hs_batch* B, int32_t iters, int32_t* finished) {
         for (int k = 0; k < iters; ++k) HS_CUDA(cudaGraphLaunch(B->exec, B->solve));
         B->iterations_run += iters;
     }
-    HS_CUDA(cudaMemcpyAsync(B->h_scal.data(), B->d_scal, sizeof(Scalars) * B->slots.size(), cudaMemcpyDeviceToHost,
+    // Slots admitted while this launch runs are not part of it: their entries
+    // in the scalars copy below are not theirs yet.
+    for (auto& sl : B->slots) sl.launched = sl.state == 1;
+    HS_CUDA(cudaMemcpyAsync(B->h_scal, B->d_scal, sizeof(Scalars) * B->slots.size(), cudaMemcpyDeviceToHost,
                             B->solve));
-    HS_CUDA(cudaStreamSynchronize(B->solve));
+    HS_CUDA(cudaEventRecord(B->launched, B->solve));
+    B->inflight = true;
+    return HS_OK;
+}
+
+int hs_batch_wait(hs_batch* B, int32_t* finished) {
+    if (!B) return hs::set_error(HS_ERR_ARG, "hs_batch_wait: NULL argument");
     int32_t nf = 0;
-    for (size_t s = 0; s < B->slots.size(); ++s) {
-        hs_batch_slot& sl = B->slots[s];
-        if (sl.state == 1 && B->h_scal[s].done) {
-            sl.state = 2;
-            B->dirty = true;
-            // copy the solution out now (the solve stream is idle)
-            HS_CUDA(cudaMemcpy(sl.x_out, sl.vec, sizeof(double) * sl.n, cudaMemcpyDeviceToHost));
-            ++nf;
+    if (B->inflight) {
+        B->inflight = false;
+        HS_CUDA(cudaEventSynchronize(B->launched));
+        for (size_t s = 0; s < B->slots.size(); ++s) {
+            hs_batch_slot& sl = B->slots[s];
+            if (sl.state == 1 && sl.launched && B->h_scal[s].done) {
+                sl.state = 2;
+                B->dirty = true;
+                // the solve stream has passed the event: x is final
+                HS_CUDA(cudaMemcpy(sl.x_out, sl.vec, sizeof(double) * sl.n, cudaMemcpyDeviceToHost));
+                ++nf;
+            }
         }
     }
     if (finished) *finished = nf;
     return HS_OK;
+}
+
+int hs_batch_step(hs_batch* B, int32_t iters, int32_t* finished) {
+    const int rc = hs_batch_launch(B, iters);
+    if (rc) return rc;
+    return hs_batch_wait(B, finished);
 }
 
 int hs_batch_poll(hs_batch* B, hs_batch_result* results, int32_t max_results, int32_t* count) {
@@ -780,6 +804,8 @@ int hs_batch_destroy(hs_batch* B) {
     for (void* p : ptrs) cudaFree(p);
     cudaStreamDestroy(B->solve);
     cudaStreamDestroy(B->setup);
+    if (B->launched) cudaEventDestroy(B->launched);
+    if (B->h_scal) cudaFreeHost(B->h_scal);
     delete B;
     return HS_OK;
 }

@@ -41,7 +41,7 @@ struct hs_matrix_s {
     int32_t* rp = nullptr;
     int32_t* ci = nullptr;
     void* v = nullptr;
-    int lpr = 8;
+    int lpr = 256;   // rows per CSR-stream block
     int64_t bytes = 0;
 };
 
@@ -49,13 +49,12 @@ namespace hsm {
 
 inline size_t dsize(int dt) { return dt == HS_F64 ? 8 : 4; }
 
+// Rows per CSR-stream block: 256 while a block's products fit its staging area
+// (2048 entries: up to 8 per row, with margin for uneven rows), 128 beyond
+// (4096 entries, 32 per row; longer blocks fold from global memory).
 int pick_lpr(int64_t nnz, int32_t n) {
     const double avg = n > 0 ? (double)nnz / n : 1.0;
-    if (avg <= 2) return 2;
-    if (avg <= 4) return 4;
-    if (avg <= 8) return 8;
-    if (avg <= 16) return 16;
-    return 32;
+    return avg <= 7.5 ? 256 : 128;
 }
 
 // Host CSR (row-wise) arrays from an hs_sparse, values as double.
@@ -143,40 +142,38 @@ int matrix_from_host(const std::vector<int32_t>& rp, const std::vector<int32_t>&
 // ---------------------------------------------------------------------------
 constexpr int kThreads = 256;
 
-template <int LPR>
-__device__ __forceinline__ void row_of(int64_t& row, int64_t& stride_rows) {
-    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    row = warp * (32 / LPR) + ((threadIdx.x & 31) / LPR);
-    stride_rows = nwarps * (32 / LPR);
-}
+// Every SpMV-shaped kernel below runs the block CSR-stream of spmv.cuh: a
+// block of BR threads owns BR consecutive rows; BR = 256 for short rows, 128
+// for long ones (the block's products must fit stream_cap<BR>).  Grid-stride
+// over row blocks.
+#define HS_CS_ROWS_LOOP(BR) \
+    for (int64_t row0 = (int64_t)blockIdx.x * (BR); row0 < n; row0 += (int64_t)gridDim.x * (BR))
+#define HS_CS_FOLD(T, BR) hsdev::csr_stream_fold<T, BR, hsdev::stream_cap<BR>()>
+#define HS_CS_SHARED(T, BR) __shared__ hsdev::CsrStream<T, BR, hsdev::stream_cap<BR>()> sh
 
 // MODE 0: y = A x; MODE 1: y = y - A x (term by term); MODE 2: y = beta y + sum (a x) alpha.
-template <typename T, int LPR, int MODE>
-__global__ void __launch_bounds__(kThreads) spmv_kernel(int32_t n, const int32_t* __restrict__ rp,
-                                                        const int32_t* __restrict__ ci, const T* __restrict__ v,
-                                                        const T* __restrict__ x, T* __restrict__ y, T alpha, T beta) {
-    int64_t row, stride;
-    row_of<LPR>(row, stride);
-    const int64_t row_base0 = row - ((threadIdx.x & 31) / LPR);
-    for (int64_t r0 = row_base0; r0 < n; r0 += stride) {
-        const int64_t rr = r0 + ((threadIdx.x & 31) / LPR);
-        const bool valid = rr < n;
-        const int mc = hsdev::warp_max_chunks<LPR>(rp, rr, valid);
-        auto fx = [&](int32_t j) { return __ldg(x + j); };
+template <typename T, int BR, int MODE>
+__global__ void __launch_bounds__(BR, 1024 / BR) spmv_kernel(int32_t n, const int32_t* __restrict__ rp,
+                                                           const int32_t* __restrict__ ci, const T* __restrict__ v,
+                                                           const T* __restrict__ x, T* __restrict__ y, T alpha,
+                                                           T beta) {
+    HS_CS_SHARED(T, BR);
+    auto fx = [&](int32_t j) { return __ldg(x + j); };
+    HS_CS_ROWS_LOOP(BR) {
+        const int64_t r = row0 + threadIdx.x;
+        const bool valid = r < n;
         T acc;
         if (MODE == 0) {
-            acc = hsdev::row_fold<LPR>(rp, ci, v, rr, valid, T(0), fx, AddOp<T>(), mc);
+            acc = HS_CS_FOLD(T, BR)(sh, n, rp, ci, v, row0, T(0), fx, AddOp<T>());
         } else if (MODE == 1) {
-            const T a0 = valid ? y[rr] : T(0);
-            acc = hsdev::row_fold<LPR>(rp, ci, v, rr, valid, a0, fx, SubOp<T>(), mc);
+            acc = HS_CS_FOLD(T, BR)(sh, n, rp, ci, v, row0, valid ? y[r] : T(0), fx, SubOp<T>());
         } else {
             T a0 = T(0);
-            if (valid && beta != T(0)) a0 = (beta == T(1)) ? y[rr] : mul_rn(y[rr], beta);
+            if (valid && beta != T(0)) a0 = (beta == T(1)) ? y[r] : mul_rn(y[r], beta);
             auto op = [alpha](T a, T p) { return add_rn(a, mul_rn(p, alpha)); };
-            acc = hsdev::row_fold<LPR>(rp, ci, v, rr, valid, a0, fx, op, mc);
+            acc = HS_CS_FOLD(T, BR)(sh, n, rp, ci, v, row0, a0, fx, op);
         }
-        if (valid && (threadIdx.x & (LPR - 1)) == 0) y[rr] = acc;
+        if (valid) y[r] = acc;
     }
 }
 
@@ -202,29 +199,27 @@ __global__ void fill_kernel(T* __restrict__ a, int64_t n, T value) {
         a[i] = value;
 }
 
-// Power iteration step (chebyshev.jl:46-51): w = l1inv .* (A v); partial sum of w.^2.
-template <int LPR>
-__global__ void __launch_bounds__(kThreads) power_spmv_kernel(int32_t n, const int32_t* __restrict__ rp,
-                                                              const int32_t* __restrict__ ci,
-                                                              const double* __restrict__ v,
-                                                              const double* __restrict__ vin,
-                                                              const double* __restrict__ l1inv,
-                                                              double* __restrict__ w, double* __restrict__ partials,
-                                                              const int* __restrict__ stop) {
+// Power iteration step (chebyshev.jl:46-51): w = l1inv .* (A v); partial sum
+// of w.^2 per block (grid <= partials capacity).
+template <int BR>
+__global__ void __launch_bounds__(BR, 1024 / BR) power_spmv_kernel(int32_t n, const int32_t* __restrict__ rp,
+                                                                 const int32_t* __restrict__ ci,
+                                                                 const double* __restrict__ v,
+                                                                 const double* __restrict__ vin,
+                                                                 const double* __restrict__ l1inv,
+                                                                 double* __restrict__ w,
+                                                                 double* __restrict__ partials,
+                                                                 const int* __restrict__ stop) {
     if (*stop) return;
-    int64_t row, stride;
-    row_of<LPR>(row, stride);
-    const int64_t row_base0 = row - ((threadIdx.x & 31) / LPR);
+    HS_CS_SHARED(double, BR);
+    auto fx = [&](int32_t j) { return __ldg(vin + j); };
     double ss = 0.0;
-    for (int64_t r0 = row_base0; r0 < n; r0 += stride) {
-        const int64_t rr = r0 + ((threadIdx.x & 31) / LPR);
-        const bool valid = rr < n;
-        const int mc = hsdev::warp_max_chunks<LPR>(rp, rr, valid);
-        auto fx = [&](int32_t j) { return __ldg(vin + j); };
-        double acc = hsdev::row_fold<LPR>(rp, ci, v, rr, valid, 0.0, fx, AddOp<double>(), mc);
-        if (valid && (threadIdx.x & (LPR - 1)) == 0) {
-            const double wi = __dmul_rn(acc, l1inv[rr]);
-            w[rr] = wi;
+    HS_CS_ROWS_LOOP(BR) {
+        const int64_t r = row0 + threadIdx.x;
+        const double acc = HS_CS_FOLD(double, BR)(sh, n, rp, ci, v, row0, 0.0, fx, AddOp<double>());
+        if (r < n) {
+            const double wi = __dmul_rn(acc, l1inv[r]);
+            w[r] = wi;
             ss = __dadd_rn(ss, __dmul_rn(wi, wi));
         }
     }
@@ -255,22 +250,19 @@ __global__ void power_normalize_kernel(int32_t n, const double* __restrict__ w, 
 }
 
 // Lanczos operator w = dm .* (A (dm .* v)), dm = sqrt(l1inv).
-template <int LPR>
-__global__ void __launch_bounds__(kThreads) lanczos_op_kernel(int32_t n, const int32_t* __restrict__ rp,
-                                                              const int32_t* __restrict__ ci,
-                                                              const double* __restrict__ v,
-                                                              const double* __restrict__ vin,
-                                                              const double* __restrict__ dm, double* __restrict__ w) {
-    int64_t row, stride;
-    row_of<LPR>(row, stride);
-    const int64_t row_base0 = row - ((threadIdx.x & 31) / LPR);
-    for (int64_t r0 = row_base0; r0 < n; r0 += stride) {
-        const int64_t rr = r0 + ((threadIdx.x & 31) / LPR);
-        const bool valid = rr < n;
-        const int mc = hsdev::warp_max_chunks<LPR>(rp, rr, valid);
-        auto fx = [&](int32_t j) { return __dmul_rn(__ldg(dm + j), __ldg(vin + j)); };
-        double acc = hsdev::row_fold<LPR>(rp, ci, v, rr, valid, 0.0, fx, AddOp<double>(), mc);
-        if (valid && (threadIdx.x & (LPR - 1)) == 0) w[rr] = __dmul_rn(dm[rr], acc);
+template <int BR>
+__global__ void __launch_bounds__(BR, 1024 / BR) lanczos_op_kernel(int32_t n, const int32_t* __restrict__ rp,
+                                                                 const int32_t* __restrict__ ci,
+                                                                 const double* __restrict__ v,
+                                                                 const double* __restrict__ vin,
+                                                                 const double* __restrict__ dm,
+                                                                 double* __restrict__ w) {
+    HS_CS_SHARED(double, BR);
+    auto fx = [&](int32_t j) { return __dmul_rn(__ldg(dm + j), __ldg(vin + j)); };
+    HS_CS_ROWS_LOOP(BR) {
+        const int64_t r = row0 + threadIdx.x;
+        const double acc = HS_CS_FOLD(double, BR)(sh, n, rp, ci, v, row0, 0.0, fx, AddOp<double>());
+        if (r < n) w[r] = __dmul_rn(dm[r], acc);
     }
 }
 
@@ -292,23 +284,20 @@ __global__ void sqrt_kernel(int32_t n, const double* __restrict__ a, double* __r
 
 // ---- Chebyshev 4th kind ----------------------------------------------------
 // r = b - A x (chebyshev.jl:165-167), z = 0 (:170)
-template <typename T, int LPR>
-__global__ void __launch_bounds__(kThreads) cheb4_init_kernel(int32_t n, const int32_t* __restrict__ rp,
-                                                              const int32_t* __restrict__ ci, const T* __restrict__ v,
-                                                              const T* __restrict__ x, const T* __restrict__ b,
-                                                              T* __restrict__ r, T* __restrict__ z) {
-    int64_t row, stride;
-    row_of<LPR>(row, stride);
-    const int64_t row_base0 = row - ((threadIdx.x & 31) / LPR);
-    for (int64_t r0 = row_base0; r0 < n; r0 += stride) {
-        const int64_t rr = r0 + ((threadIdx.x & 31) / LPR);
-        const bool valid = rr < n;
-        const int mc = hsdev::warp_max_chunks<LPR>(rp, rr, valid);
-        auto fx = [&](int32_t j) { return __ldg(x + j); };
-        const T ax = hsdev::row_fold<LPR>(rp, ci, v, rr, valid, T(0), fx, AddOp<T>(), mc);
-        if (valid && (threadIdx.x & (LPR - 1)) == 0) {
-            r[rr] = sub_rn(b[rr], ax);
-            z[rr] = T(0);
+template <typename T, int BR>
+__global__ void __launch_bounds__(BR, 1024 / BR) cheb4_init_kernel(int32_t n, const int32_t* __restrict__ rp,
+                                                                 const int32_t* __restrict__ ci,
+                                                                 const T* __restrict__ v, const T* __restrict__ x,
+                                                                 const T* __restrict__ b, T* __restrict__ r,
+                                                                 T* __restrict__ z) {
+    HS_CS_SHARED(T, BR);
+    auto fx = [&](int32_t j) { return __ldg(x + j); };
+    HS_CS_ROWS_LOOP(BR) {
+        const int64_t i = row0 + threadIdx.x;
+        const T ax = HS_CS_FOLD(T, BR)(sh, n, rp, ci, v, row0, T(0), fx, AddOp<T>());
+        if (i < n) {
+            r[i] = sub_rn(b[i], ax);
+            z[i] = T(0);
         }
     }
 }
@@ -325,55 +314,48 @@ __global__ void cheb4_init_zero_kernel(int32_t n, const IO* __restrict__ b, T* _
 }
 
 // One fused step (chebyshev.jl:176-179 with kernel :132-139).
-template <typename T, int LPR>
-__global__ void __launch_bounds__(kThreads) cheb4_step_kernel(int32_t n, const int32_t* __restrict__ rp,
-                                                              const int32_t* __restrict__ ci, const T* __restrict__ v,
-                                                              const T* __restrict__ l1inv, T ak, T bk,
-                                                              const T* __restrict__ z_old, const T* __restrict__ r_old,
-                                                              T* __restrict__ z_new, T* __restrict__ r_new,
-                                                              T* __restrict__ x) {
-    int64_t row, stride;
-    row_of<LPR>(row, stride);
-    const int64_t row_base0 = row - ((threadIdx.x & 31) / LPR);
-    for (int64_t r0 = row_base0; r0 < n; r0 += stride) {
-        const int64_t rr = r0 + ((threadIdx.x & 31) / LPR);
-        const bool valid = rr < n;
-        const int mc = hsdev::warp_max_chunks<LPR>(rp, rr, valid);
-        auto zk = [&](int32_t j) {
-            return add_rn(mul_rn(ak, __ldg(z_old + j)), mul_rn(mul_rn(bk, __ldg(l1inv + j)), __ldg(r_old + j)));
-        };
-        const T r0v = valid ? r_old[rr] : T(0);
-        const T acc = hsdev::row_fold<LPR>(rp, ci, v, rr, valid, r0v, zk, SubOp<T>(), mc);
-        if (valid && (threadIdx.x & (LPR - 1)) == 0) {
-            const T zi = zk((int32_t)rr);
-            z_new[rr] = zi;
-            x[rr] = add_rn(x[rr], zi);
-            r_new[rr] = acc;
+template <typename T, int BR>
+__global__ void __launch_bounds__(BR, 1024 / BR) cheb4_step_kernel(int32_t n, const int32_t* __restrict__ rp,
+                                                                 const int32_t* __restrict__ ci,
+                                                                 const T* __restrict__ v, const T* __restrict__ l1inv,
+                                                                 T ak, T bk, const T* __restrict__ z_old,
+                                                                 const T* __restrict__ r_old, T* __restrict__ z_new,
+                                                                 T* __restrict__ r_new, T* __restrict__ x) {
+    HS_CS_SHARED(T, BR);
+    auto zk = [&](int32_t j) {
+        return add_rn(mul_rn(ak, __ldg(z_old + j)), mul_rn(mul_rn(bk, __ldg(l1inv + j)), __ldg(r_old + j)));
+    };
+    HS_CS_ROWS_LOOP(BR) {
+        const int64_t i = row0 + threadIdx.x;
+        const bool valid = i < n;
+        const T acc = HS_CS_FOLD(T, BR)(sh, n, rp, ci, v, row0, valid ? r_old[i] : T(0), zk, SubOp<T>());
+        if (valid) {
+            const T zi = zk((int32_t)i);
+            z_new[i] = zi;
+            x[i] = add_rn(x[i], zi);
+            r_new[i] = acc;
         }
     }
 }
 
 // ---- Chebyshev 1st kind ----------------------------------------------------
 // tmp = A x; r = (l1inv (b - tmp)) inv_rho; z = c0 r   (chebyshev.jl:287-293, :237-244)
-template <typename T, int LPR>
-__global__ void __launch_bounds__(kThreads) cheb1_init_kernel(int32_t n, const int32_t* __restrict__ rp,
-                                                              const int32_t* __restrict__ ci, const T* __restrict__ v,
-                                                              const T* __restrict__ x, const T* __restrict__ b,
-                                                              const T* __restrict__ l1inv, T inv_rho, T c0,
-                                                              T* __restrict__ r, T* __restrict__ z) {
-    int64_t row, stride;
-    row_of<LPR>(row, stride);
-    const int64_t row_base0 = row - ((threadIdx.x & 31) / LPR);
-    for (int64_t r0 = row_base0; r0 < n; r0 += stride) {
-        const int64_t rr = r0 + ((threadIdx.x & 31) / LPR);
-        const bool valid = rr < n;
-        const int mc = hsdev::warp_max_chunks<LPR>(rp, rr, valid);
-        auto fx = [&](int32_t j) { return __ldg(x + j); };
-        const T tmp = hsdev::row_fold<LPR>(rp, ci, v, rr, valid, T(0), fx, AddOp<T>(), mc);
-        if (valid && (threadIdx.x & (LPR - 1)) == 0) {
-            const T ri = mul_rn(mul_rn(l1inv[rr], sub_rn(b[rr], tmp)), inv_rho);
-            r[rr] = ri;
-            z[rr] = mul_rn(c0, ri);
+template <typename T, int BR>
+__global__ void __launch_bounds__(BR, 1024 / BR) cheb1_init_kernel(int32_t n, const int32_t* __restrict__ rp,
+                                                                 const int32_t* __restrict__ ci,
+                                                                 const T* __restrict__ v, const T* __restrict__ x,
+                                                                 const T* __restrict__ b, const T* __restrict__ l1inv,
+                                                                 T inv_rho, T c0, T* __restrict__ r,
+                                                                 T* __restrict__ z) {
+    HS_CS_SHARED(T, BR);
+    auto fx = [&](int32_t j) { return __ldg(x + j); };
+    HS_CS_ROWS_LOOP(BR) {
+        const int64_t i = row0 + threadIdx.x;
+        const T tmp = HS_CS_FOLD(T, BR)(sh, n, rp, ci, v, row0, T(0), fx, AddOp<T>());
+        if (i < n) {
+            const T ri = mul_rn(mul_rn(l1inv[i], sub_rn(b[i], tmp)), inv_rho);
+            r[i] = ri;
+            z[i] = mul_rn(c0, ri);
         }
     }
 }
@@ -390,27 +372,24 @@ __global__ void cheb1_init_zero_kernel(int32_t n, const IO* __restrict__ b, cons
 }
 
 // x += z_old; r -= (l1inv (A z_old)) inv_rho; z_new = c1 z_old + c2 r   (:300-316)
-template <typename T, int LPR>
-__global__ void __launch_bounds__(kThreads) cheb1_step_kernel(int32_t n, const int32_t* __restrict__ rp,
-                                                              const int32_t* __restrict__ ci, const T* __restrict__ v,
-                                                              const T* __restrict__ l1inv, T inv_rho, T c1, T c2,
-                                                              const T* __restrict__ z_old, T* __restrict__ z_new,
-                                                              T* __restrict__ r, T* __restrict__ x) {
-    int64_t row, stride;
-    row_of<LPR>(row, stride);
-    const int64_t row_base0 = row - ((threadIdx.x & 31) / LPR);
-    for (int64_t r0 = row_base0; r0 < n; r0 += stride) {
-        const int64_t rr = r0 + ((threadIdx.x & 31) / LPR);
-        const bool valid = rr < n;
-        const int mc = hsdev::warp_max_chunks<LPR>(rp, rr, valid);
-        auto fz = [&](int32_t j) { return __ldg(z_old + j); };
-        const T tmp = hsdev::row_fold<LPR>(rp, ci, v, rr, valid, T(0), fz, AddOp<T>(), mc);
-        if (valid && (threadIdx.x & (LPR - 1)) == 0) {
-            const T zo = z_old[rr];
-            x[rr] = add_rn(x[rr], zo);
-            const T rn = sub_rn(r[rr], mul_rn(mul_rn(l1inv[rr], tmp), inv_rho));
-            r[rr] = rn;
-            z_new[rr] = add_rn(mul_rn(c1, zo), mul_rn(c2, rn));
+template <typename T, int BR>
+__global__ void __launch_bounds__(BR, 1024 / BR) cheb1_step_kernel(int32_t n, const int32_t* __restrict__ rp,
+                                                                 const int32_t* __restrict__ ci,
+                                                                 const T* __restrict__ v, const T* __restrict__ l1inv,
+                                                                 T inv_rho, T c1, T c2, const T* __restrict__ z_old,
+                                                                 T* __restrict__ z_new, T* __restrict__ r,
+                                                                 T* __restrict__ x) {
+    HS_CS_SHARED(T, BR);
+    auto fz = [&](int32_t j) { return __ldg(z_old + j); };
+    HS_CS_ROWS_LOOP(BR) {
+        const int64_t i = row0 + threadIdx.x;
+        const T tmp = HS_CS_FOLD(T, BR)(sh, n, rp, ci, v, row0, T(0), fz, AddOp<T>());
+        if (i < n) {
+            const T zo = z_old[i];
+            x[i] = add_rn(x[i], zo);
+            const T rn = sub_rn(r[i], mul_rn(mul_rn(l1inv[i], tmp), inv_rho));
+            r[i] = rn;
+            z_new[i] = add_rn(mul_rn(c1, zo), mul_rn(c2, rn));
         }
     }
 }
@@ -421,24 +400,22 @@ __global__ void axpy_one_kernel(int32_t n, T* __restrict__ x, const T* __restric
         x[i] = add_rn(x[i], z[i]);
 }
 
-inline int grid_rows(int64_t n, int lpr) {
-    const int64_t warps = (n * lpr + 31) / 32;
-    const int64_t blocks = (warps * 32 + kThreads - 1) / kThreads;
-    const int64_t cap = (int64_t)hs::num_sms() * 16;
-    return (int)std::max<int64_t>(1, std::min(blocks, cap));
+// One block per BR rows: the block scheduler streams them through the SMs,
+// each block's phases overlapping those of the other resident blocks.
+inline int grid_rows(int64_t n, int br) {
+    const int64_t blocks = (n + br - 1) / br;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(blocks, INT32_MAX));
 }
 inline int grid_elems(int64_t n) {
     const int64_t b = (n + kThreads - 1) / kThreads;
     return (int)std::max<int64_t>(1, std::min<int64_t>(b, (int64_t)hs::num_sms() * 16));
 }
 
-#define HS_LPR_DISPATCH(lpr, CALL) \
-    switch (lpr) {                  \
-        case 2: { constexpr int L = 2; CALL; } break;   \
-        case 4: { constexpr int L = 4; CALL; } break;   \
-        case 8: { constexpr int L = 8; CALL; } break;   \
-        case 16: { constexpr int L = 16; CALL; } break; \
-        default: { constexpr int L = 32; CALL; } break; \
+// L = rows per block (= threads per block) of the CSR-stream kernels.
+#define HS_LPR_DISPATCH(lpr, CALL)                        \
+    switch (lpr) {                                        \
+        case 256: { constexpr int L = 256; CALL; } break; \
+        default: { constexpr int L = 128; CALL; } break;  \
     }
 
 template <typename T>
@@ -448,11 +425,12 @@ int spmv_t(const hs_matrix* M, const void* x, void* y, double alpha, double beta
     const T* xx = static_cast<const T*>(x);
     T* yy = static_cast<T*>(y);
     if (alpha == 1.0 && beta == 0.0) {
-        HS_LPR_DISPATCH(M->lpr, (spmv_kernel<T, L, 0><<<g, kThreads, 0, st>>>(M->n, M->rp, M->ci, v, xx, yy, T(1), T(0))));
+        HS_LPR_DISPATCH(M->lpr, (spmv_kernel<T, L, 0><<<g, L, 0, st>>>(M->n, M->rp, M->ci, v, xx, yy, T(1), T(0))));
     } else if (alpha == -1.0 && beta == 1.0) {
-        HS_LPR_DISPATCH(M->lpr, (spmv_kernel<T, L, 1><<<g, kThreads, 0, st>>>(M->n, M->rp, M->ci, v, xx, yy, T(-1), T(1))));
+        HS_LPR_DISPATCH(M->lpr, (spmv_kernel<T, L, 1><<<g, L, 0, st>>>(M->n, M->rp, M->ci, v, xx, yy, T(-1), T(1))));
     } else {
-        HS_LPR_DISPATCH(M->lpr, (spmv_kernel<T, L, 2><<<g, kThreads, 0, st>>>(M->n, M->rp, M->ci, v, xx, yy, (T)alpha, (T)beta)));
+        HS_LPR_DISPATCH(M->lpr,
+                        (spmv_kernel<T, L, 2><<<g, L, 0, st>>>(M->n, M->rp, M->ci, v, xx, yy, (T)alpha, (T)beta)));
     }
     HS_LAUNCH_CHECK("spmv_kernel");
     return HS_OK;
@@ -467,6 +445,8 @@ int matrix_spmv(const hs_matrix* M, const void* x, void* y, double alpha, double
                               : hsm::spmv_t<float>(M, x, y, alpha, beta, st);
 }
 int matrix_n(const hs_matrix* M) { return M->n; }
+int64_t matrix_nnz(const hs_matrix* M) { return M->nnz; }
+int matrix_block_rows(const hs_matrix* M) { return M->lpr; }
 void matrix_arrays(const hs_matrix* M, const int32_t** rp, const int32_t** ci, const void** v, int* dtype) {
     *rp = M->rp;
     *ci = M->ci;
@@ -567,7 +547,7 @@ int cheb_smooth_t(hs_cheb* S, T* x, const void* b, int io, bool x_is_zero, cudaS
                 cheb4_init_zero_kernel<T, float><<<ge, kThreads, 0, st>>>(n, static_cast<const float*>(b), r[0], z[0], x);
             HS_LAUNCH_CHECK("cheb4_init_zero_kernel");
         } else {
-            HS_LPR_DISPATCH(M->lpr, (cheb4_init_kernel<T, L><<<g, kThreads, 0, st>>>(
+            HS_LPR_DISPATCH(M->lpr, (cheb4_init_kernel<T, L><<<g, L, 0, st>>>(
                                         n, M->rp, M->ci, v, x, static_cast<const T*>(b), r[0], z[0])));
             HS_LAUNCH_CHECK("cheb4_init_kernel");
         }
@@ -575,7 +555,7 @@ int cheb_smooth_t(hs_cheb* S, T* x, const void* b, int io, bool x_is_zero, cudaS
         for (int k = 1; k <= S->degree; ++k) {
             const T ak = (T)((double)(2 * k - 3) / (double)(2 * k + 1));
             const T bk = (T)((double)(8 * k - 4) / ((double)(2 * k + 1) * S->rho));
-            HS_LPR_DISPATCH(M->lpr, (cheb4_step_kernel<T, L><<<g, kThreads, 0, st>>>(
+            HS_LPR_DISPATCH(M->lpr, (cheb4_step_kernel<T, L><<<g, L, 0, st>>>(
                                         n, M->rp, M->ci, v, l1, ak, bk, z[cur], r[cur], z[cur ^ 1], r[cur ^ 1], x)));
             HS_LAUNCH_CHECK("cheb4_step_kernel");
             cur ^= 1;
@@ -595,7 +575,7 @@ int cheb_smooth_t(hs_cheb* S, T* x, const void* b, int io, bool x_is_zero, cudaS
                                                                       r[0], z[0], x);
         HS_LAUNCH_CHECK("cheb1_init_zero_kernel");
     } else {
-        HS_LPR_DISPATCH(M->lpr, (cheb1_init_kernel<T, L><<<g, kThreads, 0, st>>>(
+        HS_LPR_DISPATCH(M->lpr, (cheb1_init_kernel<T, L><<<g, L, 0, st>>>(
                                     n, M->rp, M->ci, v, x, static_cast<const T*>(b), l1, inv_rho, c0, r[0], z[0])));
         HS_LAUNCH_CHECK("cheb1_init_kernel");
     }
@@ -606,7 +586,7 @@ int cheb_smooth_t(hs_cheb* S, T* x, const void* b, int io, bool x_is_zero, cudaS
             const double rho_new = 1.0 / (2.0 * (1.0 + a) / (1.0 - a) - rho_s);
             const T c1 = (T)(rho_new * rho_s);
             const T c2 = (T)(4.0 * rho_new / (1.0 - a));
-            HS_LPR_DISPATCH(M->lpr, (cheb1_step_kernel<T, L><<<g, kThreads, 0, st>>>(
+            HS_LPR_DISPATCH(M->lpr, (cheb1_step_kernel<T, L><<<g, L, 0, st>>>(
                                         n, M->rp, M->ci, v, l1, inv_rho, c1, c2, z[cur], z[cur ^ 1], r[0], x)));
             HS_LAUNCH_CHECK("cheb1_step_kernel");
             cur ^= 1;
@@ -630,10 +610,33 @@ int hs_matrix_create(const hs_sparse* A, int32_t dtype, void* stream, hs_matrix*
     int rc = hsm::validate(A);
     if (rc) return rc;
     if (dtype != HS_F64 && dtype != HS_F32) return hs::set_error(HS_ERR_ARG, "unknown dtype");
-    std::vector<int32_t> rp, ci;
-    std::vector<double> v;
-    hsm::host_csr(A, rp, ci, v);
-    return hsm::matrix_from_host(rp, ci, v, dtype, static_cast<cudaStream_t>(stream), out);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    hs_matrix* M = new hs_matrix();
+    M->n = A->n;
+    M->nnz = A->nnz;
+    M->dtype = dtype;
+    M->lpr = hsm::pick_lpr(M->nnz, M->n);
+    const size_t es = hsm::dsize(dtype);
+    cudaError_t e;
+    if ((e = cudaMalloc(&M->rp, sizeof(int32_t) * (M->n + 1))) != cudaSuccess ||
+        (e = cudaMalloc(&M->ci, sizeof(int32_t) * std::max<int64_t>(1, M->nnz))) != cudaSuccess ||
+        (e = cudaMalloc(&M->v, es * std::max<int64_t>(1, M->nnz))) != cudaSuccess) {
+        hsm::destroy_matrix(M);
+        return hs::cuda_error(e, "cudaMalloc (matrix)");
+    }
+    M->bytes = (int64_t)(sizeof(int32_t) * (M->n + 1 + M->nnz) + es * M->nnz);
+    // A CSC input is transposed on the device (stable: rows keep ascending columns).
+    rc = hs::csr_from_host(A, dtype, M->rp, M->ci, M->v, st);
+    if (!rc) {
+        const cudaError_t se = cudaStreamSynchronize(st);
+        if (se != cudaSuccess) rc = hs::cuda_error(se, "hs_matrix_create");
+    }
+    if (rc) {
+        hsm::destroy_matrix(M);
+        return rc;
+    }
+    *out = M;
+    return HS_OK;
 }
 
 int hs_matrix_spmv(hs_matrix* A, const void* x, void* y, double alpha, double beta, void* stream) {
@@ -693,9 +696,11 @@ int hs_cheb_create(const hs_sparse* A, int32_t kind, int32_t degree, int32_t eig
     hsm::fill_kernel<double><<<ge, hsm::kThreads, 0, st>>>(vv, n, 1.0 / std::sqrt((double)n));
     hs::count_launch();
     cudaMemsetAsync(stop, 0, sizeof(int), st);
-    const int gr = hsm::grid_rows(n, M64->lpr);
+    // The power-iteration SpMV writes one partial per block: keep its grid within
+    // the partials buffer (kRedMaxBlocks); the kernel strides over row blocks.
+    const int gr = std::min(hsm::grid_rows(n, M64->lpr), hsdev::kRedMaxBlocks);
     for (int it = 0; it < 50; ++it) {
-        HS_LPR_DISPATCH(M64->lpr, (hsm::power_spmv_kernel<L><<<gr, hsm::kThreads, 0, st>>>(
+        HS_LPR_DISPATCH(M64->lpr, (hsm::power_spmv_kernel<L><<<gr, L, 0, st>>>(
                                       n, M64->rp, M64->ci, static_cast<const double*>(M64->v), vv, l1inv, ww, partials,
                                       stop)));
         hsm::power_finalize_kernel<<<1, hsdev::kRedThreads, 0, st>>>(partials, gr, rho_d, stop);
@@ -720,7 +725,7 @@ int hs_cheb_create(const hs_sparse* A, int32_t kind, int32_t degree, int32_t eig
         double beta = 0.0;
         const int rb = hsdev::red_blocks(n);
         for (int j = 0; j < 40 && j < n; ++j) {
-            HS_LPR_DISPATCH(M64->lpr, (hsm::lanczos_op_kernel<L><<<gr, hsm::kThreads, 0, st>>>(
+            HS_LPR_DISPATCH(M64->lpr, (hsm::lanczos_op_kernel<L><<<gr, L, 0, st>>>(
                                           n, M64->rp, M64->ci, static_cast<const double*>(M64->v), vv, dm, ww)));
             hsdev::dot_partials_kernel<double, double><<<rb, hsdev::kRedThreads, 0, st>>>(ww, vv, n, partials);
             hsdev::finalize_sum_kernel<<<1, hsdev::kRedThreads, 0, st>>>(partials, rb, sc, 0);

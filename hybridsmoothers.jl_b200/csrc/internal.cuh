@@ -7,8 +7,13 @@ namespace hs {
 
 int matrix_spmv(const hs_matrix* M, const void* x, void* y, double alpha, double beta, cudaStream_t st);
 int matrix_n(const hs_matrix* M);
+int64_t matrix_nnz(const hs_matrix* M);
+int matrix_block_rows(const hs_matrix* M);   // rows per CSR-stream block (128 or 256)
 void matrix_arrays(const hs_matrix* M, const int32_t** rp, const int32_t** ci, const void** v, int* dtype);
 int cheb_apply(hs_cheb* S, const void* r, void* z, int io, cudaStream_t st);
+// Uploads a validated host matrix as device CSR in `dtype` (a CSC input is
+// transposed on the device); rp has n+1 entries, ci and v nnz.
+int csr_from_host(const hs_sparse* A, int32_t dtype, int32_t* rp, int32_t* ci, void* v, cudaStream_t st);
 
 // The device-side pieces of an L1GS preconditioner that a batched launch needs.
 struct L1gsView {
@@ -20,5 +25,9 @@ struct L1gsView {
     int32_t sdt, sweep, cache;
 };
 int l1gs_view_of(const hs_l1gs* P, L1gsView* v);
+// Symmetric packed-cache L1GS built from a device CSR matrix (read during the
+// call only; for a symmetric matrix its rows are the CSC columns isSymA reads).
+int l1gs_create_from_matrix(const hs_matrix* M, int32_t partsize, double eta, int32_t sweep, int32_t smoother_dtype,
+                            cudaStream_t st, hs_l1gs** out);
 
 }  // namespace hs

@@ -4,31 +4,53 @@
 // test/test_preconditioners.jl:65,93) and which calls ldiv!(y, P, x) once per
 // iteration.
 //
-// PCG keeps every scalar on the device.  One iteration (SpMV + fused dot,
-// alpha, x/r update + fused norm, convergence test, M^-1 r, r.z, beta, p
-// update) is captured once as a CUDA graph and replayed in batches; the
+// PCG keeps every scalar on the device.  One iteration (SpMV fused with p.q,
+// alpha fused with the x/r update and r.r, convergence test, M^-1 r, r.z,
+// beta fused with the p update) is captured once as a CUDA graph and replayed
+// in batches; the
 // convergence test freezes x and r on the iteration that meets
 // ||r|| <= rtol ||b||, so replaying past convergence changes nothing and the
 // reported iteration count is the first one that met the test.
+//
+// Arithmetic.  Dot products and norms are compensated (Dot2) sums and every
+// vector update is separately rounded (no FMA contraction), the same
+// arithmetic the CPU restatement uses, so with the bitwise-identical SpMV and
+// preconditioners the device iterates reproduce the restatement's.
 #include <algorithm>
 #include <cmath>
 #include <vector>
 
 #include "internal.cuh"
 #include "reduce.cuh"
+#include "spmv.cuh"
 
 namespace {
 
 constexpr int kT = 256;
 
 struct PcgScalars {
-    double bb, rr, rz, pq, alpha, beta, tol2;
+    double bb, rr, rz, pq, alpha, beta, rtol;
     int done, it, conv_it, pad;
 };
 
 inline int grid_elems(int64_t n) {
     const int64_t b = (n + kT - 1) / kT;
     return (int)std::max<int64_t>(1, std::min<int64_t>(b, (int64_t)hs::num_sms() * 8));
+}
+
+// Streaming kernels work on tiles of kU x kT elements: each thread issues the
+// loads of its kU elements before using any of them, so every thread keeps kU
+// elements per stream in flight.  blockDim.x must be kT.
+constexpr int kU = 4;
+constexpr int64_t kTile = (int64_t)kU * kT;
+
+// Blocks for a tiled streaming kernel: at most 4 per SM (and kRedMaxBlocks),
+// with the tiles spread evenly over them.
+inline int tile_blocks(int64_t n) {
+    const int64_t tiles = std::max<int64_t>(1, (n + kTile - 1) / kTile);
+    const int64_t maxb = std::min<int64_t>((int64_t)hs::num_sms() * 4, hsdev::kRedMaxBlocks);
+    const int64_t per = (tiles + maxb - 1) / maxb;
+    return (int)((tiles + per - 1) / per);
 }
 
 __global__ void copy_kernel(int64_t n, const double* __restrict__ a, double* __restrict__ b) {
@@ -41,20 +63,49 @@ __global__ void zero_kernel(int64_t n, double* __restrict__ a) {
         a[i] = 0.0;
 }
 
-// partial sums of a.b
-__global__ void dot_kernel(int64_t n, const double* __restrict__ a, const double* __restrict__ b,
-                           double* __restrict__ partials) {
-    double v = 0.0;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        v += a[i] * b[i];
-    v = hsdev::block_sum(v);
-    if (threadIdx.x == 0) partials[blockIdx.x] = v;
+using hsdev::DD;
+
+__device__ __forceinline__ void store_dd(double* partials, DD v) {
+    v = hsdev::block_dd(v);
+    if (threadIdx.x == 0) {
+        partials[2 * blockIdx.x] = v.s;
+        partials[2 * blockIdx.x + 1] = v.c;
+    }
 }
 
+// compensated partial sums of a.b: partials[2*block], partials[2*block+1]
+__global__ void __launch_bounds__(kT) dot_kernel(int64_t n, const double* __restrict__ a,
+                                                 const double* __restrict__ b, double* __restrict__ partials) {
+    DD v{0.0, 0.0};
+    for (int64_t base = blockIdx.x * kTile + threadIdx.x; base < n; base += (int64_t)gridDim.x * kTile) {
+        double xa[kU], xb[kU];
+#pragma unroll
+        for (int k = 0; k < kU; ++k) {
+            const int64_t i = base + k * kT;
+            if (i < n) {
+                xa[k] = a[i];
+                xb[k] = b[i];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kU; ++k)
+            if (base + k * kT < n) hsdev::dd_add_prod(v, xa[k], xb[k]);
+    }
+    store_dd(partials, v);
+}
+
+// Sum of compensated partials; valid on thread 0.
 __device__ __forceinline__ double sum_partials(const double* __restrict__ partials, int nb) {
-    double v = 0.0;
-    for (int i = threadIdx.x; i < nb; i += blockDim.x) v += partials[i];
-    return hsdev::block_sum(v);
+    DD v{0.0, 0.0};
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) v = hsdev::dd_add(v, DD{partials[2 * i], partials[2 * i + 1]});
+    return hsdev::dd_value(hsdev::block_dd(v));
+}
+
+// The same sum (thread 0's value) on every thread of the block.
+__device__ __forceinline__ double sum_partials_all(const double* __restrict__ partials, int nb) {
+    DD v{0.0, 0.0};
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) v = hsdev::dd_add(v, DD{partials[2 * i], partials[2 * i + 1]});
+    return hsdev::dd_value(hsdev::block_dd_all(v));
 }
 
 __global__ void pcg_init_scalars(const double* __restrict__ partials_bb, const double* __restrict__ partials_rz,
@@ -66,39 +117,84 @@ __global__ void pcg_init_scalars(const double* __restrict__ partials_bb, const d
         s->bb = bb;
         s->rr = bb;
         s->rz = rz;
-        s->tol2 = rtol * rtol * bb;
+        s->rtol = rtol;
         s->done = (bb == 0.0);
         s->it = 0;
         s->conv_it = s->done ? 0 : -1;
     }
 }
 
-__global__ void pcg_alpha(const double* __restrict__ partials, int nb, PcgScalars* s) {
-    const double pq = sum_partials(partials, nb);
-    if (threadIdx.x == 0) {
-        s->pq = pq;
-        s->alpha = s->rz / pq;
+// q = A p (storage-order rows, bitwise mul!) and compensated partials of p.q.
+template <int BR>
+__global__ void __launch_bounds__(BR, 1024 / BR) pcg_spmv_dot(int32_t n, const int32_t* __restrict__ rp,
+                                                            const int32_t* __restrict__ ci,
+                                                            const double* __restrict__ v,
+                                                            const double* __restrict__ p, double* __restrict__ q,
+                                                            const PcgScalars* __restrict__ s,
+                                                            double* __restrict__ partials) {
+    __shared__ hsdev::CsrStream<double, BR, hsdev::stream_cap<BR>()> sh;
+    DD part{0.0, 0.0};
+    if (!s->done) {
+        auto fp = [&](int32_t j) { return __ldg(p + j); };
+        for (int64_t row0 = (int64_t)blockIdx.x * BR; row0 < n; row0 += (int64_t)gridDim.x * BR) {
+            const double acc = hsdev::csr_stream_fold<double, BR, hsdev::stream_cap<BR>()>(
+                sh, n, rp, ci, v, row0, 0.0, fp, hsdev::AddOp<double>());
+            const int64_t r = row0 + threadIdx.x;
+            if (r < n) {
+                q[r] = acc;
+                hsdev::dd_add_prod(part, p[r], acc);
+            }
+        }
     }
+    store_dd(partials, part);
 }
 
-// x += alpha p; r -= alpha q; partial r.r   (skipped once converged)
-__global__ void pcg_update(int64_t n, const PcgScalars* __restrict__ s, const double* __restrict__ p,
-                           const double* __restrict__ q, double* __restrict__ x, double* __restrict__ r,
-                           double* __restrict__ partials) {
+// alpha = r.z / p.q (every block sums the partials itself, in the same order,
+// so every block holds the same alpha); x += alpha p; r -= alpha q; partials
+// of r.r.  Skipped (r.r only) once converged.
+__global__ void __launch_bounds__(kT) pcg_update(int64_t n, PcgScalars* __restrict__ s, const double* __restrict__ ppq,
+                                                 int npq, const double* __restrict__ prz, int nrz,
+                                                 const double* __restrict__ p, const double* __restrict__ q,
+                                                 double* __restrict__ x, double* __restrict__ r,
+                                                 double* __restrict__ partials) {
     const bool done = s->done;
-    const double alpha = s->alpha;
-    double v = 0.0;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        double ri = r[i];
-        if (!done) {
-            x[i] += alpha * p[i];
-            ri -= alpha * q[i];
-            r[i] = ri;
-        }
-        v += ri * ri;
+    const double rz = sum_partials_all(prz, nrz);
+    const double pq = sum_partials_all(ppq, npq);
+    const double alpha = __ddiv_rn(rz, pq);
+    if (blockIdx.x == 0 && threadIdx.x == 0 && !done) {
+        s->rz = rz;
+        s->pq = pq;
+        s->alpha = alpha;
     }
-    v = hsdev::block_sum(v);
-    if (threadIdx.x == 0) partials[blockIdx.x] = v;
+    DD v{0.0, 0.0};
+    for (int64_t base = blockIdx.x * kTile + threadIdx.x; base < n; base += (int64_t)gridDim.x * kTile) {
+        double xv[kU], pv[kU], rv[kU], qv[kU];
+#pragma unroll
+        for (int k = 0; k < kU; ++k) {
+            const int64_t i = base + k * kT;
+            if (i < n) {
+                rv[k] = r[i];
+                if (!done) {
+                    xv[k] = x[i];
+                    pv[k] = p[i];
+                    qv[k] = q[i];
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kU; ++k) {
+            const int64_t i = base + k * kT;
+            if (i < n) {
+                if (!done) {
+                    x[i] = __dadd_rn(xv[k], __dmul_rn(alpha, pv[k]));
+                    rv[k] = __dsub_rn(rv[k], __dmul_rn(alpha, qv[k]));
+                    r[i] = rv[k];
+                }
+                hsdev::dd_add_prod(v, rv[k], rv[k]);
+            }
+        }
+    }
+    store_dd(partials, v);
 }
 
 __global__ void pcg_check(const double* __restrict__ partials, int nb, PcgScalars* s) {
@@ -107,7 +203,7 @@ __global__ void pcg_check(const double* __restrict__ partials, int nb, PcgScalar
         if (!s->done) {
             s->it += 1;
             s->rr = rr;
-            if (rr <= s->tol2) {
+            if (sqrt(rr) <= __dmul_rn(s->rtol, sqrt(s->bb))) {
                 s->done = 1;
                 s->conv_it = s->it;
             }
@@ -115,19 +211,28 @@ __global__ void pcg_check(const double* __restrict__ partials, int nb, PcgScalar
     }
 }
 
-__global__ void pcg_beta(const double* __restrict__ partials, int nb, PcgScalars* s) {
-    const double rz = sum_partials(partials, nb);
-    if (threadIdx.x == 0 && !s->done) {
-        s->beta = rz / s->rz;
-        s->rz = rz;
-    }
-}
-
-__global__ void pcg_p(int64_t n, const PcgScalars* __restrict__ s, const double* __restrict__ z, double* __restrict__ p) {
+// beta = r.z_new / r.z (every block sums the r.z partials itself); p = z + beta p.
+__global__ void __launch_bounds__(kT) pcg_p(int64_t n, const PcgScalars* __restrict__ s,
+                                            const double* __restrict__ prz, int nrz, const double* __restrict__ z,
+                                            double* __restrict__ p) {
     if (s->done) return;
-    const double beta = s->beta;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        p[i] = z[i] + beta * p[i];
+    const double beta = __ddiv_rn(sum_partials_all(prz, nrz), s->rz);
+    for (int64_t base = blockIdx.x * kTile + threadIdx.x; base < n; base += (int64_t)gridDim.x * kTile) {
+        double zv[kU], pv[kU];
+#pragma unroll
+        for (int k = 0; k < kU; ++k) {
+            const int64_t i = base + k * kT;
+            if (i < n) {
+                zv[k] = z[i];
+                pv[k] = p[i];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kU; ++k) {
+            const int64_t i = base + k * kT;
+            if (i < n) p[i] = __dadd_rn(zv[k], __dmul_rn(beta, pv[k]));
+        }
+    }
 }
 
 int prec_apply(int type, void* prec, const double* r, double* z, int64_t n, cudaStream_t st) {
@@ -152,13 +257,20 @@ struct DevBuf {
     }
 };
 
+// *out = sum of compensated partials (sqrt of it when sqrt_out).
+__global__ void finalize_dd_kernel(const double* __restrict__ partials, int nb, double* __restrict__ out,
+                                   int sqrt_out) {
+    const double v = sum_partials(partials, nb);
+    if (threadIdx.x == 0) *out = sqrt_out ? sqrt(v) : v;
+}
+
 double true_relres(hs_matrix* A, const double* b, const double* x, double* work, double* partials, double* scal,
                    int64_t n, cudaStream_t st, double bnorm) {
     copy_kernel<<<grid_elems(n), kT, 0, st>>>(n, b, work);
     hs::matrix_spmv(A, x, work, -1.0, 1.0, st);
     const int nb = hsdev::red_blocks(n);
     dot_kernel<<<nb, kT, 0, st>>>(n, work, work, partials);
-    hsdev::finalize_sum_kernel<<<1, hsdev::kRedThreads, 0, st>>>(partials, nb, scal, 1);
+    finalize_dd_kernel<<<1, kT, 0, st>>>(partials, nb, scal, 1);
     hs::count_launch(3);
     double v = 0;
     cudaMemcpyAsync(&v, scal, 8, cudaMemcpyDeviceToHost, st);
@@ -166,17 +278,20 @@ double true_relres(hs_matrix* A, const double* b, const double* x, double* work,
     return bnorm > 0 ? v / bnorm : 0.0;
 }
 
-// ---- GMRES helpers ---------------------------------------------------------
-// partials[i*nb + block] = V_i . w  for i < jc
+// ---- GMRES helpers (every operation separately rounded, as in the oracle) --
+// partials[2*(i*nb + block)] = compensated V_i . w  for i < jc
 __global__ void mdot_kernel(int64_t n, const double* __restrict__ V, int64_t ldv, int jc, const double* __restrict__ w,
                             double* __restrict__ partials, int nb) {
     for (int i = 0; i < jc; ++i) {
         const double* Vi = V + (size_t)i * ldv;
-        double v = 0.0;
+        DD v{0.0, 0.0};
         for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x)
-            v += Vi[r] * w[r];
-        v = hsdev::block_sum(v);
-        if (threadIdx.x == 0) partials[(size_t)i * nb + blockIdx.x] = v;
+            hsdev::dd_add_prod(v, Vi[r], w[r]);
+        v = hsdev::block_dd(v);
+        if (threadIdx.x == 0) {
+            partials[2 * ((size_t)i * nb + blockIdx.x)] = v.s;
+            partials[2 * ((size_t)i * nb + blockIdx.x) + 1] = v.c;
+        }
         __syncthreads();
     }
 }
@@ -185,24 +300,24 @@ __global__ void mdot_kernel(int64_t n, const double* __restrict__ V, int64_t ldv
 __global__ void mdot_finalize(const double* __restrict__ partials, int nb, double* __restrict__ hcol,
                               double* __restrict__ H, int m, int j) {
     const int i = blockIdx.x;
-    const double v = sum_partials(partials + (size_t)i * nb, nb);
+    const double v = sum_partials(partials + 2 * (size_t)i * nb, nb);
     if (threadIdx.x == 0) {
         hcol[i] = v;
-        H[(size_t)i * m + j] += v;
+        H[(size_t)i * m + j] = __dadd_rn(H[(size_t)i * m + j], v);
     }
 }
 
-// w -= sum_i hcol[i] V_i
+// w -= sum_i hcol[i] V_i, in order i = 0..jc-1
 __global__ void gs_update(int64_t n, const double* __restrict__ V, int64_t ldv, int jc, const double* __restrict__ hcol,
                           double* __restrict__ w) {
     for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
         double s = w[r];
-        for (int i = 0; i < jc; ++i) s -= hcol[i] * V[(size_t)i * ldv + r];
+        for (int i = 0; i < jc; ++i) s = __dsub_rn(s, __dmul_rn(hcol[i], V[(size_t)i * ldv + r]));
         w[r] = s;
     }
 }
 
-// H[j+1][j] = ||w||, V_{j+1} = w / ||w||, Givens update; flag = converged/breakdown
+// H[j+1][j] = ||w||, Givens update; flag = converged/breakdown
 __global__ void arnoldi_close(const double* __restrict__ partials, int nb, double* __restrict__ H, int m, int j,
                               double* __restrict__ cs, double* __restrict__ sn, double* __restrict__ g,
                               double* __restrict__ hn_out, int* __restrict__ flag, double tol) {
@@ -213,18 +328,18 @@ __global__ void arnoldi_close(const double* __restrict__ partials, int nb, doubl
     H[(size_t)(j + 1) * m + j] = hn;
     for (int i = 0; i < j; ++i) {
         const double a0 = H[(size_t)i * m + j], a1 = H[(size_t)(i + 1) * m + j];
-        H[(size_t)i * m + j] = cs[i] * a0 + sn[i] * a1;
-        H[(size_t)(i + 1) * m + j] = -sn[i] * a0 + cs[i] * a1;
+        H[(size_t)i * m + j] = __dadd_rn(__dmul_rn(cs[i], a0), __dmul_rn(sn[i], a1));
+        H[(size_t)(i + 1) * m + j] = __dadd_rn(__dmul_rn(-sn[i], a0), __dmul_rn(cs[i], a1));
     }
     const double a0 = H[(size_t)j * m + j], a1 = H[(size_t)(j + 1) * m + j];
-    const double den = sqrt(a0 * a0 + a1 * a1);
-    const double c = den == 0.0 ? 1.0 : a0 / den, s = den == 0.0 ? 0.0 : a1 / den;
+    const double den = sqrt(__dadd_rn(__dmul_rn(a0, a0), __dmul_rn(a1, a1)));
+    const double c = den == 0.0 ? 1.0 : __ddiv_rn(a0, den), s = den == 0.0 ? 0.0 : __ddiv_rn(a1, den);
     cs[j] = c;
     sn[j] = s;
-    H[(size_t)j * m + j] = c * a0 + s * a1;
+    H[(size_t)j * m + j] = __dadd_rn(__dmul_rn(c, a0), __dmul_rn(s, a1));
     H[(size_t)(j + 1) * m + j] = 0.0;
-    g[j + 1] = -s * g[j];
-    g[j] = c * g[j];
+    g[j + 1] = __dmul_rn(-s, g[j]);
+    g[j] = __dmul_rn(c, g[j]);
     *flag = (fabs(g[j + 1]) <= tol || hn == 0.0) ? 1 : 0;
 }
 
@@ -232,31 +347,31 @@ __global__ void scale_from(int64_t n, const double* __restrict__ w, const double
     const double h = *hn;
     if (h == 0.0) return;
     for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x)
-        out[r] = w[r] / h;
+        out[r] = __ddiv_rn(w[r], h);
 }
 
 __global__ void back_solve(const double* __restrict__ H, int m, int jend, const double* __restrict__ g, double* __restrict__ y) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     for (int i = jend - 1; i >= 0; --i) {
         double s = g[i];
-        for (int t = i + 1; t < jend; ++t) s -= H[(size_t)i * m + t] * y[t];
-        y[i] = s / H[(size_t)i * m + i];
+        for (int t = i + 1; t < jend; ++t) s = __dsub_rn(s, __dmul_rn(H[(size_t)i * m + t], y[t]));
+        y[i] = __ddiv_rn(s, H[(size_t)i * m + i]);
     }
 }
 
-// t = sum_i y_i V_i
+// t = sum_i y_i V_i, in order i = 0..jc-1 from 0
 __global__ void combine(int64_t n, const double* __restrict__ V, int64_t ldv, int jc, const double* __restrict__ y,
                         double* __restrict__ t) {
     for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
         double s = 0.0;
-        for (int i = 0; i < jc; ++i) s += y[i] * V[(size_t)i * ldv + r];
+        for (int i = 0; i < jc; ++i) s = __dadd_rn(s, __dmul_rn(y[i], V[(size_t)i * ldv + r]));
         t[r] = s;
     }
 }
 
 __global__ void add_to(int64_t n, const double* __restrict__ u, double* __restrict__ x) {
     for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x)
-        x[r] += u[r];
+        x[r] = __dadd_rn(x[r], u[r]);
 }
 
 __global__ void set_g(double* g, int m, double beta) {
@@ -304,7 +419,7 @@ int hs_pcg_solve(hs_matrix* A, int32_t prec_type, void* prec, const double* b, d
     } ws;
     int dev = 0;
     HS_CUDA(cudaGetDevice(&dev));
-    const int64_t need = 4 * n + 2 * hsdev::kRedMaxBlocks + 2 + (int64_t)(sizeof(PcgScalars) / 8 + 1);
+    const int64_t need = 4 * n + 6 * hsdev::kRedMaxBlocks + 2 + (int64_t)(sizeof(PcgScalars) / 8 + 1);
     if (ws.dev != dev || ws.cap < need) {
         if (ws.base && ws.dev == dev) cudaFree(ws.base);
         ws.base = nullptr;
@@ -318,11 +433,12 @@ int hs_pcg_solve(hs_matrix* A, int32_t prec_type, void* prec, const double* b, d
     double* p = z + n;
     double* q = p + n;
     double* pa = q + n;
-    double* pb = pa + hsdev::kRedMaxBlocks;
-    double* scal = pb + hsdev::kRedMaxBlocks;
+    double* pb = pa + 2 * hsdev::kRedMaxBlocks;
+    double* pc = pb + 2 * hsdev::kRedMaxBlocks;
+    double* scal = pc + 2 * hsdev::kRedMaxBlocks;
     PcgScalars* s = reinterpret_cast<PcgScalars*>(scal + 2);
     int rc;
-    const int ge = grid_elems(n), nb = hsdev::red_blocks(n);
+    const int ge = grid_elems(n), nb = tile_blocks(n);
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -339,20 +455,37 @@ int hs_pcg_solve(hs_matrix* A, int32_t prec_type, void* prec, const double* b, d
     hs::count_launch(4);
     HS_LAUNCH_CHECK("pcg init");
 
-    // One iteration as a graph.
+    // One iteration as a graph: q = A p with the p.q partials (pa); alpha,
+    // x/r update and r.r partials (pc); convergence test; z = M^-1 r; r.z
+    // partials (pb); beta and p update.
+    const int32_t *Arp = nullptr, *Aci = nullptr;
+    const void* Av = nullptr;
+    int Adt = 0;
+    hs::matrix_arrays(A, &Arp, &Aci, &Av, &Adt);
+    const int br = hs::matrix_block_rows(A);
+    const int nq = (int)std::max<int64_t>(
+        1, std::min<int64_t>((n + br - 1) / br, (int64_t)hsdev::kRedMaxBlocks));
     auto iteration = [&](cudaStream_t cs) -> int {
         int r2;
-        if ((r2 = hs::matrix_spmv(A, p, q, 1.0, 0.0, cs))) return r2;
-        dot_kernel<<<nb, kT, 0, cs>>>(n, p, q, pa);
-        pcg_alpha<<<1, kT, 0, cs>>>(pa, nb, s);
-        pcg_update<<<nb, kT, 0, cs>>>(n, s, p, q, x, r, pa);
-        pcg_check<<<1, kT, 0, cs>>>(pa, nb, s);
-        hs::count_launch(4);
+        int npq = nb;
+        if (Adt == HS_F64 && br == 256) {
+            pcg_spmv_dot<256><<<nq, 256, 0, cs>>>((int32_t)n, Arp, Aci, (const double*)Av, p, q, s, pa);
+            npq = nq;
+        } else if (Adt == HS_F64 && br == 128) {
+            pcg_spmv_dot<128><<<nq, 128, 0, cs>>>((int32_t)n, Arp, Aci, (const double*)Av, p, q, s, pa);
+            npq = nq;
+        } else {
+            if ((r2 = hs::matrix_spmv(A, p, q, 1.0, 0.0, cs))) return r2;
+            dot_kernel<<<nb, kT, 0, cs>>>(n, p, q, pa);
+        }
+        pcg_update<<<nb, kT, 0, cs>>>(n, s, pa, npq, pb, nb, p, q, x, r, pc);
+        pcg_check<<<1, kT, 0, cs>>>(pc, nb, s);
+        hs::count_launch(3);   // spmv (+dot), update, check
         if ((r2 = prec_apply(prec_type, prec, r, z, n, cs))) return r2;
         dot_kernel<<<nb, kT, 0, cs>>>(n, r, z, pb);
-        pcg_beta<<<1, kT, 0, cs>>>(pb, nb, s);
-        pcg_p<<<ge, kT, 0, cs>>>(n, s, z, p);
-        hs::count_launch(3);
+        pcg_p<<<nb, kT, 0, cs>>>(n, s, pb, nb, z, p);
+        hs::count_launch(1);   // dot; the check below counts pcg_p
+        HS_LAUNCH_CHECK("pcg iteration");
         return HS_OK;
     };
     // warm launch outside capture (sets kernel attributes), then capture
@@ -426,7 +559,7 @@ int hs_gmres_solve(hs_matrix* A, int32_t prec_type, void* prec, int32_t restart,
     int* flag;
     int rc;
     if ((rc = buf.alloc(&V, 8 * (size_t)n * (m + 1))) || (rc = buf.alloc(&u, 8 * n)) || (rc = buf.alloc(&w, 8 * n)) ||
-        (rc = buf.alloc(&r, 8 * n)) || (rc = buf.alloc(&partials, 8 * (size_t)hsdev::kRedMaxBlocks * (m + 1))) ||
+        (rc = buf.alloc(&r, 8 * n)) || (rc = buf.alloc(&partials, 16 * (size_t)hsdev::kRedMaxBlocks * (m + 1))) ||
         (rc = buf.alloc(&H, 8 * (size_t)(m + 1) * m)) || (rc = buf.alloc(&cs, 8 * m)) || (rc = buf.alloc(&sn, 8 * m)) ||
         (rc = buf.alloc(&g, 8 * (m + 1))) || (rc = buf.alloc(&y, 8 * m)) || (rc = buf.alloc(&hcol, 8 * (m + 1))) ||
         (rc = buf.alloc(&scal, 16)) || (rc = buf.alloc(&flag, sizeof(int))))
@@ -438,7 +571,7 @@ int hs_gmres_solve(hs_matrix* A, int32_t prec_type, void* prec, int32_t restart,
     cudaEventRecord(e0, st);
     auto norm = [&](const double* a) -> double {
         dot_kernel<<<nb, kT, 0, st>>>(n, a, a, partials);
-        hsdev::finalize_sum_kernel<<<1, hsdev::kRedThreads, 0, st>>>(partials, nb, scal, 1);
+        finalize_dd_kernel<<<1, kT, 0, st>>>(partials, nb, scal, 1);
         hs::count_launch(2);
         double v = 0;
         cudaMemcpyAsync(&v, scal, 8, cudaMemcpyDeviceToHost, st);
@@ -454,14 +587,12 @@ int hs_gmres_solve(hs_matrix* A, int32_t prec_type, void* prec, int32_t restart,
     bool conv = bnorm == 0.0;
     const double tol = rtol * bnorm;
     while (!conv && total < maxit) {
-        const double invb = 1.0 / beta;
         // V0 = r / beta
         {
             double* vb = scal + 1;
-            cudaMemcpyAsync(vb, &beta, 8, cudaMemcpyHostToDevice, st);
+            HS_CUDA(cudaMemcpyAsync(vb, &beta, 8, cudaMemcpyHostToDevice, st));
             scale_from<<<ge, kT, 0, st>>>(n, r, vb, V);
             hs::count_launch();
-            (void)invb;
         }
         HS_CUDA(cudaMemsetAsync(H, 0, 8 * (size_t)(m + 1) * m, st));
         set_g<<<1, 64, 0, st>>>(g, m, beta);

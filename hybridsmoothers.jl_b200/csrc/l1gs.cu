@@ -798,21 +798,29 @@ void transpose(const hs_sparse* A, std::vector<int32_t>& rp, std::vector<int32_t
         }
 }
 
+// `on_device`: the row-wise arrays are already in device memory (owned by the
+// caller and only read during setup; packed caches only).
 template <typename TM, typename TS>
 int setup_device(hs_l1gs* P, const int32_t* rp_h, const int32_t* ci_h, const TM* v_h, int64_t nnz,
-                 cudaStream_t st) {
+                 cudaStream_t st, bool on_device = false) {
     const int32_t n = P->n;
     int32_t *rp_d = nullptr, *ci_d = nullptr;
     TM* v_d = nullptr;
     int rc;
-    if ((rc = dmalloc(P, &rp_d, sizeof(int32_t) * (n + 1)))) return rc;
-    P->rp = rp_d;
-    if ((rc = dmalloc(P, &ci_d, sizeof(int32_t) * nnz))) return rc;
-    P->ci = ci_d;
-    if ((rc = dmalloc(P, &v_d, sizeof(TM) * nnz))) return rc;
-    HS_CUDA(cudaMemcpyAsync(rp_d, rp_h, sizeof(int32_t) * (n + 1), cudaMemcpyHostToDevice, st));
-    HS_CUDA(cudaMemcpyAsync(ci_d, ci_h, sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, st));
-    HS_CUDA(cudaMemcpyAsync(v_d, v_h, sizeof(TM) * nnz, cudaMemcpyHostToDevice, st));
+    if (on_device) {
+        rp_d = const_cast<int32_t*>(rp_h);
+        ci_d = const_cast<int32_t*>(ci_h);
+        v_d = const_cast<TM*>(v_h);
+    } else {
+        if ((rc = dmalloc(P, &rp_d, sizeof(int32_t) * (n + 1)))) return rc;
+        P->rp = rp_d;
+        if ((rc = dmalloc(P, &ci_d, sizeof(int32_t) * nnz))) return rc;
+        P->ci = ci_d;
+        if ((rc = dmalloc(P, &v_d, sizeof(TM) * nnz))) return rc;
+        HS_CUDA(cudaMemcpyAsync(rp_d, rp_h, sizeof(int32_t) * (n + 1), cudaMemcpyHostToDevice, st));
+        HS_CUDA(cudaMemcpyAsync(ci_d, ci_h, sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, st));
+        HS_CUDA(cudaMemcpyAsync(v_d, v_h, sizeof(TM) * nnz, cudaMemcpyHostToDevice, st));
+    }
 
     TS* D = nullptr;
     if ((rc = dmalloc(P, &D, sizeof(TS) * n))) return rc;
@@ -841,7 +849,9 @@ int setup_device(hs_l1gs* P, const int32_t* rp_h, const int32_t* ci_h, const TM*
     setup_rows_kernel<TM, TS><<<(n + 255) / 256, 256, 0, st>>>(n, P->ps, P->npad, rp_d, ci_d, v_d, (TM)P->eta, D,
                                                               Di, SLi, SUi);
     HS_LAUNCH_CHECK("setup_rows_kernel");
-    if (packed) {
+    if (packed && on_device) {
+        HS_CUDA(cudaStreamSynchronize(st));
+    } else if (packed) {
         HS_CUDA(cudaStreamSynchronize(st));
         cudaFree(rp_d);
         cudaFree(ci_d);
@@ -1121,10 +1131,10 @@ int l1gs_view_of(const hs_l1gs* P, L1gsView* v) {
 // ---------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------
-extern "C" {
-
-int hs_l1gs_create(const hs_sparse* A, int32_t partsize, int32_t is_sym, double eta, int32_t sweep, int32_t cache,
-                   int32_t smoother_dtype, int32_t threads, int32_t blocks, void* stream, hs_l1gs** out) {
+namespace {
+int l1gs_create_impl(const hs_sparse* A, bool on_device, int32_t partsize, int32_t is_sym, double eta, int32_t sweep,
+                     int32_t cache, int32_t smoother_dtype, int32_t threads, int32_t blocks, void* stream,
+                     hs_l1gs** out) {
     if (!out) return hs::set_error(HS_ERR_ARG, "out is NULL");
     *out = nullptr;
     if (partsize <= 0) return hs::set_error(HS_ERR_ARG, "partsize must be greater than 0");
@@ -1134,8 +1144,10 @@ int hs_l1gs_create(const hs_sparse* A, int32_t partsize, int32_t is_sym, double 
     if (cache != HS_CACHE_PACKED && cache != HS_CACHE_VIEW) return hs::set_error(HS_ERR_ARG, "unknown cache %d", cache);
     if (smoother_dtype != HS_F64 && smoother_dtype != HS_F32)
         return hs::set_error(HS_ERR_ARG, "unknown smoother dtype %d", smoother_dtype);
-    int rc = validate_sparse(A);
+    int rc = on_device ? HS_OK : validate_sparse(A);
     if (rc) return rc;
+    if (on_device && (cache != HS_CACHE_PACKED || (A->format == HS_CSC && !is_sym)))
+        return hs::set_error(HS_ERR_UNSUPPORTED, "device-resident input needs a packed cache and row-wise arrays");
     if (A->dtype == HS_F32 && smoother_dtype == HS_F64)
         return hs::set_error(HS_ERR_UNSUPPORTED, "an FP64 smoother needs an FP64 matrix");
     if (partsize > 65535) return hs::set_error(HS_ERR_UNSUPPORTED, "partsize above 65535");
@@ -1187,11 +1199,11 @@ int hs_l1gs_create(const hs_sparse* A, int32_t partsize, int32_t is_sym, double 
     }
 
     if (A->dtype == HS_F64 && smoother_dtype == HS_F64)
-        rc = setup_device<double, double>(P, rp_h, ci_h, static_cast<const double*>(v_h), A->nnz, st);
+        rc = setup_device<double, double>(P, rp_h, ci_h, static_cast<const double*>(v_h), A->nnz, st, on_device);
     else if (A->dtype == HS_F64)
-        rc = setup_device<double, float>(P, rp_h, ci_h, static_cast<const double*>(v_h), A->nnz, st);
+        rc = setup_device<double, float>(P, rp_h, ci_h, static_cast<const double*>(v_h), A->nnz, st, on_device);
     else
-        rc = setup_device<float, float>(P, rp_h, ci_h, static_cast<const float*>(v_h), A->nnz, st);
+        rc = setup_device<float, float>(P, rp_h, ci_h, static_cast<const float*>(v_h), A->nnz, st, on_device);
     if (rc) {
         release(P);
         return rc;
@@ -1215,6 +1227,30 @@ int hs_l1gs_create(const hs_sparse* A, int32_t partsize, int32_t is_sym, double 
     }
     *out = P;
     return HS_OK;
+}
+}  // namespace
+
+namespace hs {
+int l1gs_create_from_matrix(const hs_matrix* M, int32_t partsize, double eta, int32_t sweep, int32_t smoother_dtype,
+                            cudaStream_t st, hs_l1gs** out) {
+    hs_sparse d{};
+    const void* v = nullptr;
+    int dt = 0;
+    matrix_arrays(M, &d.ptr, &d.idx, &v, &dt);
+    d.n = matrix_n(M);
+    d.nnz = matrix_nnz(M);
+    d.format = HS_CSR;
+    d.dtype = dt;
+    d.val = v;
+    return l1gs_create_impl(&d, true, partsize, 1, eta, sweep, HS_CACHE_PACKED, smoother_dtype, 256, 148, st, out);
+}
+}  // namespace hs
+
+extern "C" {
+
+int hs_l1gs_create(const hs_sparse* A, int32_t partsize, int32_t is_sym, double eta, int32_t sweep, int32_t cache,
+                   int32_t smoother_dtype, int32_t threads, int32_t blocks, void* stream, hs_l1gs** out) {
+    return l1gs_create_impl(A, false, partsize, is_sym, eta, sweep, cache, smoother_dtype, threads, blocks, stream, out);
 }
 
 int hs_l1gs_apply(hs_l1gs* P, const void* x, void* y, int32_t io_dtype, void* stream) {

@@ -155,11 +155,14 @@ class _HostSparse:
             raise TypeError("A must be CSC (SparseMatrixCSC) or CSR (SparseMatrixCSR)")
         if A.shape[0] != A.shape[1]:
             raise ValueError("A must be square")
-        A = A.copy()
-        A.sort_indices()
-        A.sum_duplicates()
-        if dtype is not None:
+        if not A.has_canonical_format:
+            # sorted, duplicate-free copy; a canonical input is read in place
+            A = A.copy()
+            A.sort_indices()
+            A.sum_duplicates()
+        if dtype is not None and A.dtype != np.dtype(dtype):
             A = A.astype(dtype)
+        self._A = A
         self.ptr = np.ascontiguousarray(A.indptr, dtype=np.int32)
         self.idx = np.ascontiguousarray(A.indices, dtype=np.int32)
         self.val = np.ascontiguousarray(A.data)
@@ -247,6 +250,8 @@ class L1GSPreconditioner:
         sdt = _L.HS_F32 if (precision is not None and np.dtype(precision) == np.float32) else hA.desc.dtype
         cfg = builder.device_config
         self._h = C.c_void_p()
+        # bound now: module globals may already be gone when __del__ runs at exit
+        self._destroy = _L.lib().hs_l1gs_destroy
         torch.cuda.init()
         check(lib().hs_l1gs_create(C.byref(hA.desc), int(partsize), int(isSymA), float(eta), sweep.code,
                                    cache.code, sdt, cfg.threads, cfg.blocks, _stream_ptr(stream),
@@ -301,9 +306,10 @@ class L1GSPreconditioner:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h and _L._lib is not None:
+        destroy = getattr(self, "_destroy", None)
+        if h and destroy is not None:
             try:
-                _L._lib.hs_l1gs_destroy(h)
+                destroy(h)
             except Exception:
                 pass
             self._h = None
@@ -359,6 +365,8 @@ class DeviceSparseMatrix:
         self.n = hA.desc.n
         self.dtype = np.dtype(dtype)
         self._h = C.c_void_p()
+        # bound now: module globals may already be gone when __del__ runs at exit
+        self._destroy = _L.lib().hs_matrix_destroy
         check(lib().hs_matrix_create(C.byref(hA.desc), _dtype_code(dtype), _stream_ptr(stream), C.byref(self._h)))
 
     @property
@@ -367,9 +375,10 @@ class DeviceSparseMatrix:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h and _L._lib is not None:
+        destroy = getattr(self, "_destroy", None)
+        if h and destroy is not None:
             try:
-                _L._lib.hs_matrix_destroy(h)
+                destroy(h)
             except Exception:
                 pass
             self._h = None
@@ -408,6 +417,8 @@ class _ChebSmoother:
         sdt = _L.HS_F32 if (cfg.precision is not None and np.dtype(cfg.precision) == np.float32) else _L.HS_F64
         eig = _L.HS_EIG_LANCZOS if cfg.eig == "lanczos" else _L.HS_EIG_POWER
         self._h = C.c_void_p()
+        # bound now: module globals may already be gone when __del__ runs at exit
+        self._destroy = _L.lib().hs_cheb_destroy
         check(lib().hs_cheb_create(C.byref(hA.desc), cfg.kind, cfg.degree, eig, sdt, _stream_ptr(stream),
                                    C.byref(self._h)))
         self.smoother_dtype = np.float64 if sdt == _L.HS_F64 else np.float32
@@ -443,9 +454,10 @@ class _ChebSmoother:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h and _L._lib is not None:
+        destroy = getattr(self, "_destroy", None)
+        if h and destroy is not None:
             try:
-                _L._lib.hs_cheb_destroy(h)
+                destroy(h)
             except Exception:
                 pass
             self._h = None

@@ -102,6 +102,8 @@ PROTOTYPES = {
     "hs_batch_create": (C.c_int, [C.POINTER(hs_batch_config), _vp, C.POINTER(_vp)]),
     "hs_batch_submit": (C.c_int, [_vp, C.POINTER(hs_sparse), _vp, _vp, _i64, _i32, C.POINTER(_i32)]),
     "hs_batch_step": (C.c_int, [_vp, _i32, C.POINTER(_i32)]),
+    "hs_batch_launch": (C.c_int, [_vp, _i32]),
+    "hs_batch_wait": (C.c_int, [_vp, C.POINTER(_i32)]),
     "hs_batch_poll": (C.c_int, [_vp, C.POINTER(hs_batch_result), _i32, C.POINTER(_i32)]),
     "hs_batch_info_get": (C.c_int, [_vp, C.POINTER(hs_batch_info)]),
     "hs_batch_destroy": (C.c_int, [_vp]),

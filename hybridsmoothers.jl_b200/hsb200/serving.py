@@ -35,6 +35,7 @@ class BatchEngine:
         torch.cuda.init()
         cfg = hs_batch_config(max_slots, int(hbm_budget), partsize, rtol, maxit)
         self._h = C.c_void_p()
+        self._destroy = lib().hs_batch_destroy   # usable in __del__ at interpreter exit
         check(lib().hs_batch_create(C.byref(cfg), None, C.byref(self._h)))
         self._keep = {}      # tag -> (host sparse, b, x)
 
@@ -56,6 +57,16 @@ class BatchEngine:
     def step(self, iters=4):
         nf = C.c_int32()
         check(lib().hs_batch_step(self._h, int(iters), C.byref(nf)))
+        return nf.value
+
+    def launch(self, iters=4):
+        """Enqueue `iters` iterations of every active system and return at once."""
+        check(lib().hs_batch_launch(self._h, int(iters)))
+
+    def wait(self):
+        """Block until the last launch is done; returns how many systems finished."""
+        nf = C.c_int32()
+        check(lib().hs_batch_wait(self._h, C.byref(nf)))
         return nf.value
 
     def poll(self):
@@ -80,7 +91,7 @@ class BatchEngine:
 
     def close(self):
         if self._h:
-            lib().hs_batch_destroy(self._h)
+            self._destroy(self._h)
             self._h = None
 
     def __del__(self):
@@ -109,7 +120,9 @@ def serve(requests, max_slots=64, hbm_budget=64 << 30, iters_per_step=4, rtol=1e
     done_at, iters, conv, xs = {}, {}, {}, {}
     t0 = time.perf_counter()
     active = 0
-    while pending or waiting or active:
+
+    def admit():
+        nonlocal active
         now = time.perf_counter() - t0
         while pending and (not realtime or requests[pending[0]][0] <= now):
             i = pending.popleft()
@@ -123,16 +136,23 @@ def serve(requests, max_slots=64, hbm_budget=64 << 30, iters_per_step=4, rtol=1e
                 break
             waiting.popleft()
             active += 1
+
+    while pending or waiting or active:
         if active:
-            eng.step(iters_per_step)
+            # the GPU iterates while the host admits what has arrived meanwhile
+            eng.launch(iters_per_step)
+            admit()
+            eng.wait()
             for tag, x, it, ok, rel in eng.poll():
                 done_at[tag] = time.perf_counter() - t0
                 iters[tag], conv[tag], xs[tag] = it, ok, x
                 active -= 1
-        elif pending:
-            wait = requests[pending[0]][0] - (time.perf_counter() - t0)
-            if wait > 0:
-                time.sleep(min(wait, 0.01))
+        else:
+            admit()
+            if not active and pending:
+                wait = requests[pending[0]][0] - (time.perf_counter() - t0)
+                if wait > 0:
+                    time.sleep(min(wait, 0.01))
     total = time.perf_counter() - t0
     eng.close()
     lat = [done_at[i] - arrival[i] for i in done_at]

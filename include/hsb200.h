@@ -224,12 +224,19 @@ typedef struct {
 
 int hs_batch_create(const hs_batch_config* cfg, void* stream, hs_batch** out);
 /* Admit one system (host matrix, host b); x_host receives the solution when
- * it converges.  partsize 0 = the batch default. */
+ * it converges.  partsize 0 = the batch default.  A must be symmetric (the
+ * engine runs CG): a CSC is read as its own transpose.  May be called while a
+ * launch is in flight; the system joins at the next launch. */
 int hs_batch_submit(hs_batch* B, const hs_sparse* A, const double* b_host, double* x_host, int64_t tag,
                     int32_t partsize, int32_t* slot);
 /* Run `iters` batched PCG iterations over every active system; *finished =
  * systems that converged (or hit maxit) during this call. */
 int hs_batch_step(hs_batch* B, int32_t iters, int32_t* finished);
+/* hs_batch_step in two halves, so the host can admit the next requests while
+ * the GPU iterates: launch enqueues the iterations and returns; wait blocks
+ * until they are done and collects finished systems (as step does). */
+int hs_batch_launch(hs_batch* B, int32_t iters);
+int hs_batch_wait(hs_batch* B, int32_t* finished);
 /* Collect finished systems and release their device memory. */
 int hs_batch_poll(hs_batch* B, hs_batch_result* results, int32_t max_results, int32_t* count);
 int hs_batch_info_get(const hs_batch* B, hs_batch_info* info);

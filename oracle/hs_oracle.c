@@ -12,6 +12,8 @@
  * them.  The Krylov drivers (PCG, restarted GMRES) stand in for Krylov.jl,
  * which the reference reaches through LinearSolve.jl and does not vendor:
  * their iteration counts are this oracle's own and are not pinned to Krylov.jl.
+ * Their dot products are compensated (Dot2) and every update separately
+ * rounded, the arithmetic the device drivers use.
  */
 #include <math.h>
 #include <stdint.h>
@@ -107,18 +109,34 @@ static void prec_apply(int32_t n, const hso_prec* P, const double* r, double* z)
     free(rf);
 }
 
+/*
+ * Compensated dot product (Ogita, Rump & Oishi 2005, "Dot2"): TwoProduct via
+ * fma, TwoSum, errors accumulated separately.  As accurate as a dot in twice
+ * the working precision, so its rounded value does not depend on the order in
+ * which a parallel reduction meets the terms; the device drivers use the same
+ * accumulation, which is what lets their iterates match these.
+ */
 static double dot(int32_t n, const double* a, const double* b)
 {
-    double s = 0.0;
-    for (int32_t i = 0; i < n; ++i) s += a[i] * b[i];
-    return s;
+    double s = 0.0, c = 0.0;
+    for (int32_t i = 0; i < n; ++i) {
+        const double p = a[i] * b[i];
+        const double pe = fma(a[i], b[i], -p);
+        const double t = s + p;
+        const double bb = t - s;
+        const double q = (s - (t - bb)) + (p - bb);
+        s = t;
+        c = c + (q + pe);
+    }
+    return s + c;
 }
 
 /*
  * Preconditioned CG (Hestenes-Stiefel), x0 = 0, stop when the recursive
- * residual satisfies ||r_k||_2 <= rtol*||b||_2.  Returns the iteration count
- * (number of A*p products), or -1 if maxit was reached; *relres receives the
- * true relative residual ||b - A x||/||b|| of the returned x.
+ * residual satisfies sqrt(r.r) <= rtol*sqrt(b.b).  Every vector update is two
+ * rounded operations (the file is built with -ffp-contract=off).  Returns the
+ * iteration count (number of A*p products), or -1 if maxit was reached;
+ * *relres receives the true relative residual ||b - A x||/||b|| of x.
  */
 int32_t hso_pcg(int32_t n, const int32_t* rp, const int32_t* ci, const double* v, const double* b,
                 double* x, const hso_prec* P, double rtol, int32_t maxit, double* relres)
@@ -128,21 +146,22 @@ int32_t hso_pcg(int32_t n, const int32_t* rp, const int32_t* ci, const double* v
     double* p = z + n;
     double* q = p + n;
     for (int32_t i = 0; i < n; ++i) { x[i] = 0.0; r[i] = b[i]; }
-    double bnorm = sqrt(dot(n, b, b));
+    const double bb = dot(n, b, b);
+    const double bnorm = sqrt(bb);
     int32_t it = 0, conv = 0;
-    if (bnorm == 0.0) { conv = 1; goto done; }
+    if (bb == 0.0) { conv = 1; goto done; }
     prec_apply(n, P, r, z);
     memcpy(p, z, sizeof(double) * (size_t)n);
     double rz = dot(n, r, z);
     for (it = 1; it <= maxit; ++it) {
         hso_spmv_f64(n, rp, ci, v, p, q);
-        double alpha = rz / dot(n, p, q);
-        for (int32_t i = 0; i < n; ++i) { x[i] += alpha * p[i]; r[i] -= alpha * q[i]; }
-        double rn = sqrt(dot(n, r, r));
-        if (rn <= rtol * bnorm) { conv = 1; break; }
+        const double alpha = rz / dot(n, p, q);
+        for (int32_t i = 0; i < n; ++i) { x[i] = x[i] + alpha * p[i]; r[i] = r[i] - alpha * q[i]; }
+        const double rr = dot(n, r, r);
+        if (sqrt(rr) <= rtol * bnorm) { conv = 1; break; }
         prec_apply(n, P, r, z);
-        double rz_new = dot(n, r, z);
-        double beta = rz_new / rz;
+        const double rz_new = dot(n, r, z);
+        const double beta = rz_new / rz;
         rz = rz_new;
         for (int32_t i = 0; i < n; ++i) p[i] = z[i] + beta * p[i];
     }
@@ -160,9 +179,11 @@ done:
 
 /*
  * Restarted GMRES(m), right preconditioned (A M^-1 u = b, x = M^-1 u), x0 = 0,
- * modified Gram-Schmidt, Givens rotations.  A cycle ends when the Arnoldi
- * residual estimate |g_{j+1}| <= rtol*||b||; convergence is then confirmed on
- * the true residual ||b - A x||.  Returns total inner iterations or -1.
+ * classical Gram-Schmidt applied twice (CGS2: all projections of a pass from
+ * the same w, then w -= sum_i h_i V_i in order i = 0..j), Givens rotations.
+ * A cycle ends when |g_{j+1}| <= rtol*||b||; the restart residual is
+ * r = b - A x (term by term, as five-argument mul!) and convergence is
+ * ||r|| <= rtol*||b||.  Returns total inner iterations or -1.
  */
 int32_t hso_gmres(int32_t n, const int32_t* rp, const int32_t* ci, const double* v, const double* b,
                   double* x, const hso_prec* P, int32_t m, double rtol, int32_t maxit,
@@ -177,37 +198,43 @@ int32_t hso_gmres(int32_t n, const int32_t* rp, const int32_t* ci, const double*
     double* sn = (double*)calloc((size_t)m, sizeof(double));
     double* g = (double*)calloc((size_t)m + 1, sizeof(double));
     double* yv = (double*)calloc((size_t)m, sizeof(double));
+    double* hcol = (double*)calloc((size_t)m + 1, sizeof(double));
 #define HH(i, j) H[(size_t)(i) * m + (j)]
     for (int32_t i = 0; i < n; ++i) { x[i] = 0.0; r[i] = b[i]; }
     const double bnorm = sqrt(dot(n, b, b));
+    const double tol = rtol * bnorm;
     double beta = bnorm;
     int32_t total = 0, conv = 0;
     if (bnorm == 0.0) { conv = 1; goto out; }
     while (total < maxit) {
         for (int32_t i = 0; i < n; ++i) V[i] = r[i] / beta;
+        memset(H, 0, sizeof(double) * (size_t)(m + 1) * m);
         for (int32_t i = 0; i <= m; ++i) g[i] = 0.0;
         g[0] = beta;
         int32_t jend = 0;
         for (int32_t j = 0; j < m; ++j) {
             prec_apply(n, P, V + (size_t)j * n, u);
             hso_spmv_f64(n, rp, ci, v, u, w);
-            for (int32_t i = 0; i <= j; ++i) {
-                double h = dot(n, w, V + (size_t)i * n);
-                HH(i, j) = h;
-                const double* Vi = V + (size_t)i * n;
-                for (int32_t t = 0; t < n; ++t) w[t] -= h * Vi[t];
+            for (int32_t pass = 0; pass < 2; ++pass) {
+                for (int32_t i = 0; i <= j; ++i) hcol[i] = dot(n, V + (size_t)i * n, w);
+                for (int32_t t = 0; t < n; ++t) {
+                    double s = w[t];
+                    for (int32_t i = 0; i <= j; ++i) s = s - hcol[i] * V[(size_t)i * n + t];
+                    w[t] = s;
+                }
+                for (int32_t i = 0; i <= j; ++i) HH(i, j) = HH(i, j) + hcol[i];
             }
-            double hn = sqrt(dot(n, w, w));
+            const double hn = sqrt(dot(n, w, w));
             HH(j + 1, j) = hn;
             if (hn != 0.0)
                 for (int32_t t = 0; t < n; ++t) V[(size_t)(j + 1) * n + t] = w[t] / hn;
             for (int32_t i = 0; i < j; ++i) {
-                double a0 = HH(i, j), a1 = HH(i + 1, j);
+                const double a0 = HH(i, j), a1 = HH(i + 1, j);
                 HH(i, j) = cs[i] * a0 + sn[i] * a1;
                 HH(i + 1, j) = -sn[i] * a0 + cs[i] * a1;
             }
-            double a0 = HH(j, j), a1 = HH(j + 1, j);
-            double den = sqrt(a0 * a0 + a1 * a1);
+            const double a0 = HH(j, j), a1 = HH(j + 1, j);
+            const double den = sqrt(a0 * a0 + a1 * a1);
             cs[j] = den == 0.0 ? 1.0 : a0 / den;
             sn[j] = den == 0.0 ? 0.0 : a1 / den;
             HH(j, j) = cs[j] * a0 + sn[j] * a1;
@@ -216,29 +243,29 @@ int32_t hso_gmres(int32_t n, const int32_t* rp, const int32_t* ci, const double*
             g[j] = cs[j] * g[j];
             ++total;
             jend = j + 1;
-            if (fabs(g[j + 1]) <= rtol * bnorm || total >= maxit || hn == 0.0) break;
+            if (fabs(g[j + 1]) <= tol || hn == 0.0 || total >= maxit) break;
         }
         for (int32_t i = jend - 1; i >= 0; --i) {
             double s = g[i];
-            for (int32_t t = i + 1; t < jend; ++t) s -= HH(i, t) * yv[t];
+            for (int32_t t = i + 1; t < jend; ++t) s = s - HH(i, t) * yv[t];
             yv[i] = s / HH(i, i);
         }
-        for (int32_t t = 0; t < n; ++t) w[t] = 0.0;
-        for (int32_t i = 0; i < jend; ++i) {
-            const double* Vi = V + (size_t)i * n;
-            for (int32_t t = 0; t < n; ++t) w[t] += yv[i] * Vi[t];
+        for (int32_t t = 0; t < n; ++t) {
+            double s = 0.0;
+            for (int32_t i = 0; i < jend; ++i) s = s + yv[i] * V[(size_t)i * n + t];
+            w[t] = s;
         }
         prec_apply(n, P, w, u);
-        for (int32_t t = 0; t < n; ++t) x[t] += u[t];
-        hso_spmv_f64(n, rp, ci, v, x, w);
-        for (int32_t t = 0; t < n; ++t) r[t] = b[t] - w[t];
+        for (int32_t t = 0; t < n; ++t) x[t] = x[t] + u[t];
+        for (int32_t t = 0; t < n; ++t) r[t] = b[t];
+        hso_spmv_sub_f64(n, rp, ci, v, x, r);
         beta = sqrt(dot(n, r, r));
-        if (beta <= rtol * bnorm) { conv = 1; break; }
+        if (beta <= tol) { conv = 1; break; }
     }
 out:
     *relres = bnorm > 0 ? beta / bnorm : 0.0;
 #undef HH
-    free(V); free(w); free(H); free(cs); free(sn); free(g); free(yv);
+    free(V); free(w); free(H); free(cs); free(sn); free(g); free(yv); free(hcol);
     return conv ? total : -1;
 }
 

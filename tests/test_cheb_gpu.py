@@ -149,3 +149,14 @@ def test_lanczos_bounds():
     assert 0 < info.lanczos_min < info.lanczos_max <= 1.0 + 1e-12
     assert info.lanczos_max >= info.rho_power * (1 - 1e-6)
     assert S.rho == info.lanczos_max
+
+
+def test_power_iteration_large_grid():
+    """A matrix with more row blocks than the power iteration has partial
+    slots (80^3 rows = 2000 blocks of 256 > 1184): the kernel must stride over
+    row blocks and rho must still match the oracle's."""
+    A = W.poisson3d_7pt(80)
+    S = hsb200.build_smoother(hsb200.ChebyshevFourth(degree=4), A)
+    ref = O.OracleChebyshev(A, kind=4, degree=4)
+    assert abs(S.rho - ref.rho) <= 1e-12 * ref.rho
+    assert 0.5 < S.rho <= 1

@@ -135,3 +135,44 @@ def test_autotuner_picks_a_candidate():
     ps, cache = tuner.choose(A)
     assert ps in (8, 16, 32) and cache == "packed"
     assert tuner.choose(A) == (ps, cache)   # cached by matrix class
+
+
+def test_admission_during_launch_reuses_slot():
+    """A system submitted while a launch is in flight, into the slot a
+    finished system just left, joins at the next launch: the in-flight copy
+    of that slot's scalars (the previous occupant's, converged) must not mark
+    it finished, and its result equals the alone result bitwise."""
+    reqs = small_stream(2, seed=23)
+    (_, A1, b1), (_, A2, b2) = reqs
+    eng = serving.BatchEngine(max_slots=1)
+    assert eng.submit(A1, b1, 1, 8)
+    first = None
+    while first is None:
+        eng.step(8)
+        for tag, x, it, ok, rel in eng.poll():
+            first = (tag, it, ok)
+    assert first[0] == 1 and first[2]
+    eng.launch(4)                      # nothing active: only the scalars copy is in flight
+    assert eng.submit(A2, b2, 2, 8)    # same slot, admitted during the launch
+    assert eng.wait() == 0
+    assert eng.poll() == []
+    res = None
+    for _ in range(2000):
+        eng.launch(8)
+        eng.wait()
+        for tag, x, it, ok, rel in eng.poll():
+            res = (tag, x.copy(), it, ok)
+        if res:
+            break
+    eng.close()
+    assert res is not None and res[0] == 2 and res[3]
+    alone = serving.BatchEngine(max_slots=1)
+    alone.submit(A2, b2, 0, 8)
+    ref = None
+    while ref is None:
+        alone.step(8)
+        for tag, x, it, ok, rel in alone.poll():
+            ref = (x.copy(), it)
+    alone.close()
+    assert res[2] == ref[1]
+    np.testing.assert_array_equal(res[1], ref[0])
