@@ -97,6 +97,9 @@ PROTOTYPES = {
     "hs_cheb_set_rho": (C.c_int, [_vp, _d]),
     "hs_cheb_destroy": (C.c_int, [_vp]),
     "hs_cheb_smooth_noalloc": (C.c_int, [_i32, _i64, _vp, _vp, _vp, _vp, _i32, _i32, _d, _d, _vp, _vp, _vp]),
+    "hs_richardson_create": (C.c_int, [_vp, _vp, C.POINTER(_vp)]),
+    "hs_richardson_smooth": (C.c_int, [_vp, _vp, _vp, _i32, _vp]),
+    "hs_richardson_destroy": (C.c_int, [_vp]),
     "hs_pcg_solve": (C.c_int, [_vp, _i32, _vp, _vp, _vp, _d, _i32, _vp, C.POINTER(hs_solve_info)]),
     "hs_gmres_solve": (C.c_int, [_vp, _i32, _vp, _i32, _vp, _vp, _d, _i32, _vp, C.POINTER(hs_solve_info)]),
     "hs_batch_create": (C.c_int, [C.POINTER(hs_batch_config), _vp, C.POINTER(_vp)]),

@@ -180,6 +180,23 @@ int hs_cheb_smooth_noalloc(int32_t n, int64_t nnz, const int32_t* rp, const int3
                            double* x, const double* b, void* stream);
 
 /* ---------------------------------------------------------------------- */
+/* AMG smoother (ext/HybridSmoothersAMGExt.jl:8-33): the L1GS             */
+/* preconditioner used as a Richardson smoother inside a multigrid cycle.  */
+/* ---------------------------------------------------------------------- */
+typedef struct hs_richardson_s hs_richardson;
+/* HybridSmoother{A, s, residual, correction} (:8-13): A and P stay owned by
+ * the caller and must outlive the smoother; the residual and correction
+ * vectors (matrix dtype) are allocated here.  P must have been built from the
+ * same matrix (any sweep/cache; an FP32 smoother with an FP64 matrix works on
+ * FP64 vectors). */
+int hs_richardson_create(const hs_matrix* A, hs_l1gs* P, hs_richardson** out);
+/* AMG.smooth!(x, s, b) (:26-33): `sweeps` times (the reference: 2)
+ *   residual = A x;  residual .-= b;  correction = P \ residual;  x .-= correction
+ * with x and b device vectors in the matrix dtype; x is updated in place. */
+int hs_richardson_smooth(hs_richardson* S, void* x, const void* b, int32_t sweeps, void* stream);
+int hs_richardson_destroy(hs_richardson* S);
+
+/* ---------------------------------------------------------------------- */
 /* Krylov drivers (stand-ins for Krylov.jl's CG/GMRES reached through      */
 /* LinearSolve: test/test_preconditioners.jl:65,93).  FP64, device vectors. */
 /* ---------------------------------------------------------------------- */

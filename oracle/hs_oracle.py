@@ -396,3 +396,22 @@ def gmres(A, b, P=None, m=30, rtol=1e-8, maxit=10000):
                          _p(np.ascontiguousarray(b, dtype=np.float64)), _p(x), C.byref(s),
                          C.c_int32(m), C.c_double(rtol), C.c_int32(maxit), C.byref(rel))
     return x, int(it), float(rel.value)
+
+
+def amg_richardson(A, P, x, b, sweeps=2):
+    """AMG.smooth!(x, s::HybridSmoother, b) (ext/HybridSmoothersAMGExt.jl:26-33):
+    `sweeps` times residual = A x (three-argument mul!, row sums in ascending
+    column order from zero), residual .-= b, correction = P \\ residual,
+    x .-= correction.  P is an OracleL1GS of A; returns the new x."""
+    R = A.tocsr()
+    R.sort_indices()
+    dt = np.dtype(P.dtype)
+    v = np.ascontiguousarray(R.data.astype(dt))
+    x = np.array(x, dtype=dt)
+    b = np.ascontiguousarray(b, dtype=dt)
+    for _ in range(sweeps):
+        r = spmv(R.indptr, R.indices, v, x)
+        r = r - b
+        z = P.ldiv(r)
+        x = x - z
+    return x
