@@ -34,7 +34,9 @@
 
 namespace {
 
-constexpr int kRPB = 256;     // rows per block of the segmented kernels
+constexpr int kRPB = 256;     // rows per CSR-stream pass (= threads per CTA)
+constexpr int kSub = 4;       // passes per CTA
+constexpr int kRPC = kRPB * kSub;   // rows per CTA of the segmented kernels
 constexpr int kT = 256;
 
 struct Scalars {
@@ -52,59 +54,64 @@ __device__ __forceinline__ void store_dd(double* partials, DD v) {
     }
 }
 
+// Per slot: its CTA range (for the per-slot reductions) and scalars.
 struct SlotDev {
     int32_t n, blk0, nblk, pad;
+    Scalars* s;
+};
+
+// One CTA of the segmented vector kernels: kRPC rows of one slot, with every
+// pointer it needs, so a CTA starts after one load of its entry.
+struct BlockMap {
+    int32_t n, row0;
     const int32_t* rp;
     const int32_t* ci;
     const double* v;
     double *x, *r, *z, *p, *q;
-    Scalars* s;
+    const Scalars* s;
 };
 
-struct BlockMap {
-    int32_t slot, row0;
-};
-
-// One work item of the batched L1GS apply: 32 partitions (a group) of a slot.
+// One work item of the batched L1GS apply: 32 partitions (a group) of a slot,
+// with its stream bases, D_Dl1 and vectors already offset to the group.
 struct PrecItem {
-    int32_t slot, group;
-};
-
-struct PrecDev {
-    int32_t n, ngroups, tlen, pad;
-    int64_t npad;
+    const float* SL;
+    const float* SU;
     const float* Di;
-    const float* SLi;
-    const float* SUi;
-    const double* x;   // r
-    double* y;         // z
+    const double* x;   // r of the group's first row
+    double* y;         // z likewise
+    int64_t npad;
+    int32_t rows;      // rows of the slot from the group's first row on
+    int32_t tlen;
     const Scalars* s;
 };
 
 // ---- segmented PCG kernels --------------------------------------------------
 // Same arithmetic as the single-system driver: compensated (Dot2) dots,
-// separately rounded updates, storage-order SpMV rows.
-__global__ void __launch_bounds__(kT) seg_spmv_dot(const BlockMap* __restrict__ map, const SlotDev* __restrict__ slots,
-                                                   double* __restrict__ partials) {
+// separately rounded updates, storage-order SpMV rows.  The streaming kernels
+// load kSub elements per thread before using any.
+__global__ void __launch_bounds__(kT, 4) seg_spmv_dot(const BlockMap* __restrict__ map, double* __restrict__ partials) {
     __shared__ hsdev::CsrStream<double, kRPB, hsdev::stream_cap<kRPB>()> sh;
     const BlockMap m = map[blockIdx.x];
-    const SlotDev sd = slots[m.slot];
     DD part{0.0, 0.0};
-    if (!sd.s->done) {   // uniform over the block (one slot per block)
-        auto fp = [&](int32_t j) { return __ldg(sd.p + j); };
-        const double acc = hsdev::csr_stream_fold<double, kRPB, hsdev::stream_cap<kRPB>()>(
-            sh, sd.n, sd.rp, sd.ci, sd.v, m.row0, 0.0, fp, hsdev::AddOp<double>());
-        const int64_t r = m.row0 + threadIdx.x;
-        if (r < sd.n) {
-            sd.q[r] = acc;
-            hsdev::dd_add_prod(part, sd.p[r], acc);
+    if (!m.s->done) {   // uniform over the CTA (one slot per CTA)
+        auto fp = [&](int32_t j) { return __ldg(m.p + j); };
+        for (int sb = 0; sb < kSub; ++sb) {
+            const int64_t row0 = (int64_t)m.row0 + sb * kRPB;
+            if (row0 >= m.n) break;   // uniform
+            const double acc = hsdev::csr_stream_fold<double, kRPB, hsdev::stream_cap<kRPB>()>(
+                sh, m.n, m.rp, m.ci, m.v, row0, 0.0, fp, hsdev::AddOp<double>());
+            const int64_t r = row0 + threadIdx.x;
+            if (r < m.n) {
+                m.q[r] = acc;
+                hsdev::dd_add_prod(part, m.p[r], acc);
+            }
         }
     }
     store_dd(partials, part);
 }
 
-// Sum of a slot's block partials (valid on thread 0).  A large slot has
-// thousands of blocks: each thread loads 8 partials before adding any.
+// Sum of a slot's CTA partials (valid on thread 0).  A large slot has
+// thousands of CTAs: each thread loads 8 partials before adding any.
 __device__ __forceinline__ double slot_sum(const double* __restrict__ partials, const SlotDev& sd) {
     DD v{0.0, 0.0};
     const double2* p2 = reinterpret_cast<const double2*>(partials) + sd.blk0;
@@ -130,19 +137,31 @@ __global__ void seg_alpha(const SlotDev* __restrict__ slots, const int32_t* __re
     }
 }
 
-__global__ void __launch_bounds__(kT) seg_update(const BlockMap* __restrict__ map, const SlotDev* __restrict__ slots,
-                                                 double* __restrict__ partials) {
+__global__ void __launch_bounds__(kT) seg_update(const BlockMap* __restrict__ map, double* __restrict__ partials) {
     const BlockMap m = map[blockIdx.x];
-    const SlotDev sd = slots[m.slot];
     DD part{0.0, 0.0};
-    if (!sd.s->done) {
-        const double alpha = sd.s->alpha;
-        const int i = m.row0 + threadIdx.x;
-        if (i < sd.n) {
-            sd.x[i] = __dadd_rn(sd.x[i], __dmul_rn(alpha, sd.p[i]));
-            const double ri = __dsub_rn(sd.r[i], __dmul_rn(alpha, sd.q[i]));
-            sd.r[i] = ri;
-            hsdev::dd_add_prod(part, ri, ri);
+    if (!m.s->done) {
+        const double alpha = m.s->alpha;
+        double xv[kSub], pv[kSub], rv[kSub], qv[kSub];
+#pragma unroll
+        for (int k = 0; k < kSub; ++k) {
+            const int i = m.row0 + k * kRPB + threadIdx.x;
+            if (i < m.n) {
+                xv[k] = m.x[i];
+                pv[k] = m.p[i];
+                rv[k] = m.r[i];
+                qv[k] = m.q[i];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kSub; ++k) {
+            const int i = m.row0 + k * kRPB + threadIdx.x;
+            if (i < m.n) {
+                m.x[i] = __dadd_rn(xv[k], __dmul_rn(alpha, pv[k]));
+                const double ri = __dsub_rn(rv[k], __dmul_rn(alpha, qv[k]));
+                m.r[i] = ri;
+                hsdev::dd_add_prod(part, ri, ri);
+            }
         }
     }
     store_dd(partials, part);
@@ -166,14 +185,22 @@ __global__ void seg_check(const SlotDev* __restrict__ slots, const int32_t* __re
     }
 }
 
-__global__ void __launch_bounds__(kT) seg_dot(const BlockMap* __restrict__ map, const SlotDev* __restrict__ slots,
-                                              double* __restrict__ partials) {
+__global__ void __launch_bounds__(kT) seg_dot(const BlockMap* __restrict__ map, double* __restrict__ partials) {
     const BlockMap m = map[blockIdx.x];
-    const SlotDev sd = slots[m.slot];
     DD part{0.0, 0.0};
-    if (!sd.s->done) {
-        const int i = m.row0 + threadIdx.x;
-        if (i < sd.n) hsdev::dd_add_prod(part, sd.r[i], sd.z[i]);
+    if (!m.s->done) {
+        double rv[kSub], zv[kSub];
+#pragma unroll
+        for (int k = 0; k < kSub; ++k) {
+            const int i = m.row0 + k * kRPB + threadIdx.x;
+            if (i < m.n) {
+                rv[k] = m.r[i];
+                zv[k] = m.z[i];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kSub; ++k)
+            if (m.row0 + k * kRPB + (int)threadIdx.x < m.n) hsdev::dd_add_prod(part, rv[k], zv[k]);
     }
     store_dd(partials, part);
 }
@@ -188,13 +215,24 @@ __global__ void seg_beta(const SlotDev* __restrict__ slots, const int32_t* __res
     }
 }
 
-__global__ void __launch_bounds__(kT) seg_p(const BlockMap* __restrict__ map, const SlotDev* __restrict__ slots) {
+__global__ void __launch_bounds__(kT) seg_p(const BlockMap* __restrict__ map) {
     const BlockMap m = map[blockIdx.x];
-    const SlotDev sd = slots[m.slot];
-    if (sd.s->done) return;
-    const double beta = sd.s->beta;
-    const int i = m.row0 + threadIdx.x;
-    if (i < sd.n) sd.p[i] = __dadd_rn(sd.z[i], __dmul_rn(beta, sd.p[i]));
+    if (m.s->done) return;
+    const double beta = m.s->beta;
+    double zv[kSub], pv[kSub];
+#pragma unroll
+    for (int k = 0; k < kSub; ++k) {
+        const int i = m.row0 + k * kRPB + threadIdx.x;
+        if (i < m.n) {
+            zv[k] = m.z[i];
+            pv[k] = m.p[i];
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < kSub; ++k) {
+        const int i = m.row0 + k * kRPB + threadIdx.x;
+        if (i < m.n) m.p[i] = __dadd_rn(zv[k], __dmul_rn(beta, pv[k]));
+    }
 }
 
 // Slot initialisation after admission: x = 0, r = b, bb = b.b (z, p, rz after the first apply)
@@ -242,14 +280,16 @@ __global__ void init_scalars(const double* __restrict__ pbb, const double* __res
 }
 
 // ---- batched L1GS symmetric apply (FP32 smoother, FP64 vectors) -----------
-// Work item w -> (slot, group): 32 partitions of one slot, one lane each.
-// The packed streams of the slot are read tile by tile with 1D bulk copies
-// (one per stream row, 128 bytes) into a per-warp ring; y and D_Dl1 live in
-// registers, exactly like the single-system partsize<=32 kernel.
+// Work item -> 32 partitions (a group) of one slot, one lane each.  The packed
+// streams of the group are read tile by tile with 1D bulk copies (one per
+// stream row, 128 bytes) into a per-warp ring; y and D_Dl1 live in registers,
+// exactly like the single-system partsize<=32 kernel.  The elected lane keeps
+// the stream bases of the item it is issuing for in registers, so a refill is
+// one instruction sequence with no dependent loads.  Tiles of converged slots
+// are still fetched (they leave the tables at the next rebuild) but not used.
 template <int PS, int E, int STAGES>
 __global__ void __launch_bounds__(128, 3)
-    l1gs_batched_kernel(const PrecItem* __restrict__ items, int32_t nitems, const PrecDev* __restrict__ precs,
-                        int32_t* err) {
+    l1gs_batched_kernel(const PrecItem* __restrict__ items, int32_t nitems, int32_t* err) {
     constexpr int TLEN = PS * (PS - 1) / 2;
     constexpr int NT = (TLEN + E - 1) / E;
     constexpr int NTPG = 2 * NT;
@@ -268,19 +308,28 @@ __global__ void __launch_bounds__(128, 3)
     const int32_t my_items = w0 < nitems ? (nitems - 1 - w0) / wstride + 1 : 0;
     const int32_t total = my_items * NTPG;
 
+    int32_t cache_ii = -1;   // issue state of the elected lane
+    const float* cSL = nullptr;
+    const float* cSU = nullptr;
+    int64_t cnpad = 0;
     auto issue = [&](int32_t c) {
         const int32_t ii = c / NTPG;
+        if (ii != cache_ii) {
+            const PrecItem& it = items[w0 + ii * wstride];
+            cSL = it.SL;
+            cSU = it.SU;
+            cnpad = it.npad;
+            cache_ii = ii;
+        }
         int32_t ti = c - ii * NTPG;
-        const PrecItem it = items[w0 + ii * wstride];
-        const PrecDev& pd = precs[it.slot];
-        const float* base = ti < NT ? pd.SLi : pd.SUi;
+        const float* base = ti < NT ? cSL : cSU;
         if (ti >= NT) ti -= NT;
         const int stage = c & (STAGES - 1);
-        const int rows = pd.s->done ? 0 : min(E, pd.tlen - ti * E);   // converged slot: empty tile
+        const int rows = min(E, TLEN - ti * E);
         uint64_t* bar = bars + stage;
         hsdev::mbar_arrive_expect_tx(bar, (uint32_t)(rows * 128));
         for (int r = 0; r < rows; ++r) {
-            const float* src = base + ((int64_t)(ti * E + r)) * pd.npad + (int64_t)it.group * 32;
+            const float* src = base + (int64_t)(ti * E + r) * cnpad;
             float* dst = ring + stage * (E * 32) + r * 32;
             asm volatile(
                 "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], 128, [%2];" ::"r"(
@@ -310,8 +359,7 @@ __global__ void __launch_bounds__(128, 3)
     int32_t c = 0;
     for (int32_t ii = 0; ii < my_items; ++ii) {
         const PrecItem it = items[w0 + ii * wstride];
-        const PrecDev& pd = precs[it.slot];
-        if (pd.s->done) {   // converged: walk the (empty) tiles, leave z alone
+        if (it.s->done) {   // converged: walk the tiles, leave z alone
             for (int32_t t = 0; t < NTPG; ++t) {
                 if (!wait(c + t)) goto timeout;
                 release(c + t);
@@ -319,16 +367,13 @@ __global__ void __launch_bounds__(128, 3)
             c += NTPG;
             continue;
         }
-        const int64_t k = (int64_t)it.group * 32 + lane;
-        const int64_t rowbase = (int64_t)it.group * 32 * PS;
         float d[PS];
 #pragma unroll
-        for (int li = 0; li < PS; ++li) d[li] = pd.Di[(int64_t)li * pd.npad + k];
+        for (int li = 0; li < PS; ++li) d[li] = it.Di[(int64_t)li * it.npad + lane];
 #pragma unroll
         for (int m = 0; m < PS; ++m) {
             const int t = lane + 32 * m;
-            const int64_t row = rowbase + t;
-            xs[(t / PS) * XS + (t % PS)] = row < pd.n ? (float)pd.x[row] : 0.0f;
+            xs[(t / PS) * XS + (t % PS)] = t < it.rows ? (float)it.x[t] : 0.0f;
         }
         __syncwarp();
         float yv[PS];
@@ -372,8 +417,7 @@ __global__ void __launch_bounds__(128, 3)
 #pragma unroll
         for (int m = 0; m < PS; ++m) {
             const int t = lane + 32 * m;
-            const int64_t row = rowbase + t;
-            if (row < pd.n) pd.y[row] = (double)xs[(t / PS) * XS + (t % PS)];
+            if (t < it.rows) it.y[t] = (double)xs[(t / PS) * XS + (t % PS)];
         }
         __syncwarp();
     }
@@ -415,7 +459,6 @@ struct hs_batch_s {
     cudaStream_t solve = nullptr, setup = nullptr;
     std::vector<hs_batch_slot> slots;
     SlotDev* d_slots = nullptr;
-    PrecDev* d_precs = nullptr;
     Scalars* d_scal = nullptr;
     Scalars* h_scal = nullptr;          // pinned mirror of d_scal
     cudaEvent_t launched = nullptr;     // end of the last hs_batch_launch
@@ -467,7 +510,7 @@ int launch_batched(hs_batch* B, const hs_batch_s::Cls& cl, cudaStream_t st) {
     HS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, wpb * 32, smem));
     const int64_t want = (cl.nitems + wpb - 1) / wpb;
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)std::max(1, per_sm) * hs::num_sms()));
-    kern<<<grid, wpb * 32, smem, st>>>(B->d_items + cl.item0, cl.nitems, B->d_precs, B->err);
+    kern<<<grid, wpb * 32, smem, st>>>(B->d_items + cl.item0, cl.nitems, B->err);
     HS_LAUNCH_CHECK("l1gs_batched_kernel");
     return HS_OK;
 }
@@ -494,18 +537,50 @@ int rebuild(hs_batch* B) {
             if (sl.state != 1 || sl.ps != ps) continue;
             hs::L1gsView lv;
             hs::l1gs_view_of(sl.P, &lv);
-            for (int32_t g = 0; g < lv.ngroups; ++g) items.push_back({(int32_t)s, g});
+            const double* r = sl.vec + sl.n;
+            double* z = sl.vec + 2 * (size_t)sl.n;
+            for (int32_t g = 0; g < lv.ngroups; ++g) {
+                PrecItem it{};
+                it.SL = static_cast<const float*>(lv.SLi) + (int64_t)g * 32;
+                it.SU = static_cast<const float*>(lv.SUi) + (int64_t)g * 32;
+                it.Di = static_cast<const float*>(lv.Di) + (int64_t)g * 32;
+                const int64_t row0 = (int64_t)g * 32 * ps;
+                it.x = r + row0;
+                it.y = z + row0;
+                it.npad = lv.npad;
+                it.rows = (int32_t)std::max<int64_t>(0, (int64_t)sl.n - row0);
+                it.tlen = lv.tlen;
+                it.s = B->d_scal + s;
+                items.push_back(it);
+            }
         }
         cl.nitems = (int32_t)items.size() - cl.item0;
         if (cl.nitems) B->classes.push_back(cl);
     }
+    std::vector<SlotDev> sd(B->slots.size());
     for (size_t s = 0; s < B->slots.size(); ++s) {
         hs_batch_slot& sl = B->slots[s];
         if (sl.state != 1) continue;
         active.push_back((int32_t)s);
         sl.blk0 = (int32_t)map.size();
-        sl.nblk = (sl.n + kRPB - 1) / kRPB;
-        for (int32_t b = 0; b < sl.nblk; ++b) map.push_back({(int32_t)s, b * kRPB});
+        sl.nblk = (sl.n + kRPC - 1) / kRPC;
+        const void* mv = nullptr;
+        int mdt = 0;
+        BlockMap m{};
+        hs::matrix_arrays(sl.A, &m.rp, &m.ci, &mv, &mdt);
+        m.v = static_cast<const double*>(mv);
+        m.n = sl.n;
+        m.x = sl.vec;
+        m.r = sl.vec + sl.n;
+        m.z = sl.vec + 2 * (size_t)sl.n;
+        m.p = sl.vec + 3 * (size_t)sl.n;
+        m.q = sl.vec + 4 * (size_t)sl.n;
+        m.s = B->d_scal + s;
+        for (int32_t b = 0; b < sl.nblk; ++b) {
+            m.row0 = b * kRPC;
+            map.push_back(m);
+        }
+        sd[s] = SlotDev{sl.n, sl.blk0, sl.nblk, 0, B->d_scal + s};
     }
     if ((int32_t)map.size() > B->max_blocks || (int32_t)items.size() > B->max_items) {
         cudaFree(B->d_map);
@@ -517,47 +592,9 @@ int rebuild(hs_batch* B) {
         HS_CUDA(cudaMalloc(&B->d_partials, 2 * sizeof(double) * B->max_blocks));
         HS_CUDA(cudaMalloc(&B->d_items, sizeof(PrecItem) * B->max_items));
     }
-    // slot tables
-    std::vector<SlotDev> sd(B->slots.size());
-    std::vector<PrecDev> pd(B->slots.size());
-    for (size_t s = 0; s < B->slots.size(); ++s) {
-        const hs_batch_slot& sl = B->slots[s];
-        if (sl.state == 0) continue;
-        SlotDev d{};
-        d.n = sl.n;
-        d.blk0 = sl.blk0;
-        d.nblk = sl.nblk;
-        const void* mv = nullptr;
-        int mdt = 0;
-        hs::matrix_arrays(sl.A, &d.rp, &d.ci, &mv, &mdt);
-        d.v = static_cast<const double*>(mv);
-        d.x = sl.vec;
-        d.r = sl.vec + sl.n;
-        d.z = sl.vec + 2 * (size_t)sl.n;
-        d.p = sl.vec + 3 * (size_t)sl.n;
-        d.q = sl.vec + 4 * (size_t)sl.n;
-        d.s = B->d_scal + s;
-        sd[s] = d;
-        hs::L1gsView lv;
-        hs::l1gs_view_of(sl.P, &lv);
-        PrecDev p{};
-        p.n = lv.n;
-        p.ngroups = lv.ngroups;
-        p.tlen = lv.tlen;
-        p.npad = lv.npad;
-        p.Di = static_cast<const float*>(lv.Di);
-        p.SLi = static_cast<const float*>(lv.SLi);
-        p.SUi = static_cast<const float*>(lv.SUi);
-        p.x = d.r;
-        p.y = d.z;
-        p.s = d.s;
-        pd[s] = p;
-    }
     cudaStream_t st = B->solve;
-    if (!sd.empty()) {
+    if (!sd.empty())
         HS_CUDA(cudaMemcpyAsync(B->d_slots, sd.data(), sizeof(SlotDev) * sd.size(), cudaMemcpyHostToDevice, st));
-        HS_CUDA(cudaMemcpyAsync(B->d_precs, pd.data(), sizeof(PrecDev) * pd.size(), cudaMemcpyHostToDevice, st));
-    }
     if (!map.empty()) HS_CUDA(cudaMemcpyAsync(B->d_map, map.data(), sizeof(BlockMap) * map.size(), cudaMemcpyHostToDevice, st));
     if (!active.empty())
         HS_CUDA(cudaMemcpyAsync(B->d_active, active.data(), sizeof(int32_t) * active.size(), cudaMemcpyHostToDevice, st));
@@ -580,18 +617,18 @@ int rebuild(hs_batch* B) {
 
 int enqueue_iteration(hs_batch* B, cudaStream_t st) {
     if (B->nactive == 0) return HS_OK;
-    seg_spmv_dot<<<B->nblocks, kT, 0, st>>>(B->d_map, B->d_slots, B->d_partials);
+    seg_spmv_dot<<<B->nblocks, kT, 0, st>>>(B->d_map, B->d_partials);
     seg_alpha<<<B->nactive, kT, 0, st>>>(B->d_slots, B->d_active, B->d_partials);
-    seg_update<<<B->nblocks, kT, 0, st>>>(B->d_map, B->d_slots, B->d_partials);
+    seg_update<<<B->nblocks, kT, 0, st>>>(B->d_map, B->d_partials);
     seg_check<<<B->nactive, kT, 0, st>>>(B->d_slots, B->d_active, B->d_partials, B->cfg.maxit);
     hs::count_launch(4);
     for (const auto& cl : B->classes) {
         int rc = launch_prec_class(B, cl, st);
         if (rc) return rc;
     }
-    seg_dot<<<B->nblocks, kT, 0, st>>>(B->d_map, B->d_slots, B->d_partials);
+    seg_dot<<<B->nblocks, kT, 0, st>>>(B->d_map, B->d_partials);
     seg_beta<<<B->nactive, kT, 0, st>>>(B->d_slots, B->d_active, B->d_partials);
-    seg_p<<<B->nblocks, kT, 0, st>>>(B->d_map, B->d_slots);
+    seg_p<<<B->nblocks, kT, 0, st>>>(B->d_map);
     hs::count_launch(3);
     HS_CUDA(cudaGetLastError());
     return HS_OK;
@@ -625,7 +662,6 @@ int hs_batch_create(const hs_batch_config* cfg, void* stream, hs_batch** out) {
         (e = cudaMallocHost(&B->h_scal, sizeof(Scalars) * cfg->max_slots)) ||
         (e = cudaStreamCreateWithFlags(&B->setup, cudaStreamNonBlocking)) ||
         (e = cudaMalloc(&B->d_slots, sizeof(SlotDev) * cfg->max_slots)) ||
-        (e = cudaMalloc(&B->d_precs, sizeof(PrecDev) * cfg->max_slots)) ||
         (e = cudaMalloc(&B->d_scal, sizeof(Scalars) * cfg->max_slots)) ||
         (e = cudaMalloc(&B->d_active, sizeof(int32_t) * cfg->max_slots)) ||
         (e = cudaMalloc(&B->d_init, sizeof(double) * 4 * hsdev::kRedMaxBlocks))) {
@@ -800,7 +836,7 @@ int hs_batch_destroy(hs_batch* B) {
         if (s.state) free_slot(B, s);
     if (B->exec) cudaGraphExecDestroy(B->exec);
     if (B->graph) cudaGraphDestroy(B->graph);
-    void* ptrs[] = {B->d_slots, B->d_precs, B->d_scal, B->d_map, B->d_active, B->d_items, B->d_partials, B->d_init};
+    void* ptrs[] = {B->d_slots, B->d_scal, B->d_map, B->d_active, B->d_items, B->d_partials, B->d_init};
     for (void* p : ptrs) cudaFree(p);
     cudaStreamDestroy(B->solve);
     cudaStreamDestroy(B->setup);

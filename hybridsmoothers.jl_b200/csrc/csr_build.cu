@@ -9,6 +9,7 @@
 // each row come out in ascending column order (CSC enumerates columns in
 // order) -- exactly the host transpose's output.
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include <cub/device/device_radix_sort.cuh>
@@ -90,7 +91,26 @@ struct AsyncBufs {
 
 namespace hs {
 
+// The temporaries come from the device's default stream-ordered pool; keep
+// what it has reserved between calls (a served stream builds one matrix per
+// request) instead of returning it to the driver at every synchronisation.
+void keep_pool_reserve() {
+    static std::mutex mu;
+    static bool done[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+    std::lock_guard<std::mutex> lock(mu);
+    if (done[dev]) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    done[dev] = true;
+}
+
 int csr_from_host(const hs_sparse* A, int32_t dtype, int32_t* rp, int32_t* ci, void* v, cudaStream_t st) {
+    keep_pool_reserve();
     const int32_t n = A->n;
     const int64_t nnz = A->nnz;
     const size_t ses = A->dtype == HS_F64 ? 8 : 4;
