@@ -47,9 +47,11 @@ def parse_args():
     ap.add_argument("--soak-s", type=float, default=1.0, help="untimed load before timing, for clock samples")
     ap.add_argument("--suite", default=None,
                     help="secondary measurements instead of the headline line: pcg1d, pcg128, gmres96, mixed160, "
-                         "serving (comma-separated; prints one JSON line each)")
+                         "serving, pcgiter, batchiter (comma-separated; prints one JSON line each)")
     ap.add_argument("--serving-count", type=int, default=512)
     ap.add_argument("--serving-max", type=float, default=2e6)
+    ap.add_argument("--pcg-iters", type=int, default=40, help="iterations of the pcgiter suite")
+    ap.add_argument("--batch-steps", type=int, default=10, help="8-iteration steps of the batchiter suite")
     return ap.parse_args()
 
 
@@ -57,15 +59,16 @@ def parse_args():
 # Workloads and algorithmic bytes
 # ---------------------------------------------------------------------------
 def parse_workload(name):
-    # poisson128-l1gs-<sweep>-<cache>-ps<k>[-fp32]
+    # poisson<G>-l1gs-<sweep>-<cache>-ps<k>[-fp32]: the G^3 7-point Poisson operator
+    # (G = 128 is the headline; smaller G serve profiler captures of the same kernels)
     parts = name.split("-")
-    if parts[0] != "poisson128" or parts[1] != "l1gs":
+    if not parts[0].startswith("poisson") or not parts[0][7:].isdigit() or parts[1] != "l1gs":
         raise SystemExit(f"unknown workload {name}")
     sweep = {"fwd": "forward", "bwd": "backward", "sym": "symmetric"}[parts[2]]
     cache = parts[3]
     ps = int(parts[4][2:])
     fp32 = len(parts) > 5 and parts[5] == "fp32"
-    return dict(grid=128, sweep=sweep, cache=cache, ps=ps, fp32=fp32)
+    return dict(grid=int(parts[0][7:]), sweep=sweep, cache=cache, ps=ps, fp32=fp32)
 
 
 def packed_len(n, ps):
@@ -357,8 +360,59 @@ def suite_serving(args):
                          "choices": {str(k): v[0] for k, v in tuner.cache.items()}}}
 
 
+def suite_pcgiter(args):
+    """One PCG iteration on the 128^3 Poisson operator (FP64, L1GS symmetric packed ps16): a fixed
+    40-iteration run (rtol 0), device time per iteration.  The command whose kernel launch list is
+    summarised under profiles/."""
+    import hsb200
+    import torch
+    from hsb200 import workloads as W
+    A = W.poisson3d_7pt(128)
+    b = torch.from_numpy(W.rhs_uniform(A.shape[0])).cuda()
+    P = hsb200.L1GSPrecBuilder(hsb200.CUDABackend(), threads=256, blocks=148)(A, 16, isSymA=True)
+    M = hsb200.DeviceSparseMatrix(A)
+    x = torch.zeros_like(b)
+    iters = args.pcg_iters
+    hsb200.pcg(M, b, x, P, rtol=0.0, maxit=iters)
+    info = hsb200.pcg(M, b, x, P, rtol=0.0, maxit=iters)
+    n, nnz = A.shape[0], A.nnz
+    # algorithmic bytes of one iteration: SpMV+p.q, update+r.r, L1GS apply, r.z, p update
+    spmv = nnz * 12 + (n + 1) * 4 + 3 * 8 * n
+    upd, dot, pupd = 6 * 8 * n, 2 * 8 * n, 3 * 8 * n
+    l1gs = algorithmic_bytes(n, nnz, 16, "symmetric", "packed", 8)
+    per_iter = spmv + upd + l1gs + dot + pupd
+    us = info.ms * 1e3 / info.iterations
+    return {"suite": "pcgiter", "workload": "128^3 7-point Poisson, FP64 PCG + L1GS sym packed ps16",
+            "iterations": info.iterations, "us_per_iteration": us, "bytes_per_iteration": per_iter,
+            "GBps": per_iter / us / 1e3}
+
+
+def suite_batchiter(args):
+    """The batched engine (FP32 L1GS ps8 in FP64 PCG) on 48 requests of the serving stream, all
+    admitted: time per batched iteration while all are active."""
+    import torch
+    from hsb200 import serving
+    from hsb200 import workloads as W
+    reqs = W.serving_stream(count=48, lo=1e3, hi=2e6)
+    eng = serving.BatchEngine(max_slots=64)
+    for i, (_, A, b) in enumerate(reqs):
+        eng.submit(A, b, i, 8)
+    eng.step(1)
+    torch.cuda.synchronize()
+    steps = args.batch_steps
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        eng.step(8)
+    dt = time.perf_counter() - t0
+    info = eng.info()
+    eng.close()
+    rows = sum(A.shape[0] for _, A, _ in reqs)
+    return {"suite": "batchiter", "workload": "48 serving-stream systems, batched FP32-L1GS ps8 PCG",
+            "rows": rows, "active_after": info.active, "us_per_batched_iteration": dt / steps / 8 * 1e6}
+
+
 SUITES = {"pcg1d": suite_pcg1d, "pcg128": suite_pcg128, "gmres96": suite_gmres96, "mixed160": suite_mixed160,
-          "serving": suite_serving}
+          "serving": suite_serving, "pcgiter": suite_pcgiter, "batchiter": suite_batchiter}
 
 
 def main():
@@ -383,7 +437,7 @@ def main():
     x = W.rhs_uniform(n)
     tv = 4 if wl["fp32"] else 8
     bytes_per = algorithmic_bytes(n, nnz, wl["ps"], wl["sweep"], wl["cache"], tv)
-    config = {"workload": args.workload, "grid": "128^3", "n": n, "nnz": nnz, "partsize": wl["ps"],
+    config = {"workload": args.workload, "grid": f"{wl['grid']}^3", "n": n, "nnz": nnz, "partsize": wl["ps"],
               "sweep": wl["sweep"], "cache": wl["cache"], "matrix": "7-point Poisson, Dirichlet, FP64 CSC",
               "parallelism": f"replicas{world}" if world > 1 else "single",
               "l2": f"inputs larger than L2 ({bytes_per / 2**20:.0f} MiB per apply vs 126 MiB L2)",

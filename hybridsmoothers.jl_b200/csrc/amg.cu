@@ -5,7 +5,7 @@
 // HybridSmoother (:8-13) whose smooth! (:26-33) runs two Richardson sweeps
 //   mul!(residual, A, x); residual .-= b; ldiv!(correction, P, residual);
 //   x .-= correction
-// Here one sweep is two launches: a CSR-stream kernel that forms
+// Here one sweep is two launches: a warp CSR-stream kernel that forms
 // residual_i = (A x)_i - b_i (the row sum in storage order from zero, then one
 // rounded subtraction, as the three-argument mul! and the broadcast do), and
 // the L1GS apply.  From the second sweep on, the residual kernel also applies
@@ -32,21 +32,23 @@ struct hs_richardson_s {
 namespace {
 
 // residual = A xin - b, where xin_j = x_j (first sweep) or x_j - z_j (later
-// sweeps, also stored into xout for the rows of this block).
-template <typename T, int BR, bool UPDATE>
-__global__ void __launch_bounds__(BR, 1024 / BR)
+// sweeps, also stored into xout for the rows of this warp).  Warp CSR-stream.
+constexpr int kRT = 256;
+
+template <typename T, bool UPDATE>
+__global__ void __launch_bounds__(kRT)
     richardson_residual(int32_t n, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
                         const T* __restrict__ v, const T* __restrict__ x, const T* __restrict__ z,
                         const T* __restrict__ b, T* __restrict__ r, T* __restrict__ xout) {
-    __shared__ hsdev::CsrStream<T, BR, hsdev::stream_cap<BR>()> sh;
+    __shared__ T wbuf[kRT / 32][hsdev::kWarpCap];
+    const int warp = threadIdx.x >> 5;
     auto xin = [&](int32_t j) {
         if (UPDATE) return sub_rn(__ldg(x + j), __ldg(z + j));
         return __ldg(x + j);
     };
-    for (int64_t row0 = (int64_t)blockIdx.x * BR; row0 < n; row0 += (int64_t)gridDim.x * BR) {
-        const T acc = hsdev::csr_stream_fold<T, BR, hsdev::stream_cap<BR>()>(sh, n, rp, ci, v, row0, T(0), xin,
-                                                                             hsdev::AddOp<T>());
-        const int64_t i = row0 + threadIdx.x;
+    for (int64_t row0 = ((int64_t)blockIdx.x * (kRT / 32) + warp) * 32; row0 < n; row0 += (int64_t)gridDim.x * kRT) {
+        const T acc = hsdev::csr_warp_fold(wbuf[warp], n, rp, ci, v, row0, T(0), xin, hsdev::AddOp<T>());
+        const int64_t i = row0 + (threadIdx.x & 31);
         if (i < n) {
             r[i] = sub_rn(acc, b[i]);
             if (UPDATE) xout[i] = xin((int32_t)i);
@@ -68,8 +70,7 @@ int smooth_t(hs_richardson* S, T* x, const T* b, int sweeps, cudaStream_t st) {
     int dt = 0;
     hs::matrix_arrays(S->A, &rp, &ci, &vv, &dt);
     const T* v = static_cast<const T*>(vv);
-    const int br = hs::matrix_block_rows(S->A);
-    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((n + br - 1) / br, INT32_MAX));
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((n + kRT - 1) / kRT, INT32_MAX));
     T* r = static_cast<T*>(S->residual);
     T* z = static_cast<T*>(S->correction);
     const T* xcur = x;
@@ -78,15 +79,9 @@ int smooth_t(hs_richardson* S, T* x, const T* b, int sweeps, cudaStream_t st) {
     for (int k = 0; k < sweeps; ++k) {
         T* xnext = static_cast<T*>(S->xbuf[nb]);
         if (k == 0) {
-            if (br == 256)
-                richardson_residual<T, 256, false><<<grid, 256, 0, st>>>(n, rp, ci, v, xcur, z, b, r, nullptr);
-            else
-                richardson_residual<T, 128, false><<<grid, 128, 0, st>>>(n, rp, ci, v, xcur, z, b, r, nullptr);
+            richardson_residual<T, false><<<grid, kRT, 0, st>>>(n, rp, ci, v, xcur, z, b, r, nullptr);
         } else {
-            if (br == 256)
-                richardson_residual<T, 256, true><<<grid, 256, 0, st>>>(n, rp, ci, v, xcur, z, b, r, xnext);
-            else
-                richardson_residual<T, 128, true><<<grid, 128, 0, st>>>(n, rp, ci, v, xcur, z, b, r, xnext);
+            richardson_residual<T, true><<<grid, kRT, 0, st>>>(n, rp, ci, v, xcur, z, b, r, xnext);
             xcur = xnext;
             nb ^= 1;
         }

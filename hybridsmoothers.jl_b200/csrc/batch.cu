@@ -89,18 +89,19 @@ struct PrecItem {
 // Same arithmetic as the single-system driver: compensated (Dot2) dots,
 // separately rounded updates, storage-order SpMV rows.  The streaming kernels
 // load kSub elements per thread before using any.
-__global__ void __launch_bounds__(kT, 4) seg_spmv_dot(const BlockMap* __restrict__ map, double* __restrict__ partials) {
-    __shared__ hsdev::CsrStream<double, kRPB, hsdev::stream_cap<kRPB>()> sh;
+__global__ void __launch_bounds__(kT, 5) seg_spmv_dot(const BlockMap* __restrict__ map, double* __restrict__ partials) {
+    __shared__ double wbuf[kT / 32][hsdev::kWarpCap];
     const BlockMap m = map[blockIdx.x];
     DD part{0.0, 0.0};
     if (!m.s->done) {   // uniform over the CTA (one slot per CTA)
+        const int warp = threadIdx.x >> 5;
         auto fp = [&](int32_t j) { return __ldg(m.p + j); };
-        for (int sb = 0; sb < kSub; ++sb) {
-            const int64_t row0 = (int64_t)m.row0 + sb * kRPB;
-            if (row0 >= m.n) break;   // uniform
-            const double acc = hsdev::csr_stream_fold<double, kRPB, hsdev::stream_cap<kRPB>()>(
-                sh, m.n, m.rp, m.ci, m.v, row0, 0.0, fp, hsdev::AddOp<double>());
-            const int64_t r = row0 + threadIdx.x;
+        for (int k = 0; k < kRPC / kT; ++k) {   // the warp's 32-row chunks of this CTA
+            const int64_t row0 = (int64_t)m.row0 + (k * (kT / 32) + warp) * 32;
+            if (row0 >= m.n) break;   // uniform over the warp
+            const double acc =
+                hsdev::csr_warp_fold(wbuf[warp], m.n, m.rp, m.ci, m.v, row0, 0.0, fp, hsdev::AddOp<double>());
+            const int64_t r = row0 + (threadIdx.x & 31);
             if (r < m.n) {
                 m.q[r] = acc;
                 hsdev::dd_add_prod(part, m.p[r], acc);
@@ -286,7 +287,7 @@ __global__ void init_scalars(const double* __restrict__ pbb, const double* __res
 // exactly like the single-system partsize<=32 kernel.  The elected lane keeps
 // the stream bases of the item it is issuing for in registers, so a refill is
 // one instruction sequence with no dependent loads.  Tiles of converged slots
-// are still fetched (they leave the tables at the next rebuild) but not used.
+// are still fetched and applied until they leave the tables at the next rebuild.
 template <int PS, int E, int STAGES>
 __global__ void __launch_bounds__(128, 3)
     l1gs_batched_kernel(const PrecItem* __restrict__ items, int32_t nitems, int32_t* err) {
@@ -295,6 +296,7 @@ __global__ void __launch_bounds__(128, 3)
     constexpr int NTPG = 2 * NT;
     constexpr int XS = PS + 1;
     static_assert(PS % 2 == 0, "even partsize");
+    static_assert(E <= 32, "one lane per tile row");
     extern __shared__ __align__(128) unsigned char smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     constexpr uint32_t kRing = E * 32 * 4 * STAGES;
@@ -308,11 +310,15 @@ __global__ void __launch_bounds__(128, 3)
     const int32_t my_items = w0 < nitems ? (nitems - 1 - w0) / wstride + 1 : 0;
     const int32_t total = my_items * NTPG;
 
-    int32_t cache_ii = -1;   // issue state of the elected lane
+    // Tile refills: lane 0 posts the byte count on the stage's barrier and
+    // lanes 0..rows-1 each copy one 128-byte stream row, so a refill is one
+    // round of parallel bulk copies.  Every lane keeps the stream bases of the
+    // item it issues for (one broadcast load per item).
+    int32_t cache_ii = -1;
     const float* cSL = nullptr;
     const float* cSU = nullptr;
     int64_t cnpad = 0;
-    auto issue = [&](int32_t c) {
+    auto issue = [&](int32_t c) {   // called by the whole warp
         const int32_t ii = c / NTPG;
         if (ii != cache_ii) {
             const PrecItem& it = items[w0 + ii * wstride];
@@ -327,10 +333,10 @@ __global__ void __launch_bounds__(128, 3)
         const int stage = c & (STAGES - 1);
         const int rows = min(E, TLEN - ti * E);
         uint64_t* bar = bars + stage;
-        hsdev::mbar_arrive_expect_tx(bar, (uint32_t)(rows * 128));
-        for (int r = 0; r < rows; ++r) {
-            const float* src = base + (int64_t)(ti * E + r) * cnpad;
-            float* dst = ring + stage * (E * 32) + r * 32;
+        if (lane == 0) hsdev::mbar_arrive_expect_tx(bar, (uint32_t)(rows * 128));
+        if (lane < rows) {
+            const float* src = base + (int64_t)(ti * E + lane) * cnpad;
+            float* dst = ring + stage * (E * 32) + lane * 32;
             asm volatile(
                 "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], 128, [%2];" ::"r"(
                     hsdev::smem_u32(dst)),
@@ -344,7 +350,7 @@ __global__ void __launch_bounds__(128, 3)
     };
     auto release = [&](int32_t c) {
         __syncwarp();
-        if (lane == 0 && c + STAGES < total) {
+        if (c + STAGES < total) {
             hsdev::fence_proxy_async_smem();
             issue(c + STAGES);
         }
@@ -352,21 +358,16 @@ __global__ void __launch_bounds__(128, 3)
     if (lane == 0) {
         for (int s = 0; s < STAGES; ++s) hsdev::mbar_init(bars + s, 1);
         hsdev::fence_barrier_init();
-        for (int32_t c = 0; c < min(total, STAGES); ++c) issue(c);
     }
+    __syncwarp();
+    for (int32_t c = 0; c < min(total, STAGES); ++c) issue(c);
     __syncwarp();
 
     int32_t c = 0;
     for (int32_t ii = 0; ii < my_items; ++ii) {
+        // A converged slot's z is computed too (harmless: the dot and p kernels
+        // skip it, its r is frozen) -- no dependent load of its flag here.
         const PrecItem it = items[w0 + ii * wstride];
-        if (it.s->done) {   // converged: walk the tiles, leave z alone
-            for (int32_t t = 0; t < NTPG; ++t) {
-                if (!wait(c + t)) goto timeout;
-                release(c + t);
-            }
-            c += NTPG;
-            continue;
-        }
         float d[PS];
 #pragma unroll
         for (int li = 0; li < PS; ++li) d[li] = it.Di[(int64_t)li * it.npad + lane];
@@ -634,14 +635,28 @@ int enqueue_iteration(hs_batch* B, cudaStream_t st) {
     return HS_OK;
 }
 
+// Stream-ordered release on the solve stream: after every launch that used
+// the slot, without waiting for the device.
 void free_slot(hs_batch* B, hs_batch_slot& sl) {
-    if (sl.P) hs_l1gs_destroy(sl.P);
-    if (sl.A) hs_matrix_destroy(sl.A);
-    if (sl.vec) cudaFree(sl.vec);
+    if (sl.P) hs::l1gs_destroy_async(sl.P, B->solve);
+    if (sl.A) hs::matrix_destroy_async(sl.A, B->solve);
+    if (sl.vec) cudaFreeAsync(sl.vec, B->solve);
     B->used -= sl.bytes;
     sl = hs_batch_slot();
 }
 
+}  // namespace
+
+namespace {
+// Admission runs while the solve graph occupies the GPU: give its stream the
+// highest priority so its (small) setup kernels are scheduled ahead of the
+// queued iteration blocks instead of behind them.
+cudaError_t create_setup_stream(cudaStream_t* st) {
+    int lo = 0, hi = 0;
+    cudaError_t e = cudaDeviceGetStreamPriorityRange(&lo, &hi);
+    if (e != cudaSuccess) return e;
+    return cudaStreamCreateWithPriority(st, cudaStreamNonBlocking, hi);
+}
 }  // namespace
 
 extern "C" {
@@ -660,7 +675,7 @@ int hs_batch_create(const hs_batch_config* cfg, void* stream, hs_batch** out) {
     if ((e = cudaStreamCreateWithFlags(&B->solve, cudaStreamNonBlocking)) ||
         (e = cudaEventCreateWithFlags(&B->launched, cudaEventDisableTiming)) ||
         (e = cudaMallocHost(&B->h_scal, sizeof(Scalars) * cfg->max_slots)) ||
-        (e = cudaStreamCreateWithFlags(&B->setup, cudaStreamNonBlocking)) ||
+        (e = create_setup_stream(&B->setup)) ||
         (e = cudaMalloc(&B->d_slots, sizeof(SlotDev) * cfg->max_slots)) ||
         (e = cudaMalloc(&B->d_scal, sizeof(Scalars) * cfg->max_slots)) ||
         (e = cudaMalloc(&B->d_active, sizeof(int32_t) * cfg->max_slots)) ||
@@ -697,17 +712,20 @@ int hs_batch_submit(hs_batch* B, const hs_sparse* A, const double* b_host, doubl
     // The engine solves SPD systems (CG): a symmetric CSC's columns are its
     // rows, so the arrays are uploaded once, as CSR, and the FP32 smoother is
     // packed from that device copy (isSymA reads column i as row i).
+    // Slot memory is stream-ordered: allocated on the setup stream, released
+    // on the solve stream after the slot's last use, with no device sync.
     hs_sparse rows = *A;
     rows.format = HS_CSR;
-    int rc = hs_matrix_create(&rows, HS_F64, B->setup, &sl.A);
+    int rc = hs::matrix_create_async(&rows, HS_F64, B->setup, &sl.A);
     if (!rc) rc = hs::l1gs_create_from_matrix(sl.A, ps, 1.5, HS_SWEEP_SYMMETRIC, HS_F32, B->setup, &sl.P);
     if (!rc) {
-        cudaError_t e = cudaMalloc(&sl.vec, sizeof(double) * 6 * (size_t)A->n);
-        if (e) rc = hs::cuda_error(e, "cudaMalloc (slot vectors)");
+        cudaError_t e = cudaMallocAsync(&sl.vec, sizeof(double) * 6 * (size_t)A->n, B->setup);
+        if (e) rc = hs::cuda_error(e, "cudaMallocAsync (slot vectors)");
     }
     if (rc) {
-        if (sl.P) hs_l1gs_destroy(sl.P);
-        if (sl.A) hs_matrix_destroy(sl.A);
+        cudaStreamSynchronize(B->setup);
+        if (sl.P) hs::l1gs_destroy_async(sl.P, B->setup);
+        if (sl.A) hs::matrix_destroy_async(sl.A, B->setup);
         return rc;
     }
     sl.bytes = est;
@@ -834,6 +852,7 @@ int hs_batch_destroy(hs_batch* B) {
     cudaDeviceSynchronize();
     for (auto& s : B->slots)
         if (s.state) free_slot(B, s);
+    cudaStreamSynchronize(B->solve);   // the stream-ordered frees above
     if (B->exec) cudaGraphExecDestroy(B->exec);
     if (B->graph) cudaGraphDestroy(B->graph);
     void* ptrs[] = {B->d_slots, B->d_scal, B->d_map, B->d_active, B->d_items, B->d_partials, B->d_init};

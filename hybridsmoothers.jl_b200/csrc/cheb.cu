@@ -41,21 +41,14 @@ struct hs_matrix_s {
     int32_t* rp = nullptr;
     int32_t* ci = nullptr;
     void* v = nullptr;
-    int lpr = 256;   // rows per CSR-stream block
     int64_t bytes = 0;
+    bool stream_ordered = false;   // buffers from cudaMallocAsync
+    cudaStream_t alloc_stream = nullptr;
 };
 
 namespace hsm {
 
 inline size_t dsize(int dt) { return dt == HS_F64 ? 8 : 4; }
-
-// Rows per CSR-stream block: 256 while a block's products fit its staging area
-// (2048 entries: up to 8 per row, with margin for uneven rows), 128 beyond
-// (4096 entries, 32 per row; longer blocks fold from global memory).
-int pick_lpr(int64_t nnz, int32_t n) {
-    const double avg = n > 0 ? (double)nnz / n : 1.0;
-    return avg <= 7.5 ? 256 : 128;
-}
 
 // Host CSR (row-wise) arrays from an hs_sparse, values as double.
 void host_csr(const hs_sparse* A, std::vector<int32_t>& rp, std::vector<int32_t>& ci, std::vector<double>& v) {
@@ -109,7 +102,6 @@ int matrix_from_host(const std::vector<int32_t>& rp, const std::vector<int32_t>&
     M->n = (int32_t)rp.size() - 1;
     M->nnz = (int64_t)ci.size();
     M->dtype = dtype;
-    M->lpr = pick_lpr(M->nnz, M->n);
     const size_t es = dsize(dtype);
     cudaError_t e;
     if ((e = cudaMalloc(&M->rp, sizeof(int32_t) * rp.size())) != cudaSuccess ||
@@ -142,36 +134,36 @@ int matrix_from_host(const std::vector<int32_t>& rp, const std::vector<int32_t>&
 // ---------------------------------------------------------------------------
 constexpr int kThreads = 256;
 
-// Every SpMV-shaped kernel below runs the block CSR-stream of spmv.cuh: a
-// block of BR threads owns BR consecutive rows; BR = 256 for short rows, 128
-// for long ones (the block's products must fit stream_cap<BR>).  Grid-stride
-// over row blocks.
-#define HS_CS_ROWS_LOOP(BR) \
-    for (int64_t row0 = (int64_t)blockIdx.x * (BR); row0 < n; row0 += (int64_t)gridDim.x * (BR))
-#define HS_CS_FOLD(T, BR) hsdev::csr_stream_fold<T, BR, hsdev::stream_cap<BR>()>
-#define HS_CS_SHARED(T, BR) __shared__ hsdev::CsrStream<T, BR, hsdev::stream_cap<BR>()> sh
+// Every SpMV-shaped kernel below runs the warp CSR-stream of spmv.cuh
+// (csr_warp_fold): a warp owns 32 consecutive rows at a time and warps stride
+// over the matrix; a CTA is kThreads threads with one product window per warp.
+#define HS_WARP_SHARED(T) __shared__ T wbuf[kThreads / 32][hsdev::kWarpCap]
+#define HS_WARP_ROWS_LOOP                                                                                   \
+    const int warp_ = threadIdx.x >> 5;                                                                       \
+    for (int64_t row0 = ((int64_t)blockIdx.x * (kThreads / 32) + warp_) * 32; row0 < n;                       \
+         row0 += (int64_t)gridDim.x * kThreads)
+#define HS_WARP_FOLD(acc0, f, op) hsdev::csr_warp_fold(wbuf[warp_], n, rp, ci, v, row0, acc0, f, op)
 
 // MODE 0: y = A x; MODE 1: y = y - A x (term by term); MODE 2: y = beta y + sum (a x) alpha.
-template <typename T, int BR, int MODE>
-__global__ void __launch_bounds__(BR, 1024 / BR) spmv_kernel(int32_t n, const int32_t* __restrict__ rp,
-                                                           const int32_t* __restrict__ ci, const T* __restrict__ v,
-                                                           const T* __restrict__ x, T* __restrict__ y, T alpha,
-                                                           T beta) {
-    HS_CS_SHARED(T, BR);
+template <typename T, int MODE>
+__global__ void __launch_bounds__(kThreads) spmv_kernel(int32_t n, const int32_t* __restrict__ rp,
+                                                        const int32_t* __restrict__ ci, const T* __restrict__ v,
+                                                        const T* __restrict__ x, T* __restrict__ y, T alpha, T beta) {
+    HS_WARP_SHARED(T);
     auto fx = [&](int32_t j) { return __ldg(x + j); };
-    HS_CS_ROWS_LOOP(BR) {
-        const int64_t r = row0 + threadIdx.x;
+    HS_WARP_ROWS_LOOP {
+        const int64_t r = row0 + (threadIdx.x & 31);
         const bool valid = r < n;
         T acc;
         if (MODE == 0) {
-            acc = HS_CS_FOLD(T, BR)(sh, n, rp, ci, v, row0, T(0), fx, AddOp<T>());
+            acc = HS_WARP_FOLD(T(0), fx, AddOp<T>());
         } else if (MODE == 1) {
-            acc = HS_CS_FOLD(T, BR)(sh, n, rp, ci, v, row0, valid ? y[r] : T(0), fx, SubOp<T>());
+            acc = HS_WARP_FOLD(valid ? y[r] : T(0), fx, SubOp<T>());
         } else {
             T a0 = T(0);
             if (valid && beta != T(0)) a0 = (beta == T(1)) ? y[r] : mul_rn(y[r], beta);
             auto op = [alpha](T a, T p) { return add_rn(a, mul_rn(p, alpha)); };
-            acc = HS_CS_FOLD(T, BR)(sh, n, rp, ci, v, row0, a0, fx, op);
+            acc = HS_WARP_FOLD(a0, fx, op);
         }
         if (valid) y[r] = acc;
     }
@@ -200,23 +192,21 @@ __global__ void fill_kernel(T* __restrict__ a, int64_t n, T value) {
 }
 
 // Power iteration step (chebyshev.jl:46-51): w = l1inv .* (A v); partial sum
-// of w.^2 per block (grid <= partials capacity).
-template <int BR>
-__global__ void __launch_bounds__(BR, 1024 / BR) power_spmv_kernel(int32_t n, const int32_t* __restrict__ rp,
-                                                                 const int32_t* __restrict__ ci,
-                                                                 const double* __restrict__ v,
-                                                                 const double* __restrict__ vin,
-                                                                 const double* __restrict__ l1inv,
-                                                                 double* __restrict__ w,
-                                                                 double* __restrict__ partials,
-                                                                 const int* __restrict__ stop) {
+// of w.^2 per CTA (grid <= partials capacity).
+__global__ void __launch_bounds__(kThreads) power_spmv_kernel(int32_t n, const int32_t* __restrict__ rp,
+                                                              const int32_t* __restrict__ ci,
+                                                              const double* __restrict__ v,
+                                                              const double* __restrict__ vin,
+                                                              const double* __restrict__ l1inv,
+                                                              double* __restrict__ w, double* __restrict__ partials,
+                                                              const int* __restrict__ stop) {
     if (*stop) return;
-    HS_CS_SHARED(double, BR);
+    HS_WARP_SHARED(double);
     auto fx = [&](int32_t j) { return __ldg(vin + j); };
     double ss = 0.0;
-    HS_CS_ROWS_LOOP(BR) {
-        const int64_t r = row0 + threadIdx.x;
-        const double acc = HS_CS_FOLD(double, BR)(sh, n, rp, ci, v, row0, 0.0, fx, AddOp<double>());
+    HS_WARP_ROWS_LOOP {
+        const int64_t r = row0 + (threadIdx.x & 31);
+        const double acc = HS_WARP_FOLD(0.0, fx, AddOp<double>());
         if (r < n) {
             const double wi = __dmul_rn(acc, l1inv[r]);
             w[r] = wi;
@@ -250,18 +240,16 @@ __global__ void power_normalize_kernel(int32_t n, const double* __restrict__ w, 
 }
 
 // Lanczos operator w = dm .* (A (dm .* v)), dm = sqrt(l1inv).
-template <int BR>
-__global__ void __launch_bounds__(BR, 1024 / BR) lanczos_op_kernel(int32_t n, const int32_t* __restrict__ rp,
-                                                                 const int32_t* __restrict__ ci,
-                                                                 const double* __restrict__ v,
-                                                                 const double* __restrict__ vin,
-                                                                 const double* __restrict__ dm,
-                                                                 double* __restrict__ w) {
-    HS_CS_SHARED(double, BR);
+__global__ void __launch_bounds__(kThreads) lanczos_op_kernel(int32_t n, const int32_t* __restrict__ rp,
+                                                              const int32_t* __restrict__ ci,
+                                                              const double* __restrict__ v,
+                                                              const double* __restrict__ vin,
+                                                              const double* __restrict__ dm, double* __restrict__ w) {
+    HS_WARP_SHARED(double);
     auto fx = [&](int32_t j) { return __dmul_rn(__ldg(dm + j), __ldg(vin + j)); };
-    HS_CS_ROWS_LOOP(BR) {
-        const int64_t r = row0 + threadIdx.x;
-        const double acc = HS_CS_FOLD(double, BR)(sh, n, rp, ci, v, row0, 0.0, fx, AddOp<double>());
+    HS_WARP_ROWS_LOOP {
+        const int64_t r = row0 + (threadIdx.x & 31);
+        const double acc = HS_WARP_FOLD(0.0, fx, AddOp<double>());
         if (r < n) w[r] = __dmul_rn(dm[r], acc);
     }
 }
@@ -284,17 +272,16 @@ __global__ void sqrt_kernel(int32_t n, const double* __restrict__ a, double* __r
 
 // ---- Chebyshev 4th kind ----------------------------------------------------
 // r = b - A x (chebyshev.jl:165-167), z = 0 (:170)
-template <typename T, int BR>
-__global__ void __launch_bounds__(BR, 1024 / BR) cheb4_init_kernel(int32_t n, const int32_t* __restrict__ rp,
-                                                                 const int32_t* __restrict__ ci,
-                                                                 const T* __restrict__ v, const T* __restrict__ x,
-                                                                 const T* __restrict__ b, T* __restrict__ r,
-                                                                 T* __restrict__ z) {
-    HS_CS_SHARED(T, BR);
+template <typename T>
+__global__ void __launch_bounds__(kThreads) cheb4_init_kernel(int32_t n, const int32_t* __restrict__ rp,
+                                                              const int32_t* __restrict__ ci, const T* __restrict__ v,
+                                                              const T* __restrict__ x, const T* __restrict__ b,
+                                                              T* __restrict__ r, T* __restrict__ z) {
+    HS_WARP_SHARED(T);
     auto fx = [&](int32_t j) { return __ldg(x + j); };
-    HS_CS_ROWS_LOOP(BR) {
-        const int64_t i = row0 + threadIdx.x;
-        const T ax = HS_CS_FOLD(T, BR)(sh, n, rp, ci, v, row0, T(0), fx, AddOp<T>());
+    HS_WARP_ROWS_LOOP {
+        const int64_t i = row0 + (threadIdx.x & 31);
+        const T ax = HS_WARP_FOLD(T(0), fx, AddOp<T>());
         if (i < n) {
             r[i] = sub_rn(b[i], ax);
             z[i] = T(0);
@@ -314,21 +301,21 @@ __global__ void cheb4_init_zero_kernel(int32_t n, const IO* __restrict__ b, T* _
 }
 
 // One fused step (chebyshev.jl:176-179 with kernel :132-139).
-template <typename T, int BR>
-__global__ void __launch_bounds__(BR, 1024 / BR) cheb4_step_kernel(int32_t n, const int32_t* __restrict__ rp,
-                                                                 const int32_t* __restrict__ ci,
-                                                                 const T* __restrict__ v, const T* __restrict__ l1inv,
-                                                                 T ak, T bk, const T* __restrict__ z_old,
-                                                                 const T* __restrict__ r_old, T* __restrict__ z_new,
-                                                                 T* __restrict__ r_new, T* __restrict__ x) {
-    HS_CS_SHARED(T, BR);
+template <typename T>
+__global__ void __launch_bounds__(kThreads) cheb4_step_kernel(int32_t n, const int32_t* __restrict__ rp,
+                                                              const int32_t* __restrict__ ci, const T* __restrict__ v,
+                                                              const T* __restrict__ l1inv, T ak, T bk,
+                                                              const T* __restrict__ z_old, const T* __restrict__ r_old,
+                                                              T* __restrict__ z_new, T* __restrict__ r_new,
+                                                              T* __restrict__ x) {
+    HS_WARP_SHARED(T);
     auto zk = [&](int32_t j) {
         return add_rn(mul_rn(ak, __ldg(z_old + j)), mul_rn(mul_rn(bk, __ldg(l1inv + j)), __ldg(r_old + j)));
     };
-    HS_CS_ROWS_LOOP(BR) {
-        const int64_t i = row0 + threadIdx.x;
+    HS_WARP_ROWS_LOOP {
+        const int64_t i = row0 + (threadIdx.x & 31);
         const bool valid = i < n;
-        const T acc = HS_CS_FOLD(T, BR)(sh, n, rp, ci, v, row0, valid ? r_old[i] : T(0), zk, SubOp<T>());
+        const T acc = HS_WARP_FOLD(valid ? r_old[i] : T(0), zk, SubOp<T>());
         if (valid) {
             const T zi = zk((int32_t)i);
             z_new[i] = zi;
@@ -340,18 +327,17 @@ __global__ void __launch_bounds__(BR, 1024 / BR) cheb4_step_kernel(int32_t n, co
 
 // ---- Chebyshev 1st kind ----------------------------------------------------
 // tmp = A x; r = (l1inv (b - tmp)) inv_rho; z = c0 r   (chebyshev.jl:287-293, :237-244)
-template <typename T, int BR>
-__global__ void __launch_bounds__(BR, 1024 / BR) cheb1_init_kernel(int32_t n, const int32_t* __restrict__ rp,
-                                                                 const int32_t* __restrict__ ci,
-                                                                 const T* __restrict__ v, const T* __restrict__ x,
-                                                                 const T* __restrict__ b, const T* __restrict__ l1inv,
-                                                                 T inv_rho, T c0, T* __restrict__ r,
-                                                                 T* __restrict__ z) {
-    HS_CS_SHARED(T, BR);
+template <typename T>
+__global__ void __launch_bounds__(kThreads) cheb1_init_kernel(int32_t n, const int32_t* __restrict__ rp,
+                                                              const int32_t* __restrict__ ci, const T* __restrict__ v,
+                                                              const T* __restrict__ x, const T* __restrict__ b,
+                                                              const T* __restrict__ l1inv, T inv_rho, T c0,
+                                                              T* __restrict__ r, T* __restrict__ z) {
+    HS_WARP_SHARED(T);
     auto fx = [&](int32_t j) { return __ldg(x + j); };
-    HS_CS_ROWS_LOOP(BR) {
-        const int64_t i = row0 + threadIdx.x;
-        const T tmp = HS_CS_FOLD(T, BR)(sh, n, rp, ci, v, row0, T(0), fx, AddOp<T>());
+    HS_WARP_ROWS_LOOP {
+        const int64_t i = row0 + (threadIdx.x & 31);
+        const T tmp = HS_WARP_FOLD(T(0), fx, AddOp<T>());
         if (i < n) {
             const T ri = mul_rn(mul_rn(l1inv[i], sub_rn(b[i], tmp)), inv_rho);
             r[i] = ri;
@@ -372,18 +358,17 @@ __global__ void cheb1_init_zero_kernel(int32_t n, const IO* __restrict__ b, cons
 }
 
 // x += z_old; r -= (l1inv (A z_old)) inv_rho; z_new = c1 z_old + c2 r   (:300-316)
-template <typename T, int BR>
-__global__ void __launch_bounds__(BR, 1024 / BR) cheb1_step_kernel(int32_t n, const int32_t* __restrict__ rp,
-                                                                 const int32_t* __restrict__ ci,
-                                                                 const T* __restrict__ v, const T* __restrict__ l1inv,
-                                                                 T inv_rho, T c1, T c2, const T* __restrict__ z_old,
-                                                                 T* __restrict__ z_new, T* __restrict__ r,
-                                                                 T* __restrict__ x) {
-    HS_CS_SHARED(T, BR);
+template <typename T>
+__global__ void __launch_bounds__(kThreads) cheb1_step_kernel(int32_t n, const int32_t* __restrict__ rp,
+                                                              const int32_t* __restrict__ ci, const T* __restrict__ v,
+                                                              const T* __restrict__ l1inv, T inv_rho, T c1, T c2,
+                                                              const T* __restrict__ z_old, T* __restrict__ z_new,
+                                                              T* __restrict__ r, T* __restrict__ x) {
+    HS_WARP_SHARED(T);
     auto fz = [&](int32_t j) { return __ldg(z_old + j); };
-    HS_CS_ROWS_LOOP(BR) {
-        const int64_t i = row0 + threadIdx.x;
-        const T tmp = HS_CS_FOLD(T, BR)(sh, n, rp, ci, v, row0, T(0), fz, AddOp<T>());
+    HS_WARP_ROWS_LOOP {
+        const int64_t i = row0 + (threadIdx.x & 31);
+        const T tmp = HS_WARP_FOLD(T(0), fz, AddOp<T>());
         if (i < n) {
             const T zo = z_old[i];
             x[i] = add_rn(x[i], zo);
@@ -400,10 +385,10 @@ __global__ void axpy_one_kernel(int32_t n, T* __restrict__ x, const T* __restric
         x[i] = add_rn(x[i], z[i]);
 }
 
-// One block per BR rows: the block scheduler streams them through the SMs,
-// each block's phases overlapping those of the other resident blocks.
-inline int grid_rows(int64_t n, int br) {
-    const int64_t blocks = (n + br - 1) / br;
+// One CTA per kThreads rows (a warp per 32): the block scheduler streams them
+// through the SMs.
+inline int grid_rows(int64_t n) {
+    const int64_t blocks = (n + kThreads - 1) / kThreads;
     return (int)std::max<int64_t>(1, std::min<int64_t>(blocks, INT32_MAX));
 }
 inline int grid_elems(int64_t n) {
@@ -411,26 +396,18 @@ inline int grid_elems(int64_t n) {
     return (int)std::max<int64_t>(1, std::min<int64_t>(b, (int64_t)hs::num_sms() * 16));
 }
 
-// L = rows per block (= threads per block) of the CSR-stream kernels.
-#define HS_LPR_DISPATCH(lpr, CALL)                        \
-    switch (lpr) {                                        \
-        case 256: { constexpr int L = 256; CALL; } break; \
-        default: { constexpr int L = 128; CALL; } break;  \
-    }
-
 template <typename T>
 int spmv_t(const hs_matrix* M, const void* x, void* y, double alpha, double beta, cudaStream_t st) {
-    const int g = grid_rows(M->n, M->lpr);
+    const int g = grid_rows(M->n);
     const T* v = static_cast<const T*>(M->v);
     const T* xx = static_cast<const T*>(x);
     T* yy = static_cast<T*>(y);
     if (alpha == 1.0 && beta == 0.0) {
-        HS_LPR_DISPATCH(M->lpr, (spmv_kernel<T, L, 0><<<g, L, 0, st>>>(M->n, M->rp, M->ci, v, xx, yy, T(1), T(0))));
+        spmv_kernel<T, 0><<<g, kThreads, 0, st>>>(M->n, M->rp, M->ci, v, xx, yy, T(1), T(0));
     } else if (alpha == -1.0 && beta == 1.0) {
-        HS_LPR_DISPATCH(M->lpr, (spmv_kernel<T, L, 1><<<g, L, 0, st>>>(M->n, M->rp, M->ci, v, xx, yy, T(-1), T(1))));
+        spmv_kernel<T, 1><<<g, kThreads, 0, st>>>(M->n, M->rp, M->ci, v, xx, yy, T(-1), T(1));
     } else {
-        HS_LPR_DISPATCH(M->lpr,
-                        (spmv_kernel<T, L, 2><<<g, L, 0, st>>>(M->n, M->rp, M->ci, v, xx, yy, (T)alpha, (T)beta)));
+        spmv_kernel<T, 2><<<g, kThreads, 0, st>>>(M->n, M->rp, M->ci, v, xx, yy, (T)alpha, (T)beta);
     }
     HS_LAUNCH_CHECK("spmv_kernel");
     return HS_OK;
@@ -446,7 +423,6 @@ int matrix_spmv(const hs_matrix* M, const void* x, void* y, double alpha, double
 }
 int matrix_n(const hs_matrix* M) { return M->n; }
 int64_t matrix_nnz(const hs_matrix* M) { return M->nnz; }
-int matrix_block_rows(const hs_matrix* M) { return M->lpr; }
 void matrix_arrays(const hs_matrix* M, const int32_t** rp, const int32_t** ci, const void** v, int* dtype) {
     *rp = M->rp;
     *ci = M->ci;
@@ -469,11 +445,16 @@ struct hs_cheb_s {
 
 namespace hsm {
 
-void destroy_matrix(hs_matrix* M) {
+void destroy_matrix(hs_matrix* M, cudaStream_t free_stream = nullptr) {
     if (!M) return;
-    cudaFree(M->rp);
-    cudaFree(M->ci);
-    cudaFree(M->v);
+    void* ptrs[] = {M->rp, M->ci, M->v};
+    for (void* q : ptrs) {
+        if (!q) continue;
+        if (M->stream_ordered)
+            cudaFreeAsync(q, free_stream ? free_stream : M->alloc_stream);
+        else
+            cudaFree(q);
+    }
     delete M;
 }
 
@@ -538,7 +519,7 @@ int cheb_smooth_t(hs_cheb* S, T* x, const void* b, int io, bool x_is_zero, cudaS
     const T* l1 = static_cast<const T*>(S->l1inv);
     T* r[2] = {static_cast<T*>(S->w[0]), static_cast<T*>(S->w[1])};
     T* z[2] = {static_cast<T*>(S->w[2]), static_cast<T*>(S->w[3])};
-    const int g = grid_rows(n, M->lpr), ge = grid_elems(n);
+    const int g = grid_rows(n), ge = grid_elems(n);
     if (S->kind == 4) {
         if (x_is_zero) {
             if (io == HS_F64)
@@ -547,16 +528,16 @@ int cheb_smooth_t(hs_cheb* S, T* x, const void* b, int io, bool x_is_zero, cudaS
                 cheb4_init_zero_kernel<T, float><<<ge, kThreads, 0, st>>>(n, static_cast<const float*>(b), r[0], z[0], x);
             HS_LAUNCH_CHECK("cheb4_init_zero_kernel");
         } else {
-            HS_LPR_DISPATCH(M->lpr, (cheb4_init_kernel<T, L><<<g, L, 0, st>>>(
-                                        n, M->rp, M->ci, v, x, static_cast<const T*>(b), r[0], z[0])));
+            cheb4_init_kernel<T><<<g, kThreads, 0, st>>>(
+                                        n, M->rp, M->ci, v, x, static_cast<const T*>(b), r[0], z[0]);
             HS_LAUNCH_CHECK("cheb4_init_kernel");
         }
         int cur = 0;
         for (int k = 1; k <= S->degree; ++k) {
             const T ak = (T)((double)(2 * k - 3) / (double)(2 * k + 1));
             const T bk = (T)((double)(8 * k - 4) / ((double)(2 * k + 1) * S->rho));
-            HS_LPR_DISPATCH(M->lpr, (cheb4_step_kernel<T, L><<<g, L, 0, st>>>(
-                                        n, M->rp, M->ci, v, l1, ak, bk, z[cur], r[cur], z[cur ^ 1], r[cur ^ 1], x)));
+            cheb4_step_kernel<T><<<g, kThreads, 0, st>>>(
+                                        n, M->rp, M->ci, v, l1, ak, bk, z[cur], r[cur], z[cur ^ 1], r[cur ^ 1], x);
             HS_LAUNCH_CHECK("cheb4_step_kernel");
             cur ^= 1;
         }
@@ -575,8 +556,8 @@ int cheb_smooth_t(hs_cheb* S, T* x, const void* b, int io, bool x_is_zero, cudaS
                                                                       r[0], z[0], x);
         HS_LAUNCH_CHECK("cheb1_init_zero_kernel");
     } else {
-        HS_LPR_DISPATCH(M->lpr, (cheb1_init_kernel<T, L><<<g, L, 0, st>>>(
-                                    n, M->rp, M->ci, v, x, static_cast<const T*>(b), l1, inv_rho, c0, r[0], z[0])));
+        cheb1_init_kernel<T><<<g, kThreads, 0, st>>>(
+                                    n, M->rp, M->ci, v, x, static_cast<const T*>(b), l1, inv_rho, c0, r[0], z[0]);
         HS_LAUNCH_CHECK("cheb1_init_kernel");
     }
     double rho_s = (1.0 - a) / (1.0 + a);
@@ -586,8 +567,8 @@ int cheb_smooth_t(hs_cheb* S, T* x, const void* b, int io, bool x_is_zero, cudaS
             const double rho_new = 1.0 / (2.0 * (1.0 + a) / (1.0 - a) - rho_s);
             const T c1 = (T)(rho_new * rho_s);
             const T c2 = (T)(4.0 * rho_new / (1.0 - a));
-            HS_LPR_DISPATCH(M->lpr, (cheb1_step_kernel<T, L><<<g, L, 0, st>>>(
-                                        n, M->rp, M->ci, v, l1, inv_rho, c1, c2, z[cur], z[cur ^ 1], r[0], x)));
+            cheb1_step_kernel<T><<<g, kThreads, 0, st>>>(
+                                        n, M->rp, M->ci, v, l1, inv_rho, c1, c2, z[cur], z[cur ^ 1], r[0], x);
             HS_LAUNCH_CHECK("cheb1_step_kernel");
             cur ^= 1;
             rho_s = rho_new;
@@ -601,10 +582,8 @@ int cheb_smooth_t(hs_cheb* S, T* x, const void* b, int io, bool x_is_zero, cudaS
 
 }  // namespace hsm
 
-
-extern "C" {
-
-int hs_matrix_create(const hs_sparse* A, int32_t dtype, void* stream, hs_matrix** out) {
+namespace {
+int matrix_create_impl(const hs_sparse* A, int32_t dtype, void* stream, hs_matrix** out, bool stream_ordered) {
     if (!out) return hs::set_error(HS_ERR_ARG, "out is NULL");
     *out = nullptr;
     int rc = hsm::validate(A);
@@ -612,15 +591,19 @@ int hs_matrix_create(const hs_sparse* A, int32_t dtype, void* stream, hs_matrix*
     if (dtype != HS_F64 && dtype != HS_F32) return hs::set_error(HS_ERR_ARG, "unknown dtype");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     hs_matrix* M = new hs_matrix();
+    M->stream_ordered = stream_ordered;
+    M->alloc_stream = st;
     M->n = A->n;
     M->nnz = A->nnz;
     M->dtype = dtype;
-    M->lpr = hsm::pick_lpr(M->nnz, M->n);
     const size_t es = hsm::dsize(dtype);
     cudaError_t e;
-    if ((e = cudaMalloc(&M->rp, sizeof(int32_t) * (M->n + 1))) != cudaSuccess ||
-        (e = cudaMalloc(&M->ci, sizeof(int32_t) * std::max<int64_t>(1, M->nnz))) != cudaSuccess ||
-        (e = cudaMalloc(&M->v, es * std::max<int64_t>(1, M->nnz))) != cudaSuccess) {
+    auto alloc = [&](void** p, size_t bytes) {
+        return stream_ordered ? cudaMallocAsync(p, bytes, st) : cudaMalloc(p, bytes);
+    };
+    if ((e = alloc((void**)&M->rp, sizeof(int32_t) * (M->n + 1))) != cudaSuccess ||
+        (e = alloc((void**)&M->ci, sizeof(int32_t) * std::max<int64_t>(1, M->nnz))) != cudaSuccess ||
+        (e = alloc(&M->v, es * std::max<int64_t>(1, M->nnz))) != cudaSuccess) {
         hsm::destroy_matrix(M);
         return hs::cuda_error(e, "cudaMalloc (matrix)");
     }
@@ -637,6 +620,23 @@ int hs_matrix_create(const hs_sparse* A, int32_t dtype, void* stream, hs_matrix*
     }
     *out = M;
     return HS_OK;
+}
+
+}  // namespace
+
+namespace hs {
+// Matrix whose buffers come from the stream-ordered pool on `st`, released
+// with matrix_destroy_async (no device synchronisation).
+int matrix_create_async(const hs_sparse* A, int32_t dtype, cudaStream_t st, hs_matrix** out) {
+    return matrix_create_impl(A, dtype, st, out, true);
+}
+void matrix_destroy_async(hs_matrix* M, cudaStream_t st) { hsm::destroy_matrix(M, st); }
+}  // namespace hs
+
+extern "C" {
+
+int hs_matrix_create(const hs_sparse* A, int32_t dtype, void* stream, hs_matrix** out) {
+    return matrix_create_impl(A, dtype, stream, out, false);
 }
 
 int hs_matrix_spmv(hs_matrix* A, const void* x, void* y, double alpha, double beta, void* stream) {
@@ -698,11 +698,11 @@ int hs_cheb_create(const hs_sparse* A, int32_t kind, int32_t degree, int32_t eig
     cudaMemsetAsync(stop, 0, sizeof(int), st);
     // The power-iteration SpMV writes one partial per block: keep its grid within
     // the partials buffer (kRedMaxBlocks); the kernel strides over row blocks.
-    const int gr = std::min(hsm::grid_rows(n, M64->lpr), hsdev::kRedMaxBlocks);
+    const int gr = std::min(hsm::grid_rows(n), hsdev::kRedMaxBlocks);
     for (int it = 0; it < 50; ++it) {
-        HS_LPR_DISPATCH(M64->lpr, (hsm::power_spmv_kernel<L><<<gr, L, 0, st>>>(
+        hsm::power_spmv_kernel<<<gr, hsm::kThreads, 0, st>>>(
                                       n, M64->rp, M64->ci, static_cast<const double*>(M64->v), vv, l1inv, ww, partials,
-                                      stop)));
+                                      stop);
         hsm::power_finalize_kernel<<<1, hsdev::kRedThreads, 0, st>>>(partials, gr, rho_d, stop);
         hsm::power_normalize_kernel<<<ge, hsm::kThreads, 0, st>>>(n, ww, rho_d, vv, stop);
         hs::count_launch(3);
@@ -725,8 +725,8 @@ int hs_cheb_create(const hs_sparse* A, int32_t kind, int32_t degree, int32_t eig
         double beta = 0.0;
         const int rb = hsdev::red_blocks(n);
         for (int j = 0; j < 40 && j < n; ++j) {
-            HS_LPR_DISPATCH(M64->lpr, (hsm::lanczos_op_kernel<L><<<gr, L, 0, st>>>(
-                                          n, M64->rp, M64->ci, static_cast<const double*>(M64->v), vv, dm, ww)));
+            hsm::lanczos_op_kernel<<<gr, hsm::kThreads, 0, st>>>(
+                                          n, M64->rp, M64->ci, static_cast<const double*>(M64->v), vv, dm, ww);
             hsdev::dot_partials_kernel<double, double><<<rb, hsdev::kRedThreads, 0, st>>>(ww, vv, n, partials);
             hsdev::finalize_sum_kernel<<<1, hsdev::kRedThreads, 0, st>>>(partials, rb, sc, 0);
             double alpha = 0;
@@ -905,7 +905,6 @@ extern "C" int hs_cheb_smooth_noalloc(int32_t n, int64_t nnz, const int32_t* rp,
     M.rp = const_cast<int32_t*>(rp);
     M.ci = const_cast<int32_t*>(ci);
     M.v = const_cast<double*>(v);
-    M.lpr = hsm::pick_lpr(nnz, n);
     hs_cheb S;
     S.n = n;
     S.kind = kind;

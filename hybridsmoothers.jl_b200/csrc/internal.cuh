@@ -8,7 +8,6 @@ namespace hs {
 int matrix_spmv(const hs_matrix* M, const void* x, void* y, double alpha, double beta, cudaStream_t st);
 int matrix_n(const hs_matrix* M);
 int64_t matrix_nnz(const hs_matrix* M);
-int matrix_block_rows(const hs_matrix* M);   // rows per CSR-stream block (128 or 256)
 void matrix_arrays(const hs_matrix* M, const int32_t** rp, const int32_t** ci, const void** v, int* dtype);
 int cheb_apply(hs_cheb* S, const void* r, void* z, int io, cudaStream_t st);
 // Uploads a validated host matrix as device CSR in `dtype` (a CSC input is
@@ -29,5 +28,10 @@ int l1gs_view_of(const hs_l1gs* P, L1gsView* v);
 // call only; for a symmetric matrix its rows are the CSC columns isSymA reads).
 int l1gs_create_from_matrix(const hs_matrix* M, int32_t partsize, double eta, int32_t sweep, int32_t smoother_dtype,
                             cudaStream_t st, hs_l1gs** out);
+// Its buffers are stream-ordered: free them in order on `st` (no device sync).
+void l1gs_destroy_async(hs_l1gs* P, cudaStream_t st);
+// Device CSR matrix with stream-ordered buffers (allocated on `st`).
+int matrix_create_async(const hs_sparse* A, int32_t dtype, cudaStream_t st, hs_matrix** out);
+void matrix_destroy_async(hs_matrix* M, cudaStream_t st);
 
 }  // namespace hs

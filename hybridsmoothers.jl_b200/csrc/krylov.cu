@@ -125,21 +125,20 @@ __global__ void pcg_init_scalars(const double* __restrict__ partials_bb, const d
 }
 
 // q = A p (storage-order rows, bitwise mul!) and compensated partials of p.q.
-template <int BR>
-__global__ void __launch_bounds__(BR, 1024 / BR) pcg_spmv_dot(int32_t n, const int32_t* __restrict__ rp,
-                                                            const int32_t* __restrict__ ci,
-                                                            const double* __restrict__ v,
-                                                            const double* __restrict__ p, double* __restrict__ q,
-                                                            const PcgScalars* __restrict__ s,
-                                                            double* __restrict__ partials) {
-    __shared__ hsdev::CsrStream<double, BR, hsdev::stream_cap<BR>()> sh;
+// A warp owns 32 rows at a time (warp CSR-stream), warps stride over the matrix.
+__global__ void __launch_bounds__(kT, 5) pcg_spmv_dot(int32_t n, const int32_t* __restrict__ rp,
+                                                  const int32_t* __restrict__ ci, const double* __restrict__ v,
+                                                  const double* __restrict__ p, double* __restrict__ q,
+                                                  const PcgScalars* __restrict__ s, double* __restrict__ partials) {
+    __shared__ double wbuf[kT / 32][hsdev::kWarpCap];
     DD part{0.0, 0.0};
     if (!s->done) {
+        const int warp = threadIdx.x >> 5;
         auto fp = [&](int32_t j) { return __ldg(p + j); };
-        for (int64_t row0 = (int64_t)blockIdx.x * BR; row0 < n; row0 += (int64_t)gridDim.x * BR) {
-            const double acc = hsdev::csr_stream_fold<double, BR, hsdev::stream_cap<BR>()>(
-                sh, n, rp, ci, v, row0, 0.0, fp, hsdev::AddOp<double>());
-            const int64_t r = row0 + threadIdx.x;
+        for (int64_t row0 = ((int64_t)blockIdx.x * (kT / 32) + warp) * 32; row0 < n;
+             row0 += (int64_t)gridDim.x * kT) {
+            const double acc = hsdev::csr_warp_fold(wbuf[warp], n, rp, ci, v, row0, 0.0, fp, hsdev::AddOp<double>());
+            const int64_t r = row0 + (threadIdx.x & 31);
             if (r < n) {
                 q[r] = acc;
                 hsdev::dd_add_prod(part, p[r], acc);
@@ -462,17 +461,12 @@ int hs_pcg_solve(hs_matrix* A, int32_t prec_type, void* prec, const double* b, d
     const void* Av = nullptr;
     int Adt = 0;
     hs::matrix_arrays(A, &Arp, &Aci, &Av, &Adt);
-    const int br = hs::matrix_block_rows(A);
-    const int nq = (int)std::max<int64_t>(
-        1, std::min<int64_t>((n + br - 1) / br, (int64_t)hsdev::kRedMaxBlocks));
+    const int nq = (int)std::max<int64_t>(1, std::min<int64_t>((n + kT - 1) / kT, (int64_t)hsdev::kRedMaxBlocks));
     auto iteration = [&](cudaStream_t cs) -> int {
         int r2;
         int npq = nb;
-        if (Adt == HS_F64 && br == 256) {
-            pcg_spmv_dot<256><<<nq, 256, 0, cs>>>((int32_t)n, Arp, Aci, (const double*)Av, p, q, s, pa);
-            npq = nq;
-        } else if (Adt == HS_F64 && br == 128) {
-            pcg_spmv_dot<128><<<nq, 128, 0, cs>>>((int32_t)n, Arp, Aci, (const double*)Av, p, q, s, pa);
+        if (Adt == HS_F64) {
+            pcg_spmv_dot<<<nq, kT, 0, cs>>>((int32_t)n, Arp, Aci, (const double*)Av, p, q, s, pa);
             npq = nq;
         } else {
             if ((r2 = hs::matrix_spmv(A, p, q, 1.0, 0.0, cs))) return r2;

@@ -715,23 +715,31 @@ struct hs_l1gs_s {
     int launch_key = -1, launch_grid = 1;
     const void* launch_kernel = nullptr;
     int32_t* err_word = nullptr;
+    cudaStream_t alloc_stream = nullptr;   // set: buffers are stream-ordered (cudaMallocAsync)
+    bool stream_ordered = false;
 };
 
 namespace {
 
 template <typename T>
 int dmalloc(hs_l1gs* P, T** p, size_t bytes) {
-    cudaError_t e = cudaMalloc((void**)p, bytes ? bytes : 1);
+    cudaError_t e = P->stream_ordered ? cudaMallocAsync((void**)p, bytes ? bytes : 1, P->alloc_stream)
+                                      : cudaMalloc((void**)p, bytes ? bytes : 1);
     if (e != cudaSuccess) return hs::cuda_error(e, "cudaMalloc");
     P->bytes += (int64_t)bytes;
     return HS_OK;
 }
 
-void release(hs_l1gs* P) {
+void release(hs_l1gs* P, cudaStream_t free_stream = nullptr) {
     if (!P) return;
     void* ptrs[] = {P->D, P->Di, P->SLi, P->SUi, P->rp, P->ci, P->vs, P->dev_x, P->dev_y};
     for (void* q : ptrs)
-        if (q) cudaFree(q);
+        if (q) {
+            if (P->stream_ordered)
+                cudaFreeAsync(q, free_stream ? free_stream : P->alloc_stream);
+            else
+                cudaFree(q);
+        }
     delete P;
 }
 
@@ -1134,7 +1142,7 @@ int l1gs_view_of(const hs_l1gs* P, L1gsView* v) {
 namespace {
 int l1gs_create_impl(const hs_sparse* A, bool on_device, int32_t partsize, int32_t is_sym, double eta, int32_t sweep,
                      int32_t cache, int32_t smoother_dtype, int32_t threads, int32_t blocks, void* stream,
-                     hs_l1gs** out) {
+                     hs_l1gs** out, bool stream_ordered = false) {
     if (!out) return hs::set_error(HS_ERR_ARG, "out is NULL");
     *out = nullptr;
     if (partsize <= 0) return hs::set_error(HS_ERR_ARG, "partsize must be greater than 0");
@@ -1153,6 +1161,8 @@ int l1gs_create_impl(const hs_sparse* A, bool on_device, int32_t partsize, int32
     if (partsize > 65535) return hs::set_error(HS_ERR_UNSUPPORTED, "partsize above 65535");
 
     hs_l1gs* P = new hs_l1gs();
+    P->stream_ordered = stream_ordered;
+    P->alloc_stream = static_cast<cudaStream_t>(stream);
     P->n = A->n;
     P->ps = partsize;
     P->nparts = (int32_t)(((int64_t)A->n + partsize - 1) / partsize);
@@ -1242,8 +1252,11 @@ int l1gs_create_from_matrix(const hs_matrix* M, int32_t partsize, double eta, in
     d.format = HS_CSR;
     d.dtype = dt;
     d.val = v;
-    return l1gs_create_impl(&d, true, partsize, 1, eta, sweep, HS_CACHE_PACKED, smoother_dtype, 256, 148, st, out);
+    return l1gs_create_impl(&d, true, partsize, 1, eta, sweep, HS_CACHE_PACKED, smoother_dtype, 256, 148, st, out,
+                            true);
 }
+
+void l1gs_destroy_async(hs_l1gs* P, cudaStream_t st) { release(P, st); }
 }  // namespace hs
 
 extern "C" {

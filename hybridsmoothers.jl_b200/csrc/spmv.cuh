@@ -19,73 +19,63 @@ struct SubOp {
 };
 
 // ---------------------------------------------------------------------------
-// Block CSR-stream: a block of BR threads owns rows [row0, row0 + BR).  The
-// products a_q * f(col_q) of all its entries are formed cooperatively (one
-// entry per thread per pass: coalesced loads of ci/v and every gather in
-// flight together) into shared memory, then thread t folds its row's products
-// in storage order with `op` starting from `acc0`.  Bitwise the same sums as
-// the sequential row loop.  When the block's entries exceed CAP, the threads
-// fall back to folding straight from global memory (same arithmetic).
+// Warp CSR-stream: a warp owns 32 consecutive rows [row0, row0 + 32).  Its
+// entries are processed in windows of WCAP: the products a_q * f(col_q) of a
+// window are formed by all 32 lanes (coalesced ci/v loads, KU entries per
+// lane issued before their gathers) into the warp's private shared buffer,
+// and lane l then folds the part of row row0+l that lies in the window, in
+// storage order, continuing from the previous window.  Only __syncwarp
+// between phases: warps never wait for each other, so each SM keeps many
+// warps' loads in flight.  Bitwise the sequential row sums, any row length.
+// Every lane of the warp must call it; rows >= n get acc0 back.
 // ---------------------------------------------------------------------------
-template <typename T, int BR, int CAP>
-struct CsrStream {
-    T prod[CAP];
-    int32_t rs[BR + 1];
-};
+constexpr int kWarpCap = 256;   // products per window (2 KB of FP64 per warp)
+constexpr int kWarpKU = 4;      // entries per lane per load round
 
-// Staged products per block: 8 per row at 256 rows, 32 per row at 128 rows.
-template <int BR>
-constexpr int stream_cap() { return BR >= 256 ? 2048 : 4096; }
-
-// Entries per thread whose loads are issued before any of them is used.
-constexpr int kU = 8;
-
-// Returns (on every thread) the folded value of this thread's row, or acc0 for
-// rows >= n.  `sh` is the block's shared staging area.  The product phase
-// issues the loads of kU entries per thread (entry loads, then the dependent
-// gathers) before using any of them, so a block keeps kU x BR entries in
-// flight instead of one.
-template <typename T, int BR, int CAP, typename F, typename Op>
-__device__ __forceinline__ T csr_stream_fold(CsrStream<T, BR, CAP>& sh, int32_t n, const int32_t* __restrict__ rp,
-                                             const int32_t* __restrict__ ci, const T* __restrict__ v,
-                                             int64_t row0, T acc0, F f, Op op) {
-    const int t = threadIdx.x;
-    const int nrows = (int)min((int64_t)BR, (int64_t)n - row0);
-    __syncthreads();   // previous use of sh is finished
-    for (int i = t; i <= nrows; i += BR) sh.rs[i] = __ldg(rp + row0 + i);
-    __syncthreads();
-    const int32_t q0 = sh.rs[0];
-    const int32_t cnt = sh.rs[nrows] - q0;
+template <typename T, typename F, typename Op>
+__device__ __forceinline__ T csr_warp_fold(T* __restrict__ wbuf, int32_t n, const int32_t* __restrict__ rp,
+                                           const int32_t* __restrict__ ci, const T* __restrict__ v, int64_t row0,
+                                           T acc0, F f, Op op) {
+    const int lane = threadIdx.x & 31;
+    const int64_t r = row0 + lane;
+    const bool valid = r < n;
+    const int nrows = (int)min((int64_t)32, (int64_t)n - row0);
+    int32_t ra = 0, rb = 0;
+    if (valid) {
+        ra = __ldg(rp + r);
+        rb = __ldg(rp + r + 1);
+    }
+    const int32_t q0 = __shfl_sync(0xffffffffu, ra, 0);
+    const int32_t q1 = __shfl_sync(0xffffffffu, rb, nrows - 1);
     T acc = acc0;
-    if (cnt <= CAP) {
-        for (int32_t base = 0; base < cnt; base += kU * BR) {
-            int32_t c[kU];
-            T a[kU], b[kU];
+    for (int32_t base = q0; base < q1; base += kWarpCap) {
+        const int32_t cnt = min(kWarpCap, q1 - base);
+        for (int32_t k0 = 0; k0 < cnt; k0 += 32 * kWarpKU) {
+            int32_t c[kWarpKU];
+            T a[kWarpKU], b[kWarpKU];
 #pragma unroll
-            for (int k = 0; k < kU; ++k) {
-                const int32_t e = base + k * BR + t;
+            for (int k = 0; k < kWarpKU; ++k) {
+                const int32_t e = k0 + k * 32 + lane;
                 if (e < cnt) {
-                    c[k] = __ldg(ci + q0 + e);
-                    a[k] = __ldg(v + q0 + e);
+                    c[k] = __ldg(ci + base + e);
+                    a[k] = __ldg(v + base + e);
                 }
             }
 #pragma unroll
-            for (int k = 0; k < kU; ++k)
-                if (base + k * BR + t < cnt) b[k] = f(c[k]);
+            for (int k = 0; k < kWarpKU; ++k)
+                if (k0 + k * 32 + lane < cnt) b[k] = f(c[k]);
 #pragma unroll
-            for (int k = 0; k < kU; ++k) {
-                const int32_t e = base + k * BR + t;
-                if (e < cnt) sh.prod[e] = mul_rn(a[k], b[k]);
+            for (int k = 0; k < kWarpKU; ++k) {
+                const int32_t e = k0 + k * 32 + lane;
+                if (e < cnt) wbuf[e] = mul_rn(a[k], b[k]);
             }
         }
-        __syncthreads();
-        if (t < nrows) {
-            const int32_t a = sh.rs[t] - q0, b = sh.rs[t + 1] - q0;
-            for (int32_t e = a; e < b; ++e) acc = op(acc, sh.prod[e]);
+        __syncwarp();
+        if (valid) {
+            const int32_t lo = max(ra, base), hi = min(rb, base + cnt);
+            for (int32_t e = lo; e < hi; ++e) acc = op(acc, wbuf[e - base]);
         }
-    } else if (t < nrows) {
-        const int32_t a = sh.rs[t], b = sh.rs[t + 1];
-        for (int32_t q = a; q < b; ++q) acc = op(acc, mul_rn(__ldg(v + q), f(__ldg(ci + q))));
+        __syncwarp();
     }
     return acc;
 }
