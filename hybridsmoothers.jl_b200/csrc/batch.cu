@@ -9,9 +9,9 @@
 //   seg_alpha     alpha = rz / pq                            (one block per slot)
 //   seg_update    x += alpha p, r -= alpha q, partials of r.r
 //   seg_check     convergence test, iteration count
-//   l1gs_batched  z = M^-1 r, one launch per partsize class (FP32 smoother, FP64 in/out)
-//   seg_dot       partials of r.z
-//   seg_beta      beta = rz_new / rz
+//   l1gs_batched  z = M^-1 r and per-item partials of r.z, one launch per partsize class
+//                 (FP32 smoother, FP64 in/out)
+//   seg_beta      beta = rz_new / rz (r.z partials come from the L1GS apply)
 //   seg_p         p = z + beta p
 // The iteration is captured once as a CUDA graph per active set and replayed.
 // A slot's reductions always use the same blocks over its own rows and a
@@ -56,7 +56,7 @@ __device__ __forceinline__ void store_dd(double* partials, DD v) {
 
 // Per slot: its CTA range (for the per-slot reductions) and scalars.
 struct SlotDev {
-    int32_t n, blk0, nblk, pad;
+    int32_t n, blk0, nblk, item0, nitems, pad;
     Scalars* s;
 };
 
@@ -113,19 +113,22 @@ __global__ void __launch_bounds__(kT, 5) seg_spmv_dot(const BlockMap* __restrict
 
 // Sum of a slot's CTA partials (valid on thread 0).  A large slot has
 // thousands of CTAs: each thread loads 8 partials before adding any.
-__device__ __forceinline__ double slot_sum(const double* __restrict__ partials, const SlotDev& sd) {
+__device__ __forceinline__ double range_sum(const double* __restrict__ partials, int32_t first, int32_t count) {
     DD v{0.0, 0.0};
-    const double2* p2 = reinterpret_cast<const double2*>(partials) + sd.blk0;
-    for (int base = threadIdx.x; base < sd.nblk; base += 8 * blockDim.x) {
+    const double2* p2 = reinterpret_cast<const double2*>(partials) + first;
+    for (int base = threadIdx.x; base < count; base += 8 * blockDim.x) {
         double2 w[8];
 #pragma unroll
         for (int k = 0; k < 8; ++k)
-            if (base + k * (int)blockDim.x < sd.nblk) w[k] = p2[base + k * blockDim.x];
+            if (base + k * (int)blockDim.x < count) w[k] = p2[base + k * blockDim.x];
 #pragma unroll
         for (int k = 0; k < 8; ++k)
-            if (base + k * (int)blockDim.x < sd.nblk) v = hsdev::dd_add(v, DD{w[k].x, w[k].y});
+            if (base + k * (int)blockDim.x < count) v = hsdev::dd_add(v, DD{w[k].x, w[k].y});
     }
     return hsdev::dd_value(hsdev::block_dd(v));
+}
+__device__ __forceinline__ double slot_sum(const double* __restrict__ partials, const SlotDev& sd) {
+    return range_sum(partials, sd.blk0, sd.nblk);
 }
 
 __global__ void seg_alpha(const SlotDev* __restrict__ slots, const int32_t* __restrict__ active,
@@ -186,30 +189,12 @@ __global__ void seg_check(const SlotDev* __restrict__ slots, const int32_t* __re
     }
 }
 
-__global__ void __launch_bounds__(kT) seg_dot(const BlockMap* __restrict__ map, double* __restrict__ partials) {
-    const BlockMap m = map[blockIdx.x];
-    DD part{0.0, 0.0};
-    if (!m.s->done) {
-        double rv[kSub], zv[kSub];
-#pragma unroll
-        for (int k = 0; k < kSub; ++k) {
-            const int i = m.row0 + k * kRPB + threadIdx.x;
-            if (i < m.n) {
-                rv[k] = m.r[i];
-                zv[k] = m.z[i];
-            }
-        }
-#pragma unroll
-        for (int k = 0; k < kSub; ++k)
-            if (m.row0 + k * kRPB + (int)threadIdx.x < m.n) hsdev::dd_add_prod(part, rv[k], zv[k]);
-    }
-    store_dd(partials, part);
-}
-
+// r.z of the slot: the batched L1GS apply leaves one compensated partial per
+// work item (the slot's items are contiguous).
 __global__ void seg_beta(const SlotDev* __restrict__ slots, const int32_t* __restrict__ active,
-                         const double* __restrict__ partials) {
+                         const double* __restrict__ rz_part) {
     const SlotDev sd = slots[active[blockIdx.x]];
-    const double rz = slot_sum(partials, sd);
+    const double rz = range_sum(rz_part, sd.item0, sd.nitems);
     if (threadIdx.x == 0 && !sd.s->done) {
         sd.s->beta = __ddiv_rn(rz, sd.s->rz);
         sd.s->rz = rz;
@@ -290,7 +275,8 @@ __global__ void init_scalars(const double* __restrict__ pbb, const double* __res
 // are still fetched and applied until they leave the tables at the next rebuild.
 template <int PS, int E, int STAGES>
 __global__ void __launch_bounds__(128, 3)
-    l1gs_batched_kernel(const PrecItem* __restrict__ items, int32_t nitems, int32_t* err) {
+    l1gs_batched_kernel(const PrecItem* __restrict__ items, int32_t nitems, double* __restrict__ rz_part,
+                        int32_t* err) {
     constexpr int TLEN = PS * (PS - 1) / 2;
     constexpr int NT = (TLEN + E - 1) / E;
     constexpr int NTPG = 2 * NT;
@@ -415,10 +401,21 @@ __global__ void __launch_bounds__(128, 3)
 #pragma unroll
         for (int li = 0; li < PS; ++li) xs[lane * XS + li] = yv[li];
         __syncwarp();
+        hsdev::DD part{0.0, 0.0};   // this item's share of r.z (fused: no separate pass)
 #pragma unroll
         for (int m = 0; m < PS; ++m) {
             const int t = lane + 32 * m;
-            if (t < it.rows) it.y[t] = (double)xs[(t / PS) * XS + (t % PS)];
+            if (t < it.rows) {
+                const double z = (double)xs[(t / PS) * XS + (t % PS)];
+                it.y[t] = z;
+                hsdev::dd_add_prod(part, it.x[t], z);
+            }
+        }
+        part = hsdev::warp_dd(part);
+        if (lane == 0) {
+            const int64_t item = w0 + (int64_t)ii * wstride;
+            rz_part[2 * item] = part.s;
+            rz_part[2 * item + 1] = part.c;
         }
         __syncwarp();
     }
@@ -463,11 +460,14 @@ struct hs_batch_s {
     Scalars* d_scal = nullptr;
     Scalars* h_scal = nullptr;          // pinned mirror of d_scal
     cudaEvent_t launched = nullptr;     // end of the last hs_batch_launch
+    cudaEvent_t admitted = nullptr;     // end of the last admission's setup work
     bool inflight = false;
+    bool pending_admission = false;
     BlockMap* d_map = nullptr;
     int32_t* d_active = nullptr;
     PrecItem* d_items = nullptr;
     double* d_partials = nullptr;
+    double* d_rzpart = nullptr;   // r.z partials, one pair per L1GS work item
     double* d_init = nullptr;    // init partials (2 x 2 x kRedMaxBlocks)
     int32_t max_blocks = 0, max_items = 0;
     int64_t used = 0;
@@ -511,7 +511,7 @@ int launch_batched(hs_batch* B, const hs_batch_s::Cls& cl, cudaStream_t st) {
     HS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, wpb * 32, smem));
     const int64_t want = (cl.nitems + wpb - 1) / wpb;
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)std::max(1, per_sm) * hs::num_sms()));
-    kern<<<grid, wpb * 32, smem, st>>>(B->d_items + cl.item0, cl.nitems, B->err);
+    kern<<<grid, wpb * 32, smem, st>>>(B->d_items + cl.item0, cl.nitems, B->d_rzpart + 2 * (size_t)cl.item0, B->err);
     HS_LAUNCH_CHECK("l1gs_batched_kernel");
     return HS_OK;
 }
@@ -531,11 +531,13 @@ int rebuild(hs_batch* B) {
     std::vector<int32_t> active;
     std::vector<PrecItem> items;
     B->classes.clear();
+    std::vector<int32_t> item0(B->slots.size(), 0), nitem(B->slots.size(), 0);
     for (int ps : {8, 16, 32}) {
         hs_batch_s::Cls cl{ps, (int32_t)items.size(), 0};
         for (size_t s = 0; s < B->slots.size(); ++s) {
             const hs_batch_slot& sl = B->slots[s];
             if (sl.state != 1 || sl.ps != ps) continue;
+            item0[s] = (int32_t)items.size();
             hs::L1gsView lv;
             hs::l1gs_view_of(sl.P, &lv);
             const double* r = sl.vec + sl.n;
@@ -554,6 +556,7 @@ int rebuild(hs_batch* B) {
                 it.s = B->d_scal + s;
                 items.push_back(it);
             }
+            nitem[s] = (int32_t)items.size() - item0[s];
         }
         cl.nitems = (int32_t)items.size() - cl.item0;
         if (cl.nitems) B->classes.push_back(cl);
@@ -581,17 +584,19 @@ int rebuild(hs_batch* B) {
             m.row0 = b * kRPC;
             map.push_back(m);
         }
-        sd[s] = SlotDev{sl.n, sl.blk0, sl.nblk, 0, B->d_scal + s};
+        sd[s] = SlotDev{sl.n, sl.blk0, sl.nblk, item0[s], nitem[s], 0, B->d_scal + s};
     }
     if ((int32_t)map.size() > B->max_blocks || (int32_t)items.size() > B->max_items) {
         cudaFree(B->d_map);
         cudaFree(B->d_partials);
         cudaFree(B->d_items);
+        cudaFree(B->d_rzpart);
         B->max_blocks = std::max<int32_t>((int32_t)map.size() * 2, 1024);
         B->max_items = std::max<int32_t>((int32_t)items.size() * 2, 1024);
         HS_CUDA(cudaMalloc(&B->d_map, sizeof(BlockMap) * B->max_blocks));
         HS_CUDA(cudaMalloc(&B->d_partials, 2 * sizeof(double) * B->max_blocks));
         HS_CUDA(cudaMalloc(&B->d_items, sizeof(PrecItem) * B->max_items));
+        HS_CUDA(cudaMalloc(&B->d_rzpart, 2 * sizeof(double) * B->max_items));
     }
     cudaStream_t st = B->solve;
     if (!sd.empty())
@@ -627,10 +632,9 @@ int enqueue_iteration(hs_batch* B, cudaStream_t st) {
         int rc = launch_prec_class(B, cl, st);
         if (rc) return rc;
     }
-    seg_dot<<<B->nblocks, kT, 0, st>>>(B->d_map, B->d_partials);
-    seg_beta<<<B->nactive, kT, 0, st>>>(B->d_slots, B->d_active, B->d_partials);
+    seg_beta<<<B->nactive, kT, 0, st>>>(B->d_slots, B->d_active, B->d_rzpart);
     seg_p<<<B->nblocks, kT, 0, st>>>(B->d_map);
-    hs::count_launch(3);
+    hs::count_launch(2);
     HS_CUDA(cudaGetLastError());
     return HS_OK;
 }
@@ -674,6 +678,7 @@ int hs_batch_create(const hs_batch_config* cfg, void* stream, hs_batch** out) {
     cudaError_t e;
     if ((e = cudaStreamCreateWithFlags(&B->solve, cudaStreamNonBlocking)) ||
         (e = cudaEventCreateWithFlags(&B->launched, cudaEventDisableTiming)) ||
+        (e = cudaEventCreateWithFlags(&B->admitted, cudaEventDisableTiming)) ||
         (e = cudaMallocHost(&B->h_scal, sizeof(Scalars) * cfg->max_slots)) ||
         (e = create_setup_stream(&B->setup)) ||
         (e = cudaMalloc(&B->d_slots, sizeof(SlotDev) * cfg->max_slots)) ||
@@ -746,7 +751,10 @@ int hs_batch_submit(hs_batch* B, const hs_sparse* A, const double* b_host, doubl
                                    B->cfg.rtol);
     hs::count_launch(2);
     HS_CUDA(cudaGetLastError());
-    HS_CUDA(cudaStreamSynchronize(st));
+    // No host wait: the next launch orders the solve stream after this
+    // admission's setup work through the event.
+    HS_CUDA(cudaEventRecord(B->admitted, st));
+    B->pending_admission = true;
     sl.state = 1;
     B->slots[free_idx] = sl;
     B->used += est;
@@ -759,6 +767,10 @@ int hs_batch_launch(hs_batch* B, int32_t iters) {
     if (!B || iters < 1) return hs::set_error(HS_ERR_ARG, "hs_batch_launch: bad argument");
     if (B->inflight) return hs::set_error(HS_ERR_ARG, "hs_batch_launch: the previous launch was not waited for");
     int rc;
+    if (B->pending_admission) {
+        HS_CUDA(cudaStreamWaitEvent(B->solve, B->admitted, 0));
+        B->pending_admission = false;
+    }
     if (B->dirty && (rc = rebuild(B))) return rc;
     if (B->nactive > 0) {
         if (!B->exec) {
@@ -849,17 +861,19 @@ int hs_batch_info_get(const hs_batch* B, hs_batch_info* info) {
 
 int hs_batch_destroy(hs_batch* B) {
     if (!B) return HS_OK;
-    cudaDeviceSynchronize();
+    cudaDeviceSynchronize();   // launches and admissions in flight
     for (auto& s : B->slots)
         if (s.state) free_slot(B, s);
     cudaStreamSynchronize(B->solve);   // the stream-ordered frees above
     if (B->exec) cudaGraphExecDestroy(B->exec);
     if (B->graph) cudaGraphDestroy(B->graph);
-    void* ptrs[] = {B->d_slots, B->d_scal, B->d_map, B->d_active, B->d_items, B->d_partials, B->d_init};
+    void* ptrs[] = {B->d_slots, B->d_scal, B->d_map, B->d_active, B->d_items, B->d_partials, B->d_rzpart,
+                    B->d_init};
     for (void* p : ptrs) cudaFree(p);
     cudaStreamDestroy(B->solve);
     cudaStreamDestroy(B->setup);
     if (B->launched) cudaEventDestroy(B->launched);
+    if (B->admitted) cudaEventDestroy(B->admitted);
     if (B->h_scal) cudaFreeHost(B->h_scal);
     delete B;
     return HS_OK;

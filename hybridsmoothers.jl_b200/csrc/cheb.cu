@@ -610,7 +610,7 @@ int matrix_create_impl(const hs_sparse* A, int32_t dtype, void* stream, hs_matri
     M->bytes = (int64_t)(sizeof(int32_t) * (M->n + 1 + M->nnz) + es * M->nnz);
     // A CSC input is transposed on the device (stable: rows keep ascending columns).
     rc = hs::csr_from_host(A, dtype, M->rp, M->ci, M->v, st);
-    if (!rc) {
+    if (!rc && !stream_ordered) {   // stream-ordered callers order their own use
         const cudaError_t se = cudaStreamSynchronize(st);
         if (se != cudaSuccess) rc = hs::cuda_error(se, "hs_matrix_create");
     }

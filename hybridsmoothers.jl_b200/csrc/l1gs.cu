@@ -858,7 +858,7 @@ int setup_device(hs_l1gs* P, const int32_t* rp_h, const int32_t* ci_h, const TM*
                                                               Di, SLi, SUi);
     HS_LAUNCH_CHECK("setup_rows_kernel");
     if (packed && on_device) {
-        HS_CUDA(cudaStreamSynchronize(st));
+        if (!P->stream_ordered) HS_CUDA(cudaStreamSynchronize(st));
     } else if (packed) {
         HS_CUDA(cudaStreamSynchronize(st));
         cudaFree(rp_d);
