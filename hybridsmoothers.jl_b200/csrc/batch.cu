@@ -357,10 +357,15 @@ __global__ void __launch_bounds__(128, 3)
         float d[PS];
 #pragma unroll
         for (int li = 0; li < PS; ++li) d[li] = it.Di[(int64_t)li * it.npad + lane];
+        // r of the rows this lane moves (kept for the fused r.z when it fits in registers)
+        constexpr int KR = PS <= 16 ? PS : 1;
+        double rkeep[KR];
 #pragma unroll
         for (int m = 0; m < PS; ++m) {
             const int t = lane + 32 * m;
-            xs[(t / PS) * XS + (t % PS)] = t < it.rows ? (float)it.x[t] : 0.0f;
+            const double rv = t < it.rows ? it.x[t] : 0.0;
+            if (PS <= 16) rkeep[m < KR ? m : 0] = rv;
+            xs[(t / PS) * XS + (t % PS)] = (float)rv;
         }
         __syncwarp();
         float yv[PS];
@@ -408,7 +413,7 @@ __global__ void __launch_bounds__(128, 3)
             if (t < it.rows) {
                 const double z = (double)xs[(t / PS) * XS + (t % PS)];
                 it.y[t] = z;
-                hsdev::dd_add_prod(part, it.x[t], z);
+                hsdev::dd_add_prod(part, PS <= 16 ? rkeep[m < KR ? m : 0] : it.x[t], z);
             }
         }
         part = hsdev::warp_dd(part);
