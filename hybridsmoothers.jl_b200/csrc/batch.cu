@@ -330,7 +330,9 @@ __global__ void __launch_bounds__(128, 3)
                 : "memory");
         }
     };
+    int32_t last_wait = 0;   // the tile of the latest wait (a timeout drains from here)
     auto wait = [&](int32_t c) -> bool {
+        last_wait = c;
         const bool ok = hsdev::mbar_wait_bounded(bars + (c & (STAGES - 1)), (uint32_t)((c / STAGES) & 1));
         return __all_sync(0xffffffffu, ok);
     };
@@ -428,8 +430,8 @@ __global__ void __launch_bounds__(128, 3)
 timeout:
     if (lane == 0) hsdev::report_error(err, hsdev::kErrWaitTimeout);
     {
-        const int32_t end = min(total, c + STAGES);
-        for (int32_t cc = c; cc < end; ++cc)
+        const int32_t end = min(total, last_wait + STAGES);
+        for (int32_t cc = last_wait; cc < end; ++cc)
             (void)hsdev::mbar_wait_bounded(bars + (cc & (STAGES - 1)), (uint32_t)((cc / STAGES) & 1));
     }
 }

@@ -40,6 +40,17 @@ __host__ __device__ __forceinline__ int64_t up_idx(int64_t ps, int64_t li, int64
     return q * (q - 1) / 2 + (lj - li - 1);
 }
 
+// Row-aligned stream layout for partsize > 32 ("rows" layout).  Row r of a
+// direction (r = li forward, r = ps-1-li backward) occupies r + 1 slots
+// rounded up to a multiple of 8, from rows_off(r): slot 0 holds D_Dl1 of the
+// row, slots 1.. its terms in the order the sweep sums them, then zeros.  Every 8-slot tile belongs to
+// one row, so the apply streams whole tiles with a fixed-length inner loop
+// and receives D_Dl1 with the row's first tile.
+__host__ __device__ __forceinline__ int64_t rows_off(int64_t r) {   // sum over u = 1..r of u rounded up to 8
+    const int64_t m = r / 8, rem = r % 8;
+    return 32 * m * (m + 1) + 8 * (m + 1) * rem;
+}
+
 // ---------------------------------------------------------------------------
 // Setup: D_Dl1 and packing, one thread per row.
 //   D_Dl1: _diag_offpart_rowwise (:1101-1129) + eta rule (:1017-1022)
@@ -51,7 +62,7 @@ template <typename TM, typename TS>
 __global__ void setup_rows_kernel(int32_t n, int32_t ps, int64_t npad, const int32_t* __restrict__ rp,
                                   const int32_t* __restrict__ ci, const TM* __restrict__ v, TM eta,
                                   TS* __restrict__ D, TS* __restrict__ Di, TS* __restrict__ SLi,
-                                  TS* __restrict__ SUi) {
+                                  TS* __restrict__ SUi, int rows_layout) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int64_t k = i / ps;
@@ -67,15 +78,31 @@ __global__ void setup_rows_kernel(int32_t n, int32_t ps, int64_t npad, const int
         } else if (j < s || j > e) {
             d = add_rn(d, abs_t(val));
         } else if (j < i) {
-            if (SLi) SLi[lo_idx(li, j - s) * npad + k] = (TS)val;
+            if (SLi) SLi[(rows_layout ? rows_off(li) + 1 + (j - s) : lo_idx(li, j - s)) * npad + k] = (TS)val;
         } else {
-            if (SUi) SUi[up_idx(ps, li, j - s) * npad + k] = (TS)val;
+            if (SUi)
+                SUi[(rows_layout ? rows_off(ps - 1 - li) + (j - i) : up_idx(ps, li, j - s)) * npad + k] = (TS)val;
         }
     }
     const TM dl1star = (b >= mul_rn(eta, d)) ? TM(0) : div_rn(d, TM(2));
     const TM Dv = add_rn(b, dl1star);
     D[i] = (TS)Dv;
     if (Di) Di[li * npad + k] = (TS)Dv;
+    if (rows_layout) {
+        if (SLi) SLi[rows_off(li) * npad + k] = (TS)Dv;
+        if (SUi) SUi[rows_off(ps - 1 - li) * npad + k] = (TS)Dv;
+    }
+}
+
+// Rows layout: the missing rows of a short last partition get D_Dl1 = 1 in
+// their stream slots (their y stays 0 and adds +0.0 terms only).
+template <typename TS>
+__global__ void rows_tail_kernel(int32_t ps, int32_t lps, int64_t npad, int64_t k, TS* __restrict__ SLi,
+                                 TS* __restrict__ SUi) {
+    for (int li = lps + threadIdx.x; li < ps; li += blockDim.x) {
+        if (SLi) SLi[rows_off(li) * npad + k] = TS(1);
+        if (SUi) SUi[rows_off(ps - 1 - li) * npad + k] = TS(1);
+    }
 }
 
 template <typename T>
@@ -123,6 +150,7 @@ struct TileRing {
     uint64_t* bars;
     int32_t g0, gstride, ntiles, total;
     int lane;
+    mutable int32_t last = 0;   // the tile of the latest wait (a timeout drains from here)
 
     __device__ __forceinline__ void issue(int32_t c) const {
         const int32_t ntpg = (SWEEP == 2) ? 2 * ntiles : ntiles;
@@ -148,6 +176,7 @@ struct TileRing {
     }
     // Wait for tile c; false (on every lane) if a bounded wait ran out.
     __device__ __forceinline__ bool wait(int32_t c) const {
+        last = c;
         const bool ok = hsdev::mbar_wait_bounded(bars + (c & (STAGES - 1)), (uint32_t)((c / STAGES) & 1));
         return __all_sync(0xffffffffu, ok);
     }
@@ -160,9 +189,11 @@ struct TileRing {
             issue(c + STAGES);
         }
     }
-    // After a timeout at tile c: let copies already issued land, then return.
-    __device__ void drain(int32_t c, int32_t* err) const {
+    // After a timeout: let the copies issued for the tiles from the one that
+    // timed out on (at most STAGES of them) land, then return.
+    __device__ void drain(int32_t /*unused*/, int32_t* err) const {
         if (lane == 0) hsdev::report_error(err, hsdev::kErrWaitTimeout);
+        const int32_t c = last;
         const int32_t end = (c + STAGES < total) ? c + STAGES : total;
         for (int32_t cc = c; cc < end; ++cc)
             (void)hsdev::mbar_wait_bounded(bars + (cc & (STAGES - 1)), (uint32_t)((cc / STAGES) & 1));
@@ -403,6 +434,249 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
     return;
 timeout:
     ring.drain(c, p.err);
+}
+
+// Ring for the rows kernel: like TileRing, but the elected lane keeps the
+// coordinates of the next tile to fetch and advances them by one per refill
+// (no division per tile: a refill is a few instructions).
+template <typename T, int E, int STAGES, int SWEEP>
+struct RowRing {
+    const CUtensorMap* tmL;
+    const CUtensorMap* tmU;
+    T* buf;
+    uint64_t* bars;
+    int32_t total, ntiles, gstride;
+    int lane;
+    int32_t issued = 0, i_g = 0, i_ti = 0, i_dir = 0;   // next tile to fetch (elected lane)
+    mutable int32_t last = 0;
+
+    __device__ __forceinline__ void issue_next() {
+        const int stage = issued & (STAGES - 1);
+        const CUtensorMap* map = (SWEEP == 1 || (SWEEP == 2 && i_dir)) ? tmU : tmL;
+        hsdev::mbar_arrive_expect_tx(bars + stage, (uint32_t)(E * 32 * sizeof(T)));
+        hsdev::tma_load_2d(buf + stage * (E * 32), map, i_g * 32, i_ti * E, bars + stage);
+        ++issued;
+        if (++i_ti == ntiles) {
+            i_ti = 0;
+            if (SWEEP == 2 && !i_dir) {
+                i_dir = 1;
+            } else {
+                i_dir = 0;
+                i_g += gstride;
+            }
+        }
+    }
+    __device__ __forceinline__ void prologue(int32_t g0) {
+        if (lane == 0) {
+            i_g = g0;
+            for (int s = 0; s < STAGES; ++s) hsdev::mbar_init(bars + s, 1);
+            hsdev::fence_barrier_init();
+            const int32_t pro = total < STAGES ? total : STAGES;
+            for (int32_t c = 0; c < pro; ++c) issue_next();
+        }
+        __syncwarp();
+    }
+    __device__ __forceinline__ bool wait(int32_t c) const {
+        last = c;
+        const bool ok = hsdev::mbar_wait_bounded(bars + (c & (STAGES - 1)), (uint32_t)((c / STAGES) & 1));
+        return __all_sync(0xffffffffu, ok);
+    }
+    __device__ __forceinline__ const T* tile(int32_t c) const { return buf + (c & (STAGES - 1)) * (E * 32); }
+    __device__ __forceinline__ void release(int32_t c) {
+        __syncwarp();
+        if (lane == 0 && c + STAGES < total) {
+            hsdev::fence_proxy_async_smem();
+            issue_next();
+        }
+    }
+    __device__ void drain(int32_t* err) const {
+        if (lane == 0) hsdev::report_error(err, hsdev::kErrWaitTimeout);
+        const int32_t c = last;
+        const int32_t end = (c + STAGES < total) ? c + STAGES : total;
+        for (int32_t cc = c; cc < end; ++cc)
+            (void)hsdev::mbar_wait_bounded(bars + (cc & (STAGES - 1)), (uint32_t)((cc / STAGES) & 1));
+    }
+};
+
+// ---- partsize > 32: row-aligned streams (rows layout) ----------------------
+// Thread per partition as above.  Each row's stream segment starts with its
+// D_Dl1 and is padded to whole 8-slot tiles, so a full tile is 8 loads of
+// coefficients, 8 of y and 8 separately rounded multiply-adds with no index
+// arithmetic or predicates; only a row's last tile is predicated (padding
+// slots are never added).  Symmetric: the D_Dl1 .* y scaling of a row is
+// applied when the backward sweep reaches it (the same product, before any
+// use).  y lives in shared memory ([row][lane], stride 33).
+template <typename T, typename IO, int SWEEP, int STAGES>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+    l1gs_packed_rows_kernel(const __grid_constant__ CUtensorMap tmL, const __grid_constant__ CUtensorMap tmU,
+                            const PackedParams p) {
+    constexpr int E = 8;
+    constexpr int S = 33;
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    unsigned char* wbase = smem + (size_t)warp * p.warp_bytes;
+    T* ys = reinterpret_cast<T*>(wbase + p.ring_bytes + 8 * STAGES);
+    const IO* __restrict__ x = static_cast<const IO*>(p.x);
+    IO* __restrict__ y = static_cast<IO*>(p.y);
+    const int ps = p.ps;
+
+    const int wpb = blockDim.x >> 5;
+    const int32_t g0 = blockIdx.x * wpb + warp, gstride = gridDim.x * wpb;
+    RowRing<T, E, STAGES, SWEEP> ring;
+    ring.tmL = &tmL;
+    ring.tmU = &tmU;
+    ring.buf = reinterpret_cast<T*>(wbase);
+    ring.bars = reinterpret_cast<uint64_t*>(wbase + p.ring_bytes);
+    ring.gstride = gstride;
+    ring.ntiles = p.ntiles;
+    ring.lane = lane;
+    const int32_t my_groups = g0 < p.ngroups ? (p.ngroups - 1 - g0) / gstride + 1 : 0;
+    ring.total = my_groups * ((SWEEP == 2) ? 2 * p.ntiles : p.ntiles);
+    ring.prologue(g0);
+
+    int32_t c = 0;
+    for (int32_t gi = 0; gi < my_groups; ++gi) {
+        const int64_t g = g0 + (int64_t)gi * gstride;
+        const int64_t rowbase = g * 32 * (int64_t)ps;
+        T* yk = ys + lane;
+        {   // x -> ys[li][partition], coalesced; (partition, li) advanced without division (ps > 32)
+            int pp = 0, li = lane;
+            for (int t = lane; t < 32 * ps; t += 32) {
+                const int64_t row = rowbase + t;
+                ys[li * S + pp] = row < p.n ? (T)x[row] : T(0);
+                li += 32;
+                if (li >= ps) {
+                    li -= ps;
+                    ++pp;
+                }
+            }
+        }
+        __syncwarp();
+
+        if (SWEEP != 1) {   // forward, rows ascending: slots D, a[li][0..li-1]
+            int32_t t = c;
+            for (int li = 0; li < ps; ++li) {
+                const int len = li + 1;
+                const int nt = (len + E - 1) / E;
+                T acc = T(0);
+                if (!ring.wait(t)) goto timeout;
+                const T* tl = ring.tile(t) + lane;
+                const T d = tl[0];
+                if (nt == 1) {
+#pragma unroll
+                    for (int m = 1; m < E; ++m)
+                        if (m < len) acc = add_rn(acc, mul_rn(tl[m * 32], yk[(m - 1) * S]));
+                } else {
+                    T a[E - 1], b[E - 1];
+#pragma unroll
+                    for (int m = 1; m < E; ++m) {
+                        a[m - 1] = tl[m * 32];
+                        b[m - 1] = yk[(m - 1) * S];
+                    }
+#pragma unroll
+                    for (int m = 0; m < E - 1; ++m) acc = add_rn(acc, mul_rn(a[m], b[m]));
+                }
+                ring.release(t);
+                ++t;
+                for (int tr = 1; tr < nt; ++tr) {
+                    if (!ring.wait(t)) goto timeout;
+                    tl = ring.tile(t) + lane;
+                    const T* yy = yk + (tr * E - 1) * S;
+                    if (tr + 1 < nt || (len & (E - 1)) == 0) {
+                        T a[E], b[E];
+#pragma unroll
+                        for (int m = 0; m < E; ++m) {
+                            a[m] = tl[m * 32];
+                            b[m] = yy[m * S];
+                        }
+#pragma unroll
+                        for (int m = 0; m < E; ++m) acc = add_rn(acc, mul_rn(a[m], b[m]));
+                    } else {
+                        const int cnt = len & (E - 1);
+#pragma unroll
+                        for (int m = 0; m < E; ++m)
+                            if (m < cnt) acc = add_rn(acc, mul_rn(tl[m * 32], yy[m * S]));
+                    }
+                    ring.release(t);
+                    ++t;
+                }
+                yk[li * S] = div_rn(sub_rn(yk[li * S], acc), d);
+            }
+            c += p.ntiles;
+        }
+        if (SWEEP != 0) {   // backward, rows descending: slots D, a[li][li+1..ps-1]
+            int32_t t = c;
+            for (int q = 0; q < ps; ++q) {
+                const int li = ps - 1 - q;
+                const int len = q + 1;
+                const int nt = (len + E - 1) / E;
+                T acc = T(0);
+                if (!ring.wait(t)) goto timeout;
+                const T* tl = ring.tile(t) + lane;
+                const T d = tl[0];
+                const T* yy0 = yk + li * S;   // term slot m reads y[li + m]
+                if (nt == 1) {
+#pragma unroll
+                    for (int m = 1; m < E; ++m)
+                        if (m < len) acc = add_rn(acc, mul_rn(tl[m * 32], yy0[m * S]));
+                } else {
+                    T a[E - 1], b[E - 1];
+#pragma unroll
+                    for (int m = 1; m < E; ++m) {
+                        a[m - 1] = tl[m * 32];
+                        b[m - 1] = yy0[m * S];
+                    }
+#pragma unroll
+                    for (int m = 0; m < E - 1; ++m) acc = add_rn(acc, mul_rn(a[m], b[m]));
+                }
+                ring.release(t);
+                ++t;
+                for (int tr = 1; tr < nt; ++tr) {
+                    if (!ring.wait(t)) goto timeout;
+                    tl = ring.tile(t) + lane;
+                    const T* yy = yy0 + (tr * E) * S;
+                    if (tr + 1 < nt || (len & (E - 1)) == 0) {
+                        T a[E], b[E];
+#pragma unroll
+                        for (int m = 0; m < E; ++m) {
+                            a[m] = tl[m * 32];
+                            b[m] = yy[m * S];
+                        }
+#pragma unroll
+                        for (int m = 0; m < E; ++m) acc = add_rn(acc, mul_rn(a[m], b[m]));
+                    } else {
+                        const int cnt = len & (E - 1);
+#pragma unroll
+                        for (int m = 0; m < E; ++m)
+                            if (m < cnt) acc = add_rn(acc, mul_rn(tl[m * 32], yy[m * S]));
+                    }
+                    ring.release(t);
+                    ++t;
+                }
+                const T yi = (SWEEP == 2) ? mul_rn(d, yk[li * S]) : yk[li * S];   // y .= D_Dl1 .* y (:897)
+                yk[li * S] = div_rn(sub_rn(yi, acc), d);
+            }
+            c += p.ntiles;
+        }
+        __syncwarp();
+        {
+            int pp = 0, li = lane;
+            for (int t = lane; t < 32 * ps; t += 32) {
+                const int64_t row = rowbase + t;
+                if (row < p.n) y[row] = (IO)ys[li * S + pp];
+                li += 32;
+                if (li >= ps) {
+                    li -= ps;
+                    ++pp;
+                }
+            }
+        }
+        __syncwarp();
+    }
+    return;
+timeout:
+    ring.drain(p.err);
 }
 
 // ---------------------------------------------------------------------------
@@ -695,6 +969,8 @@ inline size_t dsize(int dt) { return dt == HS_F64 ? 8 : 4; }
 struct hs_l1gs_s {
     int32_t n = 0, ps = 0, nparts = 0, ngroups = 0, nchunks = 0, chunksize = 0;
     int64_t npad = 0, tlen = 0, S = 0;
+    int64_t tstore = 0;      // stream slots per direction (tlen, or rows_off(ps) in the rows layout)
+    int32_t rows_layout = 0; // packed partsize > 32: row-aligned streams with D_Dl1 inside
     int32_t sweep = 0, cache = 0, is_sym = 0, format = 0, mdt = 0, sdt = 0;
     double eta = 1.5;
     void* D = nullptr;
@@ -837,12 +1113,14 @@ int setup_device(hs_l1gs* P, const int32_t* rp_h, const int32_t* ci_h, const TM*
     const bool packed = P->cache == HS_CACHE_PACKED;
     const bool lower = P->sweep != HS_SWEEP_BACKWARD, upper = P->sweep != HS_SWEEP_FORWARD;
     if (packed) {
-        const int64_t dcount = (int64_t)P->ps * P->npad;
-        if ((rc = dmalloc(P, &Di, sizeof(TS) * dcount))) return rc;
-        P->Di = Di;
-        fill_kernel<TS><<<std::min<int64_t>((dcount + 255) / 256, 4096), 256, 0, st>>>(Di, dcount, TS(1));
-        HS_LAUNCH_CHECK("fill_kernel");
-        const int64_t tcount = P->tlen * P->npad;
+        if (!P->rows_layout) {   // the rows layout carries D_Dl1 inside its streams
+            const int64_t dcount = (int64_t)P->ps * P->npad;
+            if ((rc = dmalloc(P, &Di, sizeof(TS) * dcount))) return rc;
+            P->Di = Di;
+            fill_kernel<TS><<<std::min<int64_t>((dcount + 255) / 256, 4096), 256, 0, st>>>(Di, dcount, TS(1));
+            HS_LAUNCH_CHECK("fill_kernel");
+        }
+        const int64_t tcount = P->tstore * P->npad;
         if (lower && tcount > 0) {
             if ((rc = dmalloc(P, &SLi, sizeof(TS) * tcount))) return rc;
             P->SLi = SLi;
@@ -855,8 +1133,15 @@ int setup_device(hs_l1gs* P, const int32_t* rp_h, const int32_t* ci_h, const TM*
         }
     }
     setup_rows_kernel<TM, TS><<<(n + 255) / 256, 256, 0, st>>>(n, P->ps, P->npad, rp_d, ci_d, v_d, (TM)P->eta, D,
-                                                              Di, SLi, SUi);
+                                                              Di, SLi, SUi, P->rows_layout);
     HS_LAUNCH_CHECK("setup_rows_kernel");
+    if (packed && P->rows_layout) {
+        const int32_t lps = (int32_t)((int64_t)n - (int64_t)(P->nparts - 1) * P->ps);
+        if (lps < P->ps) {
+            rows_tail_kernel<TS><<<1, 256, 0, st>>>(P->ps, lps, P->npad, P->nparts - 1, SLi, SUi);
+            HS_LAUNCH_CHECK("rows_tail_kernel");
+        }
+    }
     if (packed && on_device) {
         if (!P->stream_ordered) HS_CUDA(cudaStreamSynchronize(st));
     } else if (packed) {
@@ -994,8 +1279,39 @@ int launch_packed_t(hs_l1gs* P, const void* x, void* y, cudaStream_t st) {
                                 (uint32_t)(P->ps * 33 * sizeof(T)), st, &cfg);
 }
 
+// Row-aligned streams (partsize > 32): 8-slot tiles, ring of 8 or 16 stages.
+template <typename T, typename IO, int SWEEP, int STAGES>
+int launch_rows_stages(hs_l1gs* P, const void* x, void* y, cudaStream_t st) {
+    constexpr int E = 8;
+    PackedParams p;
+    p.n = P->n;
+    p.ps = P->ps;
+    p.nparts = P->nparts;
+    p.npad = P->npad;
+    p.ngroups = P->ngroups;
+    p.tlen = (int32_t)P->tstore;
+    p.ntiles = (int32_t)(P->tstore / E);
+    p.Di = nullptr;
+    p.x = x;
+    p.y = y;
+    if (!P->err_word) P->err_word = hs::device_error_word();
+    p.err = P->err_word;
+    p.ring_bytes = (uint32_t)(E * 32 * sizeof(T) * STAGES);
+    static thread_local int cfg = -1;
+    return launch_packed_kernel(l1gs_packed_rows_kernel<T, IO, SWEEP, STAGES>, P, p,
+                                (uint32_t)(P->ps * 33 * sizeof(T)), st, &cfg);
+}
+
+template <typename T, typename IO, int SWEEP>
+int launch_rows_t(hs_l1gs* P, const void* x, void* y, cudaStream_t st) {
+    if (P->stages == 8) return launch_rows_stages<T, IO, SWEEP, 8>(P, x, y, st);
+    if (P->stages == 32) return launch_rows_stages<T, IO, SWEEP, 32>(P, x, y, st);
+    return launch_rows_stages<T, IO, SWEEP, 16>(P, x, y, st);
+}
+
 template <typename T, typename IO, int SWEEP>
 int launch_packed_cfg(hs_l1gs* P, const void* x, void* y, cudaStream_t st) {
+    if (P->rows_layout) return launch_rows_t<T, IO, SWEEP>(P, x, y, st);
     constexpr int EA = sizeof(T) == 8 ? 8 : 16;
     constexpr int EB = sizeof(T) == 8 ? 16 : 32;
     if (P->E == EA && P->stages == 4) return launch_packed_t<T, IO, SWEEP, EA, 4>(P, x, y, st);
@@ -1106,12 +1422,16 @@ void unpack_reference(const hs_l1gs* P, const TS* inter, TS* out, bool lower) {
         const int64_t boff = k * tlen;
         for (int64_t li = 0; li < aps; ++li) {
             if (lower) {
-                for (int64_t lj = 0; lj < li; ++lj)
-                    out[boff + li * (li - 1) / 2 + lj] = inter[lo_idx(li, lj) * P->npad + k];
+                for (int64_t lj = 0; lj < li; ++lj) {
+                    const int64_t e = P->rows_layout ? rows_off(li) + 1 + lj : lo_idx(li, lj);
+                    out[boff + li * (li - 1) / 2 + lj] = inter[e * P->npad + k];
+                }
             } else {
                 const int64_t row_start = li * aps - li * (li + 1) / 2;
-                for (int64_t lj = li + 1; lj < aps; ++lj)
-                    out[boff + row_start + (lj - li) - 1] = inter[up_idx(ps, li, lj) * P->npad + k];
+                for (int64_t lj = li + 1; lj < aps; ++lj) {
+                    const int64_t e = P->rows_layout ? rows_off(ps - 1 - li) + (lj - li) : up_idx(ps, li, lj);
+                    out[boff + row_start + (lj - li) - 1] = inter[e * P->npad + k];
+                }
             }
         }
     }
@@ -1169,6 +1489,8 @@ int l1gs_create_impl(const hs_sparse* A, bool on_device, int32_t partsize, int32
     P->npad = ((int64_t)P->nparts + 31) / 32 * 32;
     P->ngroups = (int32_t)(P->npad / 32);
     P->tlen = (int64_t)partsize * (partsize - 1) / 2;
+    P->rows_layout = (cache == HS_CACHE_PACKED && partsize > 32) ? 1 : 0;
+    P->tstore = P->rows_layout ? rows_off(partsize) : P->tlen;
     const int64_t lps = (int64_t)A->n - (int64_t)(P->nparts - 1) * partsize;
     P->S = P->tlen * (P->nparts - 1) + lps * (lps - 1) / 2;
     P->nchunks = blocks;  // _blockpartitioning for KA.GPU (:353-365)
@@ -1220,13 +1542,22 @@ int l1gs_create_impl(const hs_sparse* A, bool on_device, int32_t partsize, int32
     }
     if (cache == HS_CACHE_PACKED) {
         pick_tile(partsize, smoother_dtype, &P->E, &P->stages, &P->minb);
+        if (P->rows_layout) {   // one 8-slot tile per row segment; deeper ring (fewer warps per SM)
+            P->E = 8;
+            P->stages = partsize <= 96 ? 8 : 16;
+            // Tuning override: HSB200_ROWS_STAGES = 8, 16 or 32 tiles in flight per warp.
+            if (const char* env = getenv("HSB200_ROWS_STAGES")) {
+                const int st = atoi(env);
+                if (st == 8 || st == 16 || st == 32) P->stages = st;
+            }
+        }
         const uint32_t E = (uint32_t)P->E;
         const void* l = P->SLi ? P->SLi : P->SUi;
         const void* u = P->SUi ? P->SUi : P->SLi;
         if (l) {
             const size_t es = dsize(smoother_dtype);
-            if ((rc = hs::encode_tensor_map_2d(&P->tmL, l, smoother_dtype, P->npad, P->tlen, P->npad * es, 32, E)) ||
-                (rc = hs::encode_tensor_map_2d(&P->tmU, u, smoother_dtype, P->npad, P->tlen, P->npad * es, 32, E))) {
+            if ((rc = hs::encode_tensor_map_2d(&P->tmL, l, smoother_dtype, P->npad, P->tstore, P->npad * es, 32, E)) ||
+                (rc = hs::encode_tensor_map_2d(&P->tmU, u, smoother_dtype, P->npad, P->tstore, P->npad * es, 32, E))) {
                 release(P);
                 return rc;
             }
@@ -1328,7 +1659,7 @@ int hs_l1gs_get_packed(const hs_l1gs* P, int32_t which, void* out_host, int64_t 
     const size_t es = dsize(P->sdt);
     std::memset(out_host, 0, es * P->S);
     if (!src) return HS_OK;  // partsize 1: empty triangles
-    std::vector<unsigned char> inter(es * P->tlen * P->npad);
+    std::vector<unsigned char> inter(es * P->tstore * P->npad);
     HS_CUDA(cudaDeviceSynchronize());
     HS_CUDA(cudaMemcpy(inter.data(), src, inter.size(), cudaMemcpyDeviceToHost));
     if (P->sdt == HS_F64)

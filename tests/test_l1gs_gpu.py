@@ -257,3 +257,19 @@ def test_full_size_poisson128_packed_symmetric():
     ref = O.OracleL1GS(A, 16, isSymA=True, sweep="symmetric", cache="packed", nchunks=8, chunksize=16384)
     P = hsb200.L1GSPrecBuilder(hsb200.CUDABackend(), threads=256, blocks=148)(A, 16, isSymA=True)
     np.testing.assert_array_equal(gpu_apply(P, x), ref.ldiv(x))
+
+
+@pytest.mark.parametrize("ps", [40, 64])
+def test_nonfinite_input_rows_layout(ps):
+    """Partsize > 32 streams are padded to whole tiles; the padding is never
+    multiplied in, so an inf in x reaches exactly the rows the reference
+    reaches (NaN and inf positions equal to the oracle's)."""
+    A = W.poisson2d_matrix(30, eps=0.5)
+    x = np.random.default_rng(5).uniform(-1, 1, A.shape[0])
+    x[ps + 10] = np.inf
+    x[3] = np.nan
+    for sweep in ("forward", "backward", "symmetric"):
+        ref = O.OracleL1GS(A, ps, isSymA=True, sweep=sweep, cache="packed")
+        P = hsb200.L1GSPrecBuilder(hsb200.CUDABackend(), threads=256, blocks=20)(
+            A, ps, isSymA=True, sweep=SWEEPS[sweep])
+        np.testing.assert_array_equal(gpu_apply(P, x), ref.ldiv(x))
