@@ -40,15 +40,16 @@ __host__ __device__ __forceinline__ int64_t up_idx(int64_t ps, int64_t li, int64
     return q * (q - 1) / 2 + (lj - li - 1);
 }
 
-// Row-aligned stream layout for partsize > 32 ("rows" layout).  Row r of a
-// direction (r = li forward, r = ps-1-li backward) occupies r + 1 slots
-// rounded up to a multiple of 8, from rows_off(r): slot 0 holds D_Dl1 of the
-// row, slots 1.. its terms in the order the sweep sums them, then zeros.  Every 8-slot tile belongs to
-// one row, so the apply streams whole tiles with a fixed-length inner loop
-// and receives D_Dl1 with the row's first tile.
-__host__ __device__ __forceinline__ int64_t rows_off(int64_t r) {   // sum over u = 1..r of u rounded up to 8
-    const int64_t m = r / 8, rem = r % 8;
-    return 32 * m * (m + 1) + 8 * (m + 1) * rem;
+// Row-aligned stream layout for partsize > 32 ("rows" layout) with tile
+// width e (8 or 32 slots).  Row r of a direction (r = li forward, r = ps-1-li
+// backward) occupies r + 1 slots rounded up to a multiple of e, from
+// rows_off(r, e): slot 0 holds D_Dl1 of the row, slots 1.. its terms in the
+// order the sweep sums them, then zeros.  Every tile belongs to one row, so
+// the apply streams whole tiles with a fixed-length inner loop and receives
+// D_Dl1 with the row's first tile.
+__host__ __device__ __forceinline__ int64_t rows_off(int64_t r, int64_t e) {   // sum_{u=1..r} of u rounded up to e
+    const int64_t m = r / e, rem = r % e;
+    return e * e * m * (m + 1) / 2 + e * (m + 1) * rem;
 }
 
 // ---------------------------------------------------------------------------
@@ -78,10 +79,11 @@ __global__ void setup_rows_kernel(int32_t n, int32_t ps, int64_t npad, const int
         } else if (j < s || j > e) {
             d = add_rn(d, abs_t(val));
         } else if (j < i) {
-            if (SLi) SLi[(rows_layout ? rows_off(li) + 1 + (j - s) : lo_idx(li, j - s)) * npad + k] = (TS)val;
+            if (SLi) SLi[(rows_layout ? rows_off(li, rows_layout) + 1 + (j - s) : lo_idx(li, j - s)) * npad + k] = (TS)val;
         } else {
             if (SUi)
-                SUi[(rows_layout ? rows_off(ps - 1 - li) + (j - i) : up_idx(ps, li, j - s)) * npad + k] = (TS)val;
+                SUi[(rows_layout ? rows_off(ps - 1 - li, rows_layout) + (j - i) : up_idx(ps, li, j - s)) * npad + k] =
+                    (TS)val;
         }
     }
     const TM dl1star = (b >= mul_rn(eta, d)) ? TM(0) : div_rn(d, TM(2));
@@ -89,19 +91,19 @@ __global__ void setup_rows_kernel(int32_t n, int32_t ps, int64_t npad, const int
     D[i] = (TS)Dv;
     if (Di) Di[li * npad + k] = (TS)Dv;
     if (rows_layout) {
-        if (SLi) SLi[rows_off(li) * npad + k] = (TS)Dv;
-        if (SUi) SUi[rows_off(ps - 1 - li) * npad + k] = (TS)Dv;
+        if (SLi) SLi[rows_off(li, rows_layout) * npad + k] = (TS)Dv;
+        if (SUi) SUi[rows_off(ps - 1 - li, rows_layout) * npad + k] = (TS)Dv;
     }
 }
 
 // Rows layout: the missing rows of a short last partition get D_Dl1 = 1 in
 // their stream slots (their y stays 0 and adds +0.0 terms only).
 template <typename TS>
-__global__ void rows_tail_kernel(int32_t ps, int32_t lps, int64_t npad, int64_t k, TS* __restrict__ SLi,
+__global__ void rows_tail_kernel(int32_t ps, int32_t lps, int64_t npad, int64_t k, int32_t e, TS* __restrict__ SLi,
                                  TS* __restrict__ SUi) {
     for (int li = lps + threadIdx.x; li < ps; li += blockDim.x) {
-        if (SLi) SLi[rows_off(li) * npad + k] = TS(1);
-        if (SUi) SUi[rows_off(ps - 1 - li) * npad + k] = TS(1);
+        if (SLi) SLi[rows_off(li, e) * npad + k] = TS(1);
+        if (SUi) SUi[rows_off(ps - 1 - li, e) * npad + k] = TS(1);
     }
 }
 
@@ -436,6 +438,34 @@ timeout:
     ring.drain(c, p.err);
 }
 
+// Shared-memory loads issued in program order: a tile's coefficient and y
+// loads all go out before its multiply-adds, so one warp per SM sub-partition
+// (large partsizes have few partitions) waits for them once per 8 slots.
+__device__ __forceinline__ double lds_t(const double* p) {
+    double v;
+    asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"(hsdev::smem_u32(p)) : "memory");
+    return v;
+}
+__device__ __forceinline__ float lds_t(const float* p) {
+    float v;
+    asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(hsdev::smem_u32(p)) : "memory");
+    return v;
+}
+
+// acc += sum_{m<8} tl[m*32] * yy[m*S] in slot order, loads first.
+template <typename T, int S>
+__device__ __forceinline__ T fold8(T acc, const T* tl, const T* yy) {
+    T a[8], b[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        a[m] = lds_t(tl + m * 32);
+        b[m] = lds_t(yy + m * S);
+    }
+#pragma unroll
+    for (int m = 0; m < 8; ++m) acc = add_rn(acc, mul_rn(a[m], b[m]));
+    return acc;
+}
+
 // Ring for the rows kernel: like TileRing, but the elected lane keeps the
 // coordinates of the next tile to fetch and advances them by one per refill
 // (no division per tile: a refill is a few instructions).
@@ -506,11 +536,10 @@ struct RowRing {
 // slots are never added).  Symmetric: the D_Dl1 .* y scaling of a row is
 // applied when the backward sweep reaches it (the same product, before any
 // use).  y lives in shared memory ([row][lane], stride 33).
-template <typename T, typename IO, int SWEEP, int STAGES>
+template <typename T, typename IO, int SWEEP, int E, int STAGES>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32)
     l1gs_packed_rows_kernel(const __grid_constant__ CUtensorMap tmL, const __grid_constant__ CUtensorMap tmU,
                             const PackedParams p) {
-    constexpr int E = 8;
     constexpr int S = 33;
     extern __shared__ __align__(128) unsigned char smem[];
     const int warp = threadIdx.x >> 5;
@@ -568,14 +597,16 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
                     for (int m = 1; m < E; ++m)
                         if (m < len) acc = add_rn(acc, mul_rn(tl[m * 32], yk[(m - 1) * S]));
                 } else {
-                    T a[E - 1], b[E - 1];
+                    T a[7], b[7];
 #pragma unroll
-                    for (int m = 1; m < E; ++m) {
-                        a[m - 1] = tl[m * 32];
-                        b[m - 1] = yk[(m - 1) * S];
+                    for (int m = 1; m < 8; ++m) {
+                        a[m - 1] = lds_t(tl + m * 32);
+                        b[m - 1] = lds_t(yk + (m - 1) * S);
                     }
 #pragma unroll
-                    for (int m = 0; m < E - 1; ++m) acc = add_rn(acc, mul_rn(a[m], b[m]));
+                    for (int m = 0; m < 7; ++m) acc = add_rn(acc, mul_rn(a[m], b[m]));
+#pragma unroll
+                    for (int m0 = 8; m0 < E; m0 += 8) acc = fold8<T, S>(acc, tl + m0 * 32, yk + (m0 - 1) * S);
                 }
                 ring.release(t);
                 ++t;
@@ -584,14 +615,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
                     tl = ring.tile(t) + lane;
                     const T* yy = yk + (tr * E - 1) * S;
                     if (tr + 1 < nt || (len & (E - 1)) == 0) {
-                        T a[E], b[E];
 #pragma unroll
-                        for (int m = 0; m < E; ++m) {
-                            a[m] = tl[m * 32];
-                            b[m] = yy[m * S];
-                        }
-#pragma unroll
-                        for (int m = 0; m < E; ++m) acc = add_rn(acc, mul_rn(a[m], b[m]));
+                        for (int m0 = 0; m0 < E; m0 += 8) acc = fold8<T, S>(acc, tl + m0 * 32, yy + m0 * S);
                     } else {
                         const int cnt = len & (E - 1);
 #pragma unroll
@@ -621,14 +646,16 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
                     for (int m = 1; m < E; ++m)
                         if (m < len) acc = add_rn(acc, mul_rn(tl[m * 32], yy0[m * S]));
                 } else {
-                    T a[E - 1], b[E - 1];
+                    T a[7], b[7];
 #pragma unroll
-                    for (int m = 1; m < E; ++m) {
-                        a[m - 1] = tl[m * 32];
-                        b[m - 1] = yy0[m * S];
+                    for (int m = 1; m < 8; ++m) {
+                        a[m - 1] = lds_t(tl + m * 32);
+                        b[m - 1] = lds_t(yy0 + m * S);
                     }
 #pragma unroll
-                    for (int m = 0; m < E - 1; ++m) acc = add_rn(acc, mul_rn(a[m], b[m]));
+                    for (int m = 0; m < 7; ++m) acc = add_rn(acc, mul_rn(a[m], b[m]));
+#pragma unroll
+                    for (int m0 = 8; m0 < E; m0 += 8) acc = fold8<T, S>(acc, tl + m0 * 32, yy0 + m0 * S);
                 }
                 ring.release(t);
                 ++t;
@@ -637,14 +664,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
                     tl = ring.tile(t) + lane;
                     const T* yy = yy0 + (tr * E) * S;
                     if (tr + 1 < nt || (len & (E - 1)) == 0) {
-                        T a[E], b[E];
 #pragma unroll
-                        for (int m = 0; m < E; ++m) {
-                            a[m] = tl[m * 32];
-                            b[m] = yy[m * S];
-                        }
-#pragma unroll
-                        for (int m = 0; m < E; ++m) acc = add_rn(acc, mul_rn(a[m], b[m]));
+                        for (int m0 = 0; m0 < E; m0 += 8) acc = fold8<T, S>(acc, tl + m0 * 32, yy + m0 * S);
                     } else {
                         const int cnt = len & (E - 1);
 #pragma unroll
@@ -855,6 +876,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) l1gs_view_lanes_kernel(co
     uint16_t* uoff = loff + (ps + 1) * 32;
     uint16_t* lcol = uoff + (ps + 1) * 32;
     uint16_t* ucol = lcol + p.cap_lo * 32;
+    int32_t* cntl = reinterpret_cast<int32_t*>(
+        (reinterpret_cast<uintptr_t>(ucol + p.cap_up * 32) + 3) & ~uintptr_t(3));   // running list counts
+    int32_t* cntu = cntl + 32;
     const int32_t* __restrict__ rp = p.rp;
     const int32_t* __restrict__ ci = p.ci;
     const T* __restrict__ v = static_cast<const T*>(p.v);
@@ -865,63 +889,121 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) l1gs_view_lanes_kernel(co
     const int wpb = blockDim.x >> 5;
     for (int64_t g = (int64_t)blockIdx.x * wpb + warp; g < p.ngroups; g += (int64_t)gridDim.x * wpb) {
         const int64_t rowbase = g * 32 * (int64_t)ps;
-        // pass 1: stage x and D_Dl1, count in-block entries per row
-        for (int t = lane; t < 32 * ps; t += 32) {
-            const int pp = t / ps, li = t % ps;
-            const int64_t i = rowbase + t;
+        // List building, 32 consecutive rows at a time (one per lane): each
+        // lane loads its row's entries (8 at a time, all in flight) once,
+        // in-block entries get list slots from a segmented warp scan (the
+        // lanes of one partition are contiguous), and are written in row
+        // order, storage order within a row -- the reference's order.
+        if (lane < 32) {
+            cntl[lane] = 0;
+            cntu[lane] = 0;
+        }
+        __syncwarp();
+        int pp = lane / ps, li = lane - (lane / ps) * ps;
+        for (int m = 0; m < ps; ++m) {
+            const int64_t i = rowbase + 32 * m + lane;
             const bool valid = i < p.n;
             ys[li * S + pp] = valid ? (T)x[i] : T(0);
             ds[li * S + pp] = valid ? D[i] : T(1);
-            int cl = 0, cu = 0;
+            const int64_t s0 = rowbase + (int64_t)pp * ps;
+            const int64_t e0 = min(s0 + ps - 1, (int64_t)p.n - 1);
+            int32_t q0 = 0, q1 = 0;
             if (valid) {
-                const int64_t s0 = rowbase + (int64_t)pp * ps;
-                const int64_t e0 = min(s0 + ps - 1, (int64_t)p.n - 1);
-                const int32_t q1 = rp[i + 1];
-                for (int32_t q = rp[i]; q < q1; ++q) {
-                    const int64_t j = ci[q];
-                    cl += (want_lo && j >= s0 && j < i);
-                    cu += (want_up && j > i && j <= e0);
-                }
+                q0 = __ldg(rp + i);
+                q1 = __ldg(rp + i + 1);
             }
-            loff[(li + 1) * 32 + pp] = (uint16_t)cl;
-            uoff[(li + 1) * 32 + pp] = (uint16_t)cu;
-        }
-        __syncwarp();
-        {   // per-partition exclusive prefix over its rows
-            uint16_t al = 0, au = 0;
-            loff[lane] = 0;
-            uoff[lane] = 0;
-            for (int li = 1; li <= ps; ++li) {
-                al = (uint16_t)(al + loff[li * 32 + lane]);
-                au = (uint16_t)(au + uoff[li * 32 + lane]);
-                loff[li * 32 + lane] = al;
-                uoff[li * 32 + lane] = au;
-            }
-        }
-        __syncwarp();
-        // pass 2: write the entries
-        for (int t = lane; t < 32 * ps; t += 32) {
-            const int pp = t / ps, li = t % ps;
-            const int64_t i = rowbase + t;
-            if (i < p.n) {
-                const int64_t s0 = rowbase + (int64_t)pp * ps;
-                const int64_t e0 = min(s0 + ps - 1, (int64_t)p.n - 1);
-                int wl = loff[li * 32 + pp], wu = uoff[li * 32 + pp];
-                const int32_t q1 = rp[i + 1];
-                for (int32_t q = rp[i]; q < q1; ++q) {
-                    const int64_t j = ci[q];
-                    if (want_lo && j >= s0 && j < i) {
-                        lval[wl * 32 + pp] = v[q];
-                        lcol[wl * 32 + pp] = (uint16_t)(j - s0);
-                        ++wl;
-                    } else if (want_up && j > i && j <= e0) {
-                        uval[wu * 32 + pp] = v[q];
-                        ucol[wu * 32 + pp] = (uint16_t)(j - s0);
-                        ++wu;
+            // phase A: count (the first 8 entries stay in registers)
+            int32_t cfirst[8];
+            T vfirst[8];
+            int cl = 0, cu = 0;
+            for (int32_t qb = q0; qb < q1; qb += 8) {
+                int32_t c8[8];
+                T v8[8];
+#pragma unroll
+                for (int k = 0; k < 8; ++k)
+                    if (qb + k < q1) {
+                        c8[k] = __ldg(ci + qb + k);
+                        v8[k] = __ldg(v + qb + k);
                     }
+#pragma unroll
+                for (int k = 0; k < 8; ++k)
+                    if (qb + k < q1) {
+                        const int64_t j = c8[k];
+                        cl += (want_lo && j >= s0 && j < i);
+                        cu += (want_up && j > i && j <= e0);
+                        if (qb == q0) {
+                            cfirst[k] = c8[k];
+                            vfirst[k] = v8[k];
+                        }
+                    }
+            }
+            // phase B: slots = running count of the partition + exclusive prefix over its lanes
+            const unsigned seg = __match_any_sync(0xffffffffu, pp);
+            const int first = __ffs(seg) - 1, last = 31 - __clz(seg);
+            int il = cl, iu = cu;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int tl = __shfl_up_sync(0xffffffffu, il, o);
+                const int tu = __shfl_up_sync(0xffffffffu, iu, o);
+                if (lane >= o) {
+                    il += tl;
+                    iu += tu;
                 }
             }
+            const int basel = __shfl_sync(0xffffffffu, il - cl, first);
+            const int baseu = __shfl_sync(0xffffffffu, iu - cu, first);
+            int wl = cntl[pp] + (il - cl) - basel;
+            int wu = cntu[pp] + (iu - cu) - baseu;
+            loff[li * 32 + pp] = (uint16_t)wl;
+            uoff[li * 32 + pp] = (uint16_t)wu;
+            __syncwarp();
+            if (lane == last) {
+                cntl[pp] += il - basel;
+                cntu[pp] += iu - baseu;
+            }
+            __syncwarp();
+            // phase C: write the in-block entries in storage order
+            for (int32_t qb = q0; qb < q1; qb += 8) {
+                int32_t c8[8];
+                T v8[8];
+                if (qb == q0) {
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) {
+                        c8[k] = cfirst[k];
+                        v8[k] = vfirst[k];
+                    }
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 8; ++k)
+                        if (qb + k < q1) {
+                            c8[k] = __ldg(ci + qb + k);
+                            v8[k] = __ldg(v + qb + k);
+                        }
+                }
+#pragma unroll
+                for (int k = 0; k < 8; ++k)
+                    if (qb + k < q1) {
+                        const int64_t j = c8[k];
+                        if (want_lo && j >= s0 && j < i) {
+                            lval[wl * 32 + pp] = v8[k];
+                            lcol[wl * 32 + pp] = (uint16_t)(j - s0);
+                            ++wl;
+                        } else if (want_up && j > i && j <= e0) {
+                            uval[wu * 32 + pp] = v8[k];
+                            ucol[wu * 32 + pp] = (uint16_t)(j - s0);
+                            ++wu;
+                        }
+                    }
+            }
+            li += 32;
+            while (li >= ps) {
+                li -= ps;
+                ++pp;
+            }
         }
+        __syncwarp();
+        loff[ps * 32 + lane] = (uint16_t)cntl[lane];
+        uoff[ps * 32 + lane] = (uint16_t)cntu[lane];
         __syncwarp();
         // serial recurrence per lane (partition g*32 + lane)
         const int64_t k = g * 32 + lane;
@@ -970,7 +1052,7 @@ struct hs_l1gs_s {
     int32_t n = 0, ps = 0, nparts = 0, ngroups = 0, nchunks = 0, chunksize = 0;
     int64_t npad = 0, tlen = 0, S = 0;
     int64_t tstore = 0;      // stream slots per direction (tlen, or rows_off(ps) in the rows layout)
-    int32_t rows_layout = 0; // packed partsize > 32: row-aligned streams with D_Dl1 inside
+    int32_t rows_layout = 0; // packed partsize > 32: tile width of the row-aligned streams (0: classic)
     int32_t sweep = 0, cache = 0, is_sym = 0, format = 0, mdt = 0, sdt = 0;
     double eta = 1.5;
     void* D = nullptr;
@@ -1138,7 +1220,7 @@ int setup_device(hs_l1gs* P, const int32_t* rp_h, const int32_t* ci_h, const TM*
     if (packed && P->rows_layout) {
         const int32_t lps = (int32_t)((int64_t)n - (int64_t)(P->nparts - 1) * P->ps);
         if (lps < P->ps) {
-            rows_tail_kernel<TS><<<1, 256, 0, st>>>(P->ps, lps, P->npad, P->nparts - 1, SLi, SUi);
+            rows_tail_kernel<TS><<<1, 256, 0, st>>>(P->ps, lps, P->npad, P->nparts - 1, P->rows_layout, SLi, SUi);
             HS_LAUNCH_CHECK("rows_tail_kernel");
         }
     }
@@ -1185,6 +1267,32 @@ int setup_device(hs_l1gs* P, const int32_t* rp_h, const int32_t* ci_h, const TM*
     }
     HS_CUDA(cudaStreamSynchronize(st));
     return HS_OK;
+}
+
+// Ring depth of the rows kernel.  A warp serves 32 partitions and keeps its
+// y slice (ps x 33 values) and its ring in shared memory, so the depth sets
+// how many warps fit on an SM; large partsizes have few partitions, so pick
+// the depth that needs the fewest rounds of warps over the groups, then the
+// deepest ring among those.
+inline int rows_stages(int ps, int E, size_t es, int64_t ngroups) {
+    const int cand8[] = {4, 8, 16}, cand32[] = {4, 8};
+    const int* cand = E == 32 ? cand32 : cand8;
+    const int ncand = E == 32 ? 2 : 3;
+    const int64_t sms = hs::num_sms();
+    int best = cand[0];
+    int64_t best_rounds = INT64_MAX;
+    for (int c = 0; c < ncand; ++c) {
+        const int64_t wb = ((int64_t)E * 32 * es * cand[c] + 8 * cand[c] + (int64_t)ps * 33 * es + 127) / 128 * 128;
+        const int64_t wpb = std::max<int64_t>(1, std::min<int64_t>(kWarpsPerBlock, (200 * 1024) / wb));
+        const int64_t per_sm = 233472 / (wpb * wb + 1024);
+        if (per_sm < 1) continue;
+        const int64_t rounds = (ngroups + sms * per_sm * wpb - 1) / (sms * per_sm * wpb);
+        if (rounds <= best_rounds) {
+            best_rounds = rounds;
+            best = cand[c];
+        }
+    }
+    return best;
 }
 
 // Tile geometry of the packed stream: E rows x 32 lanes per TMA tile, STAGES
@@ -1279,10 +1387,9 @@ int launch_packed_t(hs_l1gs* P, const void* x, void* y, cudaStream_t st) {
                                 (uint32_t)(P->ps * 33 * sizeof(T)), st, &cfg);
 }
 
-// Row-aligned streams (partsize > 32): 8-slot tiles, ring of 8 or 16 stages.
-template <typename T, typename IO, int SWEEP, int STAGES>
+// Row-aligned streams (partsize > 32): E-slot tiles (8 or 32), a ring of STAGES.
+template <typename T, typename IO, int SWEEP, int E, int STAGES>
 int launch_rows_stages(hs_l1gs* P, const void* x, void* y, cudaStream_t st) {
-    constexpr int E = 8;
     PackedParams p;
     p.n = P->n;
     p.ps = P->ps;
@@ -1298,15 +1405,19 @@ int launch_rows_stages(hs_l1gs* P, const void* x, void* y, cudaStream_t st) {
     p.err = P->err_word;
     p.ring_bytes = (uint32_t)(E * 32 * sizeof(T) * STAGES);
     static thread_local int cfg = -1;
-    return launch_packed_kernel(l1gs_packed_rows_kernel<T, IO, SWEEP, STAGES>, P, p,
+    return launch_packed_kernel(l1gs_packed_rows_kernel<T, IO, SWEEP, E, STAGES>, P, p,
                                 (uint32_t)(P->ps * 33 * sizeof(T)), st, &cfg);
 }
 
 template <typename T, typename IO, int SWEEP>
 int launch_rows_t(hs_l1gs* P, const void* x, void* y, cudaStream_t st) {
-    if (P->stages == 8) return launch_rows_stages<T, IO, SWEEP, 8>(P, x, y, st);
-    if (P->stages == 32) return launch_rows_stages<T, IO, SWEEP, 32>(P, x, y, st);
-    return launch_rows_stages<T, IO, SWEEP, 16>(P, x, y, st);
+    if (P->rows_layout == 32) {
+        if (P->stages == 4) return launch_rows_stages<T, IO, SWEEP, 32, 4>(P, x, y, st);
+        return launch_rows_stages<T, IO, SWEEP, 32, 8>(P, x, y, st);
+    }
+    if (P->stages == 4) return launch_rows_stages<T, IO, SWEEP, 8, 4>(P, x, y, st);
+    if (P->stages == 16) return launch_rows_stages<T, IO, SWEEP, 8, 16>(P, x, y, st);
+    return launch_rows_stages<T, IO, SWEEP, 8, 8>(P, x, y, st);
 }
 
 template <typename T, typename IO, int SWEEP>
@@ -1361,7 +1472,7 @@ int launch_view_t(hs_l1gs* P, const void* x, void* y, cudaStream_t st) {
         const size_t ps = (size_t)P->ps;
         const size_t lanes_bytes = (sizeof(T) * (2 * ps * 33 + 32 * (size_t)(P->cap_lo + P->cap_up)) +
                                     sizeof(uint16_t) * (2 * (ps + 1) * 32 + 32 * (size_t)(P->cap_lo + P->cap_up)) +
-                                    127) / 128 * 128;
+                                    4 + 2 * 32 * sizeof(int32_t) + 127) / 128 * 128;
         if (lanes_bytes <= 100 * 1024 && P->cap_lo < 65535 && P->cap_up < 65535)
             return launch_view_lanes<T, IO, SWEEP>(P, x, y, st, lanes_bytes);
     }
@@ -1423,13 +1534,14 @@ void unpack_reference(const hs_l1gs* P, const TS* inter, TS* out, bool lower) {
         for (int64_t li = 0; li < aps; ++li) {
             if (lower) {
                 for (int64_t lj = 0; lj < li; ++lj) {
-                    const int64_t e = P->rows_layout ? rows_off(li) + 1 + lj : lo_idx(li, lj);
+                    const int64_t e = P->rows_layout ? rows_off(li, P->rows_layout) + 1 + lj : lo_idx(li, lj);
                     out[boff + li * (li - 1) / 2 + lj] = inter[e * P->npad + k];
                 }
             } else {
                 const int64_t row_start = li * aps - li * (li + 1) / 2;
                 for (int64_t lj = li + 1; lj < aps; ++lj) {
-                    const int64_t e = P->rows_layout ? rows_off(ps - 1 - li) + (lj - li) : up_idx(ps, li, lj);
+                    const int64_t e =
+                        P->rows_layout ? rows_off(ps - 1 - li, P->rows_layout) + (lj - li) : up_idx(ps, li, lj);
                     out[boff + row_start + (lj - li) - 1] = inter[e * P->npad + k];
                 }
             }
@@ -1489,8 +1601,10 @@ int l1gs_create_impl(const hs_sparse* A, bool on_device, int32_t partsize, int32
     P->npad = ((int64_t)P->nparts + 31) / 32 * 32;
     P->ngroups = (int32_t)(P->npad / 32);
     P->tlen = (int64_t)partsize * (partsize - 1) / 2;
-    P->rows_layout = (cache == HS_CACHE_PACKED && partsize > 32) ? 1 : 0;
-    P->tstore = P->rows_layout ? rows_off(partsize) : P->tlen;
+    // Row-aligned streams for partsize > 32: 8-slot tiles up to 96 (little
+    // padding), 32-slot tiles beyond (per-tile overhead spread over 32 slots).
+    P->rows_layout = (cache == HS_CACHE_PACKED && partsize > 32) ? (partsize <= 96 ? 8 : 32) : 0;
+    P->tstore = P->rows_layout ? rows_off(partsize, P->rows_layout) : P->tlen;
     const int64_t lps = (int64_t)A->n - (int64_t)(P->nparts - 1) * partsize;
     P->S = P->tlen * (P->nparts - 1) + lps * (lps - 1) / 2;
     P->nchunks = blocks;  // _blockpartitioning for KA.GPU (:353-365)
@@ -1542,13 +1656,14 @@ int l1gs_create_impl(const hs_sparse* A, bool on_device, int32_t partsize, int32
     }
     if (cache == HS_CACHE_PACKED) {
         pick_tile(partsize, smoother_dtype, &P->E, &P->stages, &P->minb);
-        if (P->rows_layout) {   // one 8-slot tile per row segment; deeper ring (fewer warps per SM)
-            P->E = 8;
-            P->stages = partsize <= 96 ? 8 : 16;
-            // Tuning override: HSB200_ROWS_STAGES = 8, 16 or 32 tiles in flight per warp.
+        if (P->rows_layout) {   // one tile per row segment
+            P->E = P->rows_layout;
+            P->stages = rows_stages(P->ps, P->E, dsize(smoother_dtype), P->ngroups);
+            // Tuning override: HSB200_ROWS_STAGES = tiles in flight per warp
+            // (4 or 8 with 32-slot tiles, 4, 8 or 16 with 8-slot tiles).
             if (const char* env = getenv("HSB200_ROWS_STAGES")) {
                 const int st = atoi(env);
-                if (st == 8 || st == 16 || st == 32) P->stages = st;
+                if (st == 4 || st == 8 || (P->E == 8 && st == 16)) P->stages = st;
             }
         }
         const uint32_t E = (uint32_t)P->E;
