@@ -191,7 +191,7 @@ def test_random_bitwise_fp64(ps, n, sweep, cache):
             np.testing.assert_array_equal(P.SUbuffer, ref.SU)
 
 
-@pytest.mark.parametrize("ps", [2, 16, 33, 64])
+@pytest.mark.parametrize("ps", [2, 16, 33, 64, 130])
 @pytest.mark.parametrize("sweep", ["forward", "symmetric"])
 @pytest.mark.parametrize("cache", ["packed", "view"])
 def test_fp32_and_mixed_bitwise(ps, sweep, cache):
