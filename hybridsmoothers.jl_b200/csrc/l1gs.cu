@@ -1336,8 +1336,15 @@ int launch_packed_kernel(KERN kern, hs_l1gs* P, PackedParams& p, uint32_t extra_
         int per_sm = 0;
         HS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, wpb * 32, smem));
         if (per_sm < 1) return hs::set_error(HS_ERR_UNSUPPORTED, "partsize %d needs too much shared memory", P->ps);
-        const int64_t want = (P->ngroups + wpb - 1) / wpb;
-        P->launch_grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)per_sm * hs::num_sms()));
+        // Every warp streams whole groups; size the grid so all warps get the
+        // same number of groups (the fewest rounds the resident warps allow),
+        // instead of a last round that only some warps run.
+        const int64_t slots = (int64_t)per_sm * hs::num_sms() * wpb;
+        const int64_t rounds = std::max<int64_t>(1, (P->ngroups + slots - 1) / slots);
+        int64_t grid = (P->ngroups + rounds * wpb - 1) / (rounds * wpb);
+        if (const char* env = getenv("HSB200_GRID_FULL"))   // tuning: one block per resident slot
+            if (atoi(env) == 1) grid = (P->ngroups + wpb - 1) / wpb;
+        P->launch_grid = (int)std::max<int64_t>(1, std::min<int64_t>(grid, (int64_t)per_sm * hs::num_sms()));
         P->launch_key = key;
         P->launch_kernel = (const void*)kern;
     }
