@@ -1321,9 +1321,10 @@ inline void pick_tile(int ps, int sdt, int* E, int* stages, int* minb) {
 
 
 template <typename KERN>
-int launch_packed_kernel(KERN kern, hs_l1gs* P, PackedParams& p, uint32_t extra_bytes, cudaStream_t st,
-                         int* configured_smem) {
-    p.warp_bytes = (p.ring_bytes + 8 * 8 + extra_bytes + 127) / 128 * 128;
+int launch_packed_kernel(KERN kern, hs_l1gs* P, PackedParams& p, int stages, bool balanced, uint32_t extra_bytes,
+                         cudaStream_t st, int* configured_smem) {
+    // per warp: the tile ring, one mbarrier per stage, then the kernel's slice
+    p.warp_bytes = (p.ring_bytes + 8 * stages + extra_bytes + 127) / 128 * 128;
     const int wpb = (int)std::max<int64_t>(1, std::min<int64_t>(kWarpsPerBlock, (200 * 1024) / p.warp_bytes));
     const size_t smem = (size_t)p.warp_bytes * wpb;
     // The launch shape depends only on the handle and the io type: compute it once.
@@ -1336,14 +1337,18 @@ int launch_packed_kernel(KERN kern, hs_l1gs* P, PackedParams& p, uint32_t extra_
         int per_sm = 0;
         HS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, wpb * 32, smem));
         if (per_sm < 1) return hs::set_error(HS_ERR_UNSUPPORTED, "partsize %d needs too much shared memory", P->ps);
-        // Every warp streams whole groups; size the grid so all warps get the
-        // same number of groups (the fewest rounds the resident warps allow),
-        // instead of a last round that only some warps run.
+        // Every warp streams whole groups.  Balanced: size the grid so all
+        // warps get the same number of groups (the fewest rounds the resident
+        // warps allow) instead of a last round that only some warps run -- the
+        // better shape when the stream is bandwidth-bound (FP64 coefficients).
+        // Otherwise one block per resident slot: FP32 streams move half the
+        // bytes per instruction and gain more from the extra warps in flight.
+        if (const char* env = getenv("HSB200_GRID_FULL"))   // tuning override: 1 = full, 0 = balanced
+            balanced = atoi(env) != 1;
         const int64_t slots = (int64_t)per_sm * hs::num_sms() * wpb;
         const int64_t rounds = std::max<int64_t>(1, (P->ngroups + slots - 1) / slots);
-        int64_t grid = (P->ngroups + rounds * wpb - 1) / (rounds * wpb);
-        if (const char* env = getenv("HSB200_GRID_FULL"))   // tuning: one block per resident slot
-            if (atoi(env) == 1) grid = (P->ngroups + wpb - 1) / wpb;
+        const int64_t grid = balanced ? (P->ngroups + rounds * wpb - 1) / (rounds * wpb)
+                                      : (P->ngroups + wpb - 1) / wpb;
         P->launch_grid = (int)std::max<int64_t>(1, std::min<int64_t>(grid, (int64_t)per_sm * hs::num_sms()));
         P->launch_key = key;
         P->launch_kernel = (const void*)kern;
@@ -1374,7 +1379,7 @@ int launch_packed_t(hs_l1gs* P, const void* x, void* y, cudaStream_t st) {
         static thread_local int cfg = -1;                                                                \
         constexpr int XS = (PSV % 2 == 0) ? PSV + 1 : PSV;                                               \
         return launch_packed_kernel(l1gs_packed_small_kernel<T, IO, SWEEP, PSV, E, STAGES, MB>, P, p,    \
-                                    (uint32_t)(32 * XS * sizeof(T)), st, &cfg);                          \
+                                    STAGES, sizeof(T) == 8, (uint32_t)(32 * XS * sizeof(T)), st, &cfg);  \
     }
     if constexpr (STAGES == 4) {
         switch (P->ps) {
@@ -1390,7 +1395,7 @@ int launch_packed_t(hs_l1gs* P, const void* x, void* y, cudaStream_t st) {
     }
 #undef HS_SMALL
     static thread_local int cfg = -1;
-    return launch_packed_kernel(l1gs_packed_kernel<T, IO, SWEEP, E, STAGES>, P, p,
+    return launch_packed_kernel(l1gs_packed_kernel<T, IO, SWEEP, E, STAGES>, P, p, STAGES, sizeof(T) == 8,
                                 (uint32_t)(P->ps * 33 * sizeof(T)), st, &cfg);
 }
 
@@ -1412,7 +1417,7 @@ int launch_rows_stages(hs_l1gs* P, const void* x, void* y, cudaStream_t st) {
     p.err = P->err_word;
     p.ring_bytes = (uint32_t)(E * 32 * sizeof(T) * STAGES);
     static thread_local int cfg = -1;
-    return launch_packed_kernel(l1gs_packed_rows_kernel<T, IO, SWEEP, E, STAGES>, P, p,
+    return launch_packed_kernel(l1gs_packed_rows_kernel<T, IO, SWEEP, E, STAGES>, P, p, STAGES, sizeof(T) == 8,
                                 (uint32_t)(P->ps * 33 * sizeof(T)), st, &cfg);
 }
 
