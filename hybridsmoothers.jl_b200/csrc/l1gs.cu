@@ -133,7 +133,7 @@ __global__ void convert_kernel(const TA* __restrict__ a, TB* __restrict__ b, int
 struct PackedParams {
     int32_t n, ps, nparts;
     int64_t npad;
-    int32_t ngroups;
+    int32_t gbeg, ngroups;   // groups [gbeg, ngroups) of this launch
     int32_t tlen;      // ps(ps-1)/2 stream elements per direction
     int32_t ntiles;    // ceil(tlen / E) tiles per direction
     const void* Di;
@@ -225,7 +225,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, MINB)
     ring.tmU = &tmU;
     ring.buf = reinterpret_cast<T*>(wbase);
     ring.bars = reinterpret_cast<uint64_t*>(wbase + p.ring_bytes);
-    ring.g0 = blockIdx.x * wpb + warp;
+    ring.g0 = p.gbeg + blockIdx.x * wpb + warp;
     ring.gstride = gridDim.x * wpb;
     ring.ntiles = NT;
     ring.lane = lane;
@@ -326,7 +326,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
     ring.tmU = &tmU;
     ring.buf = reinterpret_cast<T*>(wbase);
     ring.bars = reinterpret_cast<uint64_t*>(wbase + p.ring_bytes);
-    ring.g0 = blockIdx.x * wpb + warp;
+    ring.g0 = p.gbeg + blockIdx.x * wpb + warp;
     ring.gstride = gridDim.x * wpb;
     ring.ntiles = p.ntiles;
     ring.lane = lane;
@@ -551,7 +551,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
     const int ps = p.ps;
 
     const int wpb = blockDim.x >> 5;
-    const int32_t g0 = blockIdx.x * wpb + warp, gstride = gridDim.x * wpb;
+    const int32_t g0 = p.gbeg + blockIdx.x * wpb + warp, gstride = gridDim.x * wpb;
     RowRing<T, E, STAGES, SWEEP> ring;
     ring.tmL = &tmL;
     ring.tmU = &tmU;
@@ -709,7 +709,7 @@ timeout:
 // scanning its rows in global memory instead (same arithmetic).
 // ---------------------------------------------------------------------------
 struct ViewParams {
-    int32_t n, ps, nparts;
+    int32_t n, ps, kbeg, nparts;   // partitions [kbeg, nparts) of this launch
     const int32_t* rp;
     const int32_t* ci;
     const void* v;
@@ -745,7 +745,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) l1gs_view_kernel(const Vi
     const bool want_lo = SWEEP != 1, want_up = SWEEP != 0;
 
     const int wpb = blockDim.x >> 5;
-    for (int64_t k = (int64_t)blockIdx.x * wpb + warp; k < p.nparts; k += (int64_t)gridDim.x * wpb) {
+    for (int64_t k = p.kbeg + (int64_t)blockIdx.x * wpb + warp; k < p.nparts; k += (int64_t)gridDim.x * wpb) {
         const int64_t s = k * ps;
         const int64_t e = min(s + ps - 1, (int64_t)p.n - 1);
         const int aps = (int)(e - s + 1);
@@ -847,8 +847,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) l1gs_view_kernel(const Vi
 // memory, laid out [entry][lane] so each lane's reads are conflict-free and in
 // the reference's order (rows ascending, columns ascending within a row); then
 // each lane runs the serial row recurrence of its own partition.
+constexpr int kViewStage = 256;   // entries of one 32-row step staged in shared memory
+
 struct ViewLanesParams {
-    int32_t n, ps, nparts, ngroups;
+    int32_t n, ps, nparts, gbeg, ngroups;   // groups [gbeg, ngroups) of this launch
     const int32_t* rp;
     const int32_t* ci;
     const void* v;
@@ -869,8 +871,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) l1gs_view_lanes_kernel(co
     const bool want_lo = SWEEP != 1, want_up = SWEEP != 0;
     unsigned char* w = smem + (size_t)warp * p.warp_bytes;
     T* ys = reinterpret_cast<T*>(w);
-    T* ds = ys + ps * S;
-    T* lval = ds + ps * S;
+    T* lval = ys + ps * S;
     T* uval = lval + p.cap_lo * 32;
     uint16_t* loff = reinterpret_cast<uint16_t*>(uval + p.cap_up * 32);
     uint16_t* uoff = loff + (ps + 1) * 32;
@@ -879,6 +880,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) l1gs_view_lanes_kernel(co
     int32_t* cntl = reinterpret_cast<int32_t*>(
         (reinterpret_cast<uintptr_t>(ucol + p.cap_up * 32) + 3) & ~uintptr_t(3));   // running list counts
     int32_t* cntu = cntl + 32;
+    int32_t* sci = cntu + 32;   // one step's entries (kViewStage)
+    T* sv = reinterpret_cast<T*>((reinterpret_cast<uintptr_t>(sci + kViewStage) + 7) & ~uintptr_t(7));
     const int32_t* __restrict__ rp = p.rp;
     const int32_t* __restrict__ ci = p.ci;
     const T* __restrict__ v = static_cast<const T*>(p.v);
@@ -887,7 +890,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) l1gs_view_lanes_kernel(co
     IO* __restrict__ y = static_cast<IO*>(p.y);
 
     const int wpb = blockDim.x >> 5;
-    for (int64_t g = (int64_t)blockIdx.x * wpb + warp; g < p.ngroups; g += (int64_t)gridDim.x * wpb) {
+    for (int64_t g = p.gbeg + (int64_t)blockIdx.x * wpb + warp; g < p.ngroups; g += (int64_t)gridDim.x * wpb) {
         const int64_t rowbase = g * 32 * (int64_t)ps;
         // List building, 32 consecutive rows at a time (one per lane): each
         // lane loads its row's entries (8 at a time, all in flight) once,
@@ -899,43 +902,88 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) l1gs_view_lanes_kernel(co
             cntu[lane] = 0;
         }
         __syncwarp();
+        // Row pointers of steps m, m+1, m+2 in registers (lane l: row
+        // rowbase + 32 m + l; rows past n clamp to rp[n]), loaded three steps ahead.
+        auto rp_of = [&](int m) -> int32_t { return __ldg(rp + min(rowbase + 32 * m + lane, (int64_t)p.n)); };
+        int32_t r0 = rp_of(0), r1 = rp_of(1), r2 = rp_of(2);
+        // Step m handles rows rowbase + 32 m + lane.  Its entries are the
+        // contiguous range [qs, qe) of its first and the next step's first row
+        // pointer; they are loaded coalesced (lane e takes entries e, e + 32, ...)
+        // one step ahead into registers and dropped into the warp's staging
+        // buffer, from which every lane then scans its own row.  A step with
+        // more than kViewStage entries reads its rows from global memory instead
+        // (same order).
+        int32_t pc[kViewStage / 32];
+        T pv[kViewStage / 32];
+        T px = T(0);
+        auto fetch = [&](int m, int32_t qs, int32_t qe) {
+            if (m >= ps) return;
+            const int32_t cnt = qe - qs;
+            if (cnt <= kViewStage) {
+#pragma unroll
+                for (int k = 0; k < kViewStage / 32; ++k) {
+                    const int32_t e = k * 32 + lane;
+                    if (e < cnt) {
+                        pc[k] = __ldg(ci + qs + e);
+                        pv[k] = __ldg(v + qs + e);
+                    }
+                }
+            }
+            const int64_t i = rowbase + 32 * m + lane;
+            if (i < p.n) px = (T)x[i];
+        };
+        fetch(0, __shfl_sync(0xffffffffu, r0, 0), __shfl_sync(0xffffffffu, r1, 0));
         int pp = lane / ps, li = lane - (lane / ps) * ps;
         for (int m = 0; m < ps; ++m) {
             const int64_t i = rowbase + 32 * m + lane;
             const bool valid = i < p.n;
-            ys[li * S + pp] = valid ? (T)x[i] : T(0);
-            ds[li * S + pp] = valid ? D[i] : T(1);
+            const int32_t r3 = rp_of(m + 3);
+            const int32_t qs = __shfl_sync(0xffffffffu, r0, 0), qe = __shfl_sync(0xffffffffu, r1, 0);
+            const int32_t cnt = qe - qs;
+            const bool staged = cnt <= kViewStage;
+            if (staged) {
+#pragma unroll
+                for (int k = 0; k < kViewStage / 32; ++k) {
+                    const int32_t e = k * 32 + lane;
+                    if (e < cnt) {
+                        sci[e] = pc[k];
+                        sv[e] = pv[k];
+                    }
+                }
+            }
+            ys[li * S + pp] = valid ? px : T(0);
+            __syncwarp();
+            fetch(m + 1, qe, __shfl_sync(0xffffffffu, r2, 0));   // in flight while this step is processed
             const int64_t s0 = rowbase + (int64_t)pp * ps;
             const int64_t e0 = min(s0 + ps - 1, (int64_t)p.n - 1);
-            int32_t q0 = 0, q1 = 0;
-            if (valid) {
-                q0 = __ldg(rp + i);
-                q1 = __ldg(rp + i + 1);
-            }
-            // phase A: count (the first 8 entries stay in registers)
-            int32_t cfirst[8];
-            T vfirst[8];
+            int32_t q1 = __shfl_down_sync(0xffffffffu, r0, 1);
+            if (lane == 31) q1 = qe;
+            int32_t q0 = r0;
+            if (!valid) q0 = q1 = 0;
+            // entries q of this step at cb[q - qo] / vb[q - qo]: the staging, or global memory
+            const int32_t* cb = staged ? sci : ci;
+            const T* vb = staged ? sv : v;
+            const int32_t qo = staged ? qs : 0;
+            const int32_t ii = (int32_t)i, si = (int32_t)s0, ei = (int32_t)e0;
+            const int len = q1 - q0;
+            // phase A: in-block entries as bitmasks over the row's entries (rows of
+            // up to 32 entries), counted by popc; longer rows are counted in a loop
+            uint32_t mlo = 0, mup = 0;
             int cl = 0, cu = 0;
-            for (int32_t qb = q0; qb < q1; qb += 8) {
-                int32_t c8[8];
-                T v8[8];
-#pragma unroll
-                for (int k = 0; k < 8; ++k)
-                    if (qb + k < q1) {
-                        c8[k] = __ldg(ci + qb + k);
-                        v8[k] = __ldg(v + qb + k);
-                    }
-#pragma unroll
-                for (int k = 0; k < 8; ++k)
-                    if (qb + k < q1) {
-                        const int64_t j = c8[k];
-                        cl += (want_lo && j >= s0 && j < i);
-                        cu += (want_up && j > i && j <= e0);
-                        if (qb == q0) {
-                            cfirst[k] = c8[k];
-                            vfirst[k] = v8[k];
-                        }
-                    }
+            if (len <= 32) {
+                for (int b = 0; b < len; ++b) {
+                    const int32_t j = cb[q0 - qo + b];
+                    mlo |= (uint32_t)(want_lo && j >= si && j < ii) << b;
+                    mup |= (uint32_t)(want_up && j > ii && j <= ei) << b;
+                }
+                cl = __popc(mlo);
+                cu = __popc(mup);
+            } else {
+                for (int32_t q = q0; q < q1; ++q) {
+                    const int32_t j = cb[q - qo];
+                    cl += (want_lo && j >= si && j < ii);
+                    cu += (want_up && j > ii && j <= ei);
+                }
             }
             // phase B: slots = running count of the partition + exclusive prefix over its lanes
             const unsigned seg = __match_any_sync(0xffffffffu, pp);
@@ -961,40 +1009,40 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) l1gs_view_lanes_kernel(co
                 cntl[pp] += il - basel;
                 cntu[pp] += iu - baseu;
             }
-            __syncwarp();
-            // phase C: write the in-block entries in storage order
-            for (int32_t qb = q0; qb < q1; qb += 8) {
-                int32_t c8[8];
-                T v8[8];
-                if (qb == q0) {
-#pragma unroll
-                    for (int k = 0; k < 8; ++k) {
-                        c8[k] = cfirst[k];
-                        v8[k] = vfirst[k];
-                    }
-                } else {
-#pragma unroll
-                    for (int k = 0; k < 8; ++k)
-                        if (qb + k < q1) {
-                            c8[k] = __ldg(ci + qb + k);
-                            v8[k] = __ldg(v + qb + k);
-                        }
+            // phase C: write the in-block entries in storage order (set bits ascending)
+            if (len <= 32) {
+                while (mlo) {
+                    const int b = __ffs(mlo) - 1;
+                    mlo &= mlo - 1;
+                    lval[wl * 32 + pp] = vb[q0 - qo + b];
+                    lcol[wl * 32 + pp] = (uint16_t)(cb[q0 - qo + b] - si);
+                    ++wl;
                 }
-#pragma unroll
-                for (int k = 0; k < 8; ++k)
-                    if (qb + k < q1) {
-                        const int64_t j = c8[k];
-                        if (want_lo && j >= s0 && j < i) {
-                            lval[wl * 32 + pp] = v8[k];
-                            lcol[wl * 32 + pp] = (uint16_t)(j - s0);
-                            ++wl;
-                        } else if (want_up && j > i && j <= e0) {
-                            uval[wu * 32 + pp] = v8[k];
-                            ucol[wu * 32 + pp] = (uint16_t)(j - s0);
-                            ++wu;
-                        }
+                while (mup) {
+                    const int b = __ffs(mup) - 1;
+                    mup &= mup - 1;
+                    uval[wu * 32 + pp] = vb[q0 - qo + b];
+                    ucol[wu * 32 + pp] = (uint16_t)(cb[q0 - qo + b] - si);
+                    ++wu;
+                }
+            } else {
+                for (int32_t q = q0; q < q1; ++q) {
+                    const int32_t j = cb[q - qo];
+                    if (want_lo && j >= si && j < ii) {
+                        lval[wl * 32 + pp] = vb[q - qo];
+                        lcol[wl * 32 + pp] = (uint16_t)(j - si);
+                        ++wl;
+                    } else if (want_up && j > ii && j <= ei) {
+                        uval[wu * 32 + pp] = vb[q - qo];
+                        ucol[wu * 32 + pp] = (uint16_t)(j - si);
+                        ++wu;
                     }
+                }
             }
+            __syncwarp();   // staging and counts are rewritten by the next step
+            r0 = r1;
+            r1 = r2;
+            r2 = r3;
             li += 32;
             while (li >= ps) {
                 li -= ps;
@@ -1009,31 +1057,51 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) l1gs_view_lanes_kernel(co
         const int64_t k = g * 32 + lane;
         const int aps = k < p.nparts ? (int)min((int64_t)ps, (int64_t)p.n - k * ps) : 0;
         T* yk = ys + lane;
-        const T* dk = ds + lane;
+        const T* dk = D + k * ps;   // this lane's D_Dl1, loaded two rows ahead of use
         if (want_lo) {
+            int qa = loff[lane];
+            T d1 = aps > 0 ? __ldg(dk) : T(1), d2 = aps > 1 ? __ldg(dk + 1) : T(1);
             for (int li = 0; li < aps; ++li) {
+                const T d = d1;
+                d1 = d2;
+                if (li + 2 < aps) d2 = __ldg(dk + li + 2);
                 T acc = T(0);
-                const int q1 = loff[(li + 1) * 32 + lane];
-                for (int q = loff[li * 32 + lane]; q < q1; ++q)
+                const int qb = loff[(li + 1) * 32 + lane];
+                for (int q = qa; q < qb; ++q)
                     acc = add_rn(acc, mul_rn(lval[q * 32 + lane], yk[lcol[q * 32 + lane] * S]));
-                yk[li * S] = div_rn(sub_rn(yk[li * S], acc), dk[li * S]);
+                qa = qb;
+                yk[li * S] = div_rn(sub_rn(yk[li * S], acc), d);
             }
         }
-        if (SWEEP == 2)
-            for (int li = 0; li < aps; ++li) yk[li * S] = mul_rn(dk[li * S], yk[li * S]);
-        if (want_up) {
+        if (want_up) {   // symmetric: D_Dl1 .* y applied to a row when this sweep reaches it
+            int qb = aps > 0 ? uoff[aps * 32 + lane] : 0;
+            T d1 = aps > 0 ? __ldg(dk + aps - 1) : T(1), d2 = aps > 1 ? __ldg(dk + aps - 2) : T(1);
             for (int li = aps - 1; li >= 0; --li) {
+                const T d = d1;
+                d1 = d2;
+                if (li >= 2) d2 = __ldg(dk + li - 2);
+                T yi = yk[li * S];
+                if (SWEEP == 2) yi = mul_rn(d, yi);
                 T acc = T(0);
-                const int q1 = uoff[(li + 1) * 32 + lane];
-                for (int q = uoff[li * 32 + lane]; q < q1; ++q)
+                const int qa = uoff[li * 32 + lane];
+                for (int q = qa; q < qb; ++q)
                     acc = add_rn(acc, mul_rn(uval[q * 32 + lane], yk[ucol[q * 32 + lane] * S]));
-                yk[li * S] = div_rn(sub_rn(yk[li * S], acc), dk[li * S]);
+                qb = qa;
+                yk[li * S] = div_rn(sub_rn(yi, acc), d);
             }
         }
         __syncwarp();
-        for (int t = lane; t < 32 * ps; t += 32) {
-            const int64_t i = rowbase + t;
-            if (i < p.n) y[i] = (IO)ys[(t % ps) * S + t / ps];
+        {
+            int pp = lane / ps, li = lane - (lane / ps) * ps;
+            for (int t = lane; t < 32 * ps; t += 32) {
+                const int64_t i = rowbase + t;
+                if (i < p.n) y[i] = (IO)ys[li * S + pp];
+                li += 32;
+                while (li >= ps) {
+                    li -= ps;
+                    ++pp;
+                }
+            }
         }
         __syncwarp();
     }
@@ -1068,9 +1136,13 @@ struct hs_l1gs_s {
     alignas(64) CUtensorMap tmU;
     void* dev_x = nullptr;
     void* dev_y = nullptr;
+    // host-buffer apply: copy streams (in, out) and chunk events, made on first use
+    cudaStream_t hstream[2] = {nullptr, nullptr};
+    std::vector<cudaEvent_t> hev;
     int64_t bytes = 0;
     int E = 8, stages = 4, minb = 3;
     int launch_key = -1, launch_grid = 1;
+    int32_t rng_beg = 0, rng_end = -1;   // groups of the next launch (rng_end < 0: all)
     const void* launch_kernel = nullptr;
     int32_t* err_word = nullptr;
     cudaStream_t alloc_stream = nullptr;   // set: buffers are stream-ordered (cudaMallocAsync)
@@ -1090,6 +1162,9 @@ int dmalloc(hs_l1gs* P, T** p, size_t bytes) {
 
 void release(hs_l1gs* P, cudaStream_t free_stream = nullptr) {
     if (!P) return;
+    for (cudaEvent_t e : P->hev) cudaEventDestroy(e);
+    for (cudaStream_t q : P->hstream)
+        if (q) cudaStreamDestroy(q);
     void* ptrs[] = {P->D, P->Di, P->SLi, P->SUi, P->rp, P->ci, P->vs, P->dev_x, P->dev_y};
     for (void* q : ptrs)
         if (q) {
@@ -1353,7 +1428,9 @@ int launch_packed_kernel(KERN kern, hs_l1gs* P, PackedParams& p, int stages, boo
         P->launch_key = key;
         P->launch_kernel = (const void*)kern;
     }
-    kern<<<P->launch_grid, wpb * 32, smem, st>>>(P->tmL, P->tmU, p);
+    const int grid = (int)std::max<int64_t>(
+        1, std::min<int64_t>(P->launch_grid, ((int64_t)p.ngroups - p.gbeg + wpb - 1) / wpb));
+    kern<<<grid, wpb * 32, smem, st>>>(P->tmL, P->tmU, p);
     HS_LAUNCH_CHECK("l1gs_packed_kernel");
     return HS_OK;
 }
@@ -1365,7 +1442,8 @@ int launch_packed_t(hs_l1gs* P, const void* x, void* y, cudaStream_t st) {
     p.ps = P->ps;
     p.nparts = P->nparts;
     p.npad = P->npad;
-    p.ngroups = P->ngroups;
+    p.gbeg = P->rng_beg;
+    p.ngroups = P->rng_end < 0 ? P->ngroups : P->rng_end;
     p.tlen = (int32_t)P->tlen;
     p.ntiles = (int32_t)((P->tlen + E - 1) / E);
     p.Di = P->Di;
@@ -1407,7 +1485,8 @@ int launch_rows_stages(hs_l1gs* P, const void* x, void* y, cudaStream_t st) {
     p.ps = P->ps;
     p.nparts = P->nparts;
     p.npad = P->npad;
-    p.ngroups = P->ngroups;
+    p.gbeg = P->rng_beg;
+    p.ngroups = P->rng_end < 0 ? P->ngroups : P->rng_end;
     p.tlen = (int32_t)P->tstore;
     p.ntiles = (int32_t)(P->tstore / E);
     p.Di = nullptr;
@@ -1447,7 +1526,8 @@ int launch_view_lanes(hs_l1gs* P, const void* x, void* y, cudaStream_t st, size_
     p.n = P->n;
     p.ps = P->ps;
     p.nparts = P->nparts;
-    p.ngroups = P->ngroups;
+    p.gbeg = P->rng_beg;
+    p.ngroups = P->rng_end < 0 ? P->ngroups : P->rng_end;
     p.rp = P->rp;
     p.ci = P->ci;
     p.v = P->vs;
@@ -1457,23 +1537,38 @@ int launch_view_lanes(hs_l1gs* P, const void* x, void* y, cudaStream_t st, size_
     p.cap_lo = P->cap_lo;
     p.cap_up = P->cap_up;
     p.warp_bytes = (uint32_t)warp_bytes;
-    const int wpb = (int)std::max<int64_t>(1, std::min<int64_t>(kWarpsPerBlock, (200 * 1024) / p.warp_bytes));
-    const size_t smem = (size_t)p.warp_bytes * wpb;
     auto kern = l1gs_view_lanes_kernel<T, IO, SWEEP>;
     if (P->launch_kernel != (const void*)kern) {
+        // Warps per block: the choice that keeps the most warps resident (the
+        // per-block shared-memory reservation makes small blocks pay off when a
+        // warp's slice is large).
         static thread_local int configured_smem = -1;
-        if ((int)smem > configured_smem) {
-            HS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            configured_smem = (int)smem;
+        const int max_smem = (int)std::min<size_t>((size_t)kWarpsPerBlock * warp_bytes, 227 * 1024);
+        if (max_smem > configured_smem) {
+            HS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
+            configured_smem = max_smem;
         }
-        int per_sm = 0;
-        HS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, wpb * 32, smem));
-        if (per_sm < 1) return hs::set_error(HS_ERR_UNSUPPORTED, "view partition needs too much shared memory");
-        const int64_t want = (P->ngroups + wpb - 1) / wpb;
-        P->launch_grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)per_sm * hs::num_sms()));
+        int best_wpb = 0, best_warps = 0, best_per_sm = 0;
+        for (int w = kWarpsPerBlock; w >= 1; w >>= 1) {
+            if ((size_t)w * warp_bytes > (size_t)max_smem) continue;
+            int per_sm = 0;
+            HS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, w * 32, (size_t)w * warp_bytes));
+            if (per_sm * w > best_warps) {
+                best_warps = per_sm * w;
+                best_wpb = w;
+                best_per_sm = per_sm;
+            }
+        }
+        if (best_warps < 1) return hs::set_error(HS_ERR_UNSUPPORTED, "view partition needs too much shared memory");
+        const int64_t want = (P->ngroups + best_wpb - 1) / best_wpb;
+        P->launch_grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)best_per_sm * hs::num_sms()));
+        P->launch_key = best_wpb;
         P->launch_kernel = (const void*)kern;
     }
-    kern<<<P->launch_grid, wpb * 32, smem, st>>>(p);
+    const int wpb = P->launch_key;
+    const int grid = (int)std::max<int64_t>(
+        1, std::min<int64_t>(P->launch_grid, ((int64_t)p.ngroups - p.gbeg + wpb - 1) / wpb));
+    kern<<<grid, wpb * 32, (size_t)wpb * warp_bytes, st>>>(p);
     HS_LAUNCH_CHECK("l1gs_view_lanes_kernel");
     return HS_OK;
 }
@@ -1482,16 +1577,18 @@ template <typename T, typename IO, int SWEEP>
 int launch_view_t(hs_l1gs* P, const void* x, void* y, cudaStream_t st) {
     {
         const size_t ps = (size_t)P->ps;
-        const size_t lanes_bytes = (sizeof(T) * (2 * ps * 33 + 32 * (size_t)(P->cap_lo + P->cap_up)) +
+        const size_t lanes_bytes = (sizeof(T) * (ps * 33 + 32 * (size_t)(P->cap_lo + P->cap_up)) +
                                     sizeof(uint16_t) * (2 * (ps + 1) * 32 + 32 * (size_t)(P->cap_lo + P->cap_up)) +
-                                    4 + 2 * 32 * sizeof(int32_t) + 127) / 128 * 128;
+                                    4 + 2 * 32 * sizeof(int32_t) + (sizeof(int32_t) + sizeof(T)) * kViewStage + 8 +
+                                    127) / 128 * 128;
         if (lanes_bytes <= 100 * 1024 && P->cap_lo < 65535 && P->cap_up < 65535)
             return launch_view_lanes<T, IO, SWEEP>(P, x, y, st, lanes_bytes);
     }
     ViewParams p;
     p.n = P->n;
     p.ps = P->ps;
-    p.nparts = P->nparts;
+    p.kbeg = P->rng_beg * 32;
+    p.nparts = P->rng_end < 0 ? P->nparts : std::min<int32_t>(P->nparts, P->rng_end * 32);
     p.rp = P->rp;
     p.ci = P->ci;
     p.v = P->vs;
@@ -1514,7 +1611,7 @@ int launch_view_t(hs_l1gs* P, const void* x, void* y, cudaStream_t st) {
     int per_sm = 0;
     HS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, wpb * 32, smem));
     if (per_sm < 1) return hs::set_error(HS_ERR_UNSUPPORTED, "view partition needs too much shared memory");
-    const int64_t want = (P->nparts + wpb - 1) / wpb;
+    const int64_t want = ((int64_t)p.nparts - p.kbeg + wpb - 1) / wpb;
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)per_sm * hs::num_sms()));
     kern<<<grid, wpb * 32, smem, st>>>(p);
     HS_LAUNCH_CHECK("l1gs_view_kernel");
@@ -1733,20 +1830,82 @@ int hs_l1gs_apply(hs_l1gs* P, const void* x, void* y, int32_t io_dtype, void* st
     return hs::set_error(HS_ERR_UNSUPPORTED, "FP64 smoother with FP32 vectors is not provided");
 }
 
+// Host-buffer apply.  Partitions are independent (each reads only its own
+// rows of x), so the groups are cut into chunks whose host->device copy,
+// apply and device->host copy run on three streams: chunk c's apply waits
+// only for chunk c's rows of x, and its rows of y leave as soon as it ends,
+// so both copy directions and the kernels overlap.
+namespace {
+constexpr int kHostChunks = 8;
+constexpr size_t kHostChunkMin = size_t(4) << 20;   // bytes of x per chunk, at least
+}  // namespace
+
 int hs_l1gs_apply_host(hs_l1gs* P, const void* x_host, void* y_host, int32_t io_dtype, void* stream) {
     if (!P || !x_host || !y_host) return hs::set_error(HS_ERR_ARG, "hs_l1gs_apply_host: NULL argument");
-    const size_t bytes = dsize(io_dtype) * (size_t)P->n;
+    const size_t es = dsize(io_dtype);
+    const size_t bytes = es * (size_t)P->n;
     if (!P->dev_x) {
         int rc;
         if ((rc = dmalloc(P, &P->dev_x, bytes))) return rc;
         if ((rc = dmalloc(P, &P->dev_y, bytes))) return rc;
     }
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    HS_CUDA(cudaMemcpyAsync(P->dev_x, x_host, bytes, cudaMemcpyHostToDevice, st));
-    int rc = hs_l1gs_apply(P, P->dev_x, P->dev_y, io_dtype, stream);
+    const int chunks = (int)std::min<int64_t>(std::min<int64_t>(kHostChunks, P->ngroups),
+                                              std::max<size_t>(1, bytes / kHostChunkMin));
+    if (chunks <= 1) {
+        HS_CUDA(cudaMemcpyAsync(P->dev_x, x_host, bytes, cudaMemcpyHostToDevice, st));
+        int rc = hs_l1gs_apply(P, P->dev_x, P->dev_y, io_dtype, stream);
+        if (rc) return rc;
+        HS_CUDA(cudaMemcpyAsync(y_host, P->dev_y, bytes, cudaMemcpyDeviceToHost, st));
+        HS_CUDA(cudaStreamSynchronize(st));
+        return HS_OK;
+    }
+    if (!P->hstream[0]) {
+        for (cudaStream_t& q : P->hstream) HS_CUDA(cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking));
+        P->hev.resize(2 * kHostChunks + 2);
+        for (cudaEvent_t& e : P->hev) HS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    cudaStream_t in = P->hstream[0], out = P->hstream[1];
+    cudaEvent_t* ev = P->hev.data();
+    HS_CUDA(cudaEventRecord(ev[0], st));   // the copies follow earlier work on the caller's stream
+    HS_CUDA(cudaStreamWaitEvent(in, ev[0], 0));
+    HS_CUDA(cudaStreamWaitEvent(out, ev[0], 0));
+    const int64_t rows_per_group = 32 * (int64_t)P->ps;
+    const char* xs = static_cast<const char*>(x_host);
+    char* ysh = static_cast<char*>(y_host);
+    char* xd = static_cast<char*>(P->dev_x);
+    char* yd = static_cast<char*>(P->dev_y);
+    int rc = HS_OK;
+    for (int c = 0; c < chunks && rc == HS_OK; ++c) {
+        const int32_t gb = (int32_t)((int64_t)P->ngroups * c / chunks);
+        const int32_t ge = (int32_t)((int64_t)P->ngroups * (c + 1) / chunks);
+        const int64_t r0 = gb * rows_per_group, r1 = std::min<int64_t>(ge * rows_per_group, P->n);
+        if (r1 <= r0) continue;
+        const size_t off = es * (size_t)r0, len = es * (size_t)(r1 - r0);
+        cudaError_t e = cudaMemcpyAsync(xd + off, xs + off, len, cudaMemcpyHostToDevice, in);
+        if (e == cudaSuccess) e = cudaEventRecord(ev[1 + c], in);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(st, ev[1 + c], 0);
+        if (e != cudaSuccess) {
+            rc = hs::cuda_error(e, "hs_l1gs_apply_host (copy in)");
+            break;
+        }
+        P->rng_beg = gb;
+        P->rng_end = ge;
+        rc = hs_l1gs_apply(P, P->dev_x, P->dev_y, io_dtype, stream);
+        P->rng_beg = 0;
+        P->rng_end = -1;
+        if (rc) break;
+        e = cudaEventRecord(ev[1 + kHostChunks + c], st);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(out, ev[1 + kHostChunks + c], 0);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(ysh + off, yd + off, len, cudaMemcpyDeviceToHost, out);
+        if (e != cudaSuccess) rc = hs::cuda_error(e, "hs_l1gs_apply_host (copy out)");
+    }
+    // the caller's stream resumes after the last copy out
+    cudaEventRecord(ev[2 * kHostChunks + 1], out);
+    cudaStreamWaitEvent(st, ev[2 * kHostChunks + 1], 0);
+    const cudaError_t se = cudaStreamSynchronize(st);
     if (rc) return rc;
-    HS_CUDA(cudaMemcpyAsync(y_host, P->dev_y, bytes, cudaMemcpyDeviceToHost, st));
-    HS_CUDA(cudaStreamSynchronize(st));
+    if (se != cudaSuccess) return hs::cuda_error(se, "hs_l1gs_apply_host");
     return HS_OK;
 }
 

@@ -273,3 +273,28 @@ def test_nonfinite_input_rows_layout(ps):
         P = hsb200.L1GSPrecBuilder(hsb200.CUDABackend(), threads=256, blocks=20)(
             A, ps, isSymA=True, sweep=SWEEPS[sweep])
         np.testing.assert_array_equal(gpu_apply(P, x), ref.ldiv(x))
+
+
+@pytest.mark.parametrize("grid,ps,sweep,cache", [
+    ((128, 128, 128), 16, "symmetric", "packed"),   # 4 chunks of whole groups
+    ((1, 1500, 1500), 16, "symmetric", "packed"),   # ragged last group
+    ((1, 1500, 1500), 40, "forward", "packed"),     # rows layout
+    ((128, 128, 128), 16, "symmetric", "view"),
+    ((1, 1500, 1500), 64, "backward", "view"),
+])
+def test_host_apply_chunked_equals_device(grid, ps, sweep, cache):
+    """ldiv! on host vectors (the reference's generic path, l1_gauss_seidel.jl:367-384)
+    copies x in, applies and copies y out in chunks of whole partition groups on
+    overlapping streams; the result is bitwise the device-vector apply."""
+    offs = [(0, 0, 0), (-1, 0, 0), (1, 0, 0), (0, -1, 0), (0, 1, 0), (0, 0, -1), (0, 0, 1)]
+    A = W._canon(W._stencil_csr(grid, offs, [np.float64(6.0)] + [np.float64(-1.0)] * 6).tocsc(), "csc")
+    x = np.random.default_rng(11).uniform(-1, 1, A.shape[0])
+    P = hsb200.L1GSPrecBuilder(hsb200.CUDABackend(), threads=256, blocks=148)(
+        A, ps, isSymA=True, sweep=SWEEPS[sweep], cache_strategy=CACHES[cache])
+    want = gpu_apply(P, x)
+    got = np.empty_like(x)
+    hsb200.ldiv_(got, P, x)
+    np.testing.assert_array_equal(got, want)
+    got2 = np.empty_like(x)
+    hsb200.ldiv_(got2, P, x)   # the copy streams and events are reused
+    np.testing.assert_array_equal(got2, want)
