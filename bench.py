@@ -92,6 +92,53 @@ def algorithmic_bytes(n, nnz, ps, sweep, cache, tv, nonsym=False):
 # ---------------------------------------------------------------------------
 # Clock sampling (NVML) over the soak + timed window
 # ---------------------------------------------------------------------------
+def nvml_handle(dev_index):
+    """NVML handle of torch device `dev_index` (matched by UUID, then PCI bus id:
+    NVML numbers every GPU of the host, not only the visible ones)."""
+    import pynvml
+    pynvml.nvmlInit()
+    try:
+        import torch
+        props = torch.cuda.get_device_properties(dev_index)
+        u = str(props.uuid)
+        for cand in (u, "GPU-" + u):
+            try:
+                return pynvml.nvmlDeviceGetHandleByUUID(cand)
+            except Exception:
+                pass
+        bus = f"{props.pci_domain_id:08x}:{props.pci_bus_id:02x}:{props.pci_device_id:02x}.0"
+        return pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+    except Exception:
+        return pynvml.nvmlDeviceGetHandleByIndex(dev_index)
+
+
+def gpu_local_cpus(dev_index):
+    """Host CPUs on the GPU's NUMA node (NVML's ideal affinity), or None."""
+    try:
+        import pynvml
+        h = nvml_handle(dev_index)
+        words = pynvml.nvmlDeviceGetCpuAffinity(h, (os.cpu_count() + 63) // 64)
+        cpus = {64 * i + b for i, w in enumerate(words) for b in range(64) if (w >> b) & 1}
+        cpus &= os.sched_getaffinity(0)
+        return cpus or None
+    except Exception:
+        return None
+
+
+def alloc_local_pinned(dev_index, make):
+    """Run `make` (which allocates and fills pinned host buffers) on the CPUs local
+    to the GPU, so the pages land on the GPU's NUMA node; the affinity is restored."""
+    cpus = gpu_local_cpus(dev_index)
+    old = os.sched_getaffinity(0)
+    if cpus:
+        os.sched_setaffinity(0, cpus)
+    try:
+        return make()
+    finally:
+        if cpus:
+            os.sched_setaffinity(0, old)
+
+
 class ClockSampler:
     def __init__(self, dev_index, period_s=0.02):
         self.samples = []
@@ -105,7 +152,7 @@ class ClockSampler:
             import pynvml
             pynvml.nvmlInit()
             self.nv = pynvml
-            self.h = pynvml.nvmlDeviceGetHandleByIndex(dev_index)
+            self.h = nvml_handle(dev_index)
             self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
             self.ok = True
         except Exception:
@@ -535,9 +582,13 @@ def main():
     # e2e: the same apply through the C ABI with pinned host vectors
     e2e = None
     if not args.no_e2e:
-        xh = torch.empty(n, dtype=tdt, pin_memory=True)
-        xh.copy_(torch.from_numpy(x).to(tdt))
-        yh = torch.empty(n, dtype=tdt, pin_memory=True)
+        def make_host():
+            xh_ = torch.empty(n, dtype=tdt, pin_memory=True)
+            xh_.copy_(torch.from_numpy(x).to(tdt))
+            yh_ = torch.empty(n, dtype=tdt, pin_memory=True)
+            yh_.zero_()
+            return xh_, yh_
+        xh, yh = alloc_local_pinned(local_rank, make_host)
         io = _lib.HS_F32 if wl["fp32"] else _lib.HS_F64
         import ctypes
         sp_ = ctypes.c_void_p(stream.cuda_stream)

@@ -1136,8 +1136,9 @@ struct hs_l1gs_s {
     alignas(64) CUtensorMap tmU;
     void* dev_x = nullptr;
     void* dev_y = nullptr;
-    // host-buffer apply: copy streams (in, out) and chunk events, made on first use
-    cudaStream_t hstream[2] = {nullptr, nullptr};
+    // host-buffer apply: streams (copy in, copy out, then 4 apply streams) and
+    // chunk events, made on first use
+    cudaStream_t hstream[2 + 4] = {};
     std::vector<cudaEvent_t> hev;
     int64_t bytes = 0;
     int E = 8, stages = 4, minb = 3;
@@ -1832,12 +1833,72 @@ int hs_l1gs_apply(hs_l1gs* P, const void* x, void* y, int32_t io_dtype, void* st
 
 // Host-buffer apply.  Partitions are independent (each reads only its own
 // rows of x), so the groups are cut into chunks whose host->device copy,
-// apply and device->host copy run on three streams: chunk c's apply waits
+// apply and device->host copy run on separate streams: chunk c's apply waits
 // only for chunk c's rows of x, and its rows of y leave as soon as it ends,
-// so both copy directions and the kernels overlap.
+// so both copy directions and the kernels overlap (page-locked buffers on
+// the GPU's NUMA node copy fastest).
 namespace {
-constexpr int kHostChunks = 8;
+constexpr int kHostChunks = 16;
+constexpr int kHostWork = 4;                          // apply streams: chunk c on c % kHostWork
 constexpr size_t kHostChunkMin = size_t(4) << 20;   // bytes of x per chunk, at least
+// events: [0] fork, [1, 1+K) copy-in done, [1+K, 1+2K) apply done, [1+2K] copy-out done,
+// [2+2K, 2+2K+W) apply streams done
+constexpr int kEvIn = 1, kEvApply = 1 + kHostChunks, kEvOut = 1 + 2 * kHostChunks,
+              kEvWork = 2 + 2 * kHostChunks, kEvCount = 2 + 2 * kHostChunks + kHostWork;
+
+// The chunk sequence, forked from `origin` (ev[0] recorded there) and joined
+// back to it: copies in on hstream[0], chunk c's apply on work stream
+// c % kHostWork after its copy in, its copy out on hstream[1] after its apply.
+// Chunks touch disjoint rows, so their applies may run concurrently.
+int enqueue_host_chunks(hs_l1gs* P, const void* x_host, void* y_host, int32_t io_dtype, int chunks,
+                        cudaStream_t origin) {
+    cudaStream_t in = P->hstream[0], out = P->hstream[1];
+    cudaStream_t* work = P->hstream + 2;
+    cudaEvent_t* ev = P->hev.data();
+    HS_CUDA(cudaEventRecord(ev[0], origin));
+    if (in != origin) HS_CUDA(cudaStreamWaitEvent(in, ev[0], 0));
+    HS_CUDA(cudaStreamWaitEvent(out, ev[0], 0));
+    for (int w = 0; w < kHostWork; ++w) HS_CUDA(cudaStreamWaitEvent(work[w], ev[0], 0));
+    const size_t es = dsize(io_dtype);
+    const int64_t rows_per_group = 32 * (int64_t)P->ps;
+    const char* xs = static_cast<const char*>(x_host);
+    char* ysh = static_cast<char*>(y_host);
+    char* xd = static_cast<char*>(P->dev_x);
+    char* yd = static_cast<char*>(P->dev_y);
+    for (int c = 0; c < chunks; ++c) {
+        const int32_t gb = (int32_t)((int64_t)P->ngroups * c / chunks);
+        const int32_t ge = (int32_t)((int64_t)P->ngroups * (c + 1) / chunks);
+        const int64_t r0 = gb * rows_per_group, r1 = std::min<int64_t>(ge * rows_per_group, P->n);
+        if (r1 <= r0) continue;
+        const size_t off = es * (size_t)r0, len = es * (size_t)(r1 - r0);
+        cudaStream_t wk = work[c % kHostWork];
+        HS_CUDA(cudaMemcpyAsync(xd + off, xs + off, len, cudaMemcpyHostToDevice, in));
+        HS_CUDA(cudaEventRecord(ev[kEvIn + c], in));
+        HS_CUDA(cudaStreamWaitEvent(wk, ev[kEvIn + c], 0));
+        P->rng_beg = gb;
+        P->rng_end = ge;
+        const int rc = hs_l1gs_apply(P, P->dev_x, P->dev_y, io_dtype, wk);
+        P->rng_beg = 0;
+        P->rng_end = -1;
+        if (rc) return rc;
+        HS_CUDA(cudaEventRecord(ev[kEvApply + c], wk));
+        HS_CUDA(cudaStreamWaitEvent(out, ev[kEvApply + c], 0));
+        HS_CUDA(cudaMemcpyAsync(ysh + off, yd + off, len, cudaMemcpyDeviceToHost, out));
+    }
+    // join: the origin resumes after every copy out and every apply stream
+    HS_CUDA(cudaEventRecord(ev[kEvOut], out));
+    HS_CUDA(cudaStreamWaitEvent(origin, ev[kEvOut], 0));
+    for (int w = 0; w < kHostWork; ++w) {
+        HS_CUDA(cudaEventRecord(ev[kEvWork + w], work[w]));
+        HS_CUDA(cudaStreamWaitEvent(origin, ev[kEvWork + w], 0));
+    }
+    if (in != origin) {
+        HS_CUDA(cudaEventRecord(ev[kEvIn + kHostChunks - 1], in));
+        HS_CUDA(cudaStreamWaitEvent(origin, ev[kEvIn + kHostChunks - 1], 0));
+    }
+    return HS_OK;
+}
+
 }  // namespace
 
 int hs_l1gs_apply_host(hs_l1gs* P, const void* x_host, void* y_host, int32_t io_dtype, void* stream) {
@@ -1850,8 +1911,10 @@ int hs_l1gs_apply_host(hs_l1gs* P, const void* x_host, void* y_host, int32_t io_
         if ((rc = dmalloc(P, &P->dev_y, bytes))) return rc;
     }
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    const int chunks = (int)std::min<int64_t>(std::min<int64_t>(kHostChunks, P->ngroups),
-                                              std::max<size_t>(1, bytes / kHostChunkMin));
+    int64_t want = std::max<size_t>(1, bytes / kHostChunkMin);
+    if (const char* env = getenv("HSB200_HOST_CHUNKS"))   // tuning override
+        want = std::max(1, atoi(env));
+    const int chunks = (int)std::min<int64_t>(std::min<int64_t>(kHostChunks, P->ngroups), want);
     if (chunks <= 1) {
         HS_CUDA(cudaMemcpyAsync(P->dev_x, x_host, bytes, cudaMemcpyHostToDevice, st));
         int rc = hs_l1gs_apply(P, P->dev_x, P->dev_y, io_dtype, stream);
@@ -1862,47 +1925,10 @@ int hs_l1gs_apply_host(hs_l1gs* P, const void* x_host, void* y_host, int32_t io_
     }
     if (!P->hstream[0]) {
         for (cudaStream_t& q : P->hstream) HS_CUDA(cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking));
-        P->hev.resize(2 * kHostChunks + 2);
+        P->hev.resize(kEvCount);
         for (cudaEvent_t& e : P->hev) HS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     }
-    cudaStream_t in = P->hstream[0], out = P->hstream[1];
-    cudaEvent_t* ev = P->hev.data();
-    HS_CUDA(cudaEventRecord(ev[0], st));   // the copies follow earlier work on the caller's stream
-    HS_CUDA(cudaStreamWaitEvent(in, ev[0], 0));
-    HS_CUDA(cudaStreamWaitEvent(out, ev[0], 0));
-    const int64_t rows_per_group = 32 * (int64_t)P->ps;
-    const char* xs = static_cast<const char*>(x_host);
-    char* ysh = static_cast<char*>(y_host);
-    char* xd = static_cast<char*>(P->dev_x);
-    char* yd = static_cast<char*>(P->dev_y);
-    int rc = HS_OK;
-    for (int c = 0; c < chunks && rc == HS_OK; ++c) {
-        const int32_t gb = (int32_t)((int64_t)P->ngroups * c / chunks);
-        const int32_t ge = (int32_t)((int64_t)P->ngroups * (c + 1) / chunks);
-        const int64_t r0 = gb * rows_per_group, r1 = std::min<int64_t>(ge * rows_per_group, P->n);
-        if (r1 <= r0) continue;
-        const size_t off = es * (size_t)r0, len = es * (size_t)(r1 - r0);
-        cudaError_t e = cudaMemcpyAsync(xd + off, xs + off, len, cudaMemcpyHostToDevice, in);
-        if (e == cudaSuccess) e = cudaEventRecord(ev[1 + c], in);
-        if (e == cudaSuccess) e = cudaStreamWaitEvent(st, ev[1 + c], 0);
-        if (e != cudaSuccess) {
-            rc = hs::cuda_error(e, "hs_l1gs_apply_host (copy in)");
-            break;
-        }
-        P->rng_beg = gb;
-        P->rng_end = ge;
-        rc = hs_l1gs_apply(P, P->dev_x, P->dev_y, io_dtype, stream);
-        P->rng_beg = 0;
-        P->rng_end = -1;
-        if (rc) break;
-        e = cudaEventRecord(ev[1 + kHostChunks + c], st);
-        if (e == cudaSuccess) e = cudaStreamWaitEvent(out, ev[1 + kHostChunks + c], 0);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(ysh + off, yd + off, len, cudaMemcpyDeviceToHost, out);
-        if (e != cudaSuccess) rc = hs::cuda_error(e, "hs_l1gs_apply_host (copy out)");
-    }
-    // the caller's stream resumes after the last copy out
-    cudaEventRecord(ev[2 * kHostChunks + 1], out);
-    cudaStreamWaitEvent(st, ev[2 * kHostChunks + 1], 0);
+    const int rc = enqueue_host_chunks(P, x_host, y_host, io_dtype, chunks, st);
     const cudaError_t se = cudaStreamSynchronize(st);
     if (rc) return rc;
     if (se != cudaSuccess) return hs::cuda_error(se, "hs_l1gs_apply_host");

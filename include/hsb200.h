@@ -103,7 +103,11 @@ int hs_l1gs_apply(hs_l1gs* P, const void* x, void* y, int32_t io_dtype, void* st
 /*
  * The generic LinearSolve.ldiv!(y, P, x) with HOST vectors
  * (src/l1_gauss_seidel.jl:367-384): y .= x, adapt to the device, sweep,
- * copyto! back.  Synchronous; uses pinned staging owned by P.
+ * copyto! back.  Synchronous (returns when y_host holds the result); device
+ * copies of x and y are owned by P.  Vectors of 8 MB and more move in chunks
+ * of whole partition groups whose copy in, apply and copy out overlap on
+ * streams owned by P (ordered after earlier work on `stream`); page-locked
+ * buffers on the GPU's NUMA node copy fastest.
  */
 int hs_l1gs_apply_host(hs_l1gs* P, const void* x_host, void* y_host, int32_t io_dtype, void* stream);
 

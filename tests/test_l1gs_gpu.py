@@ -298,3 +298,25 @@ def test_host_apply_chunked_equals_device(grid, ps, sweep, cache):
     got2 = np.empty_like(x)
     hsb200.ldiv_(got2, P, x)   # the copy streams and events are reused
     np.testing.assert_array_equal(got2, want)
+
+
+@pytest.mark.parametrize("cache", ["packed", "view"])
+def test_host_apply_pinned_repeated(cache):
+    """Page-locked host vectors reused across calls with new contents (the
+    handle's copy streams, apply streams and events are reused): every result is
+    bitwise the device-vector apply."""
+    import ctypes
+    A = W.poisson3d_7pt(128)
+    n = A.shape[0]
+    P = hsb200.L1GSPrecBuilder(hsb200.CUDABackend(), threads=256, blocks=148)(
+        A, 16, isSymA=True, cache_strategy=CACHES[cache])
+    xh = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    yh = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    rng = np.random.default_rng(12)
+    for _ in range(3):
+        x = rng.uniform(-1, 1, n)
+        xh.copy_(torch.from_numpy(x))
+        hsb200._lib.check(hsb200.lib().hs_l1gs_apply_host(P.handle, ctypes.c_void_p(xh.data_ptr()),
+                                                          ctypes.c_void_p(yh.data_ptr()), hsb200._lib.HS_F64,
+                                                          None))
+        np.testing.assert_array_equal(yh.numpy(), gpu_apply(P, x))
