@@ -1831,12 +1831,14 @@ int hs_l1gs_apply(hs_l1gs* P, const void* x, void* y, int32_t io_dtype, void* st
     return hs::set_error(HS_ERR_UNSUPPORTED, "FP64 smoother with FP32 vectors is not provided");
 }
 
-// Host-buffer apply.  Partitions are independent (each reads only its own
-// rows of x), so the groups are cut into chunks whose host->device copy,
-// apply and device->host copy run on separate streams: chunk c's apply waits
-// only for chunk c's rows of x, and its rows of y leave as soon as it ends,
-// so both copy directions and the kernels overlap (page-locked buffers on
-// the GPU's NUMA node copy fastest).
+// Host-buffer apply.  Page-locked (mapped) host vectors are read and written
+// by the apply kernel itself over PCIe: every row of x is read once and every
+// row of y written once, so both link directions stream concurrently with no
+// staging copies.  Other host memory goes through device copies: partitions
+// are independent (each reads only its own rows of x), so the groups are cut
+// into chunks whose host->device copy, apply and device->host copy run on
+// separate streams -- chunk c's apply waits only for chunk c's rows of x, and
+// its rows of y leave as soon as it ends.
 namespace {
 constexpr int kHostChunks = 16;
 constexpr int kHostWork = 4;                          // apply streams: chunk c on c % kHostWork
@@ -1846,12 +1848,50 @@ constexpr size_t kHostChunkMin = size_t(4) << 20;   // bytes of x per chunk, at 
 constexpr int kEvIn = 1, kEvApply = 1 + kHostChunks, kEvOut = 1 + 2 * kHostChunks,
               kEvWork = 2 + 2 * kHostChunks, kEvCount = 2 + 2 * kHostChunks + kHostWork;
 
+// Start of the CUDA allocation that holds address p (driver query), or 0.
+uintptr_t allocation_start(const void* p) {
+    using Fn = CUresult (*)(void*, CUpointer_attribute, CUdeviceptr);
+    static const Fn fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuPointerGetAttribute", &f, 4000, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            return (Fn) nullptr;
+        }
+        return reinterpret_cast<Fn>(f);
+    }();
+    CUdeviceptr start = 0;
+    if (!fn || fn(&start, CU_POINTER_ATTRIBUTE_RANGE_START_ADDR, (CUdeviceptr)(uintptr_t)p) != CUDA_SUCCESS) return 0;
+    return (uintptr_t)start;
+}
+
+// Device address of a page-locked, mapped host buffer of `bytes` bytes, or
+// null: the first and the last byte must lie in the same mapped allocation,
+// so the kernel never touches an address outside it.
+void* mapped_device_pointer(const void* p, size_t bytes) {
+    const char* last = static_cast<const char*>(p) + (bytes ? bytes - 1 : 0);
+    cudaPointerAttributes a, b;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess || cudaPointerGetAttributes(&b, last) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    if (a.type != cudaMemoryTypeHost || b.type != cudaMemoryTypeHost || !a.devicePointer || !b.devicePointer)
+        return nullptr;
+    const uintptr_t s0 = allocation_start(p);
+    if (!s0 || s0 != allocation_start(last)) return nullptr;
+    if (static_cast<const char*>(b.devicePointer) - static_cast<const char*>(a.devicePointer) != last - static_cast<const char*>(p))
+        return nullptr;
+    return a.devicePointer;
+}
+
 // The chunk sequence, forked from `origin` (ev[0] recorded there) and joined
 // back to it: copies in on hstream[0], chunk c's apply on work stream
 // c % kHostWork after its copy in, its copy out on hstream[1] after its apply.
 // Chunks touch disjoint rows, so their applies may run concurrently.
-int enqueue_host_chunks(hs_l1gs* P, const void* x_host, void* y_host, int32_t io_dtype, int chunks,
-                        cudaStream_t origin) {
+int enqueue_host_chunks(hs_l1gs* P, const void* x_host, void* y_host, void* y_mapped, int32_t io_dtype,
+                        int chunks, cudaStream_t origin) {
     cudaStream_t in = P->hstream[0], out = P->hstream[1];
     cudaStream_t* work = P->hstream + 2;
     cudaEvent_t* ev = P->hev.data();
@@ -1877,10 +1917,11 @@ int enqueue_host_chunks(hs_l1gs* P, const void* x_host, void* y_host, int32_t io
         HS_CUDA(cudaStreamWaitEvent(wk, ev[kEvIn + c], 0));
         P->rng_beg = gb;
         P->rng_end = ge;
-        const int rc = hs_l1gs_apply(P, P->dev_x, P->dev_y, io_dtype, wk);
+        const int rc = hs_l1gs_apply(P, P->dev_x, y_mapped ? y_mapped : P->dev_y, io_dtype, wk);
         P->rng_beg = 0;
         P->rng_end = -1;
         if (rc) return rc;
+        if (y_mapped) continue;   // the apply wrote its rows of y to the host itself
         HS_CUDA(cudaEventRecord(ev[kEvApply + c], wk));
         HS_CUDA(cudaStreamWaitEvent(out, ev[kEvApply + c], 0));
         HS_CUDA(cudaMemcpyAsync(ysh + off, yd + off, len, cudaMemcpyDeviceToHost, out));
@@ -1905,21 +1946,37 @@ int hs_l1gs_apply_host(hs_l1gs* P, const void* x_host, void* y_host, int32_t io_
     if (!P || !x_host || !y_host) return hs::set_error(HS_ERR_ARG, "hs_l1gs_apply_host: NULL argument");
     const size_t es = dsize(io_dtype);
     const size_t bytes = es * (size_t)P->n;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // 2 (default): the apply reads x and writes y in mapped host memory; 1: x
+    // through staging copies, y written straight to the host; 0: staging
+    // copies both ways
+    int zero_copy = 2;
+    if (const char* env = getenv("HSB200_HOST_ZEROCOPY"))   // tuning override
+        zero_copy = atoi(env);
+    void* ym = zero_copy >= 1 ? mapped_device_pointer(y_host, bytes) : nullptr;
+    if (zero_copy >= 2 && ym) {
+        void* xm = mapped_device_pointer(x_host, bytes);
+        if (xm) {
+            const int rc = hs_l1gs_apply(P, xm, ym, io_dtype, stream);
+            if (rc) return rc;
+            HS_CUDA(cudaStreamSynchronize(st));
+            return HS_OK;
+        }
+    }
     if (!P->dev_x) {
         int rc;
         if ((rc = dmalloc(P, &P->dev_x, bytes))) return rc;
         if ((rc = dmalloc(P, &P->dev_y, bytes))) return rc;
     }
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
     int64_t want = std::max<size_t>(1, bytes / kHostChunkMin);
     if (const char* env = getenv("HSB200_HOST_CHUNKS"))   // tuning override
         want = std::max(1, atoi(env));
     const int chunks = (int)std::min<int64_t>(std::min<int64_t>(kHostChunks, P->ngroups), want);
     if (chunks <= 1) {
         HS_CUDA(cudaMemcpyAsync(P->dev_x, x_host, bytes, cudaMemcpyHostToDevice, st));
-        int rc = hs_l1gs_apply(P, P->dev_x, P->dev_y, io_dtype, stream);
+        int rc = hs_l1gs_apply(P, P->dev_x, ym ? ym : P->dev_y, io_dtype, stream);
         if (rc) return rc;
-        HS_CUDA(cudaMemcpyAsync(y_host, P->dev_y, bytes, cudaMemcpyDeviceToHost, st));
+        if (!ym) HS_CUDA(cudaMemcpyAsync(y_host, P->dev_y, bytes, cudaMemcpyDeviceToHost, st));
         HS_CUDA(cudaStreamSynchronize(st));
         return HS_OK;
     }
@@ -1928,7 +1985,7 @@ int hs_l1gs_apply_host(hs_l1gs* P, const void* x_host, void* y_host, int32_t io_
         P->hev.resize(kEvCount);
         for (cudaEvent_t& e : P->hev) HS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     }
-    const int rc = enqueue_host_chunks(P, x_host, y_host, io_dtype, chunks, st);
+    const int rc = enqueue_host_chunks(P, x_host, y_host, ym, io_dtype, chunks, st);
     const cudaError_t se = cudaStreamSynchronize(st);
     if (rc) return rc;
     if (se != cudaSuccess) return hs::cuda_error(se, "hs_l1gs_apply_host");

@@ -103,11 +103,13 @@ int hs_l1gs_apply(hs_l1gs* P, const void* x, void* y, int32_t io_dtype, void* st
 /*
  * The generic LinearSolve.ldiv!(y, P, x) with HOST vectors
  * (src/l1_gauss_seidel.jl:367-384): y .= x, adapt to the device, sweep,
- * copyto! back.  Synchronous (returns when y_host holds the result); device
- * copies of x and y are owned by P.  Vectors of 8 MB and more move in chunks
- * of whole partition groups whose copy in, apply and copy out overlap on
- * streams owned by P (ordered after earlier work on `stream`); page-locked
- * buffers on the GPU's NUMA node copy fastest.
+ * copyto! back.  Synchronous (returns when y_host holds the result).
+ * Page-locked (mapped) x_host and y_host, each one allocation of at least n
+ * elements, are read and written by the apply kernel itself over PCIe (zero
+ * copy).  Other host memory goes through device copies owned by P: vectors of
+ * 8 MB and more move in chunks of whole partition groups whose copy in, apply
+ * and copy out overlap on streams owned by P (ordered after earlier work on
+ * `stream`).  Buffers on the GPU's NUMA node move fastest.
  */
 int hs_l1gs_apply_host(hs_l1gs* P, const void* x_host, void* y_host, int32_t io_dtype, void* stream);
 
