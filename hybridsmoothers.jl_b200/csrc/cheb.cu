@@ -133,6 +133,11 @@ int matrix_from_host(const std::vector<int32_t>& rp, const std::vector<int32_t>&
 // Kernels
 // ---------------------------------------------------------------------------
 constexpr int kThreads = 256;
+// The plain SpMV with five resident CTAs per SM (48 registers): it is
+// latency-bound, and the extra warps measured 10-12 % faster FP64 SpMVs than
+// the unbounded register allocation (4 CTAs); six spill.  The fused Chebyshev
+// steps keep their registers (the same cap made them 22 % slower).
+constexpr int kWarpMinBlocks = 5;
 
 // Every SpMV-shaped kernel below runs the warp CSR-stream of spmv.cuh
 // (csr_warp_fold): a warp owns 32 consecutive rows at a time and warps stride
@@ -146,7 +151,7 @@ constexpr int kThreads = 256;
 
 // MODE 0: y = A x; MODE 1: y = y - A x (term by term); MODE 2: y = beta y + sum (a x) alpha.
 template <typename T, int MODE>
-__global__ void __launch_bounds__(kThreads) spmv_kernel(int32_t n, const int32_t* __restrict__ rp,
+__global__ void __launch_bounds__(kThreads, kWarpMinBlocks) spmv_kernel(int32_t n, const int32_t* __restrict__ rp,
                                                         const int32_t* __restrict__ ci, const T* __restrict__ v,
                                                         const T* __restrict__ x, T* __restrict__ y, T alpha, T beta) {
     HS_WARP_SHARED(T);
