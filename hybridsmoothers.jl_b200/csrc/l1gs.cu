@@ -1684,7 +1684,7 @@ int l1gs_view_of(const hs_l1gs* P, L1gsView* v) {
 namespace {
 int l1gs_create_impl(const hs_sparse* A, bool on_device, int32_t partsize, int32_t is_sym, double eta, int32_t sweep,
                      int32_t cache, int32_t smoother_dtype, int32_t threads, int32_t blocks, void* stream,
-                     hs_l1gs** out, bool stream_ordered = false) {
+                     hs_l1gs** out, bool stream_ordered = false, bool classic_small = false) {
     if (!out) return hs::set_error(HS_ERR_ARG, "out is NULL");
     *out = nullptr;
     if (partsize <= 0) return hs::set_error(HS_ERR_ARG, "partsize must be greater than 0");
@@ -1711,9 +1711,13 @@ int l1gs_create_impl(const hs_sparse* A, bool on_device, int32_t partsize, int32
     P->npad = ((int64_t)P->nparts + 31) / 32 * 32;
     P->ngroups = (int32_t)(P->npad / 32);
     P->tlen = (int64_t)partsize * (partsize - 1) / 2;
-    // Row-aligned streams for partsize > 32: 8-slot tiles up to 96 (little
+    // Row-aligned streams for partsize >= 32: 8-slot tiles up to 96 (little
     // padding), 32-slot tiles beyond (per-tile overhead spread over 32 slots).
-    P->rows_layout = (cache == HS_CACHE_PACKED && partsize > 32) ? (partsize <= 96 ? 8 : 32) : 0;
+    // (At 32 the register-resident kernel holds 64 FP64 values of y and D_Dl1
+    // per lane and spills; y in shared memory is faster.)
+    // classic_small: the batch engine's kernel reads the classic layout up to 32.
+    P->rows_layout =
+        (cache == HS_CACHE_PACKED && partsize >= (classic_small ? 33 : 32)) ? (partsize <= 96 ? 8 : 32) : 0;
     P->tstore = P->rows_layout ? rows_off(partsize, P->rows_layout) : P->tlen;
     const int64_t lps = (int64_t)A->n - (int64_t)(P->nparts - 1) * partsize;
     P->S = P->tlen * (P->nparts - 1) + lps * (lps - 1) / 2;
@@ -1809,7 +1813,7 @@ int l1gs_create_from_matrix(const hs_matrix* M, int32_t partsize, double eta, in
     d.dtype = dt;
     d.val = v;
     return l1gs_create_impl(&d, true, partsize, 1, eta, sweep, HS_CACHE_PACKED, smoother_dtype, 256, 148, st, out,
-                            true);
+                            true, /*classic_small=*/true);
 }
 
 void l1gs_destroy_async(hs_l1gs* P, cudaStream_t st) { release(P, st); }

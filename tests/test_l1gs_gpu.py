@@ -259,9 +259,9 @@ def test_full_size_poisson128_packed_symmetric():
     np.testing.assert_array_equal(gpu_apply(P, x), ref.ldiv(x))
 
 
-@pytest.mark.parametrize("ps", [40, 64])
+@pytest.mark.parametrize("ps", [32, 40, 64])
 def test_nonfinite_input_rows_layout(ps):
-    """Partsize > 32 streams are padded to whole tiles; the padding is never
+    """Partsize >= 32 streams are padded to whole tiles; the padding is never
     multiplied in, so an inf in x reaches exactly the rows the reference
     reaches (NaN and inf positions equal to the oracle's)."""
     A = W.poisson2d_matrix(30, eps=0.5)
