@@ -40,7 +40,7 @@ __host__ __device__ __forceinline__ int64_t up_idx(int64_t ps, int64_t li, int64
     return q * (q - 1) / 2 + (lj - li - 1);
 }
 
-// Row-aligned stream layout for partsize > 32 ("rows" layout) with tile
+// Row-aligned stream layout for partsize >= 32 ("rows" layout) with tile
 // width e (8 or 32 slots).  Row r of a direction (r = li forward, r = ps-1-li
 // backward) occupies r + 1 slots rounded up to a multiple of e, from
 // rows_off(r, e): slot 0 holds D_Dl1 of the row, slots 1.. its terms in the
@@ -528,7 +528,7 @@ struct RowRing {
     }
 };
 
-// ---- partsize > 32: row-aligned streams (rows layout) ----------------------
+// ---- partsize >= 32: row-aligned streams (rows layout) ----------------------
 // Thread per partition as above.  Each row's stream segment starts with its
 // D_Dl1 and is padded to whole 8-slot tiles, so a full tile is 8 loads of
 // coefficients, 8 of y and 8 separately rounded multiply-adds with no index
@@ -569,7 +569,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
         const int64_t g = g0 + (int64_t)gi * gstride;
         const int64_t rowbase = g * 32 * (int64_t)ps;
         T* yk = ys + lane;
-        {   // x -> ys[li][partition], coalesced; (partition, li) advanced without division (ps > 32)
+        {   // x -> ys[li][partition], coalesced; (partition, li) advanced without division (ps >= 32)
             int pp = 0, li = lane;
             for (int t = lane; t < 32 * ps; t += 32) {
                 const int64_t row = rowbase + t;
@@ -1120,7 +1120,7 @@ struct hs_l1gs_s {
     int32_t n = 0, ps = 0, nparts = 0, ngroups = 0, nchunks = 0, chunksize = 0;
     int64_t npad = 0, tlen = 0, S = 0;
     int64_t tstore = 0;      // stream slots per direction (tlen, or rows_off(ps) in the rows layout)
-    int32_t rows_layout = 0; // packed partsize > 32: tile width of the row-aligned streams (0: classic)
+    int32_t rows_layout = 0; // packed partsize >= 32: tile width of the row-aligned streams (0: classic)
     int32_t sweep = 0, cache = 0, is_sym = 0, format = 0, mdt = 0, sdt = 0;
     double eta = 1.5;
     void* D = nullptr;
@@ -1478,7 +1478,7 @@ int launch_packed_t(hs_l1gs* P, const void* x, void* y, cudaStream_t st) {
                                 (uint32_t)(P->ps * 33 * sizeof(T)), st, &cfg);
 }
 
-// Row-aligned streams (partsize > 32): E-slot tiles (8 or 32), a ring of STAGES.
+// Row-aligned streams (partsize >= 32): E-slot tiles (8 or 32), a ring of STAGES.
 template <typename T, typename IO, int SWEEP, int E, int STAGES>
 int launch_rows_stages(hs_l1gs* P, const void* x, void* y, cudaStream_t st) {
     PackedParams p;
