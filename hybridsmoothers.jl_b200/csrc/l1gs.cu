@@ -1363,7 +1363,11 @@ inline int rows_stages(int ps, int E, size_t es, int64_t ngroups) {
         const int64_t per_sm = 233472 / (wpb * wb + 1024);
         if (per_sm < 1) continue;
         const int64_t rounds = (ngroups + sms * per_sm * wpb - 1) / (sms * per_sm * wpb);
-        if (rounds <= best_rounds) {
+        // Fewest rounds first.  On a tie, a single round (every group resident
+        // at once) takes the deeper ring, more bytes in flight per warp; several
+        // rounds keep the shallower ring and its extra resident warps (at 128^3
+        // partsize 32: 4 stages, 12 warps per SM, beat 8 stages, 8 warps).
+        if (rounds < best_rounds || (rounds == best_rounds && rounds == 1)) {
             best_rounds = rounds;
             best = cand[c];
         }
