@@ -1720,6 +1720,8 @@ int l1gs_create_impl(const hs_sparse* A, bool on_device, int32_t partsize, int32
     // (At 32 the register-resident kernel holds 64 FP64 values of y and D_Dl1
     // per lane and spills; y in shared memory is faster.)
     // classic_small: the batch engine's kernel reads the classic layout up to 32.
+    // (The rows kernel needs partsize >= 32: its x staging starts lane l at row
+    // l of the group's first partition.)
     P->rows_layout =
         (cache == HS_CACHE_PACKED && partsize >= (classic_small ? 33 : 32)) ? (partsize <= 96 ? 8 : 32) : 0;
     P->tstore = P->rows_layout ? rows_off(partsize, P->rows_layout) : P->tlen;
