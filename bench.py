@@ -51,6 +51,10 @@ def parse_args():
     ap.add_argument("--serving-count", type=int, default=512)
     ap.add_argument("--serving-max", type=float, default=2e6)
     ap.add_argument("--pcg-iters", type=int, default=40, help="iterations of the pcgiter suite")
+    ap.add_argument("--no-solver-objects", action="store_true",
+                    help="leave the pcg and serving objects out of the headline line")
+    ap.add_argument("--pcg-repeats", type=int, default=10)
+    ap.add_argument("--headline-serving-count", type=int, default=128)
     ap.add_argument("--batch-steps", type=int, default=10, help="8-iteration steps of the batchiter suite")
     return ap.parse_args()
 
@@ -220,6 +224,17 @@ def profiled_traffic(workload):
         return None
 
 
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
 # ---------------------------------------------------------------------------
 # CPU leg (the oracle restatement; the reference itself is Julia)
 # ---------------------------------------------------------------------------
@@ -261,6 +276,83 @@ def _pcg_runs(M, b, P, reps, rtol=1e-8):
 
 def _pct(v, q):
     return float(np.percentile(np.asarray(v), q))
+
+
+def headline_pcg(A, b, repeats):
+    """The metric's solver half on the 128^3 workload: PCG to 1e-8 with the
+    headline smoother (L1GS symmetric packed partsize 16, FP64), repeated;
+    device time per solve (CUDA events inside the driver) and wall time with
+    b copied in from the host and x copied back."""
+    import torch
+    import hsb200
+    from oracle import hs_oracle as O
+    P = hsb200.L1GSPrecBuilder(hsb200.CUDABackend(), threads=256, blocks=148)(A, 16, isSymA=True)
+    M = hsb200.DeviceSparseMatrix(A)
+    bh = torch.from_numpy(np.ascontiguousarray(b)).pin_memory()
+    xh = torch.empty_like(bh).pin_memory()
+    bd = bh.cuda()
+    x = torch.zeros_like(bd)
+    hsb200.pcg(M, bd, x, P, rtol=1e-8)   # warm (kernel attributes, workspace, graph)
+    dev_ms, wall_ms, it, rel = [], [], None, None
+    for _ in range(repeats):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        bd.copy_(bh, non_blocking=True)
+        info = hsb200.pcg(M, bd, x, P, rtol=1e-8)
+        xh.copy_(x)
+        wall_ms.append((time.perf_counter() - t0) * 1e3)
+        dev_ms.append(info.ms)
+        it, rel = info.iterations, info.relres
+    t0 = time.perf_counter()
+    _, it_ref, _ = O.pcg(A, b, O.OracleL1GS(A, 16, isSymA=True, sweep="symmetric", cache="packed"))
+    oracle_s = time.perf_counter() - t0
+    return {"workload": "128^3 7-point Poisson, b~U[-1,1], PCG to ||r|| <= 1e-8 ||b||, "
+                        "L1GS symmetric packed partsize 16 FP64",
+            "repeats": repeats, "iterations": it, "iterations_oracle": it_ref, "relres": rel,
+            "solves_per_s": round(1e3 / float(np.median(dev_ms)), 3),
+            "p50_ms": round(_pct(dev_ms, 50), 3), "p99_ms": round(_pct(dev_ms, 99), 3),
+            "e2e_solves_per_s": round(1e3 / float(np.median(wall_ms)), 3),
+            "e2e_p50_ms": round(_pct(wall_ms, 50), 3), "e2e_p99_ms": round(_pct(wall_ms, 99), 3),
+            "oracle_solve_s": round(oracle_s, 1), "oracle_threads": O.omp_threads()}
+
+
+def headline_serving(count):
+    """Cut-down serving stream (the first `count` requests of the seeded
+    stream): served, batched FP32-smoother PCG against the plain FP64 drop-in
+    (one build + PCG after another).  The autotuner starts empty and runs
+    inside the served wall time."""
+    from hsb200 import serving
+    from hsb200 import workloads as W
+    from hsb200.autotune import Autotuner
+    t0 = time.perf_counter()
+    reqs = W.serving_stream(count=count, lo=1e3, hi=2e6)
+    gen_s = time.perf_counter() - t0
+    rows = sum(A.shape[0] for _, A, _ in reqs)
+    serving.solve_sequential(reqs[:2], partsize=16)   # warm: kernel attributes, pools
+    seq = serving.solve_sequential(reqs, partsize=16)
+    tuner = Autotuner(trial_iters=20)
+    closed = serving.serve([(0.0, A, b) for _, A, b in reqs], max_slots=64, iters_per_step=8,
+                           partsize_of=tuner.partsize_of)
+    rate = 0.8 * closed["solves_per_s"]
+    rng = np.random.default_rng(1)
+    t = np.cumsum(rng.exponential(1.0 / rate, size=len(reqs)))
+    opened = serving.serve([(float(t[i]), A, b) for i, (_, A, b) in enumerate(reqs)], max_slots=64,
+                           iters_per_step=8, partsize_of=tuner.partsize_of)
+    return {"workload": f"{len(reqs)} seeded 2D-5pt/3D-7pt variable-coefficient SPD systems, n log-uniform "
+                        f"[1e3, 2e6] ({rows} rows), PCG to 1e-8",
+            "generate_s": round(gen_s, 1),
+            "plain_fp64_dropin": {"solves_per_s": round(seq["solves_per_s"], 3), "p50_ms": round(seq["p50_s"] * 1e3, 2),
+                                  "p99_ms": round(seq["p99_s"] * 1e3, 2)},
+            "served_fp32_batched_closed_loop": {"solves_per_s": round(closed["solves_per_s"], 3),
+                                                "p50_ms": round(closed["p50_s"] * 1e3, 2),
+                                                "p99_ms": round(closed["p99_s"] * 1e3, 2),
+                                                "autotune_trial_s_inside": round(sum(tr[2] for tr in tuner.trials), 2)},
+            "served_fp32_batched_poisson": {"rate_per_s": round(rate, 2),
+                                            "solves_per_s": round(opened["solves_per_s"], 3),
+                                            "p50_ms": round(opened["p50_s"] * 1e3, 2),
+                                            "p99_ms": round(opened["p99_s"] * 1e3, 2)},
+            "served_vs_plain_closed_loop": round(closed["solves_per_s"] / seq["solves_per_s"], 3),
+            "served_vs_plain_poisson": round(opened["solves_per_s"] / seq["solves_per_s"], 3)}
 
 
 def suite_pcg1d(args):
@@ -514,6 +606,7 @@ def main():
                "vs_baseline": None, "dtype": "f32" if wl["fp32"] else "f64", "data": "synthetic",
                "config": config,
                "cpu_baseline": {"value": round(v, 3), "unit": "GB/s", "cores": threads, "kind": "port",
+                                "cpu_model": cpu_model(),
                                 "sample": f"{args.steps} full applies of the 128^3 workload (C restatement of "
                                           "the reference algorithm, OpenMP; the Julia reference cannot run here)"},
                "e2e": {"value": round(v, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -621,8 +714,14 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         reps, el, threads = cpu_apply_rate(A, wl, x, budget_s=10.0)
         cpu = {"value": round(bytes_per * reps / el / 1e9, 3), "unit": "GB/s", "cores": threads, "kind": "port",
+               "cpu_model": cpu_model(),
                "sample": f"{reps} full applies of the 128^3 workload in {el:.1f} s (C restatement of the "
                          "reference algorithm, OpenMP over partitions)"}
+
+    solver = {}
+    if rank == 0 and world == 1 and not args.no_solver_objects:
+        solver["pcg"] = headline_pcg(A, x, args.pcg_repeats)
+        solver["serving"] = headline_serving(args.headline_serving_count)
 
     if world > 1:
         dist.destroy_process_group()
@@ -642,6 +741,7 @@ def main():
         "gpu_launches": int(launches),
         "clocks": clocks.summary(),
     }
+    out.update(solver)
     print(json.dumps(out))
 
 

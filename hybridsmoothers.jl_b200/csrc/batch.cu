@@ -509,11 +509,7 @@ int launch_batched(hs_batch* B, const hs_batch_s::Cls& cl, cudaStream_t st) {
     const int wpb = 4;
     const size_t smem = (size_t)wb * wpb;
     auto kern = l1gs_batched_kernel<PS, 16, 4>;
-    static int configured = 0;
-    if (!configured) {
-        HS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        configured = 1;
-    }
+    if (int rc = hs::ensure_dynamic_smem((const void*)kern, (int)smem)) return rc;
     int per_sm = 0;
     HS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, wpb * 32, smem));
     const int64_t want = (cl.nitems + wpb - 1) / wpb;
@@ -713,6 +709,12 @@ int hs_batch_submit(hs_batch* B, const hs_sparse* A, const double* b_host, doubl
             break;
         }
     const int64_t est = slot_estimate(A->n, A->nnz, ps);
+    // A request larger than the whole budget can never be admitted: say so
+    // (HS_ERR_ARG) instead of "not now" (HS_ERR_BUDGET), so a caller waiting
+    // for memory to free up does not wait forever.
+    if (est > B->cfg.hbm_budget)
+        return hs::set_error(HS_ERR_ARG, "system needs %lld bytes, more than the whole HBM budget %lld",
+                             (long long)est, (long long)B->cfg.hbm_budget);
     if (free_idx < 0 || B->used + est > B->cfg.hbm_budget)
         return hs::set_error(HS_ERR_BUDGET, "no free slot or HBM budget (%lld + %lld > %lld)", (long long)B->used,
                              (long long)est, (long long)B->cfg.hbm_budget);
@@ -734,12 +736,16 @@ int hs_batch_submit(hs_batch* B, const hs_sparse* A, const double* b_host, doubl
         cudaError_t e = cudaMallocAsync(&sl.vec, sizeof(double) * 6 * (size_t)A->n, B->setup);
         if (e) rc = hs::cuda_error(e, "cudaMallocAsync (slot vectors)");
     }
-    if (rc) {
+    // Every failure from here on releases what the slot holds (in stream
+    // order on the setup stream, after the work already queued there).
+    auto fail = [&](int code) {
         cudaStreamSynchronize(B->setup);
+        if (sl.vec) cudaFreeAsync(sl.vec, B->setup);
         if (sl.P) hs::l1gs_destroy_async(sl.P, B->setup);
         if (sl.A) hs::matrix_destroy_async(sl.A, B->setup);
-        return rc;
-    }
+        return code;
+    };
+    if (rc) return fail(rc);
     sl.bytes = est;
     const int32_t n = A->n;
     double* x = sl.vec;
@@ -748,19 +754,21 @@ int hs_batch_submit(hs_batch* B, const hs_sparse* A, const double* b_host, doubl
     double* p = z + n;
     double* b = p + 2 * (size_t)n;
     cudaStream_t st = B->setup;
-    HS_CUDA(cudaMemcpyAsync(b, b_host, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+    cudaError_t ce = cudaMemcpyAsync(b, b_host, sizeof(double) * n, cudaMemcpyHostToDevice, st);
+    if (ce != cudaSuccess) return fail(hs::cuda_error(ce, "hs_batch_submit: copy of b"));
     const int g = (int)std::min<int64_t>((n + kT - 1) / kT, hsdev::kRedMaxBlocks);
     init_vectors<<<g, kT, 0, st>>>(n, b, x, r);
     hs::count_launch();
-    if ((rc = hs_l1gs_apply(sl.P, r, z, HS_F64, st))) return rc;
+    if ((rc = hs_l1gs_apply(sl.P, r, z, HS_F64, st))) return fail(rc);
     init_p_partials<<<g, kT, 0, st>>>(n, z, p, r, b, B->d_init, B->d_init + 2 * hsdev::kRedMaxBlocks);
     init_scalars<<<1, kT, 0, st>>>(B->d_init, B->d_init + 2 * hsdev::kRedMaxBlocks, g, B->d_scal + free_idx,
                                    B->cfg.rtol);
     hs::count_launch(2);
-    HS_CUDA(cudaGetLastError());
+    if ((ce = cudaGetLastError()) != cudaSuccess) return fail(hs::cuda_error(ce, "hs_batch_submit: setup kernels"));
     // No host wait: the next launch orders the solve stream after this
     // admission's setup work through the event.
-    HS_CUDA(cudaEventRecord(B->admitted, st));
+    if ((ce = cudaEventRecord(B->admitted, st)) != cudaSuccess)
+        return fail(hs::cuda_error(ce, "hs_batch_submit: cudaEventRecord"));
     B->pending_admission = true;
     sl.state = 1;
     B->slots[free_idx] = sl;

@@ -3,7 +3,9 @@
 #include <cudaTypedefs.h>
 
 #include <cstring>
+#include <map>
 #include <mutex>
+#include <utility>
 
 #include "hs_common.cuh"
 
@@ -62,6 +64,23 @@ int num_sms() {
         g_sm_count[dev] = v > 0 ? v : 148;
     }
     return g_sm_count[dev];
+}
+
+int ensure_dynamic_smem(const void* kern, int bytes) {
+    // The attribute is a property of the kernel on one device: remember the
+    // largest value set per (kernel, device), so a host thread that drives
+    // several GPUs raises it on each of them.
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, int> done;
+    int dev = 0;
+    HS_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(mu);
+    int& have = done[std::make_pair(kern, dev)];
+    if (bytes > have) {
+        HS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+        have = bytes;
+    }
+    return HS_OK;
 }
 
 int set_singular_col(int32_t col1) {

@@ -23,6 +23,9 @@ void count_launch(int64_t k = 1);
 int32_t* device_error_word();   // device pointer to the bounded-wait error word
 int num_sms();
 int set_singular_col(int32_t col1);
+// Raises the dynamic shared-memory limit of `kern` on the current device to
+// at least `bytes` (cached per kernel and device).
+int ensure_dynamic_smem(const void* kern, int bytes);
 
 }  // namespace hs
 

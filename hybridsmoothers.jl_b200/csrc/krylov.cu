@@ -390,12 +390,28 @@ int hs_pcg_solve(hs_matrix* A, int32_t prec_type, void* prec, const double* b, d
     // allowed on the legacy default stream), ordered after and before the
     // caller's stream by events.
     cudaStream_t caller = static_cast<cudaStream_t>(stream);
-    static thread_local cudaStream_t own = nullptr;
-    static thread_local cudaEvent_t join = nullptr;
-    if (!own) {
-        HS_CUDA(cudaStreamCreateWithFlags(&own, cudaStreamNonBlocking));
-        HS_CUDA(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+    // Stream, event and workspace are kept per calling thread and per device
+    // (a stream belongs to the device it was made on): repeated solves (a
+    // Krylov loop inside a time stepper, a served stream) pay no
+    // cudaMalloc/cudaFree, and no device synchronisation of cudaFree, per
+    // solve.  The workspace grows on demand.
+    int dev = 0;
+    HS_CUDA(cudaGetDevice(&dev));
+    constexpr int kMaxDevices = 64;
+    if (dev < 0 || dev >= kMaxDevices) return hs::set_error(HS_ERR_UNSUPPORTED, "device ordinal %d above 63", dev);
+    static thread_local struct Ctx {
+        cudaStream_t own = nullptr;
+        cudaEvent_t join = nullptr;
+        int64_t cap = 0;
+        double* base = nullptr;
+    } ctxs[kMaxDevices];
+    Ctx& ws = ctxs[dev];
+    if (!ws.own) {
+        HS_CUDA(cudaStreamCreateWithFlags(&ws.own, cudaStreamNonBlocking));
+        HS_CUDA(cudaEventCreateWithFlags(&ws.join, cudaEventDisableTiming));
     }
+    cudaStream_t own = ws.own;
+    cudaEvent_t join = ws.join;
     HS_CUDA(cudaEventRecord(join, caller));
     HS_CUDA(cudaStreamWaitEvent(own, join, 0));
     cudaStream_t st = own;
@@ -408,23 +424,15 @@ int hs_pcg_solve(hs_matrix* A, int32_t prec_type, void* prec, const double* b, d
         }
     } rejoin{own, caller, join};
     const int64_t n = hs::matrix_n(A);
-    // Workspace kept per thread and device, grown on demand: repeated solves
-    // (a Krylov loop inside a time stepper, a served stream) do not pay
-    // cudaMalloc/cudaFree (and the device synchronisation of cudaFree) per solve.
-    static thread_local struct Ws {
-        int dev = -1;
-        int64_t cap = 0;
-        double* base = nullptr;
-    } ws;
-    int dev = 0;
-    HS_CUDA(cudaGetDevice(&dev));
     const int64_t need = 4 * n + 6 * hsdev::kRedMaxBlocks + 2 + (int64_t)(sizeof(PcgScalars) / 8 + 1);
-    if (ws.dev != dev || ws.cap < need) {
-        if (ws.base && ws.dev == dev) cudaFree(ws.base);
+    if (ws.cap < need) {
+        if (ws.base) {
+            HS_CUDA(cudaStreamSynchronize(own));   // earlier solves on this device may still read it
+            cudaFree(ws.base);
+        }
         ws.base = nullptr;
         ws.cap = 0;
         HS_CUDA(cudaMalloc(&ws.base, sizeof(double) * need));
-        ws.dev = dev;
         ws.cap = need;
     }
     double* r = ws.base;
@@ -438,9 +446,21 @@ int hs_pcg_solve(hs_matrix* A, int32_t prec_type, void* prec, const double* b, d
     PcgScalars* s = reinterpret_cast<PcgScalars*>(scal + 2);
     int rc;
     const int ge = grid_elems(n), nb = tile_blocks(n);
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
+    // Timing events and the iteration graph are released on every return path.
+    struct Owned {
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        ~Owned() {
+            if (exec) cudaGraphExecDestroy(exec);
+            if (graph) cudaGraphDestroy(graph);
+            if (e0) cudaEventDestroy(e0);
+            if (e1) cudaEventDestroy(e1);
+        }
+    } own_res;
+    HS_CUDA(cudaEventCreate(&own_res.e0));
+    HS_CUDA(cudaEventCreate(&own_res.e1));
+    cudaEvent_t e0 = own_res.e0, e1 = own_res.e1;
     cudaEventRecord(e0, st);
     // x = 0, r = b, z = M^-1 r, p = z
     zero_kernel<<<ge, kT, 0, st>>>(n, x);
@@ -483,8 +503,8 @@ int hs_pcg_solve(hs_matrix* A, int32_t prec_type, void* prec, const double* b, d
         return HS_OK;
     };
     // warm launch outside capture (sets kernel attributes), then capture
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
+    cudaGraph_t& graph = own_res.graph;
+    cudaGraphExec_t& exec = own_res.exec;
     bool use_graph = true;
     if ((rc = iteration(st))) return rc;
     int launches_per_iter = 0;
@@ -526,10 +546,6 @@ int hs_pcg_solve(hs_matrix* A, int32_t prec_type, void* prec, const double* b, d
     cudaEventSynchronize(e1);
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    if (exec) cudaGraphExecDestroy(exec);
-    if (graph) cudaGraphDestroy(graph);
     const double bnorm = std::sqrt(hsc.bb);
     info->iterations = hsc.done ? hsc.conv_it : hsc.it;
     info->converged = hsc.done ? 1 : 0;
@@ -559,9 +575,16 @@ int hs_gmres_solve(hs_matrix* A, int32_t prec_type, void* prec, int32_t restart,
         (rc = buf.alloc(&scal, 16)) || (rc = buf.alloc(&flag, sizeof(int))))
         return rc;
     const int ge = grid_elems(n), nb = hsdev::red_blocks(n);
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
+    struct Events {   // released on every return path
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        ~Events() {
+            if (e0) cudaEventDestroy(e0);
+            if (e1) cudaEventDestroy(e1);
+        }
+    } evs;
+    HS_CUDA(cudaEventCreate(&evs.e0));
+    HS_CUDA(cudaEventCreate(&evs.e1));
+    cudaEvent_t e0 = evs.e0, e1 = evs.e1;
     cudaEventRecord(e0, st);
     auto norm = [&](const double* a) -> double {
         dot_kernel<<<nb, kT, 0, st>>>(n, a, a, partials);
@@ -628,8 +651,6 @@ int hs_gmres_solve(hs_matrix* A, int32_t prec_type, void* prec, int32_t restart,
     cudaEventSynchronize(e1);
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     HS_CUDA(cudaGetLastError());
     info->iterations = total;
     info->converged = conv ? 1 : 0;

@@ -1402,7 +1402,7 @@ inline void pick_tile(int ps, int sdt, int* E, int* stages, int* minb) {
 
 template <typename KERN>
 int launch_packed_kernel(KERN kern, hs_l1gs* P, PackedParams& p, int stages, bool balanced, uint32_t extra_bytes,
-                         cudaStream_t st, int* configured_smem) {
+                         cudaStream_t st) {
     // per warp: the tile ring, one mbarrier per stage, then the kernel's slice
     p.warp_bytes = (p.ring_bytes + 8 * stages + extra_bytes + 127) / 128 * 128;
     const int wpb = (int)std::max<int64_t>(1, std::min<int64_t>(kWarpsPerBlock, (200 * 1024) / p.warp_bytes));
@@ -1410,10 +1410,8 @@ int launch_packed_kernel(KERN kern, hs_l1gs* P, PackedParams& p, int stages, boo
     // The launch shape depends only on the handle and the io type: compute it once.
     const int key = (int)sizeof(p) ^ (int)p.warp_bytes ^ (wpb << 20);
     if (P->launch_key != key || P->launch_kernel != (const void*)kern) {
-        if ((int)smem > *configured_smem) {
-            HS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            *configured_smem = (int)smem;
-        }
+        int rc = hs::ensure_dynamic_smem((const void*)kern, (int)smem);
+        if (rc) return rc;
         int per_sm = 0;
         HS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, wpb * 32, smem));
         if (per_sm < 1) return hs::set_error(HS_ERR_UNSUPPORTED, "partsize %d needs too much shared memory", P->ps);
@@ -1459,10 +1457,9 @@ int launch_packed_t(hs_l1gs* P, const void* x, void* y, cudaStream_t st) {
     p.ring_bytes = (uint32_t)(E * 32 * sizeof(T) * STAGES);
 #define HS_SMALL(PSV, MB)                                                                                \
     {                                                                                                    \
-        static thread_local int cfg = -1;                                                                \
         constexpr int XS = (PSV % 2 == 0) ? PSV + 1 : PSV;                                               \
         return launch_packed_kernel(l1gs_packed_small_kernel<T, IO, SWEEP, PSV, E, STAGES, MB>, P, p,    \
-                                    STAGES, sizeof(T) == 8, (uint32_t)(32 * XS * sizeof(T)), st, &cfg);  \
+                                    STAGES, sizeof(T) == 8, (uint32_t)(32 * XS * sizeof(T)), st);        \
     }
     if constexpr (STAGES == 4) {
         switch (P->ps) {
@@ -1477,9 +1474,8 @@ int launch_packed_t(hs_l1gs* P, const void* x, void* y, cudaStream_t st) {
         }
     }
 #undef HS_SMALL
-    static thread_local int cfg = -1;
     return launch_packed_kernel(l1gs_packed_kernel<T, IO, SWEEP, E, STAGES>, P, p, STAGES, sizeof(T) == 8,
-                                (uint32_t)(P->ps * 33 * sizeof(T)), st, &cfg);
+                                (uint32_t)(P->ps * 33 * sizeof(T)), st);
 }
 
 // Row-aligned streams (partsize >= 32): E-slot tiles (8 or 32), a ring of STAGES.
@@ -1500,9 +1496,8 @@ int launch_rows_stages(hs_l1gs* P, const void* x, void* y, cudaStream_t st) {
     if (!P->err_word) P->err_word = hs::device_error_word();
     p.err = P->err_word;
     p.ring_bytes = (uint32_t)(E * 32 * sizeof(T) * STAGES);
-    static thread_local int cfg = -1;
     return launch_packed_kernel(l1gs_packed_rows_kernel<T, IO, SWEEP, E, STAGES>, P, p, STAGES, sizeof(T) == 8,
-                                (uint32_t)(P->ps * 33 * sizeof(T)), st, &cfg);
+                                (uint32_t)(P->ps * 33 * sizeof(T)), st);
 }
 
 template <typename T, typename IO, int SWEEP>
@@ -1547,12 +1542,8 @@ int launch_view_lanes(hs_l1gs* P, const void* x, void* y, cudaStream_t st, size_
         // Warps per block: the choice that keeps the most warps resident (the
         // per-block shared-memory reservation makes small blocks pay off when a
         // warp's slice is large).
-        static thread_local int configured_smem = -1;
         const int max_smem = (int)std::min<size_t>((size_t)kWarpsPerBlock * warp_bytes, 227 * 1024);
-        if (max_smem > configured_smem) {
-            HS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
-            configured_smem = max_smem;
-        }
+        if (int rc = hs::ensure_dynamic_smem((const void*)kern, max_smem)) return rc;
         int best_wpb = 0, best_warps = 0, best_per_sm = 0;
         for (int w = kWarpsPerBlock; w >= 1; w >>= 1) {
             if ((size_t)w * warp_bytes > (size_t)max_smem) continue;
@@ -1608,11 +1599,7 @@ int launch_view_t(hs_l1gs* P, const void* x, void* y, cudaStream_t st) {
     const int wpb = (int)std::max<int64_t>(1, std::min<int64_t>(kWarpsPerBlock, (200 * 1024) / p.warp_bytes));
     const size_t smem = (size_t)p.warp_bytes * wpb;
     auto kern = l1gs_view_kernel<T, IO, SWEEP>;
-    static thread_local int configured_smem = -1;
-    if ((int)smem > configured_smem) {
-        HS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        configured_smem = (int)smem;
-    }
+    if (int rc = hs::ensure_dynamic_smem((const void*)kern, (int)smem)) return rc;
     int per_sm = 0;
     HS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, wpb * 32, smem));
     if (per_sm < 1) return hs::set_error(HS_ERR_UNSUPPORTED, "view partition needs too much shared memory");

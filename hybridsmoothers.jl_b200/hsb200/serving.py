@@ -154,6 +154,10 @@ def serve(requests, max_slots=64, hbm_budget=64 << 30, iters_per_step=4, rtol=1e
                 active -= 1
         else:
             admit()
+            if not active and waiting:
+                # nothing runs, so nothing will free up: the head request can never fit
+                raise RuntimeError(f"request {waiting[0]} cannot be admitted by an idle engine "
+                                   f"(max_slots={max_slots}, hbm_budget={hbm_budget})")
             if not active and pending:
                 wait = requests[pending[0]][0] - (time.perf_counter() - t0)
                 if wait > 0:

@@ -168,18 +168,21 @@ int hs_cheb_set_rho(hs_cheb* S, double rho);
 int hs_cheb_destroy(hs_cheb* S);
 
 /*
- * smooth!(x, s, b) for callers that cannot call cudaMalloc where they smooth
- * (a runtime that owns the whole device pool, code under an allocator lock, a
- * serving loop that forbids allocation on its hot path).  No counterpart in
- * the reference.  The caller passes every operand as a device buffer: the CSR
+ * Chebyshev smoothing of x in place, for callers that cannot call cudaMalloc
+ * where they smooth (a runtime that owns the whole device pool, code under an
+ * allocator lock, a serving loop that forbids allocation on its hot path).
+ * No counterpart in the reference.  The caller passes every operand as a
+ * device buffer: the CSR
  * matrix (rp, ci, v; FP64, sorted columns), l1inv = 1 ./ (l1 row sums), kind
  * (4 or 1), degree, rho and, for the 1st kind, astar (see hs_cheb_info), and
  * x (updated in place) and b, all FP64.  The function allocates nothing: its
  * work vectors live in a static device array of 4 * 262144 doubles (8 MiB,
  * held on every GPU that loads the library), so n may not exceed 262144
  * (HS_ERR_ARG otherwise).  The first call on a device looks up that array's
- * device address; make it before any stream capture.  All calls share the
- * array, so calls whose GPU work overlaps race.
+ * device address and keeps it; make it before any stream capture.  The kept
+ * address belongs to the device's context: after cudaDeviceReset on that
+ * device, do not call this function again in the same process.  All calls
+ * share the array, so calls whose GPU work overlaps race.
  */
 int hs_cheb_smooth_noalloc(int32_t n, int64_t nnz, const int32_t* rp, const int32_t* ci, const double* v,
                            const double* l1inv, int32_t kind, int32_t degree, double rho, double astar,

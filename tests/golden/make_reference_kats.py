@@ -76,4 +76,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: make_reference_kats.py <path of the HybridSmoothers.jl checkout>")
+    main(sys.argv[1])
