@@ -63,7 +63,7 @@ def parse_args():
 # Workloads and algorithmic bytes
 # ---------------------------------------------------------------------------
 def parse_workload(name):
-    # poisson<G>-l1gs-<sweep>-<cache>-ps<k>[-fp32]: the G^3 7-point Poisson operator
+    # poisson<G>-l1gs-<sweep>-<cache>-ps<k>[-fp32][-tpp<t>][-reference|-any]: the G^3 7-point Poisson operator
     # (G = 128 is the headline; smaller G serve profiler captures of the same kernels)
     parts = name.split("-")
     if not parts[0].startswith("poisson") or not parts[0][7:].isdigit() or parts[1] != "l1gs":
@@ -71,8 +71,15 @@ def parse_workload(name):
     sweep = {"fwd": "forward", "bwd": "backward", "sym": "symmetric"}[parts[2]]
     cache = parts[3]
     ps = int(parts[4][2:])
-    fp32 = len(parts) > 5 and parts[5] == "fp32"
-    return dict(grid=int(parts[0][7:]), sweep=sweep, cache=cache, ps=ps, fp32=fp32)
+    fp32 = "fp32" in parts[5:]
+    tpp = 0   # threads per partition: 0 = the library's choice
+    order = None   # summation order: the library's choice, "reference" or "any"
+    for extra in parts[5:]:
+        if extra.startswith("tpp"):
+            tpp = int(extra[3:])
+        elif extra in ("reference", "any"):
+            order = extra
+    return dict(grid=int(parts[0][7:]), sweep=sweep, cache=cache, ps=ps, fp32=fp32, tpp=tpp, order=order)
 
 
 def packed_len(n, ps):
@@ -629,7 +636,9 @@ def main():
     cache = hsb200.PackedBufferCache() if wl["cache"] == "packed" else hsb200.MatrixViewCache()
     P = hsb200.L1GSPrecBuilder(hsb200.CUDABackend(local_rank), threads=256, blocks=148)(
         A, wl["ps"], isSymA=True, sweep=sweep, cache_strategy=cache,
-        precision=np.float32 if wl["fp32"] else None)
+        precision=np.float32 if wl["fp32"] else None, threads_per_part=wl["tpp"], order=wl["order"])
+    config["threads_per_part"] = P.threads_per_part
+    config["order"] = P.order
     tdt = torch.float32 if wl["fp32"] else torch.float64
     xd = torch.from_numpy(x).to(device="cuda", dtype=tdt)
     yd = torch.empty_like(xd)

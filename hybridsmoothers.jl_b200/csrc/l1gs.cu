@@ -29,6 +29,7 @@
 #include <vector>
 
 #include "internal.cuh"
+#include "l1gs_coop.cuh"
 
 namespace {
 
@@ -59,11 +60,14 @@ __host__ __device__ __forceinline__ int64_t rows_off(int64_t r, int64_t e) {   /
 // TM is the matrix value type (the type D_Dl1 is computed in), TS the
 // smoother type it is stored in.
 // ---------------------------------------------------------------------------
+// With a cooperative layout (coop.G > 0) the triangles go to SC instead, in
+// the column-block order of l1gs_coop.cuh (coop_dirs: 1 lower, 2 upper).
 template <typename TM, typename TS>
 __global__ void setup_rows_kernel(int32_t n, int32_t ps, int64_t npad, const int32_t* __restrict__ rp,
                                   const int32_t* __restrict__ ci, const TM* __restrict__ v, TM eta,
                                   TS* __restrict__ D, TS* __restrict__ Di, TS* __restrict__ SLi,
-                                  TS* __restrict__ SUi, int rows_layout) {
+                                  TS* __restrict__ SUi, int rows_layout, hscoop::Layout coop, int coop_dirs,
+                                  TS* __restrict__ SC) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int64_t k = i / ps;
@@ -79,11 +83,18 @@ __global__ void setup_rows_kernel(int32_t n, int32_t ps, int64_t npad, const int
         } else if (j < s || j > e) {
             d = add_rn(d, abs_t(val));
         } else if (j < i) {
-            if (SLi) SLi[(rows_layout ? rows_off(li, rows_layout) + 1 + (j - s) : lo_idx(li, j - s)) * npad + k] = (TS)val;
+            if (SC) {
+                if (coop_dirs & 1) SC[hscoop::lower_idx(coop, k, li, j - s)] = (TS)val;
+            } else if (SLi) {
+                SLi[(rows_layout ? rows_off(li, rows_layout) + 1 + (j - s) : lo_idx(li, j - s)) * npad + k] = (TS)val;
+            }
         } else {
-            if (SUi)
+            if (SC) {
+                if (coop_dirs & 2) SC[hscoop::upper_idx(coop, k, li, j - s)] = (TS)val;
+            } else if (SUi) {
                 SUi[(rows_layout ? rows_off(ps - 1 - li, rows_layout) + (j - i) : up_idx(ps, li, j - s)) * npad + k] =
                     (TS)val;
+            }
         }
     }
     const TM dl1star = (b >= mul_rn(eta, d)) ? TM(0) : div_rn(d, TM(2));
@@ -452,9 +463,36 @@ __device__ __forceinline__ float lds_t(const float* p) {
     return v;
 }
 
+// A row's running sum.  NACC = 1: one sum in the order the terms arrive --
+// ascending column, the reference's order, bit-identical.  NACC = 4: the term
+// in tile slot m goes to partial sum m % 4 and the row's total is
+// (s0 + s1) + (s2 + s3); four independent add chains instead of one, a
+// different rounding (relative 1e-12 of the reference in FP64).
+template <typename T, int NACC>
+struct RowAcc;
+template <typename T>
+struct RowAcc<T, 1> {
+    T a = T(0);
+    __device__ __forceinline__ void add(int, T p) { a = add_rn(a, p); }
+    __device__ __forceinline__ T total() const { return a; }
+};
+template <typename T>
+struct RowAcc<T, 4> {
+    T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
+    __device__ __forceinline__ void add(int m, T p) {   // m is a compile-time slot index after unrolling
+        switch (m & 3) {
+            case 0: a0 = add_rn(a0, p); break;
+            case 1: a1 = add_rn(a1, p); break;
+            case 2: a2 = add_rn(a2, p); break;
+            default: a3 = add_rn(a3, p); break;
+        }
+    }
+    __device__ __forceinline__ T total() const { return add_rn(add_rn(a0, a1), add_rn(a2, a3)); }
+};
+
 // acc += sum_{m<8} tl[m*32] * yy[m*S] in slot order, loads first.
-template <typename T, int S>
-__device__ __forceinline__ T fold8(T acc, const T* tl, const T* yy) {
+template <typename T, int S, typename ACC>
+__device__ __forceinline__ void fold8(ACC& acc, const T* tl, const T* yy) {
     T a[8], b[8];
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
@@ -462,8 +500,7 @@ __device__ __forceinline__ T fold8(T acc, const T* tl, const T* yy) {
         b[m] = lds_t(yy + m * S);
     }
 #pragma unroll
-    for (int m = 0; m < 8; ++m) acc = add_rn(acc, mul_rn(a[m], b[m]));
-    return acc;
+    for (int m = 0; m < 8; ++m) acc.add(m, mul_rn(a[m], b[m]));
 }
 
 // Ring for the rows kernel: like TileRing, but the elected lane keeps the
@@ -536,7 +573,7 @@ struct RowRing {
 // slots are never added).  Symmetric: the D_Dl1 .* y scaling of a row is
 // applied when the backward sweep reaches it (the same product, before any
 // use).  y lives in shared memory ([row][lane], stride 33).
-template <typename T, typename IO, int SWEEP, int E, int STAGES>
+template <typename T, typename IO, int SWEEP, int E, int STAGES, int NACC>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32)
     l1gs_packed_rows_kernel(const __grid_constant__ CUtensorMap tmL, const __grid_constant__ CUtensorMap tmU,
                             const PackedParams p) {
@@ -588,14 +625,14 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
             for (int li = 0; li < ps; ++li) {
                 const int len = li + 1;
                 const int nt = (len + E - 1) / E;
-                T acc = T(0);
+                RowAcc<T, NACC> acc;
                 if (!ring.wait(t)) goto timeout;
                 const T* tl = ring.tile(t) + lane;
                 const T d = tl[0];
                 if (nt == 1) {
 #pragma unroll
                     for (int m = 1; m < E; ++m)
-                        if (m < len) acc = add_rn(acc, mul_rn(tl[m * 32], yk[(m - 1) * S]));
+                        if (m < len) acc.add(m, mul_rn(tl[m * 32], yk[(m - 1) * S]));
                 } else {
                     T a[7], b[7];
 #pragma unroll
@@ -604,9 +641,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
                         b[m - 1] = lds_t(yk + (m - 1) * S);
                     }
 #pragma unroll
-                    for (int m = 0; m < 7; ++m) acc = add_rn(acc, mul_rn(a[m], b[m]));
+                    for (int m = 0; m < 7; ++m) acc.add(m + 1, mul_rn(a[m], b[m]));
 #pragma unroll
-                    for (int m0 = 8; m0 < E; m0 += 8) acc = fold8<T, S>(acc, tl + m0 * 32, yk + (m0 - 1) * S);
+                    for (int m0 = 8; m0 < E; m0 += 8) fold8<T, S>(acc, tl + m0 * 32, yk + (m0 - 1) * S);
                 }
                 ring.release(t);
                 ++t;
@@ -616,17 +653,17 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
                     const T* yy = yk + (tr * E - 1) * S;
                     if (tr + 1 < nt || (len & (E - 1)) == 0) {
 #pragma unroll
-                        for (int m0 = 0; m0 < E; m0 += 8) acc = fold8<T, S>(acc, tl + m0 * 32, yy + m0 * S);
+                        for (int m0 = 0; m0 < E; m0 += 8) fold8<T, S>(acc, tl + m0 * 32, yy + m0 * S);
                     } else {
                         const int cnt = len & (E - 1);
 #pragma unroll
                         for (int m = 0; m < E; ++m)
-                            if (m < cnt) acc = add_rn(acc, mul_rn(tl[m * 32], yy[m * S]));
+                            if (m < cnt) acc.add(m, mul_rn(tl[m * 32], yy[m * S]));
                     }
                     ring.release(t);
                     ++t;
                 }
-                yk[li * S] = div_rn(sub_rn(yk[li * S], acc), d);
+                yk[li * S] = div_rn(sub_rn(yk[li * S], acc.total()), d);
             }
             c += p.ntiles;
         }
@@ -636,7 +673,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
                 const int li = ps - 1 - q;
                 const int len = q + 1;
                 const int nt = (len + E - 1) / E;
-                T acc = T(0);
+                RowAcc<T, NACC> acc;
                 if (!ring.wait(t)) goto timeout;
                 const T* tl = ring.tile(t) + lane;
                 const T d = tl[0];
@@ -644,7 +681,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
                 if (nt == 1) {
 #pragma unroll
                     for (int m = 1; m < E; ++m)
-                        if (m < len) acc = add_rn(acc, mul_rn(tl[m * 32], yy0[m * S]));
+                        if (m < len) acc.add(m, mul_rn(tl[m * 32], yy0[m * S]));
                 } else {
                     T a[7], b[7];
 #pragma unroll
@@ -653,9 +690,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
                         b[m - 1] = lds_t(yy0 + m * S);
                     }
 #pragma unroll
-                    for (int m = 0; m < 7; ++m) acc = add_rn(acc, mul_rn(a[m], b[m]));
+                    for (int m = 0; m < 7; ++m) acc.add(m + 1, mul_rn(a[m], b[m]));
 #pragma unroll
-                    for (int m0 = 8; m0 < E; m0 += 8) acc = fold8<T, S>(acc, tl + m0 * 32, yy0 + m0 * S);
+                    for (int m0 = 8; m0 < E; m0 += 8) fold8<T, S>(acc, tl + m0 * 32, yy0 + m0 * S);
                 }
                 ring.release(t);
                 ++t;
@@ -665,18 +702,18 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
                     const T* yy = yy0 + (tr * E) * S;
                     if (tr + 1 < nt || (len & (E - 1)) == 0) {
 #pragma unroll
-                        for (int m0 = 0; m0 < E; m0 += 8) acc = fold8<T, S>(acc, tl + m0 * 32, yy + m0 * S);
+                        for (int m0 = 0; m0 < E; m0 += 8) fold8<T, S>(acc, tl + m0 * 32, yy + m0 * S);
                     } else {
                         const int cnt = len & (E - 1);
 #pragma unroll
                         for (int m = 0; m < E; ++m)
-                            if (m < cnt) acc = add_rn(acc, mul_rn(tl[m * 32], yy[m * S]));
+                            if (m < cnt) acc.add(m, mul_rn(tl[m * 32], yy[m * S]));
                     }
                     ring.release(t);
                     ++t;
                 }
                 const T yi = (SWEEP == 2) ? mul_rn(d, yk[li * S]) : yk[li * S];   // y .= D_Dl1 .* y (:897)
-                yk[li * S] = div_rn(sub_rn(yi, acc), d);
+                yk[li * S] = div_rn(sub_rn(yi, acc.total()), d);
             }
             c += p.ntiles;
         }
@@ -1121,6 +1158,19 @@ struct hs_l1gs_s {
     int64_t npad = 0, tlen = 0, S = 0;
     int64_t tstore = 0;      // stream slots per direction (tlen, or rows_off(ps) in the rows layout)
     int32_t rows_layout = 0; // packed partsize >= 32: tile width of the row-aligned streams (0: classic)
+    // Threads per partition of the packed sweep: 1 (thread per partition,
+    // interleaved or rows layout) or 4/8/16/32 (cooperative kernel, coop layout).
+    int32_t tpp = 1;
+    // Partial sums per row of the thread-per-partition rows kernel: 1 (the
+    // reference's order) or 4 (reordered; options.order == 2).
+    int32_t nacc = 1;
+    int32_t order = 1;           // 1: reference summation order everywhere; 2: reordered where faster
+    int32_t coop_m = 0;          // rows per lane of the cooperative kernel
+    int32_t coop_ngroups = 0;    // groups of G = 32/tpp partitions
+    hscoop::Layout coop;
+    hscoop::Geometry coop_geo;
+    void* SC = nullptr;          // cooperative streams (all directions)
+    hscoop::LaunchCache coop_lc;
     int32_t sweep = 0, cache = 0, is_sym = 0, format = 0, mdt = 0, sdt = 0;
     double eta = 1.5;
     void* D = nullptr;
@@ -1144,6 +1194,7 @@ struct hs_l1gs_s {
     int E = 8, stages = 4, minb = 3;
     int launch_key = -1, launch_grid = 1;
     int32_t rng_beg = 0, rng_end = -1;   // groups of the next launch (rng_end < 0: all)
+    int32_t io_groups = 0, io_group_parts = 32;   // the groups rng_beg/rng_end count
     const void* launch_kernel = nullptr;
     int32_t* err_word = nullptr;
     cudaStream_t alloc_stream = nullptr;   // set: buffers are stream-ordered (cudaMallocAsync)
@@ -1166,7 +1217,7 @@ void release(hs_l1gs* P, cudaStream_t free_stream = nullptr) {
     for (cudaEvent_t e : P->hev) cudaEventDestroy(e);
     for (cudaStream_t q : P->hstream)
         if (q) cudaStreamDestroy(q);
-    void* ptrs[] = {P->D, P->Di, P->SLi, P->SUi, P->rp, P->ci, P->vs, P->dev_x, P->dev_y};
+    void* ptrs[] = {P->D, P->Di, P->SLi, P->SUi, P->SC, P->rp, P->ci, P->vs, P->dev_x, P->dev_y};
     for (void* q : ptrs)
         if (q) {
             if (P->stream_ordered)
@@ -1270,7 +1321,13 @@ int setup_device(hs_l1gs* P, const int32_t* rp_h, const int32_t* ci_h, const TM*
     TS *Di = nullptr, *SLi = nullptr, *SUi = nullptr;
     const bool packed = P->cache == HS_CACHE_PACKED;
     const bool lower = P->sweep != HS_SWEEP_BACKWARD, upper = P->sweep != HS_SWEEP_FORWARD;
-    if (packed) {
+    TS* SC = nullptr;
+    if (packed && P->tpp > 1) {
+        const int64_t count = (int64_t)P->coop_ngroups * P->coop.Lgp;
+        if ((rc = dmalloc(P, &SC, sizeof(TS) * count))) return rc;
+        P->SC = SC;
+        HS_CUDA(cudaMemsetAsync(SC, 0, sizeof(TS) * count, st));
+    } else if (packed) {
         if (!P->rows_layout) {   // the rows layout carries D_Dl1 inside its streams
             const int64_t dcount = (int64_t)P->ps * P->npad;
             if ((rc = dmalloc(P, &Di, sizeof(TS) * dcount))) return rc;
@@ -1290,8 +1347,9 @@ int setup_device(hs_l1gs* P, const int32_t* rp_h, const int32_t* ci_h, const TM*
             HS_CUDA(cudaMemsetAsync(SUi, 0, sizeof(TS) * tcount, st));
         }
     }
+    const int coop_dirs = (lower ? 1 : 0) | (upper ? 2 : 0);
     setup_rows_kernel<TM, TS><<<(n + 255) / 256, 256, 0, st>>>(n, P->ps, P->npad, rp_d, ci_d, v_d, (TM)P->eta, D,
-                                                              Di, SLi, SUi, P->rows_layout);
+                                                              Di, SLi, SUi, P->rows_layout, P->coop, coop_dirs, SC);
     HS_LAUNCH_CHECK("setup_rows_kernel");
     if (packed && P->rows_layout) {
         const int32_t lps = (int32_t)((int64_t)n - (int64_t)(P->nparts - 1) * P->ps);
@@ -1479,7 +1537,7 @@ int launch_packed_t(hs_l1gs* P, const void* x, void* y, cudaStream_t st) {
 }
 
 // Row-aligned streams (partsize >= 32): E-slot tiles (8 or 32), a ring of STAGES.
-template <typename T, typename IO, int SWEEP, int E, int STAGES>
+template <typename T, typename IO, int SWEEP, int E, int STAGES, int NACC>
 int launch_rows_stages(hs_l1gs* P, const void* x, void* y, cudaStream_t st) {
     PackedParams p;
     p.n = P->n;
@@ -1496,19 +1554,25 @@ int launch_rows_stages(hs_l1gs* P, const void* x, void* y, cudaStream_t st) {
     if (!P->err_word) P->err_word = hs::device_error_word();
     p.err = P->err_word;
     p.ring_bytes = (uint32_t)(E * 32 * sizeof(T) * STAGES);
-    return launch_packed_kernel(l1gs_packed_rows_kernel<T, IO, SWEEP, E, STAGES>, P, p, STAGES, sizeof(T) == 8,
+    return launch_packed_kernel(l1gs_packed_rows_kernel<T, IO, SWEEP, E, STAGES, NACC>, P, p, STAGES, sizeof(T) == 8,
                                 (uint32_t)(P->ps * 33 * sizeof(T)), st);
+}
+
+template <typename T, typename IO, int SWEEP, int NACC>
+int launch_rows_n(hs_l1gs* P, const void* x, void* y, cudaStream_t st) {
+    if (P->rows_layout == 32) {
+        if (P->stages == 4) return launch_rows_stages<T, IO, SWEEP, 32, 4, NACC>(P, x, y, st);
+        return launch_rows_stages<T, IO, SWEEP, 32, 8, NACC>(P, x, y, st);
+    }
+    if (P->stages == 4) return launch_rows_stages<T, IO, SWEEP, 8, 4, NACC>(P, x, y, st);
+    if (P->stages == 16) return launch_rows_stages<T, IO, SWEEP, 8, 16, NACC>(P, x, y, st);
+    return launch_rows_stages<T, IO, SWEEP, 8, 8, NACC>(P, x, y, st);
 }
 
 template <typename T, typename IO, int SWEEP>
 int launch_rows_t(hs_l1gs* P, const void* x, void* y, cudaStream_t st) {
-    if (P->rows_layout == 32) {
-        if (P->stages == 4) return launch_rows_stages<T, IO, SWEEP, 32, 4>(P, x, y, st);
-        return launch_rows_stages<T, IO, SWEEP, 32, 8>(P, x, y, st);
-    }
-    if (P->stages == 4) return launch_rows_stages<T, IO, SWEEP, 8, 4>(P, x, y, st);
-    if (P->stages == 16) return launch_rows_stages<T, IO, SWEEP, 8, 16>(P, x, y, st);
-    return launch_rows_stages<T, IO, SWEEP, 8, 8>(P, x, y, st);
+    if (P->nacc == 4) return launch_rows_n<T, IO, SWEEP, 4>(P, x, y, st);
+    return launch_rows_n<T, IO, SWEEP, 1>(P, x, y, st);
 }
 
 template <typename T, typename IO, int SWEEP>
@@ -1610,8 +1674,27 @@ int launch_view_t(hs_l1gs* P, const void* x, void* y, cudaStream_t st) {
     return HS_OK;
 }
 
+int launch_coop(hs_l1gs* P, const void* x, void* y, int io, cudaStream_t st) {
+    hscoop::Params p;
+    p.n = P->n;
+    p.ps = P->ps;
+    p.gbeg = P->rng_beg;
+    p.gend = P->rng_end < 0 ? P->coop_ngroups : P->rng_end;
+    p.Lg = (int32_t)P->coop.Lg;
+    p.Lgp = P->coop.Lgp;
+    p.geo = P->coop_geo;
+    p.SC = P->SC;
+    p.D = P->D;
+    p.x = x;
+    p.y = y;
+    if (!P->err_word) P->err_word = hs::device_error_word();
+    p.err = P->err_word;
+    return hscoop::launch(P->sdt, io, P->sweep, P->tpp, P->coop_m, p, &P->coop_lc, st);
+}
+
 template <typename T, typename IO>
 int launch_apply(hs_l1gs* P, const void* x, void* y, cudaStream_t st) {
+    if (P->cache == HS_CACHE_PACKED && P->tpp > 1) return launch_coop(P, x, y, dtype_of<IO>::value, st);
     if (P->cache == HS_CACHE_PACKED) {
         switch (P->sweep) {
             case HS_SWEEP_FORWARD: return launch_packed_cfg<T, IO, 0>(P, x, y, st);
@@ -1635,12 +1718,20 @@ void unpack_reference(const hs_l1gs* P, const TS* inter, TS* out, bool lower) {
         for (int64_t li = 0; li < aps; ++li) {
             if (lower) {
                 for (int64_t lj = 0; lj < li; ++lj) {
+                    if (P->tpp > 1) {
+                        out[boff + li * (li - 1) / 2 + lj] = inter[hscoop::lower_idx(P->coop, k, li, lj)];
+                        continue;
+                    }
                     const int64_t e = P->rows_layout ? rows_off(li, P->rows_layout) + 1 + lj : lo_idx(li, lj);
                     out[boff + li * (li - 1) / 2 + lj] = inter[e * P->npad + k];
                 }
             } else {
                 const int64_t row_start = li * aps - li * (li + 1) / 2;
                 for (int64_t lj = li + 1; lj < aps; ++lj) {
+                    if (P->tpp > 1) {
+                        out[boff + row_start + (lj - li) - 1] = inter[hscoop::upper_idx(P->coop, k, li, lj)];
+                        continue;
+                    }
                     const int64_t e =
                         P->rows_layout ? rows_off(ps - 1 - li, P->rows_layout) + (lj - li) : up_idx(ps, li, lj);
                     out[boff + row_start + (lj - li) - 1] = inter[e * P->npad + k];
@@ -1673,9 +1764,29 @@ int l1gs_view_of(const hs_l1gs* P, L1gsView* v) {
 // C ABI
 // ---------------------------------------------------------------------------
 namespace {
+// Threads per partition when the caller leaves it open (0).  One thread per
+// partition (the reference's order) while the partitions give every SM about
+// six warps of 32 partitions; below that (large partsizes, small matrices)
+// lanes share a partition, eight rows per lane where the partsize allows it
+// (measured fastest on the 128^3 and 96^3 Poisson operators: partsize
+// 64 / 8 lanes, 128 / 16, 256 / 32).  Partsizes below 32 always keep one
+// thread per partition.
+int auto_threads_per_part(int32_t ps, int64_t nparts) {
+    if (ps < 32) return 1;
+    if (nparts / 32 >= 6 * (int64_t)hs::num_sms()) return 1;
+    int tpp = 4;
+    while (tpp < 32 && tpp * 8 < ps) tpp *= 2;
+    const int m = hscoop::rows_per_lane(ps, tpp);
+    if (m && hscoop::supported(ps, tpp, m)) return tpp;
+    tpp = ps <= 128 ? 16 : 32;   // partsizes that are not lanes x rows
+    const int m2 = hscoop::rows_per_lane(ps, tpp);
+    return (m2 && hscoop::supported(ps, tpp, m2)) ? tpp : 1;
+}
+
 int l1gs_create_impl(const hs_sparse* A, bool on_device, int32_t partsize, int32_t is_sym, double eta, int32_t sweep,
                      int32_t cache, int32_t smoother_dtype, int32_t threads, int32_t blocks, void* stream,
-                     hs_l1gs** out, bool stream_ordered = false, bool classic_small = false) {
+                     hs_l1gs** out, bool stream_ordered = false, bool classic_small = false,
+                     int32_t threads_per_part = 0, int32_t order = 0) {
     if (!out) return hs::set_error(HS_ERR_ARG, "out is NULL");
     *out = nullptr;
     if (partsize <= 0) return hs::set_error(HS_ERR_ARG, "partsize must be greater than 0");
@@ -1692,6 +1803,13 @@ int l1gs_create_impl(const hs_sparse* A, bool on_device, int32_t partsize, int32
     if (A->dtype == HS_F32 && smoother_dtype == HS_F64)
         return hs::set_error(HS_ERR_UNSUPPORTED, "an FP64 smoother needs an FP64 matrix");
     if (partsize > 65535) return hs::set_error(HS_ERR_UNSUPPORTED, "partsize above 65535");
+    if (order < 0 || order > 2) return hs::set_error(HS_ERR_ARG, "order must be 0, 1 or 2 (got %d)", order);
+    if (order == 1 && threads_per_part > 1)
+        return hs::set_error(HS_ERR_ARG, "the reference summation order needs one thread per partition");
+    if (threads_per_part != 0 && threads_per_part != 1 && threads_per_part != 4 && threads_per_part != 8 &&
+        threads_per_part != 16 && threads_per_part != 32)
+        return hs::set_error(HS_ERR_ARG, "threads per partition must be 0 (automatic), 1, 4, 8, 16 or 32 (got %d)",
+                             threads_per_part);
 
     hs_l1gs* P = new hs_l1gs();
     P->stream_ordered = stream_ordered;
@@ -1712,6 +1830,48 @@ int l1gs_create_impl(const hs_sparse* A, bool on_device, int32_t partsize, int32
     P->rows_layout =
         (cache == HS_CACHE_PACKED && partsize >= (classic_small ? 33 : 32)) ? (partsize <= 96 ? 8 : 32) : 0;
     P->tstore = P->rows_layout ? rows_off(partsize, P->rows_layout) : P->tlen;
+    {   // threads per partition of the packed sweep
+        int tpp = threads_per_part;
+        const bool coop_ok = cache == HS_CACHE_PACKED && !classic_small && partsize >= 2;
+        if (!coop_ok || order == 1) {
+            tpp = 1;
+        } else if (tpp == 0) {
+            tpp = auto_threads_per_part(partsize, P->nparts);
+        }
+        if (tpp > 1) {
+            const int m = hscoop::rows_per_lane(partsize, tpp);
+            if (!m || !hscoop::supported(partsize, tpp, m)) {
+                if (threads_per_part != 0) {
+                    delete P;
+                    return hs::set_error(HS_ERR_UNSUPPORTED, "partsize %d with %d threads per partition is not provided",
+                                         partsize, tpp);
+                }
+                tpp = 1;
+            } else {
+                const size_t es = dsize(smoother_dtype);
+                P->tpp = tpp;
+                P->coop_m = m;
+                P->rows_layout = 0;
+                P->tstore = 0;
+                P->coop = hscoop::make_layout(partsize, tpp, sweep != HS_SWEEP_BACKWARD, sweep != HS_SWEEP_FORWARD, es);
+                P->coop_ngroups = (int32_t)(((int64_t)P->nparts + P->coop.G - 1) / P->coop.G);
+                P->coop_geo = hscoop::make_geometry(P->coop, es);
+                if (P->coop.Lg > INT32_MAX / 2) {
+                    delete P;
+                    return hs::set_error(HS_ERR_UNSUPPORTED, "partsize %d is too large for %d threads per partition",
+                                         partsize, tpp);
+                }
+            }
+        }
+        P->tpp = tpp;
+    }
+    // Summation order: reordered partial sums only when asked for (order 2)
+    // and only in the rows kernel (thread per partition, partsize >= 32).
+    P->order = (order == 2 || (order == 0 && P->tpp > 1)) ? 2 : 1;
+    P->nacc = (P->order == 2 && P->tpp == 1 && P->rows_layout) ? 4 : 1;
+    // Host-chunked applies cut the work into whole groups of this many partitions.
+    P->io_groups = P->tpp > 1 ? P->coop_ngroups : P->ngroups;
+    P->io_group_parts = P->tpp > 1 ? P->coop.G : 32;
     const int64_t lps = (int64_t)A->n - (int64_t)(P->nparts - 1) * partsize;
     P->S = P->tlen * (P->nparts - 1) + lps * (lps - 1) / 2;
     P->nchunks = blocks;  // _blockpartitioning for KA.GPU (:353-365)
@@ -1761,7 +1921,10 @@ int l1gs_create_impl(const hs_sparse* A, bool on_device, int32_t partsize, int32
         release(P);
         return rc;
     }
-    if (cache == HS_CACHE_PACKED) {
+    if (cache == HS_CACHE_PACKED && P->tpp > 1) {
+        std::memset(&P->tmL, 0, sizeof(CUtensorMap));
+        std::memset(&P->tmU, 0, sizeof(CUtensorMap));
+    } else if (cache == HS_CACHE_PACKED) {
         pick_tile(partsize, smoother_dtype, &P->E, &P->stages, &P->minb);
         if (P->rows_layout) {   // one tile per row segment
             P->E = P->rows_layout;
@@ -1817,6 +1980,13 @@ extern "C" {
 int hs_l1gs_create(const hs_sparse* A, int32_t partsize, int32_t is_sym, double eta, int32_t sweep, int32_t cache,
                    int32_t smoother_dtype, int32_t threads, int32_t blocks, void* stream, hs_l1gs** out) {
     return l1gs_create_impl(A, false, partsize, is_sym, eta, sweep, cache, smoother_dtype, threads, blocks, stream, out);
+}
+
+int hs_l1gs_create_opts(const hs_sparse* A, int32_t partsize, int32_t is_sym, double eta, int32_t sweep,
+                        int32_t cache, int32_t smoother_dtype, int32_t threads, int32_t blocks,
+                        const hs_l1gs_options* opts, void* stream, hs_l1gs** out) {
+    return l1gs_create_impl(A, false, partsize, is_sym, eta, sweep, cache, smoother_dtype, threads, blocks, stream, out,
+                            false, false, opts ? opts->threads_per_part : 0, opts ? opts->order : 0);
 }
 
 int hs_l1gs_apply(hs_l1gs* P, const void* x, void* y, int32_t io_dtype, void* stream) {
@@ -1897,14 +2067,14 @@ int enqueue_host_chunks(hs_l1gs* P, const void* x_host, void* y_host, void* y_ma
     HS_CUDA(cudaStreamWaitEvent(out, ev[0], 0));
     for (int w = 0; w < kHostWork; ++w) HS_CUDA(cudaStreamWaitEvent(work[w], ev[0], 0));
     const size_t es = dsize(io_dtype);
-    const int64_t rows_per_group = 32 * (int64_t)P->ps;
+    const int64_t rows_per_group = (int64_t)P->io_group_parts * P->ps;
     const char* xs = static_cast<const char*>(x_host);
     char* ysh = static_cast<char*>(y_host);
     char* xd = static_cast<char*>(P->dev_x);
     char* yd = static_cast<char*>(P->dev_y);
     for (int c = 0; c < chunks; ++c) {
-        const int32_t gb = (int32_t)((int64_t)P->ngroups * c / chunks);
-        const int32_t ge = (int32_t)((int64_t)P->ngroups * (c + 1) / chunks);
+        const int32_t gb = (int32_t)((int64_t)P->io_groups * c / chunks);
+        const int32_t ge = (int32_t)((int64_t)P->io_groups * (c + 1) / chunks);
         const int64_t r0 = gb * rows_per_group, r1 = std::min<int64_t>(ge * rows_per_group, P->n);
         if (r1 <= r0) continue;
         const size_t off = es * (size_t)r0, len = es * (size_t)(r1 - r0);
@@ -1968,7 +2138,7 @@ int hs_l1gs_apply_host(hs_l1gs* P, const void* x_host, void* y_host, int32_t io_
     int64_t want = std::max<size_t>(1, bytes / kHostChunkMin);
     if (const char* env = getenv("HSB200_HOST_CHUNKS"))   // tuning override
         want = std::max(1, atoi(env));
-    const int chunks = (int)std::min<int64_t>(std::min<int64_t>(kHostChunks, P->ngroups), want);
+    const int chunks = (int)std::min<int64_t>(std::min<int64_t>(kHostChunks, P->io_groups), want);
     if (chunks <= 1) {
         HS_CUDA(cudaMemcpyAsync(P->dev_x, x_host, bytes, cudaMemcpyHostToDevice, st));
         int rc = hs_l1gs_apply(P, P->dev_x, ym ? ym : P->dev_y, io_dtype, stream);
@@ -2005,6 +2175,8 @@ int hs_l1gs_info_get(const hs_l1gs* P, hs_l1gs_info* info) {
     info->packed_len = P->S;
     info->device_bytes = P->bytes;
     info->eta = P->eta;
+    info->threads_per_part = P->tpp;
+    info->order = (P->tpp > 1 || P->nacc > 1) ? 2 : 1;
     return HS_OK;
 }
 
@@ -2018,14 +2190,15 @@ int hs_l1gs_get_diag(const hs_l1gs* P, void* out_host) {
 int hs_l1gs_get_packed(const hs_l1gs* P, int32_t which, void* out_host, int64_t capacity) {
     if (!P || !out_host) return hs::set_error(HS_ERR_ARG, "hs_l1gs_get_packed: NULL argument");
     if (P->cache != HS_CACHE_PACKED) return hs::set_error(HS_ERR_ARG, "not a packed-cache preconditioner");
-    const void* src = which == 0 ? P->SLi : P->SUi;
+    const void* src = P->tpp > 1 ? P->SC : (which == 0 ? P->SLi : P->SUi);
     const bool has = which == 0 ? P->sweep != HS_SWEEP_BACKWARD : P->sweep != HS_SWEEP_FORWARD;
     if (!has) return hs::set_error(HS_ERR_ARG, "this sweep has no %s buffer", which == 0 ? "SL" : "SU");
     if (capacity < P->S) return hs::set_error(HS_ERR_ARG, "capacity %lld < %lld", (long long)capacity, (long long)P->S);
     const size_t es = dsize(P->sdt);
     std::memset(out_host, 0, es * P->S);
     if (!src) return HS_OK;  // partsize 1: empty triangles
-    std::vector<unsigned char> inter(es * P->tstore * P->npad);
+    std::vector<unsigned char> inter(P->tpp > 1 ? es * (size_t)P->coop_ngroups * P->coop.Lgp
+                                                : es * P->tstore * P->npad);
     HS_CUDA(cudaDeviceSynchronize());
     HS_CUDA(cudaMemcpy(inter.data(), src, inter.size(), cudaMemcpyDeviceToHost));
     if (P->sdt == HS_F64)

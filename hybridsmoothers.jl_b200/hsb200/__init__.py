@@ -221,11 +221,19 @@ class L1GSPrecBuilder:
         return cfg.chunks if isinstance(cfg, CPUConfig) else cfg.blocks
 
     def __call__(self, A, partsize=None, isSymA=False, eta=1.5, sweep=None, cache_strategy=None,
-                 precision=None, stream=None):
+                 precision=None, stream=None, threads_per_part=0, order=None):
         """builder(A, partsize; isSymA, η, sweep, cache_strategy) (:287-313).
 
         precision: None (the matrix type) or np.float32 for an FP32 smoother
         built from an FP64 matrix.
+        threads_per_part: 0 (the library chooses), 1 (one thread per
+        partition: every row summed in the reference's order, bit-identical)
+        or 4/8/16/32 lanes sharing a partition (forward sweeps stay
+        bit-identical; backward/symmetric agree to rounding).  Packed caches
+        only; a matrix-view cache always uses 1.
+        order: None (the library chooses), "reference" (every row summed in
+        the reference's order: bit-identical results) or "any" (the library
+        may reorder a row's sum: relative 1e-12 of the reference in FP64).
         """
         if isinstance(self.backend, CPU):
             raise NotImplementedError("the KA.CPU() backend is not part of this library (B200 only)")
@@ -237,14 +245,18 @@ class L1GSPrecBuilder:
         if isinstance(A, Symmetric):
             A = A.materialize()
             isSymA = True
+        codes = {None: 0, "reference": 1, "any": 2}
+        if order not in codes:
+            raise ValueError("order must be None, 'reference' or 'any'")
         return L1GSPreconditioner(self, A, partsize, bool(isSymA), float(eta), sweep, cache_strategy,
-                                  precision, stream)
+                                  precision, stream, int(threads_per_part), codes[order])
 
 
 class L1GSPreconditioner:
     """L1GSPreconditioner(partitioning, sweep) (src/l1_gauss_seidel.jl:180-183)."""
 
-    def __init__(self, builder, A, partsize, isSymA, eta, sweep, cache, precision, stream):
+    def __init__(self, builder, A, partsize, isSymA, eta, sweep, cache, precision, stream, threads_per_part=0,
+                 order=0):
         import torch
         hA = _HostSparse(A)
         sdt = _L.HS_F32 if (precision is not None and np.dtype(precision) == np.float32) else hA.desc.dtype
@@ -253,9 +265,10 @@ class L1GSPreconditioner:
         # bound now: module globals may already be gone when __del__ runs at exit
         self._destroy = _L.lib().hs_l1gs_destroy
         torch.cuda.init()
-        check(lib().hs_l1gs_create(C.byref(hA.desc), int(partsize), int(isSymA), float(eta), sweep.code,
-                                   cache.code, sdt, cfg.threads, cfg.blocks, _stream_ptr(stream),
-                                   C.byref(self._h)))
+        opts = _L.hs_l1gs_options(int(threads_per_part), int(order))
+        check(lib().hs_l1gs_create_opts(C.byref(hA.desc), int(partsize), int(isSymA), float(eta), sweep.code,
+                                        cache.code, sdt, cfg.threads, cfg.blocks, C.byref(opts),
+                                        _stream_ptr(stream), C.byref(self._h)))
         info = _L.hs_l1gs_info()
         check(lib().hs_l1gs_info_get(self._h, C.byref(info)))
         self.info = info
@@ -265,6 +278,8 @@ class L1GSPreconditioner:
         self.smoother_dtype = np.float64 if sdt == _L.HS_F64 else np.float32
         self.partitioning = BlockPartitioning(info.partsize, info.nparts, info.nchunks, info.chunksize,
                                               builder.backend)
+        self.threads_per_part = info.threads_per_part
+        self.order = "reference" if info.order == 1 else "any"
 
     # -- introspection (P.sweep.op.D_DL1, .L.SLbuffer, .U.SUbuffer) --------
     @property

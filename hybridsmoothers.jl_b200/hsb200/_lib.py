@@ -44,7 +44,12 @@ class hs_l1gs_info(C.Structure):
     _fields_ = [("n", C.c_int32), ("partsize", C.c_int32), ("nparts", C.c_int32), ("nchunks", C.c_int32),
                 ("chunksize", C.c_int32), ("sweep", C.c_int32), ("cache", C.c_int32), ("is_sym", C.c_int32),
                 ("format", C.c_int32), ("matrix_dtype", C.c_int32), ("smoother_dtype", C.c_int32),
-                ("packed_len", C.c_int64), ("device_bytes", C.c_int64), ("eta", C.c_double)]
+                ("packed_len", C.c_int64), ("device_bytes", C.c_int64), ("eta", C.c_double),
+                ("threads_per_part", C.c_int32), ("order", C.c_int32)]
+
+
+class hs_l1gs_options(C.Structure):
+    _fields_ = [("threads_per_part", C.c_int32), ("order", C.c_int32)]
 
 
 class hs_cheb_info(C.Structure):
@@ -82,6 +87,8 @@ PROTOTYPES = {
                                  C.POINTER(_vp)]),
     "hs_l1gs_apply": (C.c_int, [_vp, _vp, _vp, _i32, _vp]),
     "hs_l1gs_apply_host": (C.c_int, [_vp, _vp, _vp, _i32, _vp]),
+    "hs_l1gs_create_opts": (C.c_int, [C.POINTER(hs_sparse), _i32, _i32, _d, _i32, _i32, _i32, _i32, _i32,
+                                      C.POINTER(hs_l1gs_options), _vp, C.POINTER(_vp)]),
     "hs_l1gs_info_get": (C.c_int, [_vp, C.POINTER(hs_l1gs_info)]),
     "hs_l1gs_get_diag": (C.c_int, [_vp, _vp]),
     "hs_l1gs_get_packed": (C.c_int, [_vp, _i32, _vp, _i64]),

@@ -73,7 +73,28 @@ typedef struct {
     int64_t packed_len;        /* S: length of SLbuffer/SUbuffer in the reference layout */
     int64_t device_bytes;      /* device memory held by the preconditioner */
     double eta;
+    int32_t threads_per_part;  /* 1, or the lanes sharing a partition (see hs_l1gs_options) */
+    int32_t order;             /* 1: every row summed in the reference's order; 2: reordered */
 } hs_l1gs_info;
+
+/* Build options beyond the reference's arguments. */
+typedef struct {
+    /* Threads that share one partition of a packed sweep.  0: chosen by the
+     * library; 1: one thread per partition, which sums every row in the
+     * reference's order (bit-identical results); 4, 8, 16 or 32: lanes of a
+     * warp share a partition (for large partsizes, where partitions are too
+     * few to keep the GPU busy one thread each).  With several lanes, forward
+     * sweeps stay bit-identical; backward and symmetric sweeps add a row's
+     * terms in descending column order and agree with the reference's
+     * ascending order to rounding.  Matrix-view caches always use 1. */
+    int32_t threads_per_part;
+    /* Summation order of each row's terms.  0: chosen by the library; 1: the
+     * reference's ascending order everywhere (bit-identical to the reference;
+     * requires threads_per_part 0 or 1); 2: the library may reorder (partial
+     * sums combined at the end of the row), agreeing with the reference to
+     * rounding: relative 1e-12 in FP64. */
+    int32_t order;
+} hs_l1gs_options;
 
 /* ---------------------------------------------------------------------- */
 /* L1 Gauss-Seidel                                                        */
@@ -91,6 +112,12 @@ typedef struct {
 int hs_l1gs_create(const hs_sparse* A, int32_t partsize, int32_t is_sym, double eta,
                    int32_t sweep, int32_t cache, int32_t smoother_dtype, int32_t threads,
                    int32_t blocks, void* stream, hs_l1gs** out);
+
+/* hs_l1gs_create with build options (NULL = defaults): the same builder call
+ * (src/l1_gauss_seidel.jl:287-313) plus the threads-per-partition choice. */
+int hs_l1gs_create_opts(const hs_sparse* A, int32_t partsize, int32_t is_sym, double eta,
+                        int32_t sweep, int32_t cache, int32_t smoother_dtype, int32_t threads,
+                        int32_t blocks, const hs_l1gs_options* opts, void* stream, hs_l1gs** out);
 
 /*
  * LinearSolve.ldiv!(y, P, x) on device vectors (src/l1_gauss_seidel.jl:367-384

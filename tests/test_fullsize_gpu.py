@@ -69,7 +69,7 @@ def test_poisson128_l1gs_bitwise(poisson128, ps, cache, sweep):
     A, x = poisson128
     ref = O.OracleL1GS(A, ps, isSymA=True, sweep=sweep, cache=cache)
     P = hsb200.L1GSPrecBuilder(hsb200.CUDABackend(), threads=256, blocks=148)(
-        A, ps, isSymA=True, sweep=SWEEPS[sweep], cache_strategy=CACHES[cache])
+        A, ps, isSymA=True, sweep=SWEEPS[sweep], cache_strategy=CACHES[cache], order="reference")
     np.testing.assert_array_equal(gpu_apply(P, x), ref.ldiv(x))
 
 

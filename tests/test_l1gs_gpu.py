@@ -182,7 +182,7 @@ def test_random_bitwise_fp64(ps, n, sweep, cache):
         M = A.asformat(fmt)
         ref = O.OracleL1GS(M, ps, isSymA=isSym, sweep=sweep, cache=cache)
         P = hsb200.L1GSPrecBuilder(hsb200.CUDABackend(), threads=256, blocks=20)(
-            M, ps, isSymA=isSym, sweep=SWEEPS[sweep], cache_strategy=CACHES[cache])
+            M, ps, isSymA=isSym, sweep=SWEEPS[sweep], cache_strategy=CACHES[cache], order="reference")
         np.testing.assert_array_equal(P.D_DL1, ref.D)
         np.testing.assert_array_equal(gpu_apply(P, x), ref.ldiv(x))
         if cache == "packed" and sweep != "backward":
@@ -203,10 +203,11 @@ def test_fp32_and_mixed_bitwise(ps, sweep, cache):
     # FP32 matrix, FP32 vectors
     A32 = A.astype(np.float32)
     ref = O.OracleL1GS(A32, ps, isSymA=True, sweep=sweep, cache=cache)
-    P = b(A32, ps, isSymA=True, sweep=SWEEPS[sweep], cache_strategy=CACHES[cache])
+    P = b(A32, ps, isSymA=True, sweep=SWEEPS[sweep], cache_strategy=CACHES[cache], order="reference")
     np.testing.assert_array_equal(gpu_apply(P, x.astype(np.float32), torch.float32), ref.ldiv(x.astype(np.float32)))
     # FP64 matrix, FP32 smoother, FP64 vectors
-    Pm = b(A, ps, isSymA=True, sweep=SWEEPS[sweep], cache_strategy=CACHES[cache], precision=np.float32)
+    Pm = b(A, ps, isSymA=True, sweep=SWEEPS[sweep], cache_strategy=CACHES[cache], precision=np.float32,
+           order="reference")
     D64 = O.OracleL1GS(A, ps, isSymA=True, sweep=sweep, cache=cache).D
     np.testing.assert_array_equal(Pm.D_DL1, D64.astype(np.float32))
     y = gpu_apply(Pm, x, torch.float64)
@@ -235,7 +236,7 @@ def test_poisson3d_bitwise(ps, cache):
     for sweep in ("forward", "backward", "symmetric"):
         ref = O.OracleL1GS(A, ps, isSymA=True, sweep=sweep, cache=cache)
         P = hsb200.L1GSPrecBuilder(hsb200.CUDABackend(), threads=256, blocks=148)(
-            A, ps, isSymA=True, sweep=SWEEPS[sweep], cache_strategy=CACHES[cache])
+            A, ps, isSymA=True, sweep=SWEEPS[sweep], cache_strategy=CACHES[cache], order="reference")
         np.testing.assert_array_equal(gpu_apply(P, x), ref.ldiv(x))
 
 
@@ -271,7 +272,7 @@ def test_nonfinite_input_rows_layout(ps):
     for sweep in ("forward", "backward", "symmetric"):
         ref = O.OracleL1GS(A, ps, isSymA=True, sweep=sweep, cache="packed")
         P = hsb200.L1GSPrecBuilder(hsb200.CUDABackend(), threads=256, blocks=20)(
-            A, ps, isSymA=True, sweep=SWEEPS[sweep])
+            A, ps, isSymA=True, sweep=SWEEPS[sweep], order="reference")
         np.testing.assert_array_equal(gpu_apply(P, x), ref.ldiv(x))
 
 

@@ -30,7 +30,8 @@ def true_relres(A, x, b):
 
 def single_pcg_iters(A, b, ps):
     P = hsb200.L1GSPrecBuilder(hsb200.CUDABackend(), threads=256, blocks=148)(A, ps, isSymA=True,
-                                                                             precision=np.float32)
+                                                                             precision=np.float32,
+                                                                             order="reference")
     M = hsb200.DeviceSparseMatrix(A)
     bd = torch.from_numpy(b).cuda()
     x = torch.zeros_like(bd)
