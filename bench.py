@@ -326,25 +326,25 @@ def headline_pcg(A, b, repeats):
 def headline_serving(count):
     """Cut-down serving stream (the first `count` requests of the seeded
     stream): served, batched FP32-smoother PCG against the plain FP64 drop-in
-    (one build + PCG after another).  The autotuner starts empty and runs
-    inside the served wall time."""
+    (one build + PCG after another).  The partsize tuner starts empty and
+    learns inside the served wall time, from the served solves themselves."""
     from hsb200 import serving
     from hsb200 import workloads as W
-    from hsb200.autotune import Autotuner
+    from hsb200.autotune import OnlineTuner
     t0 = time.perf_counter()
     reqs = W.serving_stream(count=count, lo=1e3, hi=2e6)
     gen_s = time.perf_counter() - t0
     rows = sum(A.shape[0] for _, A, _ in reqs)
     serving.solve_sequential(reqs[:2], partsize=16)   # warm: kernel attributes, pools
     seq = serving.solve_sequential(reqs, partsize=16)
-    tuner = Autotuner(trial_iters=20)
-    closed = serving.serve([(0.0, A, b) for _, A, b in reqs], max_slots=64, iters_per_step=8,
-                           partsize_of=tuner.partsize_of)
+    tuner = OnlineTuner()
+    closed = serving.serve([(0.0, A, b) for _, A, b in reqs], max_slots=64, iters_per_step=8, tuner=tuner)
     rate = 0.8 * closed["solves_per_s"]
     rng = np.random.default_rng(1)
     t = np.cumsum(rng.exponential(1.0 / rate, size=len(reqs)))
+    tuner2 = OnlineTuner()
     opened = serving.serve([(float(t[i]), A, b) for i, (_, A, b) in enumerate(reqs)], max_slots=64,
-                           iters_per_step=8, partsize_of=tuner.partsize_of)
+                           iters_per_step=8, tuner=tuner2)
     return {"workload": f"{len(reqs)} seeded 2D-5pt/3D-7pt variable-coefficient SPD systems, n log-uniform "
                         f"[1e3, 2e6] ({rows} rows), PCG to 1e-8",
             "generate_s": round(gen_s, 1),
@@ -353,7 +353,9 @@ def headline_serving(count):
             "served_fp32_batched_closed_loop": {"solves_per_s": round(closed["solves_per_s"], 3),
                                                 "p50_ms": round(closed["p50_s"] * 1e3, 2),
                                                 "p99_ms": round(closed["p99_s"] * 1e3, 2),
-                                                "autotune_trial_s_inside": round(sum(tr[2] for tr in tuner.trials), 2)},
+                                                "partsize_tuning": "online (no trial solves), per class: " +
+                                                json.dumps({str(k): min(v, key=lambda c: float(np.mean(v[c])))
+                                                            for k, v in tuner.obs.items()})},
             "served_fp32_batched_poisson": {"rate_per_s": round(rate, 2),
                                             "solves_per_s": round(opened["solves_per_s"], 3),
                                             "p50_ms": round(opened["p50_s"] * 1e3, 2),
@@ -473,26 +475,22 @@ def suite_serving(args):
     """Workload 5: stream of SPD systems, served + batched FP32-smoother PCG vs the plain FP64 drop-in."""
     from hsb200 import serving
     from hsb200 import workloads as W
-    from hsb200.autotune import Autotuner
+    from hsb200.autotune import OnlineTuner
     t0 = time.perf_counter()
     reqs = W.serving_stream(count=args.serving_count, lo=1e3, hi=args.serving_max)
     gen_s = time.perf_counter() - t0
     rows = sum(A.shape[0] for _, A, _ in reqs)
     seq = serving.solve_sequential(reqs, partsize=16)
-    tuner = Autotuner(trial_iters=20)
-    t1 = time.perf_counter()
-    for _, A, _ in reqs:
-        tuner.choose(A)
-    tune_s = time.perf_counter() - t1
-    # closed loop (all requests waiting at t=0): throughput
-    closed = serving.serve([(0.0, A, b) for _, A, b in reqs], max_slots=64, iters_per_step=8,
-                           partsize_of=tuner.partsize_of)
+    # closed loop (all requests waiting at t=0): throughput; the partsize
+    # tuner learns from the served solves, inside the timed run
+    tuner = OnlineTuner()
+    closed = serving.serve([(0.0, A, b) for _, A, b in reqs], max_slots=64, iters_per_step=8, tuner=tuner)
     # open loop: Poisson arrivals at 80% of the served throughput
     rate = 0.8 * closed["solves_per_s"]
     rng = np.random.default_rng(1)
     t = np.cumsum(rng.exponential(1.0 / rate, size=len(reqs)))
     opened = serving.serve([(float(t[i]), A, b) for i, (_, A, b) in enumerate(reqs)], max_slots=64,
-                           iters_per_step=8, partsize_of=tuner.partsize_of)
+                           iters_per_step=8, tuner=OnlineTuner())
     return {"suite": "serving", "workload": f"{len(reqs)} 2D-5pt/3D-7pt variable-coefficient SPD systems, "
                                              f"n log-uniform [1e3, {args.serving_max:.0e}], PCG 1e-8",
             "total_rows": rows, "generate_s": gen_s,
@@ -502,8 +500,9 @@ def suite_serving(args):
             "served_fp32_batched_poisson": {"rate_per_s": rate, "solves_per_s": opened["solves_per_s"],
                                             "p50_s": opened["p50_s"], "p99_s": opened["p99_s"]},
             "speedup_closed_loop": closed["solves_per_s"] / seq["solves_per_s"],
-            "autotune": {"classes": len(tuner.cache), "seconds": tune_s,
-                         "choices": {str(k): v[0] for k, v in tuner.cache.items()}}}
+            "partsize_tuning": {"classes": len(tuner.obs),
+                                "choices": {str(k): min(v, key=lambda c: float(np.mean(v[c])))
+                                            for k, v in tuner.obs.items()}}}
 
 
 def suite_pcgiter(args):

@@ -54,6 +54,27 @@ __global__ void convert_values(int64_t m, const TS* __restrict__ a, TD* __restri
         b[i] = (TD)a[i];
 }
 
+// DiagonalIndices (src/l1_gauss_seidel.jl:422-436) on the uploaded CSC:
+// diag[c] = position of A[c,c] in rowval (binary search of the sorted
+// column); a missing or zero diagonal records its column in *bad
+// (atomicMin: the smallest such column, the one the reference's ascending
+// loop throws SingularException for).
+template <typename TS>
+__global__ void diag_indices_kernel(int32_t n, const int32_t* __restrict__ ptr, const int32_t* __restrict__ rows,
+                                    const TS* __restrict__ val, int32_t* __restrict__ diag, int32_t* __restrict__ bad) {
+    for (int32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        int32_t lo = ptr[c], hi = ptr[c + 1];   // first position with rows[pos] >= c in [lo, hi)
+        while (lo < hi) {
+            const int32_t mid = lo + (hi - lo) / 2;
+            if (rows[mid] < c) lo = mid + 1;
+            else hi = mid;
+        }
+        const bool ok = lo < ptr[c + 1] && rows[lo] == c && val[lo] != TS(0);
+        diag[c] = ok ? lo : -1;
+        if (!ok) atomicMin(bad, c);
+    }
+}
+
 int grid_for(int64_t m) { return (int)std::max<int64_t>(1, std::min<int64_t>((m + 255) / 256, 8192)); }
 
 template <typename TS, typename TD>
@@ -109,7 +130,8 @@ void keep_pool_reserve() {
     done[dev] = true;
 }
 
-int csr_from_host(const hs_sparse* A, int32_t dtype, int32_t* rp, int32_t* ci, void* v, cudaStream_t st) {
+int csr_from_host(const hs_sparse* A, int32_t dtype, int32_t* rp, int32_t* ci, void* v, cudaStream_t st,
+                  int32_t* diag, int32_t* bad) {
     keep_pool_reserve();
     const int32_t n = A->n;
     const int64_t nnz = A->nnz;
@@ -142,6 +164,17 @@ int csr_from_host(const hs_sparse* A, int32_t dtype, int32_t* rp, int32_t* ci, v
     if (nnz > 0) {
         HS_CUDA(cudaMemcpyAsync(rows_in, A->idx, sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, st));
         HS_CUDA(cudaMemcpyAsync(val, A->val, ses * nnz, cudaMemcpyHostToDevice, st));
+    }
+    if (diag) {
+        if (A->dtype == HS_F64)
+            diag_indices_kernel<double><<<grid_for(n), 256, 0, st>>>(n, static_cast<const int32_t*>(ptr),
+                                                                     static_cast<const int32_t*>(rows_in),
+                                                                     static_cast<const double*>(val), diag, bad);
+        else
+            diag_indices_kernel<float><<<grid_for(n), 256, 0, st>>>(n, static_cast<const int32_t*>(ptr),
+                                                                    static_cast<const int32_t*>(rows_in),
+                                                                    static_cast<const float*>(val), diag, bad);
+        HS_LAUNCH_CHECK("diag_indices_kernel");
     }
     expand_columns<<<grid_for(n), 256, 0, st>>>(n, static_cast<const int32_t*>(ptr), static_cast<int32_t*>(col));
     iota_kernel<<<grid_for(nnz), 256, 0, st>>>(nnz, static_cast<int32_t*>(pos));

@@ -11,8 +11,12 @@ int64_t matrix_nnz(const hs_matrix* M);
 void matrix_arrays(const hs_matrix* M, const int32_t** rp, const int32_t** ci, const void** v, int* dtype);
 int cheb_apply(hs_cheb* S, const void* r, void* z, int io, cudaStream_t st);
 // Uploads a validated host matrix as device CSR in `dtype` (a CSC input is
-// transposed on the device); rp has n+1 entries, ci and v nnz.
-int csr_from_host(const hs_sparse* A, int32_t dtype, int32_t* rp, int32_t* ci, void* v, cudaStream_t st);
+// transposed on the device); rp has n+1 entries, ci and v nnz.  For a CSC
+// input, a non-null `diag` (n entries) receives DiagonalIndices and *bad
+// (initialised by the caller to n) the smallest column whose diagonal is
+// missing or zero.
+int csr_from_host(const hs_sparse* A, int32_t dtype, int32_t* rp, int32_t* ci, void* v, cudaStream_t st,
+                  int32_t* diag = nullptr, int32_t* bad = nullptr);
 
 // The device-side pieces of an L1GS preconditioner that a batched launch needs.
 struct L1gsView {

@@ -30,6 +30,7 @@ constexpr int kT = 256;
 
 struct PcgScalars {
     double bb, rr, rz, pq, alpha, beta, rtol;
+    double eps, rnorm;   // Krylov.jl test: sqrt(r.z) <= eps = atol + rtol sqrt(r0.z0)
     int done, it, conv_it, pad;
 };
 
@@ -108,8 +109,10 @@ __device__ __forceinline__ double sum_partials_all(const double* __restrict__ pa
     return hsdev::dd_value(hsdev::block_dd_all(v));
 }
 
+// kjl: Krylov.jl's stopping test (sqrt(r.z) <= atol + rtol sqrt(r0.z0)),
+// else ||r|| <= rtol ||b||.
 __global__ void pcg_init_scalars(const double* __restrict__ partials_bb, const double* __restrict__ partials_rz,
-                                 int nb, PcgScalars* s, double rtol) {
+                                 int nb, PcgScalars* s, double rtol, double atol, int kjl) {
     const double bb = sum_partials(partials_bb, nb);
     __syncthreads();
     const double rz = sum_partials(partials_rz, nb);
@@ -118,9 +121,30 @@ __global__ void pcg_init_scalars(const double* __restrict__ partials_bb, const d
         s->rr = bb;
         s->rz = rz;
         s->rtol = rtol;
-        s->done = (bb == 0.0);
+        s->rnorm = sqrt(rz);
+        s->eps = __dadd_rn(atol, __dmul_rn(rtol, s->rnorm));
+        s->done = kjl ? (rz == 0.0 || s->rnorm <= s->eps) : (bb == 0.0);
         s->it = 0;
         s->conv_it = s->done ? 0 : -1;
+    }
+}
+
+// Krylov.jl's test after z = M^-1 r: rNorm = sqrt(r.z) <= eps (or rNorm + 1
+// <= 1); a non-positive p.q (no curvature) stops without convergence.
+__global__ void kjl_check(const double* __restrict__ partials, int nb, PcgScalars* s) {
+    const double rz = sum_partials(partials, nb);
+    if (threadIdx.x == 0 && !s->done) {
+        s->it += 1;
+        if (!(s->pq > 0.0)) {
+            s->done = 2;
+            return;
+        }
+        const double rn = sqrt(rz);
+        s->rnorm = rn;
+        if (rn <= s->eps || __dadd_rn(rn, 1.0) <= 1.0) {
+            s->done = 1;
+            s->conv_it = s->it;
+        }
     }
 }
 
@@ -377,15 +401,103 @@ __global__ void set_g(double* g, int m, double beta) {
     for (int i = threadIdx.x; i <= m; i += blockDim.x) g[i] = (i == 0) ? beta : 0.0;
 }
 
-}  // namespace
+// ---- Krylov.jl GMRES helpers ---------------------------------------------
+// q -= h V_i with h = V_i.q summed from the partials by every block in the
+// same order; block 0 records h as R[i][k].
+__global__ void __launch_bounds__(kT) mgs_axpy(int64_t n, const double* __restrict__ partials, int nb,
+                                               const double* __restrict__ Vi, double* __restrict__ q,
+                                               double* __restrict__ Rik) {
+    const double h = sum_partials_all(partials, nb);
+    if (blockIdx.x == 0 && threadIdx.x == 0) *Rik = h;
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x)
+        q[r] = __dsub_rn(q[r], __dmul_rn(h, Vi[r]));
+}
 
-extern "C" {
+__device__ __forceinline__ double sgn(double a) { return a < 0.0 ? -1.0 : 1.0; }
 
-int hs_pcg_solve(hs_matrix* A, int32_t prec_type, void* prec, const double* b, double* x, double rtol, int32_t maxit,
-                 void* stream, hs_solve_info* info) {
+// Symmetric Givens reflection [c s; s -c] [a; b] = [rho; 0] (Krylov.jl's
+// sym_givens; Golub & Van Loan / Bindel, Demmel & Kahan).
+__device__ void sym_givens(double a, double b, double* c, double* s, double* rho) {
+    if (b == 0.0) {
+        *c = (a == 0.0) ? 1.0 : sgn(a);
+        *s = 0.0;
+        *rho = fabs(a);
+    } else if (a == 0.0) {
+        *c = 0.0;
+        *s = sgn(b);
+        *rho = fabs(b);
+    } else if (fabs(b) > fabs(a)) {
+        const double t = __ddiv_rn(a, b);
+        *s = __ddiv_rn(sgn(b), sqrt(__dadd_rn(1.0, __dmul_rn(t, t))));
+        *c = __dmul_rn(*s, t);
+        *rho = __ddiv_rn(b, *s);
+    } else {
+        const double t = __ddiv_rn(b, a);
+        *c = __ddiv_rn(sgn(a), sqrt(__dadd_rn(1.0, __dmul_rn(t, t))));
+        *s = __dmul_rn(*c, t);
+        *rho = __ddiv_rn(a, *c);
+    }
+}
+
+// Closes inner iteration k: Hbis = ||q||, previous reflections applied to
+// column k of R, a new one from (R_kk, Hbis), zeta = s_k z_k, z_k = c_k z_k,
+// z_{k+1} = zeta; scal[0] = Hbis, scal[1] = |zeta|; flag = solved | 2*breakdown.
+__global__ void kjl_arnoldi_close(const double* __restrict__ partials, int nb, double* __restrict__ R, int m, int k,
+                                  double* __restrict__ c, double* __restrict__ sv, double* __restrict__ z,
+                                  double* __restrict__ scal, int* __restrict__ flag, double eps, double btol) {
+    const double qq = sum_partials(partials, nb);
+    if (threadIdx.x != 0) return;
+    const double hbis = sqrt(qq);
+    for (int i = 0; i < k; ++i) {
+        const double ri = R[(size_t)i * m + k], ri1 = R[(size_t)(i + 1) * m + k];
+        const double tmp = __dadd_rn(__dmul_rn(c[i], ri), __dmul_rn(sv[i], ri1));
+        R[(size_t)(i + 1) * m + k] = __dsub_rn(__dmul_rn(sv[i], ri), __dmul_rn(c[i], ri1));
+        R[(size_t)i * m + k] = tmp;
+    }
+    double ck, sk, rho;
+    sym_givens(R[(size_t)k * m + k], hbis, &ck, &sk, &rho);
+    c[k] = ck;
+    sv[k] = sk;
+    R[(size_t)k * m + k] = rho;
+    const double zeta = __dmul_rn(sk, z[k]);
+    z[k] = __dmul_rn(ck, z[k]);
+    z[k + 1] = zeta;
+    const double rn = fabs(zeta);
+    scal[0] = hbis;
+    scal[1] = rn;
+    const bool solved = rn <= eps || __dadd_rn(rn, 1.0) <= 1.0;
+    *flag = (solved ? 1 : 0) | (hbis <= btol ? 2 : 0);
+}
+
+// y = R \ z over the first kk columns: y_i = (z_i - sum_{j>i, from the last}
+// R_ij y_j) / R_ii, or 0 where |R_ii| <= btol.
+__global__ void kjl_back_solve(const double* __restrict__ R, int m, int kk, const double* __restrict__ z,
+                               double* __restrict__ y, double btol) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    for (int i = kk - 1; i >= 0; --i) {
+        double yi = z[i];
+        for (int j = kk - 1; j > i; --j) yi = __dsub_rn(yi, __dmul_rn(R[(size_t)i * m + j], y[j]));
+        const double rii = R[(size_t)i * m + i];
+        y[i] = fabs(rii) <= btol ? 0.0 : __ddiv_rn(yi, rii);
+    }
+}
+
+// w = b - w
+__global__ void rsub_kernel(int64_t n, const double* __restrict__ b, double* __restrict__ w) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        w[i] = __dsub_rn(b[i], w[i]);
+}
+
+// One PCG driver, two stopping tests: kjl = false, ||r|| <= rtol ||b||
+// checked after the x/r update (hs_pcg_solve); kjl = true, Krylov.jl's cg
+// test checked after z = M^-1 r (hs_cg_krylovjl).
+int pcg_impl(hs_matrix* A, int32_t prec_type, void* prec, const double* b, double* x, double atol, double rtol,
+             int32_t maxit, void* stream, hs_solve_info* info, bool kjl) {
     if (!A || !b || !x || !info) return hs::set_error(HS_ERR_ARG, "hs_pcg_solve: NULL argument");
     if (prec_type != HS_PREC_NONE && !prec) return hs::set_error(HS_ERR_ARG, "preconditioner handle is NULL");
+    if (kjl && maxit == 0) maxit = 2 * hs::matrix_n(A);   // Krylov.jl's itmax = 0: 2n
     if (maxit < 1) return hs::set_error(HS_ERR_ARG, "maxit must be positive");
+    if (!(rtol >= 0.0) || !(atol >= 0.0)) return hs::set_error(HS_ERR_ARG, "tolerances must be non-negative");
     // The solve runs on a private non-blocking stream (graph capture is not
     // allowed on the legacy default stream), ordered after and before the
     // caller's stream by events.
@@ -470,7 +582,7 @@ int hs_pcg_solve(hs_matrix* A, int32_t prec_type, void* prec, const double* b, d
     copy_kernel<<<ge, kT, 0, st>>>(n, z, p);
     dot_kernel<<<nb, kT, 0, st>>>(n, b, b, pa);
     dot_kernel<<<nb, kT, 0, st>>>(n, r, z, pb);
-    pcg_init_scalars<<<1, kT, 0, st>>>(pa, pb, nb, s, rtol);
+    pcg_init_scalars<<<1, kT, 0, st>>>(pa, pb, nb, s, rtol, atol, kjl ? 1 : 0);
     hs::count_launch(4);
     HS_LAUNCH_CHECK("pcg init");
 
@@ -493,12 +605,13 @@ int hs_pcg_solve(hs_matrix* A, int32_t prec_type, void* prec, const double* b, d
             dot_kernel<<<nb, kT, 0, cs>>>(n, p, q, pa);
         }
         pcg_update<<<nb, kT, 0, cs>>>(n, s, pa, npq, pb, nb, p, q, x, r, pc);
-        pcg_check<<<1, kT, 0, cs>>>(pc, nb, s);
-        hs::count_launch(3);   // spmv (+dot), update, check
+        if (!kjl) pcg_check<<<1, kT, 0, cs>>>(pc, nb, s);
+        hs::count_launch(kjl ? 2 : 3);   // spmv (+dot), update, check
         if ((r2 = prec_apply(prec_type, prec, r, z, n, cs))) return r2;
         dot_kernel<<<nb, kT, 0, cs>>>(n, r, z, pb);
+        if (kjl) kjl_check<<<1, kT, 0, cs>>>(pb, nb, s);
         pcg_p<<<nb, kT, 0, cs>>>(n, s, pb, nb, z, p);
-        hs::count_launch(1);   // dot; the check below counts pcg_p
+        hs::count_launch(kjl ? 2 : 1);   // dot (+ check); the check below counts pcg_p
         HS_LAUNCH_CHECK("pcg iteration");
         return HS_OK;
     };
@@ -547,12 +660,153 @@ int hs_pcg_solve(hs_matrix* A, int32_t prec_type, void* prec, const double* b, d
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
     const double bnorm = std::sqrt(hsc.bb);
-    info->iterations = hsc.done ? hsc.conv_it : hsc.it;
-    info->converged = hsc.done ? 1 : 0;
+    const bool conv = hsc.done == 1;
+    info->iterations = conv ? hsc.conv_it : hsc.it;
+    info->converged = conv ? 1 : 0;
     info->ms = ms;
     info->relres = true_relres(A, b, x, q, pa, scal, n, st, bnorm);
+    info->rnorm = kjl ? hsc.rnorm : std::sqrt(hsc.rr);
     HS_CUDA(cudaGetLastError());
-    if (!hsc.done) return hs::set_error(HS_ERR_NOT_CONVERGED, "PCG did not converge in %d iterations", maxit);
+    if (hsc.done == 2) return hs::set_error(HS_ERR_NOT_CONVERGED, "CG stopped: p.q <= 0 (no positive curvature)");
+    if (!conv) return hs::set_error(HS_ERR_NOT_CONVERGED, "PCG did not converge in %d iterations", maxit);
+    return HS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hs_pcg_solve(hs_matrix* A, int32_t prec_type, void* prec, const double* b, double* x, double rtol, int32_t maxit,
+                 void* stream, hs_solve_info* info) {
+    return pcg_impl(A, prec_type, prec, b, x, 0.0, rtol, maxit, stream, info, false);
+}
+
+int hs_cg_krylovjl(hs_matrix* A, int32_t prec_type, void* prec, const double* b, double* x, double atol, double rtol,
+                   int32_t itmax, void* stream, hs_solve_info* info) {
+    return pcg_impl(A, prec_type, prec, b, x, atol, rtol, itmax, stream, info, true);
+}
+
+// Krylov.jl's gmres with restart and a left preconditioner (LinearSolve's
+// KrylovJL_GMRES with Pl = P, restart length `memory`): the residual
+// estimate |zeta| of ||M^-1 (b - A x)|| is tested against
+// atol + rtol ||M^-1 b|| after every inner iteration.
+int hs_gmres_krylovjl(hs_matrix* A, int32_t prec_type, void* prec, int32_t memory, const double* b, double* x,
+                      double atol, double rtol, int32_t itmax, void* stream, hs_solve_info* info) {
+    if (!A || !b || !x || !info) return hs::set_error(HS_ERR_ARG, "hs_gmres_krylovjl: NULL argument");
+    if (prec_type != HS_PREC_NONE && !prec) return hs::set_error(HS_ERR_ARG, "preconditioner handle is NULL");
+    if (memory < 1 || memory > 1024) return hs::set_error(HS_ERR_ARG, "memory (restart length) must be in 1..1024");
+    if (itmax < 0 || !(rtol >= 0.0) || !(atol >= 0.0)) return hs::set_error(HS_ERR_ARG, "bad itmax or tolerances");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int64_t n = hs::matrix_n(A);
+    if (itmax == 0) itmax = (int32_t)std::min<int64_t>(2 * n, INT32_MAX);
+    const int m = memory;
+    const double btol = std::pow(2.220446049250313e-16, 0.75);
+    DevBuf buf;
+    double *V, *w, *q, *partials, *R, *c, *sv, *z, *y, *scal;
+    int* flag;
+    int rc;
+    if ((rc = buf.alloc(&V, 8 * (size_t)n * (m + 1))) || (rc = buf.alloc(&w, 8 * n)) || (rc = buf.alloc(&q, 8 * n)) ||
+        (rc = buf.alloc(&partials, 16 * (size_t)hsdev::kRedMaxBlocks)) ||
+        (rc = buf.alloc(&R, 8 * (size_t)(m + 1) * m)) || (rc = buf.alloc(&c, 8 * m)) || (rc = buf.alloc(&sv, 8 * m)) ||
+        (rc = buf.alloc(&z, 8 * (m + 1))) || (rc = buf.alloc(&y, 8 * m)) || (rc = buf.alloc(&scal, 16)) ||
+        (rc = buf.alloc(&flag, sizeof(int))))
+        return rc;
+    const int ge = grid_elems(n), nb = hsdev::red_blocks(n);
+    struct Events {   // released on every return path
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        ~Events() {
+            if (e0) cudaEventDestroy(e0);
+            if (e1) cudaEventDestroy(e1);
+        }
+    } evs;
+    HS_CUDA(cudaEventCreate(&evs.e0));
+    HS_CUDA(cudaEventCreate(&evs.e1));
+    cudaEventRecord(evs.e0, st);
+    auto norm_to = [&](const double* a, double* out) {   // *out = ||a|| on the device
+        dot_kernel<<<nb, kT, 0, st>>>(n, a, a, partials);
+        finalize_dd_kernel<<<1, kT, 0, st>>>(partials, nb, out, 1);
+        hs::count_launch(2);
+    };
+    auto read = [&](const double* d) -> double {
+        double v = 0;
+        cudaMemcpyAsync(&v, d, 8, cudaMemcpyDeviceToHost, st);
+        cudaStreamSynchronize(st);
+        return v;
+    };
+    zero_kernel<<<ge, kT, 0, st>>>(n, x);
+    hs::count_launch();
+    // r0 = M \ b in V_0's storage; beta0 = ||r0||
+    if ((rc = prec_apply(prec_type, prec, b, V, n, st))) return rc;
+    norm_to(V, scal + 1);
+    double beta = read(scal + 1);
+    double rn = beta;
+    const double eps = atol + rtol * rn;
+    int32_t iter = 0, npass = 0;
+    bool solved = rn <= eps, breakdown = false;
+    while (!(solved || iter >= itmax || breakdown)) {
+        HS_CUDA(cudaMemsetAsync(R, 0, 8 * (size_t)(m + 1) * m, st));
+        HS_CUDA(cudaMemsetAsync(z, 0, 8 * (size_t)(m + 1), st));
+        if (npass >= 1) {   // r0 = M \ (b - A x)
+            if ((rc = hs::matrix_spmv(A, x, w, 1.0, 0.0, st))) return rc;
+            rsub_kernel<<<ge, kT, 0, st>>>(n, b, w);
+            hs::count_launch();
+            if ((rc = prec_apply(prec_type, prec, w, V, n, st))) return rc;
+            norm_to(V, scal + 1);
+            beta = read(scal + 1);
+        }
+        HS_CUDA(cudaMemcpyAsync(z, &beta, 8, cudaMemcpyHostToDevice, st));
+        scale_from<<<ge, kT, 0, st>>>(n, V, scal + 1, V);   // V_0 = r0 / beta
+        hs::count_launch();
+        ++npass;
+        int k = 0;
+        while (true) {
+            const double* Vk = V + (size_t)k * n;
+            if ((rc = hs::matrix_spmv(A, Vk, w, 1.0, 0.0, st))) return rc;
+            if ((rc = prec_apply(prec_type, prec, w, q, n, st))) return rc;
+            for (int i = 0; i <= k; ++i) {   // modified Gram-Schmidt
+                const double* Vi = V + (size_t)i * n;
+                dot_kernel<<<nb, kT, 0, st>>>(n, Vi, q, partials);
+                mgs_axpy<<<ge, kT, 0, st>>>(n, partials, nb, Vi, q, R + (size_t)i * m + k);
+                hs::count_launch(2);
+            }
+            dot_kernel<<<nb, kT, 0, st>>>(n, q, q, partials);
+            kjl_arnoldi_close<<<1, kT, 0, st>>>(partials, nb, R, m, k, c, sv, z, scal, flag, eps, btol);
+            hs::count_launch(2);
+            int hflag = 0;
+            HS_CUDA(cudaMemcpyAsync(&hflag, flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+            HS_CUDA(cudaStreamSynchronize(st));
+            ++iter;
+            ++k;
+            solved = (hflag & 1) != 0;
+            breakdown = (hflag & 2) != 0;
+            if (solved || breakdown || k >= m || iter >= itmax) break;
+            scale_from<<<ge, kT, 0, st>>>(n, q, scal, V + (size_t)k * n);   // V_k = q / Hbis
+            hs::count_launch();
+        }
+        rn = read(scal + 1);
+        kjl_back_solve<<<1, 32, 0, st>>>(R, m, k, z, y, btol);
+        combine<<<ge, kT, 0, st>>>(n, V, n, k, y, w);
+        add_to<<<ge, kT, 0, st>>>(n, w, x);
+        hs::count_launch(3);
+    }
+    cudaEventRecord(evs.e1, st);
+    cudaEventSynchronize(evs.e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, evs.e0, evs.e1);
+    // true relative residual of x
+    copy_kernel<<<ge, kT, 0, st>>>(n, b, w);
+    hs::count_launch();
+    if ((rc = hs::matrix_spmv(A, x, w, -1.0, 1.0, st))) return rc;
+    norm_to(w, scal);
+    norm_to(b, scal + 1);
+    const double rr = read(scal), bn = read(scal + 1);
+    HS_CUDA(cudaGetLastError());
+    info->iterations = iter;
+    info->converged = solved ? 1 : 0;
+    info->relres = bn > 0 ? rr / bn : 0.0;
+    info->rnorm = rn;
+    info->ms = ms;
+    if (!solved) return hs::set_error(HS_ERR_NOT_CONVERGED, "GMRES did not converge in %d iterations", itmax);
     return HS_OK;
 }
 
@@ -655,6 +909,7 @@ int hs_gmres_solve(hs_matrix* A, int32_t prec_type, void* prec, int32_t restart,
     info->iterations = total;
     info->converged = conv ? 1 : 0;
     info->relres = bnorm > 0 ? beta / bnorm : 0.0;
+    info->rnorm = beta;
     info->ms = ms;
     if (!conv) return hs::set_error(HS_ERR_NOT_CONVERGED, "GMRES did not converge in %d iterations", maxit);
     return HS_OK;

@@ -30,6 +30,7 @@
 
 #include "internal.cuh"
 #include "l1gs_coop.cuh"
+#include "l1gs_seg.cuh"
 
 namespace {
 
@@ -1171,6 +1172,10 @@ struct hs_l1gs_s {
     hscoop::Geometry coop_geo;
     void* SC = nullptr;          // cooperative streams (all directions)
     hscoop::LaunchCache coop_lc;
+    // Matrix-view cache up to partsize 128: per-group segment lists of the
+    // in-block entries (the row-wise arrays are released after the build).
+    hsseg::View seg;
+    bool use_seg = false;
     int32_t sweep = 0, cache = 0, is_sym = 0, format = 0, mdt = 0, sdt = 0;
     double eta = 1.5;
     void* D = nullptr;
@@ -1217,6 +1222,7 @@ void release(hs_l1gs* P, cudaStream_t free_stream = nullptr) {
     for (cudaEvent_t e : P->hev) cudaEventDestroy(e);
     for (cudaStream_t q : P->hstream)
         if (q) cudaStreamDestroy(q);
+    hsseg::destroy(&P->seg);
     void* ptrs[] = {P->D, P->Di, P->SLi, P->SUi, P->SC, P->rp, P->ci, P->vs, P->dev_x, P->dev_y};
     for (void* q : ptrs)
         if (q) {
@@ -1252,64 +1258,55 @@ int validate_sparse(const hs_sparse* A) {
     return HS_OK;
 }
 
-// DiagonalIndices (src/l1_gauss_seidel.jl:422-436) on the host.
-template <typename TM>
-int diag_indices(const hs_sparse* A, std::vector<int32_t>& diag) {
-    const TM* val = static_cast<const TM*>(A->val);
-    diag.resize(A->n);
-    for (int32_t col = 0; col < A->n; ++col) {
-        const int32_t r1 = A->ptr[col], r2 = A->ptr[col + 1] - 1;
-        const int32_t* first = std::lower_bound(A->idx + r1, A->idx + r2 + 1, col);
-        const int32_t pos = (int32_t)(first - A->idx);
-        if (pos > r2 || A->idx[pos] != col || val[pos] == TM(0)) {
-            hs::set_error(HS_ERR_SINGULAR, "SingularException(%d): missing or zero diagonal", col + 1);
-            return hs::set_singular_col(col + 1);
-        }
-        diag[col] = pos;
+// Largest in-block strict-lower (caps[0]) and strict-upper (caps[1]) entry
+// count of any partition, from device row-wise arrays (the view kernels size
+// their shared-memory lists by it).  Thread per partition.
+__global__ void view_caps_kernel(int32_t n, int32_t ps, int32_t nparts, const int32_t* __restrict__ rp,
+                                 const int32_t* __restrict__ ci, int32_t* __restrict__ caps) {
+    for (int32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nparts; k += gridDim.x * blockDim.x) {
+        const int64_t s = (int64_t)k * ps, e = min(s + ps - 1, (int64_t)n - 1);
+        int32_t cl = 0, cu = 0;
+        for (int64_t i = s; i <= e; ++i)
+            for (int32_t q = rp[i]; q < rp[i + 1]; ++q) {
+                const int64_t j = ci[q];
+                cl += (j >= s && j < i);
+                cu += (j > i && j <= e);
+            }
+        atomicMax(caps, cl);
+        atomicMax(caps + 1, cu);
     }
-    return HS_OK;
 }
 
-// Stable CSC -> CSR transpose: iterating columns in order leaves every row's
-// entries in ascending column order.
-template <typename TM>
-void transpose(const hs_sparse* A, std::vector<int32_t>& rp, std::vector<int32_t>& ci, std::vector<TM>& v) {
-    const int32_t n = A->n;
-    const TM* val = static_cast<const TM*>(A->val);
-    rp.assign(n + 1, 0);
-    for (int64_t q = 0; q < A->nnz; ++q) rp[A->idx[q] + 1]++;
-    for (int32_t i = 0; i < n; ++i) rp[i + 1] += rp[i];
-    std::vector<int32_t> cur(rp.begin(), rp.end() - 1);
-    ci.resize(A->nnz);
-    v.resize(A->nnz);
-    for (int32_t col = 0; col < n; ++col)
-        for (int32_t q = A->ptr[col]; q < A->ptr[col + 1]; ++q) {
-            const int32_t r = A->idx[q];
-            ci[cur[r]] = col;
-            v[cur[r]] = val[q];
-            cur[r]++;
-        }
-}
+// Where setup_device finds the row-wise arrays.
+enum class Rows {
+    Host,            // host memory: uploaded here, released after setup (packed) or kept (view)
+    DeviceBorrowed,  // device memory owned by the caller, read during setup only (packed caches)
+    DeviceOwned      // device memory allocated for this handle (P->bytes counts it): kept or freed like Host
+};
 
-// `on_device`: the row-wise arrays are already in device memory (owned by the
-// caller and only read during setup; packed caches only).
 template <typename TM, typename TS>
 int setup_device(hs_l1gs* P, const int32_t* rp_h, const int32_t* ci_h, const TM* v_h, int64_t nnz,
-                 cudaStream_t st, bool on_device = false) {
+                 cudaStream_t st, Rows where = Rows::Host) {
     const int32_t n = P->n;
     int32_t *rp_d = nullptr, *ci_d = nullptr;
     TM* v_d = nullptr;
     int rc;
-    if (on_device) {
+    const bool on_device = where == Rows::DeviceBorrowed;
+    if (where != Rows::Host) {
         rp_d = const_cast<int32_t*>(rp_h);
         ci_d = const_cast<int32_t*>(ci_h);
         v_d = const_cast<TM*>(v_h);
+        if (where == Rows::DeviceOwned) {
+            P->rp = rp_d;
+            P->ci = ci_d;
+        }
     } else {
         if ((rc = dmalloc(P, &rp_d, sizeof(int32_t) * (n + 1)))) return rc;
         P->rp = rp_d;
         if ((rc = dmalloc(P, &ci_d, sizeof(int32_t) * nnz))) return rc;
         P->ci = ci_d;
         if ((rc = dmalloc(P, &v_d, sizeof(TM) * nnz))) return rc;
+        P->vs = v_d;   // the handle owns it from here (kept, converted or released below)
         HS_CUDA(cudaMemcpyAsync(rp_d, rp_h, sizeof(int32_t) * (n + 1), cudaMemcpyHostToDevice, st));
         HS_CUDA(cudaMemcpyAsync(ci_d, ci_h, sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, st));
         HS_CUDA(cudaMemcpyAsync(v_d, v_h, sizeof(TM) * nnz, cudaMemcpyHostToDevice, st));
@@ -1368,6 +1365,22 @@ int setup_device(hs_l1gs* P, const int32_t* rp_h, const int32_t* ci_h, const TM*
         P->bytes -= (int64_t)(sizeof(int32_t) * (n + 1 + nnz) + sizeof(TM) * nnz);
         P->rp = nullptr;
         P->ci = nullptr;
+        P->vs = nullptr;
+    } else if (P->ps <= hsseg::kMaxPartsize) {
+        // segment lists from the rows; the apply needs nothing else of the matrix
+        if ((rc = hsseg::build<TM, TS>(n, P->ps, P->nparts, rp_d, ci_d, v_d, lower, upper, &P->seg, st))) return rc;
+        P->bytes += P->seg.bytes;
+        P->use_seg = true;
+        HS_CUDA(cudaStreamSynchronize(st));
+        if (!on_device) {
+            cudaFree(rp_d);
+            cudaFree(ci_d);
+            cudaFree(v_d);
+            P->bytes -= (int64_t)(sizeof(int32_t) * (n + 1 + nnz) + sizeof(TM) * nnz);
+        }
+        P->rp = nullptr;
+        P->ci = nullptr;
+        P->vs = nullptr;
     } else {
         if (std::is_same<TM, TS>::value) {
             P->vs = v_d;
@@ -1383,17 +1396,34 @@ int setup_device(hs_l1gs* P, const int32_t* rp_h, const int32_t* ci_h, const TM*
         }
         // Shared-memory capacity: the largest in-block lower/upper count of any partition.
         int32_t ml = 0, mu = 0;
-        for (int64_t k = 0; k < P->nparts; ++k) {
-            const int64_t s = k * P->ps, e = std::min<int64_t>(s + P->ps - 1, n - 1);
-            int32_t cl = 0, cu = 0;
-            for (int64_t i = s; i <= e; ++i)
-                for (int32_t q = rp_h[i]; q < rp_h[i + 1]; ++q) {
-                    const int64_t j = ci_h[q];
-                    cl += (j >= s && j < i);
-                    cu += (j > i && j <= e);
-                }
-            ml = std::max(ml, cl);
-            mu = std::max(mu, cu);
+        if (where == Rows::Host) {
+            for (int64_t k = 0; k < P->nparts; ++k) {
+                const int64_t s = k * P->ps, e = std::min<int64_t>(s + P->ps - 1, n - 1);
+                int32_t cl = 0, cu = 0;
+                for (int64_t i = s; i <= e; ++i)
+                    for (int32_t q = rp_h[i]; q < rp_h[i + 1]; ++q) {
+                        const int64_t j = ci_h[q];
+                        cl += (j >= s && j < i);
+                        cu += (j > i && j <= e);
+                    }
+                ml = std::max(ml, cl);
+                mu = std::max(mu, cu);
+            }
+        } else {
+            int32_t* caps = nullptr;
+            HS_CUDA(cudaMalloc(&caps, 2 * sizeof(int32_t)));
+            cudaMemsetAsync(caps, 0, 2 * sizeof(int32_t), st);
+            view_caps_kernel<<<std::max(1, std::min((P->nparts + 255) / 256, 4096)), 256, 0, st>>>(
+                n, P->ps, P->nparts, P->rp, P->ci, caps);
+            int32_t hc[2] = {0, 0};
+            cudaError_t e1 = cudaGetLastError();
+            if (e1 == cudaSuccess) e1 = cudaMemcpyAsync(hc, caps, sizeof(hc), cudaMemcpyDeviceToHost, st);
+            if (e1 == cudaSuccess) e1 = cudaStreamSynchronize(st);
+            cudaFree(caps);
+            if (e1 != cudaSuccess) return hs::cuda_error(e1, "view_caps_kernel");
+            hs::count_launch();
+            ml = hc[0];
+            mu = hc[1];
         }
         const int32_t limit = 4096;
         P->cap_lo = lower ? std::min(ml, limit) : 0;
@@ -1524,9 +1554,12 @@ int launch_packed_t(hs_l1gs* P, const void* x, void* y, cudaStream_t st) {
             case 2: HS_SMALL(2, 4)
             case 4: HS_SMALL(4, 4)
             case 8: HS_SMALL(8, 4)
+            case 12: HS_SMALL(12, 4)
             case 16:
                 if (P->minb == 4) HS_SMALL(16, 4)
                 HS_SMALL(16, 3)
+            case 24: HS_SMALL(24, 3)
+            case 31: HS_SMALL(31, 3)
             case 32: HS_SMALL(32, 3)
             default: break;
         }
@@ -1695,6 +1728,11 @@ int launch_coop(hs_l1gs* P, const void* x, void* y, int io, cudaStream_t st) {
 template <typename T, typename IO>
 int launch_apply(hs_l1gs* P, const void* x, void* y, cudaStream_t st) {
     if (P->cache == HS_CACHE_PACKED && P->tpp > 1) return launch_coop(P, x, y, dtype_of<IO>::value, st);
+    if (P->cache == HS_CACHE_VIEW && P->use_seg) {
+        if (!P->err_word) P->err_word = hs::device_error_word();
+        return hsseg::launch(P->sdt, dtype_of<IO>::value, P->sweep, P->seg, P->n, P->ps, P->rng_beg,
+                             P->rng_end < 0 ? P->ngroups : P->rng_end, P->D, x, y, P->err_word, st);
+    }
     if (P->cache == HS_CACHE_PACKED) {
         switch (P->sweep) {
             case HS_SWEEP_FORWARD: return launch_packed_cfg<T, IO, 0>(P, x, y, st);
@@ -1887,36 +1925,65 @@ int l1gs_create_impl(const hs_sparse* A, bool on_device, int32_t partsize, int32
 
     // Row i of the preconditioner is read from: the CSR row; column i of a
     // CSC when isSymA (:1218-1229); the true row of a non-symmetric CSC,
-    // after DiagonalIndices validated the diagonal (:619, :422-436).
-    std::vector<int32_t> trp, tci;
-    std::vector<double> tv64;
-    std::vector<float> tv32;
+    // after DiagonalIndices validated the diagonal (:619, :422-436).  The
+    // non-symmetric CSC is uploaded as it is; DiagonalIndices and the
+    // transpose to rows run on the device.
     const int32_t* rp_h = A->ptr;
     const int32_t* ci_h = A->idx;
     const void* v_h = A->val;
+    Rows where = on_device ? Rows::DeviceBorrowed : Rows::Host;
     if (A->format == HS_CSC && !is_sym) {
-        rc = A->dtype == HS_F64 ? diag_indices<double>(A, P->diag) : diag_indices<float>(A, P->diag);
+        int32_t *rp_d = nullptr, *ci_d = nullptr, *dg = nullptr;
+        void* v_d = nullptr;
+        const size_t mes = dsize(A->dtype);
+        if ((rc = dmalloc(P, &rp_d, sizeof(int32_t) * ((size_t)A->n + 1))) ||
+            (rc = dmalloc(P, &ci_d, sizeof(int32_t) * (size_t)A->nnz)) ||
+            (rc = dmalloc(P, (char**)&v_d, mes * (size_t)A->nnz)) ||
+            (rc = dmalloc(P, &dg, sizeof(int32_t) * ((size_t)A->n + 1)))) {
+            cudaFree(rp_d);
+            cudaFree(ci_d);
+            cudaFree(v_d);
+            cudaFree(dg);
+            delete P;
+            return rc;
+        }
+        P->rp = rp_d;   // released with the handle on every path below
+        P->ci = ci_d;
+        P->vs = v_d;
+        int32_t* bad = dg + A->n;
+        int32_t nb = A->n, first_bad = 0;
+        cudaError_t e = cudaMemcpyAsync(bad, &nb, sizeof(int32_t), cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) rc = hs::csr_from_host(A, A->dtype, rp_d, ci_d, v_d, st, dg, bad);
+        else rc = hs::cuda_error(e, "DiagonalIndices");
+        if (!rc) {
+            P->diag.resize(A->n);
+            e = cudaMemcpyAsync(&first_bad, bad, sizeof(int32_t), cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(P->diag.data(), dg, sizeof(int32_t) * A->n, cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) rc = hs::cuda_error(e, "DiagonalIndices");
+        }
+        cudaFree(dg);
+        P->bytes -= (int64_t)(sizeof(int32_t) * ((size_t)A->n + 1));
+        if (!rc && first_bad < A->n) {
+            hs::set_error(HS_ERR_SINGULAR, "SingularException(%d): missing or zero diagonal", first_bad + 1);
+            rc = hs::set_singular_col(first_bad + 1);
+        }
         if (rc) {
             release(P);
             return rc;
         }
-        if (A->dtype == HS_F64) {
-            transpose<double>(A, trp, tci, tv64);
-            v_h = tv64.data();
-        } else {
-            transpose<float>(A, trp, tci, tv32);
-            v_h = tv32.data();
-        }
-        rp_h = trp.data();
-        ci_h = tci.data();
+        rp_h = rp_d;   // setup_device keeps the arrays (view cache) or releases them (packed)
+        ci_h = ci_d;
+        v_h = v_d;
+        where = Rows::DeviceOwned;
     }
 
     if (A->dtype == HS_F64 && smoother_dtype == HS_F64)
-        rc = setup_device<double, double>(P, rp_h, ci_h, static_cast<const double*>(v_h), A->nnz, st, on_device);
+        rc = setup_device<double, double>(P, rp_h, ci_h, static_cast<const double*>(v_h), A->nnz, st, where);
     else if (A->dtype == HS_F64)
-        rc = setup_device<double, float>(P, rp_h, ci_h, static_cast<const double*>(v_h), A->nnz, st, on_device);
+        rc = setup_device<double, float>(P, rp_h, ci_h, static_cast<const double*>(v_h), A->nnz, st, where);
     else
-        rc = setup_device<float, float>(P, rp_h, ci_h, static_cast<const float*>(v_h), A->nnz, st, on_device);
+        rc = setup_device<float, float>(P, rp_h, ci_h, static_cast<const float*>(v_h), A->nnz, st, where);
     if (rc) {
         release(P);
         return rc;

@@ -1,0 +1,68 @@
+// Matrix-view L1 Gauss-Seidel sweep over per-group segment lists.
+//
+// Reference: the MatrixViewCache sweep of src/l1_gauss_seidel.jl
+// (:1588-1597, :1600-1737) scans row i of the (adapted, device-resident)
+// matrix on every apply and sums the entries with start <= j < i (forward) or
+// i < j <= end (backward) in storage order -- ascending column.  Those
+// entries never change, so here they are gathered once, at build time, into
+// one stream per group of 32 partitions (lane = partition, as in the packed
+// sweeps): for each row of the partitions, in the order the sweep reaches
+// them, a number of slots equal to the largest count of any of the 32
+// partitions' rows there; slot k of row li holds, for every lane, the value
+// and the local column (j - start) of that partition's k-th in-block entry
+// ([value x 32][column x 32] per slot).  A lane adds only its own row's
+// entries (its count per row is kept beside the stream), in storage order,
+// with separately rounded multiply and add -- the reference's sequence, so
+// results are bit-identical; the zeros that fill short rows are never read
+// into a sum.  The apply streams exactly these slots (no out-of-block entry,
+// no row pointer) through a per-warp ring filled by 1D bulk copies.
+#pragma once
+
+#include <stdint.h>
+
+#include "hs_common.cuh"
+
+namespace hsseg {
+
+constexpr int kSlotsPerChunk(int es) { return es == 8 ? 6 : 10; }   // chunks of 1920 bytes, whole slots
+constexpr int kMaxPartsize = 128;                                    // y and D_Dl1 slices in shared memory
+
+// Device arrays of a segment-list view (one direction).
+struct Dir {
+    unsigned char* stream = nullptr;   // slots: [value x 32][uint16 column x 32]
+    int64_t* base = nullptr;           // first slot of each group
+    int32_t* total = nullptr;          // slots of each group
+    uint16_t* off = nullptr;           // [group][row]: first slot of the row (in the sweep's row order)
+    uint8_t* maxc = nullptr;           // [group][row]: slots of the row
+    uint8_t* cnt = nullptr;            // [group][row][lane]: the lane's own entries in the row
+    int64_t slots = 0;                 // all groups
+};
+
+struct View {
+    Dir lo, up;
+    int32_t ngroups = 0;
+    int64_t bytes = 0;   // device memory held
+};
+
+// Builds the lists from a device CSR (row-wise arrays of the preconditioner's
+// rows) in smoother type TS; sizes in P's geometry.  Allocates with
+// cudaMalloc (accounted in view->bytes).
+template <typename TM, typename TS>
+int build(int32_t n, int32_t ps, int32_t nparts, const int32_t* rp, const int32_t* ci, const TM* v, bool lower,
+          bool upper, View* view, cudaStream_t st);
+void destroy(View* view);
+
+struct Params {
+    int32_t n, ps, gbeg, gend;
+    Dir lo, up;
+    const void* D;
+    const void* x;
+    void* y;
+    int32_t* err;
+    uint32_t warp_bytes, ring_off, bars_off, ys_off, ds_off, nst;
+};
+
+int launch(int sdt, int io, int sweep, const View& view, int32_t n, int32_t ps, int32_t gbeg, int32_t gend,
+           const void* D, const void* x, void* y, int32_t* err, cudaStream_t st);
+
+}  // namespace hsseg

@@ -41,8 +41,9 @@ __all__ = [
     "CPU", "CUDABackend", "GPUConfig", "CPUConfig", "L1GSPrecBuilder", "L1GSPreconditioner",
     "ForwardSweep", "BackwardSweep", "SymmetricSweep", "PackedBufferCache", "MatrixViewCache",
     "Symmetric", "ldiv_", "backslash", "ChebyshevFourth", "ChebyshevFirst", "build_smoother",
-    "smooth_", "DeviceSparseMatrix", "mul_", "pcg", "gmres", "HSError", "SingularException",
-    "kernel_launches", "BlockPartitioning",
+    "smooth_", "DeviceSparseMatrix", "mul_", "pcg", "gmres", "cg_krylovjl", "gmres_krylovjl", "LinearProblem",
+    "KrylovJL_CG", "KrylovJL_GMRES", "solve", "HSError", "SingularException", "kernel_launches",
+    "BlockPartitioning",
 ]
 
 
@@ -524,3 +525,89 @@ def gmres(A, b, x, P=None, restart=30, rtol=1e-8, maxit=10000, stream=None):
     if st not in (_L.HS_OK, _L.HS_ERR_NOT_CONVERGED):
         check(st)
     return info
+
+
+def cg_krylovjl(A, b, x, P=None, atol=0.0, rtol=1e-8, itmax=0, stream=None):
+    """Krylov.jl's cg with M = P applied by ldiv! (FP64, device vectors):
+    stops when sqrt(r.z) <= atol + rtol sqrt(r0.z0), z = M^-1 r.  itmax 0 = 2n.
+    Returns hs_solve_info (iterations = Krylov.jl's niter)."""
+    import torch
+    t, h = _prec_args(P)
+    info = _L.hs_solve_info()
+    st = lib().hs_cg_krylovjl(A.handle, t, h, _dev_ptr(b, torch.float64), _dev_ptr(x, torch.float64), float(atol),
+                              float(rtol), int(itmax), _stream_ptr(stream), C.byref(info))
+    if st not in (_L.HS_OK, _L.HS_ERR_NOT_CONVERGED):
+        check(st)
+    return info
+
+
+def gmres_krylovjl(A, b, x, P=None, memory=30, atol=0.0, rtol=1e-8, itmax=0, stream=None):
+    """Krylov.jl's gmres with restart length `memory` and left preconditioner
+    M = P (as LinearSolve passes Pl): stops when the estimate of
+    ||M^-1 (b - A x)|| is at most atol + rtol ||M^-1 b||.  itmax 0 = 2n."""
+    import torch
+    t, h = _prec_args(P)
+    info = _L.hs_solve_info()
+    st = lib().hs_gmres_krylovjl(A.handle, t, h, int(memory), _dev_ptr(b, torch.float64), _dev_ptr(x, torch.float64),
+                                 float(atol), float(rtol), int(itmax), _stream_ptr(stream), C.byref(info))
+    if st not in (_L.HS_OK, _L.HS_ERR_NOT_CONVERGED):
+        check(st)
+    return info
+
+
+# ---------------------------------------------------------------------------
+# The caller's interface: LinearSolve.jl's solve(LinearProblem(A, b), alg; Pl)
+# (README.md:27-29, test/test_preconditioners.jl:65,93) on the device drivers.
+# ---------------------------------------------------------------------------
+class LinearProblem:
+    """LinearProblem(A, b): A a scipy.sparse CSC/CSR matrix, b a numpy vector."""
+
+    def __init__(self, A, b):
+        self.A, self.b = A, np.asarray(b, dtype=np.float64)
+
+
+class KrylovJL_CG:
+    """KrylovJL_CG(): Krylov.jl's cg."""
+
+
+class KrylovJL_GMRES:
+    """KrylovJL_GMRES(; gmres_restart = 0): Krylov.jl's gmres, restarted every
+    gmres_restart iterations; 0 (LinearSolve's default) runs without restart,
+    here for up to min(n, 1024) iterations (the Krylov basis is allocated up
+    front; beyond that it restarts)."""
+
+    def __init__(self, gmres_restart=0):
+        if gmres_restart < 0:
+            raise ValueError("gmres_restart must be >= 0")
+        self.gmres_restart = int(gmres_restart)
+
+
+class LinearSolution:
+    def __init__(self, u, info):
+        self.u = u
+        self.iters = int(info.iterations)
+        self.converged = bool(info.converged)
+        self.relres = float(info.relres)
+        self.resid = float(info.rnorm)
+        self.ms = float(info.ms)
+
+
+DEFAULT_TOL = float(np.sqrt(np.finfo(np.float64).eps))   # LinearSolve's default abstol and reltol
+
+
+def solve(prob, alg, Pl=None, abstol=DEFAULT_TOL, reltol=DEFAULT_TOL, maxiters=0, stream=None):
+    """solve(prob, alg; Pl, abstol, reltol, maxiters) -> solution with .u (host
+    vector) and .iters, on the device: the matrix and b are uploaded, Krylov.jl's
+    cg or gmres runs with Pl applied by ldiv! each iteration."""
+    import torch
+    A = DeviceSparseMatrix(prob.A, stream=stream)
+    b = torch.from_numpy(np.ascontiguousarray(prob.b)).cuda()
+    x = torch.zeros_like(b)
+    if isinstance(alg, KrylovJL_CG):
+        info = cg_krylovjl(A, b, x, Pl, atol=abstol, rtol=reltol, itmax=maxiters, stream=stream)
+    elif isinstance(alg, KrylovJL_GMRES):
+        memory = alg.gmres_restart if alg.gmres_restart > 0 else min(A.n, 1024)
+        info = gmres_krylovjl(A, b, x, Pl, memory=memory, atol=abstol, rtol=reltol, itmax=maxiters, stream=stream)
+    else:
+        raise TypeError("alg must be KrylovJL_CG() or KrylovJL_GMRES()")
+    return LinearSolution(x.cpu().numpy(), info)

@@ -59,7 +59,8 @@ class hs_cheb_info(C.Structure):
 
 
 class hs_solve_info(C.Structure):
-    _fields_ = [("iterations", C.c_int32), ("converged", C.c_int32), ("relres", C.c_double), ("ms", C.c_double)]
+    _fields_ = [("iterations", C.c_int32), ("converged", C.c_int32), ("relres", C.c_double), ("ms", C.c_double),
+                ("rnorm", C.c_double)]
 
 
 class hs_batch_config(C.Structure):
@@ -109,6 +110,8 @@ PROTOTYPES = {
     "hs_richardson_destroy": (C.c_int, [_vp]),
     "hs_pcg_solve": (C.c_int, [_vp, _i32, _vp, _vp, _vp, _d, _i32, _vp, C.POINTER(hs_solve_info)]),
     "hs_gmres_solve": (C.c_int, [_vp, _i32, _vp, _i32, _vp, _vp, _d, _i32, _vp, C.POINTER(hs_solve_info)]),
+    "hs_cg_krylovjl": (C.c_int, [_vp, _i32, _vp, _vp, _vp, _d, _d, _i32, _vp, C.POINTER(hs_solve_info)]),
+    "hs_gmres_krylovjl": (C.c_int, [_vp, _i32, _vp, _i32, _vp, _vp, _d, _d, _i32, _vp, C.POINTER(hs_solve_info)]),
     "hs_batch_create": (C.c_int, [C.POINTER(hs_batch_config), _vp, C.POINTER(_vp)]),
     "hs_batch_submit": (C.c_int, [_vp, C.POINTER(hs_sparse), _vp, _vp, _i64, _i32, C.POINTER(_i32)]),
     "hs_batch_step": (C.c_int, [_vp, _i32, C.POINTER(_i32)]),

@@ -106,10 +106,13 @@ def percentile(v, q):
 
 
 def serve(requests, max_slots=64, hbm_budget=64 << 30, iters_per_step=4, rtol=1e-8, partsize_of=None,
-          realtime=True, maxit=5000, admit_per_step=8):
+          realtime=True, maxit=5000, admit_per_step=8, tuner=None):
     """Continuous-batching replay of [(arrival_s, A, b)].
 
-    partsize_of(A) -> 8/16/32 (the autotuner); default 16.  At most
+    partsize_of(A) -> 8/16/32 (e.g. Autotuner.partsize_of); default 16.
+    tuner: an OnlineTuner (partsize_for(A, tag) at admission, observe(tag,
+    iterations) when the solve finishes), which learns the partsize from
+    the served solves themselves.  At most
     `admit_per_step` requests are admitted per step once systems are running,
     so their host-side preparation overlaps the GPU's iterations instead of
     delaying the first launch.
@@ -135,8 +138,13 @@ def serve(requests, max_slots=64, hbm_budget=64 << 30, iters_per_step=4, rtol=1e
         while waiting and admitted < admit_per_step:
             i = waiting[0]
             _, A, b = requests[i]
-            ps = partsize_of(A) if partsize_of else 16
+            if tuner is not None:
+                ps = tuner.partsize_for(A, i)
+            else:
+                ps = partsize_of(A) if partsize_of else 16
             if not eng.submit(A, b, i, ps):
+                if tuner is not None:
+                    tuner.cancel(i)   # not admitted now: its partsize is handed out again later
                 break
             waiting.popleft()
             active += 1
@@ -152,6 +160,8 @@ def serve(requests, max_slots=64, hbm_budget=64 << 30, iters_per_step=4, rtol=1e
                 done_at[tag] = time.perf_counter() - t0
                 iters[tag], conv[tag], xs[tag] = it, ok, x
                 active -= 1
+                if tuner is not None and tag in tuner.tags:
+                    tuner.observe(tag, it)
         else:
             admit()
             if not active and waiting:

@@ -242,12 +242,33 @@ typedef struct {
     int32_t converged;
     double relres;      /* true ||b - A x|| / ||b|| at exit */
     double ms;          /* device time of the solve */
+    double rnorm;       /* the residual norm the stopping test used, at exit */
 } hs_solve_info;
 
+/* This library's PCG: stops when the recursive residual satisfies
+ * ||r|| <= rtol ||b||. */
 int hs_pcg_solve(hs_matrix* A, int32_t prec_type, void* prec, const double* b, double* x,
                  double rtol, int32_t maxit, void* stream, hs_solve_info* info);
+/* This library's restarted GMRES(m), right preconditioned (CGS2): stops when
+ * ||b - A x|| <= rtol ||b||. */
 int hs_gmres_solve(hs_matrix* A, int32_t prec_type, void* prec, int32_t restart, const double* b,
                    double* x, double rtol, int32_t maxit, void* stream, hs_solve_info* info);
+
+/* Krylov.jl's cg as LinearSolve.solve(LinearProblem(A, b), KrylovJL_CG(); Pl = P)
+ * runs it (test/test_preconditioners.jl:93, README.md:29): M = P applied with
+ * ldiv!, x0 = 0, stop when sqrt(r.z) <= atol + rtol sqrt(r0.z0) with z = M^-1 r
+ * (the preconditioned residual norm).  itmax 0 = 2n.  info->iterations is
+ * Krylov.jl's niter, info->rnorm the final sqrt(r.z). */
+int hs_cg_krylovjl(hs_matrix* A, int32_t prec_type, void* prec, const double* b, double* x,
+                   double atol, double rtol, int32_t itmax, void* stream, hs_solve_info* info);
+/* Krylov.jl's gmres as KrylovJL_GMRES(gmres_restart = memory) with Pl = P
+ * runs it (test/test_preconditioners.jl:65): left preconditioner, modified
+ * Gram-Schmidt, symmetric Givens reflections, restart after `memory` inner
+ * iterations; stop when the estimate of ||M^-1 (b - A x)|| is at most
+ * atol + rtol ||M^-1 b||.  itmax 0 = 2n. */
+int hs_gmres_krylovjl(hs_matrix* A, int32_t prec_type, void* prec, int32_t memory, const double* b,
+                      double* x, double atol, double rtol, int32_t itmax, void* stream,
+                      hs_solve_info* info);
 
 /* ---------------------------------------------------------------------- */
 /* Batched, served PCG (no counterpart in the reference: the serving and   */

@@ -9,10 +9,12 @@
  * known-answer vector in the reference's test suite
  * (test/test_preconditioners.jl, test/test_chebyshev.jl, test/gpu/gpu.jl) and
  * the a* table of src/chebyshev.jl:208-210; tests/test_oracle_kat.py checks
- * them.  The Krylov drivers (PCG, restarted GMRES) stand in for Krylov.jl,
- * which the reference reaches through LinearSolve.jl and does not vendor:
- * their iteration counts are this oracle's own and are not pinned to Krylov.jl.
- * Their dot products are compensated (Dot2) and every update separately
+ * them.  Two pairs of Krylov drivers: hso_cg_kjl / hso_gmres_kjl restate
+ * Krylov.jl's cg and gmres as the reference calls them through LinearSolve.jl
+ * (Krylov.jl is not vendored: restated from its published algorithms, the
+ * reference's call sites test/test_preconditioners.jl:65,93 and README.md:29);
+ * hso_pcg / hso_gmres are this project's own drivers (true-residual stopping,
+ * CGS2).  Dot products are compensated (Dot2) and every update separately
  * rounded, the arithmetic the device drivers use.
  */
 #include <math.h>
@@ -267,6 +269,196 @@ out:
 #undef HH
     free(V); free(w); free(H); free(cs); free(sn); free(g); free(yv); free(hcol);
     return conv ? total : -1;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Krylov.jl's CG and GMRES as LinearSolve.jl's KrylovJL_CG / KrylovJL_GMRES */
+/* call them with Pl = P (test/test_preconditioners.jl:65,93): M = P applied */
+/* with ldiv! (z = P \ r), x0 = 0, stopping at rNorm <= atol + rtol*rNorm0.  */
+/* Restated from the published algorithms of Krylov.jl (0.9/0.10, src/cg.jl  */
+/* and src/gmres.jl; not vendored in the reference).  Dot products and norms */
+/* are the compensated sums above (Krylov.jl calls BLAS, whose summation     */
+/* order is the library's own); updates are separately rounded.              */
+/* ------------------------------------------------------------------------ */
+
+/*
+ * cg!: r = b, z = M \ r, p = z, gamma = r.z, rNorm = sqrt(gamma),
+ * eps = atol + rtol*rNorm; each iteration q = A p, alpha = gamma / p.q,
+ * x += alpha p, r -= alpha q, z = M \ r, gamma' = r.z, rNorm = sqrt(gamma');
+ * stop when rNorm <= eps (or rNorm + 1 <= 1), else p = z + (gamma'/gamma) p.
+ * A non-positive p.q (zero or negative curvature) stops without convergence.
+ * itmax 0 means 2n.  Returns the iteration count (Krylov.jl's niter), or -1
+ * when not solved; *relres = ||b - A x|| / ||b||, *rnorm = the final rNorm.
+ */
+int32_t hso_cg_kjl(int32_t n, const int32_t* rp, const int32_t* ci, const double* v, const double* b, double* x,
+                   const hso_prec* P, double atol, double rtol, int32_t itmax, double* relres, double* rnorm)
+{
+    double* r = (double*)malloc(sizeof(double) * (size_t)n * 4);
+    double* z = r + n;
+    double* p = z + n;
+    double* q = p + n;
+    if (itmax <= 0) itmax = 2 * n;
+    for (int32_t i = 0; i < n; ++i) { x[i] = 0.0; r[i] = b[i]; }
+    prec_apply(n, P, r, z);
+    memcpy(p, z, sizeof(double) * (size_t)n);
+    double gamma = dot(n, r, z);
+    double rn = sqrt(gamma);
+    const double eps = atol + rtol * rn;
+    int32_t iter = 0, solved = (gamma == 0.0) || (rn <= eps), failed = 0;
+    while (!solved && iter < itmax) {
+        hso_spmv_f64(n, rp, ci, v, p, q);
+        const double pq = dot(n, p, q);
+        if (!(pq > 0.0)) { failed = 1; break; }
+        const double alpha = gamma / pq;
+        for (int32_t i = 0; i < n; ++i) { x[i] = x[i] + alpha * p[i]; r[i] = r[i] - alpha * q[i]; }
+        prec_apply(n, P, r, z);
+        const double gnew = dot(n, r, z);
+        rn = sqrt(gnew);
+        ++iter;
+        solved = (rn <= eps) || (rn + 1.0 <= 1.0);
+        if (!solved) {
+            const double beta = gnew / gamma;
+            gamma = gnew;
+            for (int32_t i = 0; i < n; ++i) p[i] = z[i] + beta * p[i];
+        }
+    }
+    const double bnorm = sqrt(dot(n, b, b));
+    hso_spmv_f64(n, rp, ci, v, x, q);
+    for (int32_t i = 0; i < n; ++i) q[i] = b[i] - q[i];
+    *relres = bnorm > 0 ? sqrt(dot(n, q, q)) / bnorm : 0.0;
+    *rnorm = rn;
+    free(r);
+    return (solved && !failed) ? iter : -1;
+}
+
+/*
+ * Symmetric Givens reflection [c s; s -c] [a; b] = [rho; 0] (the stable
+ * form of Golub & Van Loan / Bindel, Demmel & Kahan that Krylov.jl's
+ * sym_givens computes).
+ */
+static void sym_givens(double a, double b, double* c, double* s, double* rho)
+{
+    if (b == 0.0) {
+        *c = (a == 0.0) ? 1.0 : copysign(1.0, a);
+        *s = 0.0;
+        *rho = fabs(a);
+    } else if (a == 0.0) {
+        *c = 0.0;
+        *s = copysign(1.0, b);
+        *rho = fabs(b);
+    } else if (fabs(b) > fabs(a)) {
+        const double t = a / b;
+        *s = copysign(1.0, b) / sqrt(1.0 + t * t);
+        *c = *s * t;
+        *rho = b / *s;
+    } else {
+        const double t = b / a;
+        *c = copysign(1.0, a) / sqrt(1.0 + t * t);
+        *s = *c * t;
+        *rho = a / *c;
+    }
+}
+
+/*
+ * gmres! with restart = true and memory m, left preconditioner M:
+ * r0 = M \ (b - A x) (x = 0 first), beta = ||r0||, eps = atol + rtol*beta0.
+ * A cycle sets z_1 = beta, V_1 = r0 / beta; inner iteration k: q = M \ (A V_k),
+ * modified Gram-Schmidt R_ik = V_i.q, q -= R_ik V_i (i = 1..k, in order),
+ * Hbis = ||q||, the previous reflections applied to column k of R, a new one
+ * from sym_givens(R_kk, Hbis), zeta_{k+1} = s_k z_k, z_k = c_k z_k,
+ * rNorm = |zeta_{k+1}|; the cycle ends when rNorm <= eps (or rNorm + 1 <= 1),
+ * k = m, the iteration cap, or breakdown (Hbis <= btol = eps(double)^(3/4));
+ * otherwise V_{k+1} = q / Hbis, z_{k+1} = zeta_{k+1}.  Then y = R \ z by back
+ * substitution (columns from the last; y_i = 0 where |R_ii| <= btol) and
+ * x += sum_i y_i V_i.  Returns niter (total inner iterations) or -1.
+ */
+int32_t hso_gmres_kjl(int32_t n, const int32_t* rp, const int32_t* ci, const double* v, const double* b, double* x,
+                      const hso_prec* P, int32_t m, double atol, double rtol, int32_t itmax, double* relres,
+                      double* rnorm)
+{
+    const double btol = pow(2.220446049250313e-16, 0.75);
+    double* V = (double*)malloc(sizeof(double) * (size_t)n * (m + 1));
+    double* w = (double*)malloc(sizeof(double) * (size_t)n * 3);
+    double* q = w + n;
+    double* xr = q + n;
+    double* R = (double*)calloc((size_t)(m + 1) * m, sizeof(double));
+    double* c = (double*)calloc((size_t)m, sizeof(double));
+    double* s = (double*)calloc((size_t)m, sizeof(double));
+    double* z = (double*)calloc((size_t)m + 1, sizeof(double));
+    double* yv = (double*)calloc((size_t)m, sizeof(double));
+#define RR(i, j) R[(size_t)(i) * m + (j)]
+    if (itmax <= 0) itmax = 2 * n;
+    for (int32_t i = 0; i < n; ++i) x[i] = 0.0;
+    prec_apply(n, P, b, V);   /* r0 = M \ b, in V_1's storage */
+    double beta = sqrt(dot(n, V, V));
+    double rn = beta;
+    const double eps = atol + rtol * rn;
+    int32_t iter = 0, npass = 0, solved = rn <= eps, breakdown = 0;
+    while (!(solved || iter >= itmax || breakdown)) {
+        memset(R, 0, sizeof(double) * (size_t)(m + 1) * m);
+        memset(z, 0, sizeof(double) * (size_t)(m + 1));
+        if (npass >= 1) {
+            hso_spmv_f64(n, rp, ci, v, x, w);
+            for (int32_t i = 0; i < n; ++i) w[i] = b[i] - w[i];
+            prec_apply(n, P, w, V);
+            beta = sqrt(dot(n, V, V));
+        }
+        z[0] = beta;
+        for (int32_t i = 0; i < n; ++i) V[i] = V[i] / beta;
+        ++npass;
+        int32_t k = 0;
+        int32_t inner_done = 0;
+        while (!inner_done) {
+            const double* Vk = V + (size_t)k * n;
+            hso_spmv_f64(n, rp, ci, v, Vk, w);
+            prec_apply(n, P, w, q);
+            for (int32_t i = 0; i <= k; ++i) {
+                const double* Vi = V + (size_t)i * n;
+                const double h = dot(n, Vi, q);
+                RR(i, k) = h;
+                for (int32_t t = 0; t < n; ++t) q[t] = q[t] - h * Vi[t];
+            }
+            const double hbis = sqrt(dot(n, q, q));
+            for (int32_t i = 0; i < k; ++i) {
+                const double tmp = c[i] * RR(i, k) + s[i] * RR(i + 1, k);
+                RR(i + 1, k) = s[i] * RR(i, k) - c[i] * RR(i + 1, k);
+                RR(i, k) = tmp;
+            }
+            sym_givens(RR(k, k), hbis, &c[k], &s[k], &RR(k, k));
+            const double zeta = s[k] * z[k];
+            z[k] = c[k] * z[k];
+            rn = fabs(zeta);
+            ++iter;
+            ++k;
+            solved = (rn <= eps) || (rn + 1.0 <= 1.0);
+            breakdown = hbis <= btol;
+            inner_done = solved || breakdown || k >= m || iter >= itmax;
+            if (!inner_done) {
+                double* Vn = V + (size_t)k * n;
+                for (int32_t t = 0; t < n; ++t) Vn[t] = q[t] / hbis;
+                z[k] = zeta;
+            }
+        }
+        for (int32_t i = k - 1; i >= 0; --i) {
+            double yi = z[i];
+            for (int32_t j = k - 1; j > i; --j) yi = yi - RR(i, j) * yv[j];
+            yv[i] = fabs(RR(i, i)) <= btol ? 0.0 : yi / RR(i, i);
+        }
+        for (int32_t t = 0; t < n; ++t) xr[t] = 0.0;
+        for (int32_t i = 0; i < k; ++i) {
+            const double* Vi = V + (size_t)i * n;
+            for (int32_t t = 0; t < n; ++t) xr[t] = xr[t] + yv[i] * Vi[t];
+        }
+        for (int32_t t = 0; t < n; ++t) x[t] = x[t] + xr[t];
+    }
+    const double bnorm = sqrt(dot(n, b, b));
+    hso_spmv_f64(n, rp, ci, v, x, w);
+    for (int32_t i = 0; i < n; ++i) w[i] = b[i] - w[i];
+    *relres = bnorm > 0 ? sqrt(dot(n, w, w)) / bnorm : 0.0;
+    *rnorm = rn;
+#undef RR
+    free(V); free(w); free(R); free(c); free(s); free(z); free(yv);
+    return solved ? iter : -1;
 }
 
 int32_t hso_omp_max_threads(void)

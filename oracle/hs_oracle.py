@@ -64,6 +64,8 @@ def lib():
             getattr(L, "hso_cheb1_astar" + sfx).argtypes = [C.c_int32]
         L.hso_pcg.restype = C.c_int32
         L.hso_gmres.restype = C.c_int32
+        L.hso_cg_kjl.restype = C.c_int32
+        L.hso_gmres_kjl.restype = C.c_int32
         L.hso_omp_max_threads.restype = C.c_int32
         _lib = L
     return _lib
@@ -396,6 +398,39 @@ def gmres(A, b, P=None, m=30, rtol=1e-8, maxit=10000):
                          _p(np.ascontiguousarray(b, dtype=np.float64)), _p(x), C.byref(s),
                          C.c_int32(m), C.c_double(rtol), C.c_int32(maxit), C.byref(rel))
     return x, int(it), float(rel.value)
+
+
+def cg_krylovjl(A, b, P=None, atol=0.0, rtol=1e-8, itmax=0):
+    """Krylov.jl's cg (M = P applied with ldiv!), restated in
+    hs_oracle.c:hso_cg_kjl.  Returns (x, niter or -1, true relative residual,
+    final preconditioned residual norm)."""
+    Ar = A.tocsr().astype(np.float64)
+    Ar.sort_indices()
+    n = Ar.shape[0]
+    x = np.zeros(n)
+    rel, rn = C.c_double(), C.c_double()
+    s, keep = _prec_struct(P)
+    it = lib().hso_cg_kjl(C.c_int32(n), _p(_i32(Ar.indptr)), _p(_i32(Ar.indices)), _p(Ar.data),
+                          _p(np.ascontiguousarray(b, dtype=np.float64)), _p(x), C.byref(s), C.c_double(atol),
+                          C.c_double(rtol), C.c_int32(itmax), C.byref(rel), C.byref(rn))
+    return x, int(it), float(rel.value), float(rn.value)
+
+
+def gmres_krylovjl(A, b, P=None, memory=30, atol=0.0, rtol=1e-8, itmax=0):
+    """Krylov.jl's gmres with restart (memory = restart length) and left
+    preconditioner M = P (as LinearSolve passes Pl), restated in
+    hs_oracle.c:hso_gmres_kjl.  Returns (x, niter or -1, true relative
+    residual, final residual estimate)."""
+    Ar = A.tocsr().astype(np.float64)
+    Ar.sort_indices()
+    n = Ar.shape[0]
+    x = np.zeros(n)
+    rel, rn = C.c_double(), C.c_double()
+    s, keep = _prec_struct(P)
+    it = lib().hso_gmres_kjl(C.c_int32(n), _p(_i32(Ar.indptr)), _p(_i32(Ar.indices)), _p(Ar.data),
+                             _p(np.ascontiguousarray(b, dtype=np.float64)), _p(x), C.byref(s), C.c_int32(memory),
+                             C.c_double(atol), C.c_double(rtol), C.c_int32(itmax), C.byref(rel), C.byref(rn))
+    return x, int(it), float(rel.value), float(rn.value)
 
 
 def amg_richardson(A, P, x, b, sweeps=2):

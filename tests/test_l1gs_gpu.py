@@ -168,8 +168,8 @@ def random_matrix(n, density, seed, sym=False):
     return W._canon(A.tocsc())
 
 
-CASES = [(1, 37), (2, 40), (3, 100), (5, 101), (16, 1000), (17, 999), (31, 700), (32, 2048), (33, 1111),
-         (64, 3000), (100, 2345), (256, 4000)]
+CASES = [(1, 37), (2, 40), (3, 100), (5, 101), (12, 1234), (16, 1000), (17, 999), (24, 2000), (31, 700),
+         (32, 2048), (33, 1111), (64, 3000), (100, 2345), (256, 4000)]
 
 
 @pytest.mark.parametrize("ps,n", CASES)
