@@ -480,6 +480,16 @@ def suite_serving(args):
     reqs = W.serving_stream(count=args.serving_count, lo=1e3, hi=args.serving_max)
     gen_s = time.perf_counter() - t0
     rows = sum(A.shape[0] for _, A, _ in reqs)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world > 1:
+        # one engine per GPU over its share of the stream (closed loop)
+        closed = serving.serve_sharded([(0.0, A, b) for _, A, b in reqs], max_slots=64, iters_per_step=8,
+                                       tuner=OnlineTuner())
+        return {"suite": "serving", "workload": f"{len(reqs)} 2D-5pt/3D-7pt variable-coefficient SPD systems, "
+                                                 f"n log-uniform [1e3, {args.serving_max:.0e}], PCG 1e-8",
+                "ranks": world, "total_rows": rows, "generate_s": gen_s,
+                "served_fp32_batched_closed_loop": {"solves_per_s": closed["solves_per_s"], "p50_s": closed["p50_s"],
+                                                    "p99_s": closed["p99_s"], "wall_s": closed["wall_s"]}}
     seq = serving.solve_sequential(reqs, partsize=16)
     # closed loop (all requests waiting at t=0): throughput; the partsize
     # tuner learns from the served solves, inside the timed run
@@ -565,11 +575,19 @@ def main():
     if args.suite:
         import torch
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        if world > 1:   # only the serving suite shards (requests across ranks, no collective on the solves)
+            import torch.distributed as dist
+            from datetime import timedelta
+            dist.init_process_group("gloo", timeout=timedelta(seconds=600))
         for name in args.suite.split(","):
             t0 = time.perf_counter()
             res = SUITES[name](args)
             res["seconds"] = round(time.perf_counter() - t0, 1)
-            print(json.dumps(res), flush=True)
+            if int(os.environ.get("RANK", "0")) == 0:
+                print(json.dumps(res), flush=True)
+        if world > 1:
+            dist.destroy_process_group()
         return
     wl = parse_workload(args.workload)
     rank = int(os.environ.get("RANK", "0"))

@@ -31,6 +31,7 @@
 #pragma once
 
 #include <algorithm>
+#include <cstdlib>
 
 #include "hs_common.cuh"
 
@@ -86,13 +87,24 @@ struct Geometry {
 
 inline Geometry make_geometry(const Layout& L, size_t es) {
     Geometry g;
-    const uint32_t che = (uint32_t)(2048 / es);
+    // Tuning overrides: HSB200_COOP_CHUNK = chunk bytes (1024, 2048 or 4096),
+    // HSB200_COOP_AHEAD = chunks kept in flight beyond a column block (1..8).
+    uint32_t chunk_bytes = 2048, ahead = 2;
+    if (const char* env = getenv("HSB200_COOP_CHUNK")) {
+        const int v = atoi(env);
+        if (v == 1024 || v == 2048 || v == 4096) chunk_bytes = (uint32_t)v;
+    }
+    if (const char* env = getenv("HSB200_COOP_AHEAD")) {
+        const int v = atoi(env);
+        if (v >= 1 && v <= 8) ahead = (uint32_t)v;
+    }
+    const uint32_t che = (uint32_t)(chunk_bytes / es);
     while ((1u << g.che_log2) < che) ++g.che_log2;
     const int64_t maxcol = (int64_t)L.G * (L.ps - 1);        // entries of the longest column block
     g.ntail = (uint32_t)std::max<int64_t>(1, (maxcol + che - 1) / che);
-    // A column block spans at most ntail + 1 chunks; keep at least two more in flight.
+    // A column block spans at most ntail + 1 chunks; keep `ahead` more in flight.
     g.nst = 4;
-    while (g.nst < g.ntail + 3) g.nst *= 2;
+    while (g.nst < g.ntail + 1 + ahead) g.nst *= 2;
     const size_t ring = (size_t)(g.nst + g.ntail) * che * es;
     g.bars_off = (uint32_t)ring;
     g.ys_off = (uint32_t)((ring + 8 * g.nst + 15) / 16 * 16);

@@ -106,19 +106,21 @@ def percentile(v, q):
 
 
 def serve(requests, max_slots=64, hbm_budget=64 << 30, iters_per_step=4, rtol=1e-8, partsize_of=None,
-          realtime=True, maxit=5000, admit_per_step=8, tuner=None):
+          realtime=True, maxit=5000, admit_per_step=8, tuner=None, engine_factory=None):
     """Continuous-batching replay of [(arrival_s, A, b)].
 
     partsize_of(A) -> 8/16/32 (e.g. Autotuner.partsize_of); default 16.
     tuner: an OnlineTuner (partsize_for(A, tag) at admission, observe(tag,
     iterations) when the solve finishes), which learns the partsize from
-    the served solves themselves.  At most
+    the served solves themselves.  engine_factory(max_slots, hbm_budget,
+    rtol, maxit) builds the engine (default: BatchEngine).  At most
     `admit_per_step` requests are admitted per step once systems are running,
     so their host-side preparation overlaps the GPU's iterations instead of
     delaying the first launch.
     Returns dict with per-request latency, iterations, results and totals.
     """
-    eng = BatchEngine(max_slots=max_slots, hbm_budget=hbm_budget, rtol=rtol, maxit=maxit)
+    factory = engine_factory or (lambda ms, hb, rt, mi: BatchEngine(max_slots=ms, hbm_budget=hb, rtol=rt, maxit=mi))
+    eng = factory(max_slots, hbm_budget, rtol, maxit)
     order = sorted(range(len(requests)), key=lambda i: requests[i][0])
     pending = deque(order)
     waiting = deque()
@@ -201,3 +203,29 @@ def solve_sequential(requests, partsize=16, rtol=1e-8, precision=None, maxit=500
     total = time.perf_counter() - t0
     return {"wall_s": total, "solves_per_s": len(requests) / total, "latency_s": lat, "iterations": iters,
             "p50_s": percentile(lat, 50), "p99_s": percentile(lat, 99)}
+
+
+def serve_sharded(requests, **kw):
+    """serve() across the ranks of a process group, one GPU each: rank r
+    takes requests r, r + world, ... (each arrives at its own time) and runs
+    its own engine; no collective touches the solves.  Returns, on every
+    rank, the whole job's figures: solves/s = all solves / the slowest
+    rank's wall time, p50/p99 over all requests, and {request: x}."""
+    import torch.distributed as dist
+    from . import distributed as D
+    rank, world = (dist.get_rank(), dist.get_world_size()) if dist.is_initialized() else (0, 1)
+    mine = D.shard(list(range(len(requests))), rank, world)
+    res = serve([requests[i] for i in mine], **kw)
+    local = {"lat": res["latency_s"], "wall": res["wall_s"],
+             "x": {mine[k]: v for k, v in res["x"].items()},
+             "it": {mine[k]: v for k, v in res["iterations"].items()}}
+    parts = [local]
+    if world > 1:
+        parts = [None] * world
+        dist.all_gather_object(parts, local)
+    lat = [t for p_ in parts for t in p_["lat"]]
+    wall = max(p_["wall"] for p_ in parts)
+    xs = {k: v for p_ in parts for k, v in p_["x"].items()}
+    its = {k: v for p_ in parts for k, v in p_["it"].items()}
+    return {"solves": len(xs), "wall_s": wall, "solves_per_s": len(xs) / wall, "p50_s": percentile(lat, 50),
+            "p99_s": percentile(lat, 99), "x": xs, "iterations": its, "ranks": world}

@@ -96,17 +96,25 @@ mutable struct L1GSPreconditioner{T}
     n::Int
 end
 
+struct HsL1gsOptions
+    threads_per_part::Int32   # 0: the library's choice; 1: thread per partition; 4/8/16/32 lanes
+    order::Int32              # 0: the library's choice; 1: the reference's summation order; 2: reordered
+end
+
 function (b::L1GSPrecBuilder)(A::SparseMatrixCSC{T}, partsize::Integer = b.device_config.blocks;
                               isSymA::Bool = false, η = 1.5, sweep::AbstractSweep = SymmetricSweep(),
                               cache_strategy::AbstractCacheStrategy = PackedBufferCache(),
-                              precision::Type = T) where {T}
+                              precision::Type = T, threads_per_part::Integer = 0,
+                              order::Symbol = :auto) where {T}
     partsize == 0 && error("partsize must be greater than 0")
     h = Ref{Ptr{Cvoid}}(C_NULL)
+    opts = HsL1gsOptions(threads_per_part, order === :reference ? 1 : order === :any ? 2 : 0)
     with_desc(A) do d
-        check(ccall((:hs_l1gs_create, libhsb200), Cint,
-                    (Ref{HsSparse}, Int32, Int32, Cdouble, Int32, Int32, Int32, Int32, Int32, Ptr{Cvoid}, Ref{Ptr{Cvoid}}),
+        check(ccall((:hs_l1gs_create_opts, libhsb200), Cint,
+                    (Ref{HsSparse}, Int32, Int32, Cdouble, Int32, Int32, Int32, Int32, Int32, Ref{HsL1gsOptions},
+                     Ptr{Cvoid}, Ref{Ptr{Cvoid}}),
                     d, partsize, isSymA, η, code(sweep), code(cache_strategy), dtcode(precision),
-                    b.device_config.threads, b.device_config.blocks, stream().handle, h))
+                    b.device_config.threads, b.device_config.blocks, opts, stream().handle, h))
     end
     P = L1GSPreconditioner{precision}(h[], size(A, 1))
     finalizer(p -> ccall((:hs_l1gs_destroy, libhsb200), Cint, (Ptr{Cvoid},), p.handle), P)
@@ -180,3 +188,40 @@ export L1GSPrecBuilder, ForwardSweep, BackwardSweep, SymmetricSweep, PackedBuffe
        ChebyshevFourth, ChebyshevFirst, smooth!
 
 end # module
+
+# The callers of ldiv!: Krylov.jl's cg and gmres as LinearSolve runs them with
+# Pl = P, on the device (hs_cg_krylovjl / hs_gmres_krylovjl).  A device matrix
+# handle comes from hs_matrix_create; the solvers apply P once per iteration.
+struct HsSolveInfo
+    iterations::Int32
+    converged::Int32
+    relres::Cdouble
+    ms::Cdouble
+    rnorm::Cdouble
+end
+
+prec_code(::Nothing) = (Int32(0), C_NULL)
+prec_code(P::L1GSPreconditioner) = (Int32(1), P.handle)
+prec_code(S::ChebyshevSmoother) = (Int32(2), S.handle)
+
+function krylov_cg!(x::CuArray{Float64}, A::Ptr{Cvoid}, b::CuArray{Float64}, Pl = nothing;
+                    atol = sqrt(eps(Float64)), rtol = sqrt(eps(Float64)), itmax::Integer = 0)
+    t, h = prec_code(Pl)
+    info = Ref{HsSolveInfo}()
+    st = ccall((:hs_cg_krylovjl, libhsb200), Cint,
+               (Ptr{Cvoid}, Int32, Ptr{Cvoid}, CuPtr{Float64}, CuPtr{Float64}, Cdouble, Cdouble, Int32, Ptr{Cvoid},
+                Ref{HsSolveInfo}), A, t, h, b, x, atol, rtol, itmax, stream().handle, info)
+    st == 6 || check(st)   # 6: not converged, reported in info
+    return info[]
+end
+
+function krylov_gmres!(x::CuArray{Float64}, A::Ptr{Cvoid}, b::CuArray{Float64}, Pl = nothing; memory::Integer = 20,
+                       atol = sqrt(eps(Float64)), rtol = sqrt(eps(Float64)), itmax::Integer = 0)
+    t, h = prec_code(Pl)
+    info = Ref{HsSolveInfo}()
+    st = ccall((:hs_gmres_krylovjl, libhsb200), Cint,
+               (Ptr{Cvoid}, Int32, Ptr{Cvoid}, Int32, CuPtr{Float64}, CuPtr{Float64}, Cdouble, Cdouble, Int32,
+                Ptr{Cvoid}, Ref{HsSolveInfo}), A, t, h, memory, b, x, atol, rtol, itmax, stream().handle, info)
+    st == 6 || check(st)
+    return info[]
+end
