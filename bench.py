@@ -88,14 +88,32 @@ def packed_len(n, ps):
     return ps * (ps - 1) * (nparts - 1) // 2 + lps * (lps - 1) // 2
 
 
-def algorithmic_bytes(n, nnz, ps, sweep, cache, tv, nonsym=False):
+SEG_MAX_PARTSIZE = 128   # views up to this partsize run the segment-list kernel
+
+
+def inblock_entries(A, ps):
+    """Strictly lower and strictly upper in-block entries of the row-wise
+    matrix (partition = ps consecutive rows and columns)."""
+    C = A.tocoo()
+    same = (C.row // ps) == (C.col // ps)
+    return int(np.count_nonzero(same & (C.col < C.row))), int(np.count_nonzero(same & (C.col > C.row)))
+
+
+def algorithmic_bytes(n, nnz, ps, sweep, cache, tv, nonsym=False, inblock=None):
     """Per-apply bytes: packed Tv*(S + 3N) per direction, symmetric fused
-    Tv*(2S + 3N); view nnz*(Ti+Tv) + (N+1)*Ti + 3*Tv*N (+ N*Ti for the
-    non-symmetric DiagonalIndices path)."""
+    Tv*(2S + 3N).  View up to partsize 128 (segment lists): the in-block
+    entries each direction reads, E_d*(Tv + 2) (value and 2-byte local
+    column), plus 3*Tv*N; larger partsizes scan the rows:
+    nnz*(Ti+Tv) + (N+1)*Ti + 3*Tv*N (+ N*Ti for the non-symmetric
+    DiagonalIndices path)."""
     ti = 4
     if cache == "packed":
         S = packed_len(n, ps)
         return tv * ((2 if sweep == "symmetric" else 1) * S + 3 * n)
+    if ps <= SEG_MAX_PARTSIZE and inblock is not None:
+        lo, up = inblock
+        e = (lo if sweep != "backward" else 0) + (up if sweep != "forward" else 0)
+        return e * (tv + 2) + 3 * tv * n
     b = nnz * (ti + tv) + (n + 1) * ti + 3 * tv * n
     return b + (n * ti if nonsym else 0)
 
@@ -599,7 +617,8 @@ def main():
     n, nnz = A.shape[0], A.nnz
     x = W.rhs_uniform(n)
     tv = 4 if wl["fp32"] else 8
-    bytes_per = algorithmic_bytes(n, nnz, wl["ps"], wl["sweep"], wl["cache"], tv)
+    bytes_per = algorithmic_bytes(n, nnz, wl["ps"], wl["sweep"], wl["cache"], tv,
+                                  inblock=inblock_entries(A, wl["ps"]) if wl["cache"] == "view" else None)
     config = {"workload": args.workload, "grid": f"{wl['grid']}^3", "n": n, "nnz": nnz, "partsize": wl["ps"],
               "sweep": wl["sweep"], "cache": wl["cache"], "matrix": "7-point Poisson, Dirichlet, FP64 CSC",
               "parallelism": f"replicas{world}" if world > 1 else "single",

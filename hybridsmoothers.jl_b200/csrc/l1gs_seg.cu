@@ -36,9 +36,9 @@ __global__ void seg_count_kernel(int32_t n, int32_t ps, const int32_t* __restric
     }
 }
 
-// One warp per (group, row): the lanes' counts (interleaved) and their maximum.
-__global__ void seg_max_kernel(int32_t n, int32_t ps, int32_t nparts, int64_t items, const int32_t* __restrict__ cnt,
-                               uint8_t* __restrict__ maxc, uint8_t* __restrict__ cnti) {
+// One warp per (group, row): the largest count of the 32 partitions' rows.
+__global__ void seg_max_kernel(int32_t n, int32_t ps, int32_t psq, int32_t nparts, int64_t items,
+                               const int32_t* __restrict__ cnt, uint8_t* __restrict__ maxc) {
     const int lane = threadIdx.x & 31;
     for (int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; w < items;
          w += ((int64_t)gridDim.x * blockDim.x) >> 5) {
@@ -46,23 +46,34 @@ __global__ void seg_max_kernel(int32_t n, int32_t ps, int32_t nparts, int64_t it
         const int64_t k = g * 32 + lane, row = k * ps + li;
         const int32_t c = (k < nparts && row < n) ? cnt[row] : 0;
         const unsigned m = __reduce_max_sync(FULL, (unsigned)c);
-        cnti[w * 32 + lane] = (uint8_t)c;
-        if (lane == 0) maxc[w] = (uint8_t)m;
+        if (lane == 0) maxc[g * psq + li] = (uint8_t)m;
     }
 }
 
 // Per group: the first slot of every row in the sweep's row order (ascending
 // rows for the lower lists, descending for the upper), and the group's total.
-__global__ void seg_off_kernel(int32_t ngroups, int32_t ps, const uint8_t* __restrict__ maxc,
+__global__ void seg_off_kernel(int32_t ngroups, int32_t ps, int32_t psq, const uint8_t* __restrict__ maxc,
                                uint16_t* __restrict__ off, int32_t* __restrict__ total, int descending) {
     for (int32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < ngroups; g += gridDim.x * blockDim.x) {
         int32_t acc = 0;
         for (int32_t t = 0; t < ps; ++t) {
             const int64_t li = descending ? ps - 1 - t : t;
             off[(int64_t)g * ps + li] = (uint16_t)acc;
-            acc += maxc[(int64_t)g * ps + li];
+            acc += maxc[(int64_t)g * psq + li];
         }
         total[g] = acc;
+    }
+}
+
+// Every slot's columns start as `ps` (the zero row); the scatter then writes
+// the real entries over them.
+template <typename TS>
+__global__ void seg_pad_kernel(int64_t slots, int32_t ps, unsigned char* __restrict__ stream) {
+    constexpr int64_t SB = 32 * (sizeof(TS) + 2);
+    const int64_t m = slots * 32;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < m; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t slot = e >> 5, lane = e & 31;
+        reinterpret_cast<uint16_t*>(stream + slot * SB + 32 * sizeof(TS))[lane] = (uint16_t)ps;
     }
 }
 
@@ -111,20 +122,30 @@ int dalloc(hsseg::View* view, T** out, size_t bytes) {
 // ---------------------------------------------------------------------------
 // Apply: warp per group of 32 partitions, lane = partition.
 // ---------------------------------------------------------------------------
+constexpr int kTab = 32;   // (group, direction) pairs whose stream position a warp keeps in shared memory
+
+struct TabEnt {
+    int64_t base;   // first slot
+    int32_t tot;    // slots
+    int32_t pad;
+};
+
 template <typename T, typename IO, int SWEEP>
-__global__ void __launch_bounds__(kSegWarps * 32) l1gs_seg_kernel(const hsseg::Params p) {
+__global__ void __launch_bounds__(kSegWarps * 32, 1) l1gs_seg_kernel(const hsseg::Params p) {
     constexpr int S = 33;
     constexpr uint32_t SB = 32 * (sizeof(T) + 2);                 // bytes per slot
-    constexpr uint32_t K = hsseg::kSlotsPerChunk(sizeof(T));      // slots per chunk
+    constexpr int K = hsseg::kSlotsPerChunk(sizeof(T));           // slots per chunk
     constexpr uint32_t CHB = K * SB;                              // bytes per chunk
+    constexpr int NDIR = SWEEP == 2 ? 2 : 1;
     extern __shared__ __align__(128) unsigned char smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int ps = p.ps;
+    const int ps = p.ps, psq = (ps + 3) & ~3;
     const uint32_t nst = p.nst;
     unsigned char* wbase = smem + (size_t)warp * p.warp_bytes;
     unsigned char* ring = wbase + p.ring_off;
     uint64_t* bars = reinterpret_cast<uint64_t*>(wbase + p.bars_off);
-    T* ys = reinterpret_cast<T*>(wbase + p.ys_off);   // y of row li, lane's partition: ys[li * S + lane]
+    TabEnt* tab = reinterpret_cast<TabEnt*>(wbase + p.tab_off);
+    T* ys = reinterpret_cast<T*>(wbase + p.ys_off);   // y of row li, lane's partition: ys[li * S + lane]; row ps: +0
     T* ds = reinterpret_cast<T*>(wbase + p.ds_off);
     const T* __restrict__ D = static_cast<const T*>(p.D);
     const IO* __restrict__ x = static_cast<const IO*>(p.x);
@@ -132,45 +153,61 @@ __global__ void __launch_bounds__(kSegWarps * 32) l1gs_seg_kernel(const hsseg::P
     const int wpb = blockDim.x >> 5;
     const int32_t q0 = p.gbeg + blockIdx.x * wpb + warp, qstride = gridDim.x * wpb;
     const int32_t my_groups = q0 < p.gend ? (p.gend - 1 - q0) / qstride + 1 : 0;
-    constexpr int NDIR = SWEEP == 2 ? 2 : 1;
+    const int32_t npairs = my_groups * NDIR;   // (group, direction) pairs, in sweep order
     auto dir_of = [&](int d) -> const hsseg::Dir& { return (SWEEP == 1 || d == 1) ? p.up : p.lo; };
 
-    // Producer (lane 0): walks (group, direction, chunk) of this warp's streams.
-    int32_t issued = 0, pgi = 0, pd = 0, pc = 0, pnch = -1;
+    // Stream positions of this warp's pairs (the first kTab into the table)
+    // and the number of chunks of all of them.
+    int32_t nch_lane = 0;
+    for (int32_t pi = lane; pi < npairs; pi += 32) {
+        const int64_t g = q0 + (int64_t)(pi / NDIR) * qstride;
+        const hsseg::Dir& dd = dir_of(pi % NDIR);
+        const int32_t tot = dd.total[g];
+        if (pi < kTab) {
+            tab[pi].base = dd.base[g];
+            tab[pi].tot = tot;
+        }
+        nch_lane += (tot + K - 1) / K;
+    }
+    const int32_t total = (int32_t)__reduce_add_sync(FULL, (unsigned)nch_lane);
+    ys[ps * S + lane] = T(0);
+    __syncwarp();
+
+    // Producer (lane 0): walks the pairs' chunks in order.
+    int32_t issued = 0, ppi = 0, pc = 0, pnch = -1, ptot = 0;
     const unsigned char* psrc = nullptr;
-    int32_t ptot = 0;
-    auto advance = [&]() -> bool {   // position on the next non-empty (group, direction); false at the end
-        while (pgi < my_groups) {
+    auto advance = [&]() -> bool {   // position on the next chunk; false at the end
+        while (ppi < npairs) {
             if (pnch < 0) {
-                const int64_t g = q0 + (int64_t)pgi * qstride;
-                const hsseg::Dir& dd = dir_of(pd);
-                ptot = dd.total[g];
-                pnch = (int32_t)((ptot + K - 1) / K);
-                psrc = dd.stream + dd.base[g] * SB;
+                const hsseg::Dir& dd = dir_of(ppi % NDIR);
+                int64_t b;
+                if (ppi < kTab) {
+                    b = tab[ppi].base;
+                    ptot = tab[ppi].tot;
+                } else {
+                    const int64_t g = q0 + (int64_t)(ppi / NDIR) * qstride;
+                    b = dd.base[g];
+                    ptot = dd.total[g];
+                }
+                pnch = (ptot + K - 1) / K;
+                psrc = dd.stream + b * SB;
                 pc = 0;
             }
             if (pc < pnch) return true;
             pnch = -1;
-            if (++pd == NDIR) {
-                pd = 0;
-                ++pgi;
-            }
+            ++ppi;
         }
         return false;
     };
-    auto issue_next = [&]() -> bool {
-        if (!advance()) return false;
+    auto issue_next = [&]() {
+        if (!advance()) return;
         const uint32_t s = (uint32_t)issued & (nst - 1u);
-        const uint32_t bytes = (uint32_t)min((int32_t)K, ptot - pc * (int32_t)K) * SB;
+        const uint32_t bytes = (uint32_t)min(K, ptot - pc * K) * SB;
         hsdev::mbar_arrive_expect_tx(bars + s, bytes);
         hsdev::bulk_load(ring + (size_t)s * CHB, psrc + (size_t)pc * CHB, bytes, bars + s);
         ++issued;
         ++pc;
-        return true;
     };
-    int32_t total = 0;   // chunks of all this warp's streams (each lane counts)
-    for (int32_t gi = 0; gi < my_groups; ++gi)
-        for (int d = 0; d < NDIR; ++d) total += (dir_of(d).total[q0 + (int64_t)gi * qstride] + K - 1) / K;
     if (lane == 0) {
         for (uint32_t s = 0; s < nst; ++s) hsdev::mbar_init(bars + s, 1);
         hsdev::fence_barrier_init();
@@ -187,8 +224,7 @@ __global__ void __launch_bounds__(kSegWarps * 32) l1gs_seg_kernel(const hsseg::P
         }
         return true;
     };
-    auto release = [&](int32_t upto) {
-        if (upto <= freed) return;
+    auto release = [&](int32_t upto) {   // chunks below `upto` are consumed: refill their stages
         freed = upto;
         __syncwarp();
         if (lane == 0) {
@@ -197,76 +233,117 @@ __global__ void __launch_bounds__(kSegWarps * 32) l1gs_seg_kernel(const hsseg::P
         }
     };
 
-    int32_t cbase = 0;   // first chunk of the current (group, direction)
+    // (partition, row) of this lane's t-th element of a group, t = lane + 32 u
+    const int dq = 32 / ps, dr = 32 - dq * ps;
+    int32_t ch = 0;   // chunk of the next slot
     for (int32_t gi = 0; gi < my_groups && ok; ++gi) {
         const int64_t g = q0 + (int64_t)gi * qstride;
         const int64_t rowbase = g * 32 * (int64_t)ps;
-        {   // x and D_Dl1 of the group's rows -> [li][partition], coalesced
-            int pp = lane / ps, li = lane - (lane / ps) * ps;
+        const int32_t nrows = (int32_t)min((int64_t)32 * ps, (int64_t)p.n - rowbase);
+        // x and D_Dl1 of the group's rows -> [li][partition], all loads in flight at once
+        if constexpr (sizeof(IO) == sizeof(T)) {
+            int pp = lane / ps, li = lane - pp * ps;
             for (int t = lane; t < 32 * ps; t += 32) {
-                const int64_t row = rowbase + t;
-                const bool valid = row < p.n;
-                ys[li * S + pp] = valid ? (T)x[row] : T(0);
-                ds[li * S + pp] = valid ? D[row] : T(1);
-                li += 32;
-                while (li >= ps) {
+                T* yd = ys + li * S + pp;
+                T* dd = ds + li * S + pp;
+                if (t < nrows) {
+                    hsdev::cp_async<sizeof(T)>(yd, x + rowbase + t);
+                    hsdev::cp_async<sizeof(T)>(dd, D + rowbase + t);
+                } else {
+                    *yd = T(0);
+                    *dd = T(1);
+                }
+                li += dr;
+                pp += dq;
+                if (li >= ps) {
                     li -= ps;
                     ++pp;
                 }
             }
+        } else {   // FP64 vectors, FP32 smoother: x converted on the way in
+            int pp = lane / ps, li = lane - pp * ps;
+            for (int t0 = lane; t0 < 32 * ps; t0 += 32 * 8) {
+                IO xv[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const int t = t0 + 32 * u;
+                    xv[u] = t < nrows ? x[rowbase + t] : IO(0);
+                }
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const int t = t0 + 32 * u;
+                    if (t < 32 * ps) {
+                        T* dd = ds + li * S + pp;
+                        ys[li * S + pp] = (T)xv[u];
+                        if (t < nrows)
+                            hsdev::cp_async<sizeof(T)>(dd, D + rowbase + t);
+                        else
+                            *dd = T(1);
+                    }
+                    li += dr;
+                    pp += dq;
+                    if (li >= ps) {
+                        li -= ps;
+                        ++pp;
+                    }
+                }
+            }
         }
+        // slots per row of each direction: bytes [4 lane, 4 lane + 4) of the group's row list
+        uint32_t mw[NDIR];
+#pragma unroll
+        for (int d = 0; d < NDIR; ++d)
+            mw[d] = 4 * lane < psq ? *reinterpret_cast<const uint32_t*>(dir_of(d).maxc + g * psq + 4 * lane) : 0u;
+        hsdev::cp_async_wait_all();
         __syncwarp();
         T* yk = ys + lane;
         const T* dk = ds + lane;
-        for (int d = 0; d < NDIR && ok; ++d) {
+#pragma unroll
+        for (int d = 0; d < NDIR; ++d) {
+            if (!ok) break;
             const bool lowerdir = SWEEP == 0 || (SWEEP == 2 && d == 0);
-            const hsseg::Dir& dd = lowerdir ? p.lo : p.up;
-            const int32_t nch = (dd.total[g] + (int32_t)K - 1) / (int32_t)K;
-            const uint8_t* __restrict__ mx = dd.maxc + g * ps;
-            const uint16_t* __restrict__ of = dd.off + g * ps;
-            const uint8_t* __restrict__ cn = dd.cnt + g * ps * 32 + lane;
+            int wi = 0;   // slot of the next entry inside chunk ch
             for (int t = 0; t < ps; ++t) {
                 const int li = lowerdir ? t : ps - 1 - t;
-                const int m = __ldg(mx + li);
-                const int o = __ldg(of + li);
-                const int c = __ldg(cn + li * 32);
+                const int m = (int)((__shfl_sync(FULL, mw[d], li >> 2) >> ((li & 3) * 8)) & 0xffu);
+                const T dv = dk[li * S];
+                T yi = yk[li * S];
                 T acc = T(0);
                 for (int k = 0; k < m; ++k) {
-                    const int32_t slot = o + k;
-                    const int32_t chunk = cbase + slot / (int32_t)K;
-                    if (chunk >= ready && !wait_upto(chunk)) {
+                    if (ch >= ready && !wait_upto(ch)) {
                         ok = false;
                         break;
                     }
-                    if (k < c) {
-                        const unsigned char* sp =
-                            ring + (size_t)((uint32_t)chunk & (nst - 1u)) * CHB + (size_t)(slot % (int32_t)K) * SB;
-                        const T a = reinterpret_cast<const T*>(sp)[lane];
-                        const int col = reinterpret_cast<const uint16_t*>(sp + 32 * sizeof(T))[lane];
-                        acc = add_rn(acc, mul_rn(a, yk[col * S]));
-                    }
+                    const unsigned char* sp = ring + (size_t)((uint32_t)ch & (nst - 1u)) * CHB + (size_t)wi * SB;
+                    const T a = reinterpret_cast<const T*>(sp)[lane];
+                    const int col = reinterpret_cast<const uint16_t*>(sp + 32 * sizeof(T))[lane];
+                    acc = add_rn(acc, mul_rn(a, yk[col * S]));
                     // a finished chunk goes back at once: a row may span more chunks than the ring holds
-                    if ((slot + 1) % (int32_t)K == 0) release(cbase + (slot + 1) / (int32_t)K);
+                    if (++wi == K) {
+                        wi = 0;
+                        ++ch;
+                        release(ch);
+                    }
                 }
                 if (!ok) break;
-                const T dv = dk[li * S];
-                T yi = yk[li * S];
                 if (SWEEP == 2 && !lowerdir) yi = mul_rn(dv, yi);   // y .= D_Dl1 .* y (:897) as the row is reached
                 yk[li * S] = div_rn(sub_rn(yi, acc), dv);
             }
             if (!ok) break;
-            release(cbase + nch);
-            cbase += nch;
+            if (wi > 0) {   // the pair's last, partly used chunk
+                ++ch;
+                release(ch);
+            }
         }
         if (!ok) break;
         __syncwarp();
         {
-            int pp = lane / ps, li = lane - (lane / ps) * ps;
-            for (int t = lane; t < 32 * ps; t += 32) {
-                const int64_t row = rowbase + t;
-                if (row < p.n) y[row] = (IO)ys[li * S + pp];
-                li += 32;
-                while (li >= ps) {
+            int pp = lane / ps, li = lane - pp * ps;
+            for (int t = lane; t < nrows; t += 32) {
+                y[rowbase + t] = (IO)ys[li * S + pp];
+                li += dr;
+                pp += dq;
+                if (li >= ps) {
                     li -= ps;
                     ++pp;
                 }
@@ -275,6 +352,9 @@ __global__ void __launch_bounds__(kSegWarps * 32) l1gs_seg_kernel(const hsseg::P
         __syncwarp();
     }
     if (!ok) {
+        // A bounded wait ran out: record it, let the copies in flight land
+        // (bounded), and return.
+        hsdev::cp_async_wait_all();
         if (lane == 0) hsdev::report_error(p.err, hsdev::kErrWaitTimeout);
         const int32_t end = __shfl_sync(FULL, issued, 0);
         for (int32_t c = ready; c < end; ++c)
@@ -288,10 +368,10 @@ int launch_t(const hsseg::View& view, hsseg::Params& p, cudaStream_t st) {
     p.nst = 4;
     p.ring_off = 0;
     p.bars_off = p.nst * CHB;
-    p.ys_off = (p.bars_off + 8 * p.nst + 15) / 16 * 16;
-    const uint32_t slice = (uint32_t)(33 * p.ps * sizeof(T));
-    p.ds_off = (p.ys_off + slice + 15) / 16 * 16;
-    p.warp_bytes = (p.ds_off + slice + 127) / 128 * 128;
+    p.tab_off = (p.bars_off + 8 * p.nst + 15) / 16 * 16;
+    p.ys_off = p.tab_off + kTab * (uint32_t)sizeof(TabEnt);
+    p.ds_off = (p.ys_off + (uint32_t)(33 * (p.ps + 1) * sizeof(T)) + 15) / 16 * 16;
+    p.warp_bytes = (p.ds_off + (uint32_t)(33 * p.ps * sizeof(T)) + 127) / 128 * 128;
     auto kern = l1gs_seg_kernel<T, IO, SWEEP>;
     int best_w = 0, best_warps = 0, best_per_sm = 0;
     for (int w = kSegWarps; w >= 1; w >>= 1) {
@@ -335,13 +415,16 @@ int build(int32_t n, int32_t ps, int32_t nparts, const int32_t* rp, const int32_
           bool upper, View* view, cudaStream_t st) {
     if (ps > kMaxPartsize) return hs::set_error(HS_ERR_UNSUPPORTED, "segment lists need partsize <= %d", kMaxPartsize);
     const int32_t ngroups = (int32_t)(((int64_t)nparts + 31) / 32);
+    const int32_t psq = (ps + 3) & ~3;
     view->ngroups = ngroups;
     const int64_t items = (int64_t)ngroups * ps;
     Tmp tmp;
     int32_t *cntL = nullptr, *qL = nullptr, *cntU = nullptr, *qU = nullptr;
+    uint16_t* off = nullptr;
     int rc;
     if ((rc = tmp.get(&cntL, 4 * (size_t)n)) || (rc = tmp.get(&qL, 4 * (size_t)n)) ||
-        (rc = tmp.get(&cntU, 4 * (size_t)n)) || (rc = tmp.get(&qU, 4 * (size_t)n)))
+        (rc = tmp.get(&cntU, 4 * (size_t)n)) || (rc = tmp.get(&qU, 4 * (size_t)n)) ||
+        (rc = tmp.get(&off, 2 * (size_t)items)))
         return rc;
     seg_count_kernel<<<grid_of(n), 256, 0, st>>>(n, ps, rp, ci, cntL, qL, cntU, qU);
     HS_LAUNCH_CHECK("seg_count_kernel");
@@ -351,13 +434,13 @@ int build(int32_t n, int32_t ps, int32_t nparts, const int32_t* rp, const int32_
         Dir& dd = d == 0 ? view->lo : view->up;
         const int32_t* cnt = d == 0 ? cntL : cntU;
         const int32_t* q0 = d == 0 ? qL : qU;
-        if ((rc = dalloc(view, &dd.maxc, (size_t)items)) || (rc = dalloc(view, &dd.cnt, 32 * (size_t)items)) ||
-            (rc = dalloc(view, &dd.off, 2 * (size_t)items)) || (rc = dalloc(view, &dd.total, 4 * (size_t)ngroups)) ||
+        if ((rc = dalloc(view, &dd.maxc, (size_t)ngroups * psq)) || (rc = dalloc(view, &dd.total, 4 * (size_t)ngroups)) ||
             (rc = dalloc(view, &dd.base, 8 * (size_t)ngroups)))
             return rc;
-        seg_max_kernel<<<grid_of(items * 32), 256, 0, st>>>(n, ps, nparts, items, cnt, dd.maxc, dd.cnt);
-        seg_off_kernel<<<grid_of(ngroups), 256, 0, st>>>(ngroups, ps, dd.maxc, dd.off, dd.total, d == 1);
-        hs::count_launch();
+        HS_CUDA(cudaMemsetAsync(dd.maxc, 0, (size_t)ngroups * psq, st));
+        seg_max_kernel<<<grid_of(items * 32), 256, 0, st>>>(n, ps, psq, nparts, items, cnt, dd.maxc);
+        HS_LAUNCH_CHECK("seg_max_kernel");
+        seg_off_kernel<<<grid_of(ngroups), 256, 0, st>>>(ngroups, ps, psq, dd.maxc, off, dd.total, d == 1);
         HS_LAUNCH_CHECK("seg_off_kernel");
         std::vector<int32_t> tot(ngroups);
         std::vector<int64_t> base(ngroups);
@@ -372,9 +455,13 @@ int build(int32_t n, int32_t ps, int32_t nparts, const int32_t* rp, const int32_
         HS_CUDA(cudaMemcpyAsync(dd.base, base.data(), 8 * (size_t)ngroups, cudaMemcpyHostToDevice, st));
         if ((rc = dalloc(view, &dd.stream, (size_t)(acc * SB)))) return rc;
         HS_CUDA(cudaMemsetAsync(dd.stream, 0, (size_t)(acc * SB), st));
-        seg_scatter_kernel<TM, TS><<<grid_of(n), 256, 0, st>>>(n, ps, ci, v, cnt, q0, dd.off, dd.base, dd.stream);
+        if (acc > 0) {
+            seg_pad_kernel<TS><<<grid_of(acc * 32), 256, 0, st>>>(acc, ps, dd.stream);
+            HS_LAUNCH_CHECK("seg_pad_kernel");
+        }
+        seg_scatter_kernel<TM, TS><<<grid_of(n), 256, 0, st>>>(n, ps, ci, v, cnt, q0, off, dd.base, dd.stream);
         HS_LAUNCH_CHECK("seg_scatter_kernel");
-        HS_CUDA(cudaStreamSynchronize(st));   // the host base vector goes out of scope
+        HS_CUDA(cudaStreamSynchronize(st));   // the host base vector and the scratch go out of scope
     }
     return HS_OK;
 }
@@ -391,9 +478,7 @@ void destroy(View* view) {
         cudaFree(dd->stream);
         cudaFree(dd->base);
         cudaFree(dd->total);
-        cudaFree(dd->off);
         cudaFree(dd->maxc);
-        cudaFree(dd->cnt);
         *dd = Dir();
     }
     view->bytes = 0;

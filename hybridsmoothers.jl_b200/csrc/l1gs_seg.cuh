@@ -10,12 +10,17 @@
 // them, a number of slots equal to the largest count of any of the 32
 // partitions' rows there; slot k of row li holds, for every lane, the value
 // and the local column (j - start) of that partition's k-th in-block entry
-// ([value x 32][column x 32] per slot).  A lane adds only its own row's
-// entries (its count per row is kept beside the stream), in storage order,
-// with separately rounded multiply and add -- the reference's sequence, so
-// results are bit-identical; the zeros that fill short rows are never read
-// into a sum.  The apply streams exactly these slots (no out-of-block entry,
-// no row pointer) through a per-warp ring filled by 1D bulk copies.
+// ([value x 32][column x 32] per slot).  A lane's slots past its own count
+// hold the value 0 and the column `ps`, a row of y that is always +0: adding
+// 0 * 0 leaves an accumulator unchanged bit for bit (an accumulator that
+// starts at +0 is never -0), so every lane runs the same slots without a
+// count.  Each lane adds its row's entries in storage order with separately
+// rounded multiply and add -- the reference's sequence, so results are
+// bit-identical.  The apply streams exactly these slots (no out-of-block
+// entry, no row pointer) through a per-warp ring filled by 1D bulk copies;
+// the per-row slot counts of a group arrive in one 4-byte load per lane and
+// are read back by shuffles, and the slot offsets are running sums, so the
+// row loop touches no global memory.
 #pragma once
 
 #include <stdint.h>
@@ -32,9 +37,7 @@ struct Dir {
     unsigned char* stream = nullptr;   // slots: [value x 32][uint16 column x 32]
     int64_t* base = nullptr;           // first slot of each group
     int32_t* total = nullptr;          // slots of each group
-    uint16_t* off = nullptr;           // [group][row]: first slot of the row (in the sweep's row order)
-    uint8_t* maxc = nullptr;           // [group][row]: slots of the row
-    uint8_t* cnt = nullptr;            // [group][row][lane]: the lane's own entries in the row
+    uint8_t* maxc = nullptr;           // [group][row], row stride ps rounded up to 4: slots of the row
     int64_t slots = 0;                 // all groups
 };
 
@@ -59,7 +62,7 @@ struct Params {
     const void* x;
     void* y;
     int32_t* err;
-    uint32_t warp_bytes, ring_off, bars_off, ys_off, ds_off, nst;
+    uint32_t warp_bytes, ring_off, bars_off, tab_off, ys_off, ds_off, nst;
 };
 
 int launch(int sdt, int io, int sweep, const View& view, int32_t n, int32_t ps, int32_t gbeg, int32_t gend,

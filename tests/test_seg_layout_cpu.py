@@ -3,11 +3,13 @@
 
 The emulation builds the per-group streams with the build kernels' formulas
 (in-block counts, per-row maximum over the group's 32 partitions, row offsets
-in the sweep's order, group bases), then runs the apply lane by lane: the
-warp's chunks are "copied" into a 4-stage ring in issue order, each read
-asserts that its chunk has landed and has not been released, finished
-chunks are released inside a row, and every lane adds only its own row's
-entries.  Results must equal the oracle's view path bit for bit.
+in the sweep's order, group bases, padding slots holding 0 and the column
+`ps`), then runs the apply lane by lane: the warp's chunks are "copied" into
+a 4-stage ring in issue order, each read asserts that its chunk has landed
+and has not been released, finished chunks are released inside a row, the
+slot position is a running (chunk, slot) pair, and every lane runs all of
+the row's slots -- its padding adds 0 * y[ps] with y[ps] = +0.  Results must
+equal the oracle's view path bit for bit, non-finite inputs included.
 """
 import numpy as np
 import pytest
@@ -69,7 +71,7 @@ def build(A_rows, ps, dtype):
         base = np.concatenate([[0], np.cumsum(total)[:-1]]).astype(int)
         slots = int(total.sum())
         vals = np.zeros((slots, 32), dtype=dtype)
-        cols = np.zeros((slots, 32), dtype=np.int64)
+        cols = np.full((slots, 32), ps, dtype=np.int64)
         for i in range(n):
             k, li = divmod(i, ps)
             g, lane = divmod(k, 32)
@@ -126,9 +128,9 @@ def emulate(A_rows, ps, sweep, D, x, dtype, warps=2, K=6):
                 nch = -(-int(dirs[d]["total"][g]) // K)
                 chunks += [(d, g, c) for c in range(nch)]
         ring = Ring(chunks)
-        cbase = 0
+        ch = 0
         for g in groups:
-            ys = np.zeros((ps, 32), dtype=dtype)
+            ys = np.zeros((ps + 1, 32), dtype=dtype)   # row ps: the padding slots' target, +0
             ds = np.ones((ps, 32), dtype=dtype)
             for lane in range(32):
                 for li in range(ps):
@@ -138,29 +140,36 @@ def emulate(A_rows, ps, sweep, D, x, dtype, warps=2, K=6):
                         ds[li, lane] = D[row]
             for d in order:
                 dd = dirs[d]
-                nch = -(-int(dd["total"][g]) // K)
+                start = ch
+                wi = 0
+                o = 0      # running slot offset of the row (the stored offsets, recomputed)
                 rows = range(ps) if d == "lo" else range(ps - 1, -1, -1)
-                for li in rows:
-                    m, o = dd["maxc"][g, li], dd["off"][g, li]
-                    acc = np.zeros(32, dtype=dtype)
-                    for k in range(m):
-                        slot = o + k
-                        chunk = cbase + slot // K
-                        ring.wait_upto(chunk)
-                        ring.check(chunk)
-                        for lane in range(32):
-                            if k < dd["cnti"][g, li, lane]:
-                                a = dd["vals"][dd["base"][g] + slot, lane]
-                                col = dd["cols"][dd["base"][g] + slot, lane]
-                                acc[lane] = acc[lane] + a * ys[col, lane]
-                        if (slot + 1) % K == 0:
-                            ring.release(cbase + (slot + 1) // K)
-                    yi = ys[li].copy()
-                    if sweep == "symmetric" and d == "up":
-                        yi = ds[li] * yi
-                    ys[li] = (yi - acc) / ds[li]
-                ring.release(cbase + nch)
-                cbase += nch
+                with np.errstate(all="ignore"):
+                    for li in rows:
+                        m = dd["maxc"][g, li]
+                        assert dd["off"][g, li] == o
+                        acc = np.zeros(32, dtype=dtype)
+                        for k in range(m):
+                            assert (ch - start) * K + wi == o + k
+                            ring.wait_upto(ch)
+                            ring.check(ch)
+                            a = dd["vals"][dd["base"][g] + o + k]
+                            col = dd["cols"][dd["base"][g] + o + k]
+                            acc = acc + a * ys[col, np.arange(32)]
+                            wi += 1
+                            if wi == K:
+                                wi = 0
+                                ch += 1
+                                ring.release(ch)
+                        o += m
+                        yi = ys[li].copy()
+                        if sweep == "symmetric" and d == "up":
+                            yi = ds[li] * yi
+                        ys[li] = (yi - acc) / ds[li]
+                if wi > 0:
+                    ch += 1
+                    ring.release(ch)
+                assert ch - start == -(-int(dd["total"][g]) // K)
             for lane in range(32):
                 for li in range(ps):
                     row = (g * 32 + lane) * ps + li
@@ -200,3 +209,23 @@ def test_seg_emulation_stencil_fp32():
     ref = O.OracleL1GS(A, 16, isSymA=True, sweep="symmetric", cache="view")
     got = emulate(rows_of(A, True), 16, "symmetric", ref.D, x, np.float32)
     np.testing.assert_array_equal(got, ref.ldiv(x))
+
+
+@pytest.mark.parametrize("sweep", ["forward", "backward", "symmetric"])
+def test_seg_emulation_nonfinite(sweep):
+    """Padding slots add 0 * y[ps] with y[ps] = +0: a lane whose own rows
+    are shorter than the group's maximum must not pick up an inf or NaN of
+    another row (0 * inf would be NaN)."""
+    rng = np.random.default_rng(7)
+    n, ps = 700, 16
+    A = sp.random(n, n, density=8.0 / n, random_state=rng, format="csc")
+    A.data = rng.uniform(-1, 1, A.nnz)
+    A = A + sp.diags(rng.uniform(3, 5, n) + abs(A).sum(axis=1).A.ravel())
+    A = W._canon(A.tocsc())
+    x = rng.uniform(-1, 1, n)
+    x[[3, 40, 41, 333]] = [np.inf, -np.inf, np.nan, np.inf]
+    ref = O.OracleL1GS(A, ps, isSymA=True, sweep=sweep, cache="view")
+    with np.errstate(all="ignore"):
+        want = ref.ldiv(x)
+    got = emulate(rows_of(A, True), ps, sweep, ref.D, x, np.float64)
+    np.testing.assert_array_equal(got, want)
