@@ -1711,6 +1711,7 @@ int launch_coop(hs_l1gs* P, const void* x, void* y, int io, cudaStream_t st) {
     hscoop::Params p;
     p.n = P->n;
     p.ps = P->ps;
+    p.blk = P->coop.blk;
     p.gbeg = P->rng_beg;
     p.gend = P->rng_end < 0 ? P->coop_ngroups : P->rng_end;
     p.Lg = (int32_t)P->coop.Lg;
@@ -1802,15 +1803,17 @@ int l1gs_view_of(const hs_l1gs* P, L1gsView* v) {
 // C ABI
 // ---------------------------------------------------------------------------
 namespace {
-// Threads per partition when the caller leaves it open (0).  One thread per
+// Threads per partition when the caller leaves it open (0).  Partsizes from
+// 32 that are multiples of 8 take the blocked kernel (8 lanes per partition,
+// off-diagonal 8 x 8 tiles as dense products).  Otherwise one thread per
 // partition (the reference's order) while the partitions give every SM about
 // six warps of 32 partitions; below that (large partsizes, small matrices)
-// lanes share a partition, eight rows per lane where the partsize allows it
-// (measured fastest on the 128^3 and 96^3 Poisson operators: partsize
-// 64 / 8 lanes, 128 / 16, 256 / 32).  Partsizes below 32 always keep one
-// thread per partition.
+// the column-block kernel's lanes share a partition, eight rows per lane
+// where the partsize allows it.  Partsizes below 32 always keep one thread per
+// partition.
 int auto_threads_per_part(int32_t ps, int64_t nparts) {
     if (ps < 32) return 1;
+    if (hscoop::blk_ok(ps, hscoop::kBlkB)) return hscoop::kBlkB;
     if (nparts / 32 >= 6 * (int64_t)hs::num_sms()) return 1;
     int tpp = 4;
     while (tpp < 32 && tpp * 8 < ps) tpp *= 2;
@@ -1842,8 +1845,11 @@ int l1gs_create_impl(const hs_sparse* A, bool on_device, int32_t partsize, int32
         return hs::set_error(HS_ERR_UNSUPPORTED, "an FP64 smoother needs an FP64 matrix");
     if (partsize > 65535) return hs::set_error(HS_ERR_UNSUPPORTED, "partsize above 65535");
     if (order < 0 || order > 2) return hs::set_error(HS_ERR_ARG, "order must be 0, 1 or 2 (got %d)", order);
-    if (order == 1 && threads_per_part > 1)
-        return hs::set_error(HS_ERR_ARG, "the reference summation order needs one thread per partition");
+    if (order == 1 && threads_per_part > 1 &&
+        !(sweep == HS_SWEEP_FORWARD && cache == HS_CACHE_PACKED && hscoop::blk_ok(partsize, threads_per_part)))
+        return hs::set_error(HS_ERR_ARG,
+                             "the reference summation order needs one thread per partition (or, for forward "
+                             "sweeps, 8 lanes per partition and a partsize that is a multiple of 8)");
     if (threads_per_part != 0 && threads_per_part != 1 && threads_per_part != 4 && threads_per_part != 8 &&
         threads_per_part != 16 && threads_per_part != 32)
         return hs::set_error(HS_ERR_ARG, "threads per partition must be 0 (automatic), 1, 4, 8, 16 or 32 (got %d)",
@@ -1871,14 +1877,18 @@ int l1gs_create_impl(const hs_sparse* A, bool on_device, int32_t partsize, int32
     {   // threads per partition of the packed sweep
         int tpp = threads_per_part;
         const bool coop_ok = cache == HS_CACHE_PACKED && !classic_small && partsize >= 2;
-        if (!coop_ok || order == 1) {
+        if (!coop_ok) {
             tpp = 1;
         } else if (tpp == 0) {
             tpp = auto_threads_per_part(partsize, P->nparts);
         }
+        // The reference's summation order: one thread per partition, or the
+        // blocked kernel's forward sweep (it adds in that order too).
+        if (order == 1 && tpp > 1 && !(sweep == HS_SWEEP_FORWARD && hscoop::blk_ok(partsize, tpp))) tpp = 1;
         if (tpp > 1) {
-            const int m = hscoop::rows_per_lane(partsize, tpp);
-            if (!m || !hscoop::supported(partsize, tpp, m)) {
+            const bool blk = hscoop::blk_ok(partsize, tpp);
+            const int m = blk ? partsize / tpp : hscoop::rows_per_lane(partsize, tpp);
+            if (!blk && (!m || !hscoop::supported(partsize, tpp, m))) {
                 if (threads_per_part != 0) {
                     delete P;
                     return hs::set_error(HS_ERR_UNSUPPORTED, "partsize %d with %d threads per partition is not provided",
@@ -1905,7 +1915,8 @@ int l1gs_create_impl(const hs_sparse* A, bool on_device, int32_t partsize, int32
     }
     // Summation order: reordered partial sums only when asked for (order 2)
     // and only in the rows kernel (thread per partition, partsize >= 32).
-    P->order = (order == 2 || (order == 0 && P->tpp > 1)) ? 2 : 1;
+    const bool exact_order = P->tpp == 1 || (P->coop.blk && sweep == HS_SWEEP_FORWARD);
+    P->order = (order == 2 || (order == 0 && !exact_order)) ? 2 : 1;
     P->nacc = (P->order == 2 && P->tpp == 1 && P->rows_layout) ? 4 : 1;
     // Host-chunked applies cut the work into whole groups of this many partitions.
     P->io_groups = P->tpp > 1 ? P->coop_ngroups : P->ngroups;
@@ -2243,7 +2254,8 @@ int hs_l1gs_info_get(const hs_l1gs* P, hs_l1gs_info* info) {
     info->device_bytes = P->bytes;
     info->eta = P->eta;
     info->threads_per_part = P->tpp;
-    info->order = (P->tpp > 1 || P->nacc > 1) ? 2 : 1;
+    const bool exact = (P->tpp == 1 && P->nacc == 1) || (P->tpp > 1 && P->coop.blk && P->sweep == HS_SWEEP_FORWARD);
+    info->order = exact ? 1 : 2;
     return HS_OK;
 }
 

@@ -37,6 +37,26 @@
 
 namespace hscoop {
 
+// Blocked variant ("blk", partsizes that are multiples of 8): B = 8 lanes per
+// partition, G = 4 partitions per warp, the partition cut into 8 x 8 tiles.
+// The sweep is left-looking by row block: row block I first adds the
+// off-diagonal tiles (I, J) of the blocks solved before it -- a dense
+// product with y of those blocks, lanes = rows, no dependence between
+// steps -- and then solves its diagonal tile, where the solved row's value is
+// broadcast to the block's lanes by a shuffle.  Forward, row i adds its terms
+// in ascending j (tiles J = 0, 1, ... then the diagonal tile's columns), the
+// reference's order, so forward sweeps are bit-identical; backward and
+// symmetric sweeps agree to rounding.  Stream order per direction and group:
+//   lower: for I = 0 .. nb-1: tiles (I, 0 .. I-1), then diagonal tile I
+//   upper: for I = nb-1 .. 0: tiles (I, I+1 .. nb-1), then diagonal tile I
+// An off-diagonal warp tile (the G partitions' tiles) is 32 x 8 entries,
+// [column / V][lane][column % V] with lane = g * 8 + row and V = 16 bytes /
+// element size, so a lane reads V columns of its row with one 16-byte load;
+// a diagonal warp tile keeps only its strict triangle, column by column in
+// the order of the solve (lower: columns 0..6, rows below; upper: columns
+// 7..1, rows above), partitions side by side inside a column.
+constexpr int kBlkB = 8;
+
 // Entries of direction blocks 0..t-1: G * sum_{u<t} (ps-1-u).
 __host__ __device__ __forceinline__ int64_t colbase(int64_t ps, int64_t G, int64_t t) {
     return G * (t * (ps - 1) - t * (t - 1) / 2);
@@ -44,16 +64,21 @@ __host__ __device__ __forceinline__ int64_t colbase(int64_t ps, int64_t G, int64
 
 struct Layout {
     int32_t ps = 0, G = 0;
+    int32_t blk = 0, V = 0;  // blocked variant; elements per 16 bytes
     int64_t Ld = 0;          // entries per direction per group: G*ps*(ps-1)/2
     int64_t Lg = 0;          // entries of one group stream (Ld, or 2*Ld for both directions)
     int64_t Lgp = 0;         // group stride in the buffer: Lg rounded up to 128 bytes
     int64_t upper_off = 0;   // first upper entry inside a group stream (0, or Ld)
 };
 
+inline bool blk_ok(int ps, int tpp) { return tpp == kBlkB && ps >= kBlkB && ps % kBlkB == 0; }
+
 inline Layout make_layout(int ps, int tpp, bool lower, bool upper, size_t es) {
     Layout L;
     L.ps = ps;
     L.G = 32 / tpp;
+    L.blk = blk_ok(ps, tpp) ? 1 : 0;
+    L.V = (int32_t)(16 / es);
     L.Ld = (int64_t)L.G * ps * (ps - 1) / 2;
     L.Lg = (lower && upper) ? 2 * L.Ld : L.Ld;
     const int64_t q = 128 / (int64_t)es;
@@ -65,10 +90,30 @@ inline Layout make_layout(int ps, int tpp, bool lower, bool upper, size_t es) {
 // Position of a_{li,lj} (local row/column of partition k) in the stream.
 __host__ __device__ __forceinline__ int64_t lower_idx(const Layout& L, int64_t k, int64_t li, int64_t lj) {
     const int64_t q = k / L.G, g = k - q * L.G;
+    if (L.blk) {
+        constexpr int64_t B = kBlkB, TILE = 32 * B;
+        const int64_t G = L.G, V = L.V, DG = G * B * (B - 1) / 2;
+        const int64_t I = li / B, ii = li - I * B, J = lj / B, jj = lj - J * B;
+        const int64_t rs = TILE * (I * (I - 1) / 2) + I * DG;   // row block I's first entry
+        const int64_t off = J < I ? rs + J * TILE + (jj / V) * 32 * V + (g * B + ii) * V + jj % V
+                                  : rs + I * TILE + G * (jj * (B - 1) - jj * (jj - 1) / 2) + g * (B - 1 - jj) +
+                                        (ii - jj - 1);
+        return q * L.Lgp + off;
+    }
     return q * L.Lgp + colbase(L.ps, L.G, lj) + (li - lj - 1) * L.G + g;
 }
 __host__ __device__ __forceinline__ int64_t upper_idx(const Layout& L, int64_t k, int64_t li, int64_t lj) {
     const int64_t q = k / L.G, g = k - q * L.G;
+    if (L.blk) {
+        constexpr int64_t B = kBlkB, TILE = 32 * B;
+        const int64_t G = L.G, V = L.V, DG = G * B * (B - 1) / 2;
+        const int64_t I = li / B, ii = li - I * B, J = lj / B, jj = lj - J * B;
+        const int64_t m = L.ps / B - 1 - I;                     // row blocks after I (consumed before it)
+        const int64_t rs = TILE * (m * (m - 1) / 2) + m * DG;
+        const int64_t off = J > I ? rs + (J - I - 1) * TILE + (jj / V) * 32 * V + (g * B + ii) * V + jj % V
+                                  : rs + m * TILE + G * (B * (B - 1) / 2 - jj * (jj + 1) / 2) + g * jj + ii;
+        return q * L.Lgp + L.upper_off + off;
+    }
     return q * L.Lgp + L.upper_off + colbase(L.ps, L.G, L.ps - 1 - lj) + li * L.G + g;
 }
 
@@ -100,7 +145,8 @@ inline Geometry make_geometry(const Layout& L, size_t es) {
     }
     const uint32_t che = (uint32_t)(chunk_bytes / es);
     while ((1u << g.che_log2) < che) ++g.che_log2;
-    const int64_t maxcol = (int64_t)L.G * (L.ps - 1);        // entries of the longest column block
+    // entries of the longest linear run: a column block, or a blocked off-diagonal warp tile
+    const int64_t maxcol = L.blk ? 32 * kBlkB : (int64_t)L.G * (L.ps - 1);
     g.ntail = (uint32_t)std::max<int64_t>(1, (maxcol + che - 1) / che);
     // A column block spans at most ntail + 1 chunks; keep `ahead` more in flight.
     g.nst = 4;
@@ -110,12 +156,14 @@ inline Geometry make_geometry(const Layout& L, size_t es) {
     g.ys_off = (uint32_t)((ring + 8 * g.nst + 15) / 16 * 16);
     const size_t rows = (size_t)L.G * L.ps * es;
     g.ds_off = (uint32_t)(g.ys_off + (rows + 15) / 16 * 16);
-    g.warp_bytes = (uint32_t)((g.ds_off + rows + 127) / 128 * 128);
+    // the blocked kernel keeps D_Dl1 in registers: y only
+    g.warp_bytes = (uint32_t)((g.ds_off + (L.blk ? 0 : rows) + 127) / 128 * 128);
     return g;
 }
 
 struct Params {
     int32_t n, ps;
+    int32_t blk;             // blocked layout and kernel
     int32_t gbeg, gend;      // groups [gbeg, gend) of this launch
     int32_t Lg;              // entries of one group stream
     int64_t Lgp;             // group stride in the buffer
@@ -138,6 +186,8 @@ bool supported(int ps, int tpp, int m);
 
 // Launches the sweep for smoother type sdt (HS_F64/HS_F32) and vector type io.
 int launch(int sdt, int io, int sweep, int tpp, int m, const Params& p, LaunchCache* lc, cudaStream_t st);
+// The blocked kernel (l1gs_blk.cu).
+int launch_blk(int sdt, int io, int sweep, const Params& p, LaunchCache* lc, cudaStream_t st);
 
 // Rows per lane for (partsize, lanes per partition): the smallest power of
 // two from 4 to 16 that covers ps, or 0.

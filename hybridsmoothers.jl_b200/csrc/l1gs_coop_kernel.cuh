@@ -265,9 +265,9 @@ int launch_t(const Params& p, LaunchCache* lc, cudaStream_t st) {
 
 // The (lanes per partition, rows per lane) pairs with kernels: every pair for
 // partsizes that are exactly lanes x rows, 16 and 32 lanes for the others
-// (keep in step with hscoop::supported).
+// (keep in step with hscoop::supported; 8 lanes run the blocked kernel).
 #define HS_COOP_EXACT_PAIRS(X) \
-    X(4, 4) X(4, 8) X(4, 16) X(8, 4) X(8, 8) X(8, 16) X(16, 4) X(16, 8) X(16, 16) X(32, 4) X(32, 8) X(32, 16)
+    X(4, 4) X(4, 8) X(4, 16) X(16, 4) X(16, 8) X(16, 16) X(32, 4) X(32, 8) X(32, 16)
 #define HS_COOP_GENERIC_PAIRS(X) X(16, 4) X(16, 8) X(16, 16) X(32, 4) X(32, 8) X(32, 16)
 
 template <typename T, typename IO, int SWEEP>

@@ -1,0 +1,265 @@
+"""CPU check of the blocked cooperative sweep's layout, ring protocol and order
+of operations (csrc/l1gs_coop.cuh "blocked variant", csrc/l1gs_blk.cu),
+before any GPU run.
+
+The stream is built with the layout's index formulas (restated below from
+hscoop::lower_idx / upper_idx), checked to be a bijection onto each group's
+stream, and read back the way the kernel reads it: per row block, the
+off-diagonal warp tiles as 16-byte vectors from the ring's linear address
+(`(vg + pos) & rmask` plus the lane's offset), then the diagonal tile's
+columns; every ring read asserts that its chunk has landed, has not been
+released and holds the intended stream entry.  The arithmetic is the
+kernel's: dense products in column order for the off-diagonal tiles, the
+diagonal solve with the solved value broadcast, separately rounded multiply
+and add, rows past n held at 0.  Forward sweeps must equal the oracle bit for
+bit, backward and symmetric sweeps within 1e-12.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from hsb200 import workloads as W
+from oracle import hs_oracle as O
+from test_coop_layout_cpu import Ring
+
+B = 8
+G = 4
+TILE = 32 * B
+DG = G * B * (B - 1) // 2
+
+
+def make_layout(ps, lower, upper, es):
+    Ld = G * ps * (ps - 1) // 2
+    Lg = 2 * Ld if (lower and upper) else Ld
+    q = 128 // es
+    return dict(ps=ps, G=G, V=16 // es, Ld=Ld, Lg=Lg, Lgp=(Lg + q - 1) // q * q, upper_off=Ld if lower else 0)
+
+
+def lower_idx(L, k, li, lj):
+    q, g = divmod(k, G)
+    V = L["V"]
+    I, ii = divmod(li, B)
+    J, jj = divmod(lj, B)
+    rs = TILE * (I * (I - 1) // 2) + I * DG
+    if J < I:
+        off = rs + J * TILE + (jj // V) * 32 * V + (g * B + ii) * V + jj % V
+    else:
+        off = rs + I * TILE + G * (jj * (B - 1) - jj * (jj - 1) // 2) + g * (B - 1 - jj) + (ii - jj - 1)
+    return q * L["Lgp"] + off
+
+
+def upper_idx(L, k, li, lj):
+    q, g = divmod(k, G)
+    V = L["V"]
+    I, ii = divmod(li, B)
+    J, jj = divmod(lj, B)
+    m = L["ps"] // B - 1 - I
+    rs = TILE * (m * (m - 1) // 2) + m * DG
+    if J > I:
+        off = rs + (J - I - 1) * TILE + (jj // V) * 32 * V + (g * B + ii) * V + jj % V
+    else:
+        off = rs + m * TILE + G * (B * (B - 1) // 2 - jj * (jj + 1) // 2) + g * jj + ii
+    return q * L["Lgp"] + L["upper_off"] + off
+
+
+def ring_geometry(es):
+    """hscoop::make_geometry for the blocked layout: 2 KiB chunks, the
+    longest linear run one off-diagonal warp tile."""
+    che = 2048 // es
+    ntail = max(1, -(-TILE // che))
+    st = 4
+    while st < ntail + 3:
+        st *= 2
+    return che, st, ntail
+
+
+def build_stream(A, ps, sweep, dtype):
+    R = A.tocsr()
+    n = A.shape[0]
+    es = np.dtype(dtype).itemsize
+    lower, upper = sweep != "backward", sweep != "forward"
+    L = make_layout(ps, lower, upper, es)
+    nparts = -(-n // ps)
+    ngroups = -(-nparts // G)
+    SC = np.zeros(ngroups * L["Lgp"], dtype=dtype)
+    for i in range(n):
+        k, li = divmod(i, ps)
+        s = k * ps
+        e = min(s + ps - 1, n - 1)
+        for p in range(R.indptr[i], R.indptr[i + 1]):
+            j = R.indices[p]
+            if s <= j < i and lower:
+                SC[lower_idx(L, k, li, j - s)] = R.data[p]
+            elif i < j <= e and upper:
+                SC[upper_idx(L, k, li, j - s)] = R.data[p]
+    return L, SC, ngroups
+
+
+def emulate(A, ps, sweep, D, x, dtype, warps=3):
+    T = np.dtype(dtype).type
+    es = np.dtype(dtype).itemsize
+    n = A.shape[0]
+    L, SC, ngroups = build_stream(A, ps, sweep, dtype)
+    che, st, ntail = ring_geometry(es)
+    V = L["V"]
+    nb = ps // B
+    y = np.zeros(n, dtype=dtype)
+    for w in range(warps):
+        groups = list(range(w, ngroups, warps))
+        ring = Ring(SC, L, groups, che, st, ntail, es)
+        nchg = ring.nchg
+        for gi, q in enumerate(groups):
+            c0 = gi * nchg
+            vg = c0 * che
+            base = q * L["Lgp"]
+            rowbase = q * G * ps
+            ys = np.zeros(G * ps, dtype=dtype)
+            pos = 0
+
+            def have(length):
+                ring.wait_upto(c0 + (pos + length - 1) // che)
+
+            def consumed():
+                ring.release(c0 + pos // che)
+
+            def rd(off):   # ring read at group-stream position pos + off
+                return ring.read(vg + pos, off, base + pos + off)
+
+            def tile(acc, J):
+                for lane in range(32):
+                    g, r = divmod(lane, B)
+                    for pv in range(B // V):
+                        for c in range(V):
+                            a = rd(pv * 32 * V + lane * V + c)
+                            acc[lane] = T(acc[lane] + T(a * ys[g * ps + J * B + pv * V + c]))
+                return acc
+
+            rows = [[rowbase + g * ps + I * B + r for g, r in (divmod(l, B) for l in range(32))] for I in range(nb)]
+            with np.errstate(all="ignore"):
+                if sweep != "backward":
+                    for I in range(nb):
+                        valid = [rr < n for rr in rows[I]]
+                        xr = [T(x[rr]) if v else T(0) for rr, v in zip(rows[I], valid)]
+                        dr = [D[rr] if v else T(1) for rr, v in zip(rows[I], valid)]
+                        acc = [T(0)] * 32
+                        for J in range(I):
+                            have(TILE)
+                            acc = tile(acc, J)
+                            pos += TILE
+                            consumed()
+                        have(DG)
+                        yown = [T(0)] * 32
+                        for c in range(B):
+                            v = [T((xr[l] - acc[l]) / dr[l]) for l in range(32)]
+                            for lane in range(32):
+                                g, r = divmod(lane, B)
+                                yc = v[g * B + c]
+                                if r == c:
+                                    yown[lane] = v[lane]
+                                if c < B - 1 and r > c:
+                                    a = rd(G * (c * (B - 1) - c * (c - 1) // 2) + g * (B - 1 - c) + (r - c - 1))
+                                    acc[lane] = T(acc[lane] + T(a * yc))
+                        for lane in range(32):
+                            g, r = divmod(lane, B)
+                            ys[g * ps + I * B + r] = yown[lane] if valid[lane] else T(0)
+                        pos += DG
+                        consumed()
+                if sweep != "forward":
+                    for I in range(nb - 1, -1, -1):
+                        valid = [rr < n for rr in rows[I]]
+                        dr = [D[rr] if v else T(1) for rr, v in zip(rows[I], valid)]
+                        if sweep == "symmetric":
+                            xr = [T(dr[l] * ys[(l // B) * ps + I * B + l % B]) for l in range(32)]
+                        else:
+                            xr = [T(x[rr]) if v else T(0) for rr, v in zip(rows[I], valid)]
+                        acc = [T(0)] * 32
+                        for J in range(I + 1, nb):
+                            have(TILE)
+                            acc = tile(acc, J)
+                            pos += TILE
+                            consumed()
+                        have(DG)
+                        yown = [T(0)] * 32
+                        for c in range(B - 1, -1, -1):
+                            v = [T((xr[l] - acc[l]) / dr[l]) for l in range(32)]
+                            for lane in range(32):
+                                g, r = divmod(lane, B)
+                                yc = v[g * B + c]
+                                if r == c:
+                                    yown[lane] = v[lane]
+                                if c > 0 and r < c:
+                                    a = rd(G * (B * (B - 1) // 2 - c * (c + 1) // 2) + g * c + r)
+                                    acc[lane] = T(acc[lane] + T(a * yc))
+                        for lane in range(32):
+                            g, r = divmod(lane, B)
+                            ys[g * ps + I * B + r] = yown[lane] if valid[lane] else T(0)
+                        pos += DG
+                        consumed()
+            assert pos == L["Lg"]
+            ring.release(c0 + nchg)
+            for t in range(G * ps):
+                if rowbase + t < n:
+                    y[rowbase + t] = ys[t]
+        assert ring.ready == ring.issued == ring.total
+    return y
+
+
+@pytest.mark.parametrize("ps", [8, 16, 32, 64])
+def test_blk_layout_is_a_bijection(ps):
+    """Every strict-triangle slot of every partition maps to a distinct entry
+    of its group's stream, and the stream has no holes."""
+    for es in (8, 4):
+        for lower, upper in ((True, False), (False, True), (True, True)):
+            L = make_layout(ps, lower, upper, es)
+            seen = set()
+            for k in range(2 * G):
+                for li in range(ps):
+                    for lj in range(ps):
+                        if lj < li and lower:
+                            p = lower_idx(L, k, li, lj)
+                        elif lj > li and upper:
+                            p = upper_idx(L, k, li, lj)
+                        else:
+                            continue
+                        assert p not in seen
+                        seen.add(p)
+                        q = k // G
+                        assert q * L["Lgp"] <= p < q * L["Lgp"] + L["Lg"]
+            assert len(seen) == 2 * L["Lg"]
+
+
+@pytest.mark.parametrize("ps,n", [(8, 77), (16, 150), (24, 333), (32, 300), (40, 257), (64, 500), (128, 700)])
+@pytest.mark.parametrize("sweep", ["forward", "backward", "symmetric"])
+def test_blk_emulation_matches_oracle(ps, n, sweep):
+    A = W.poisson2d_matrix(int(math.ceil(math.sqrt(n))), eps=0.3)
+    A = A[:n, :n].tocsc()
+    A.sort_indices()
+    rng = np.random.default_rng(ps + n)
+    A.data = A.data * rng.uniform(0.5, 1.5, A.nnz)   # distinct values: a misplaced entry shows
+    x = rng.uniform(-1, 1, n)
+    ref = O.OracleL1GS(A, ps, isSymA=False, sweep=sweep, cache="packed")
+    want = ref.ldiv(x)
+    got = emulate(A, ps, sweep, ref.D, x, np.float64)
+    if sweep == "forward":
+        np.testing.assert_array_equal(got, want)
+    else:
+        np.testing.assert_allclose(got, want, rtol=1e-12, atol=1e-12 * np.abs(want).max())
+
+
+def test_blk_emulation_fp32_and_nonfinite():
+    A = W.poisson2d_matrix(18, eps=0.3).astype(np.float32)
+    n = A.shape[0]
+    x = np.random.default_rng(1).uniform(-1, 1, n).astype(np.float32)
+    x[[5, 100, 200]] = [np.inf, np.nan, -np.inf]
+    for sweep in ("forward", "symmetric"):
+        ref = O.OracleL1GS(A, 24, isSymA=True, sweep=sweep, cache="packed")
+        with np.errstate(all="ignore"):
+            want = ref.ldiv(x)
+        got = emulate(A, 24, sweep, ref.D, x, np.float32)
+        if sweep == "forward":
+            np.testing.assert_array_equal(got, want)
+        else:
+            fin = np.isfinite(want)
+            np.testing.assert_array_equal(np.isfinite(got), fin)
+            np.testing.assert_allclose(got[fin], want[fin], rtol=1e-5, atol=1e-5 * np.abs(want[fin]).max())

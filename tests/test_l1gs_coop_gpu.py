@@ -1,7 +1,8 @@
 """GPU parity of the packed sweeps that reorder a row's sum, against the
-oracle: the cooperative sweep (several lanes per partition,
-csrc/l1gs_coop_kernel.cuh) and the rows kernel with partial sums
-(order="any", csrc/l1gs.cu).
+oracle: the cooperative sweeps (several lanes per partition: the column-block
+kernel, csrc/l1gs_coop_kernel.cuh, for 4, 16 and 32 lanes; the blocked
+kernel, csrc/l1gs_blk.cu, for 8 lanes and partsizes that are multiples of 8)
+and the rows kernel with partial sums (order="any", csrc/l1gs.cu).
 
 Forward sweeps add each row's terms in the reference's ascending order and are
 compared bitwise.  Backward and symmetric sweeps add them in descending order,
@@ -68,8 +69,10 @@ def random_matrix(n, density, seed):
 
 # (partsize, lanes per partition, n): ragged last partitions, groups with
 # padding partitions, every instantiated (lanes, rows-per-lane) pair -- exact
-# fits for 4 and 8 lanes, exact and other partsizes for 16 and 32
+# fits for 4 lanes, exact and other partsizes for 16 and 32; 8 lanes: the
+# blocked kernel at one to 64 row blocks per partition
 COOP_CASES = [(16, 4, 1000), (32, 4, 999), (64, 4, 3000), (32, 8, 2048), (64, 8, 3000), (128, 8, 4000),
+              (8, 8, 777), (24, 8, 1001), (40, 8, 999), (56, 8, 3001), (256, 8, 5000), (512, 8, 4100),
               (5, 16, 301), (17, 16, 500), (33, 16, 1111), (64, 16, 4000), (100, 16, 2345), (256, 16, 4000),
               (2, 32, 50), (20, 32, 700), (128, 32, 3001), (256, 32, 4000), (300, 32, 2500), (512, 32, 3000)]
 
@@ -93,7 +96,7 @@ def test_coop_random_fp64(ps, tpp, n, sweep):
             np.testing.assert_array_equal(P.SUbuffer, ref.SU)
 
 
-@pytest.mark.parametrize("ps,tpp", [(16, 4), (33, 16), (64, 16), (130, 32)])
+@pytest.mark.parametrize("ps,tpp", [(16, 4), (33, 16), (64, 16), (130, 32), (32, 8), (72, 8), (256, 8)])
 @pytest.mark.parametrize("sweep", ["forward", "symmetric"])
 def test_coop_fp32_and_mixed(ps, tpp, sweep):
     A = W.poisson2d_matrix(40, eps=0.3)
@@ -138,18 +141,20 @@ def test_coop_in_place_and_host_apply():
     np.testing.assert_array_equal(got, want)
 
 
-@pytest.mark.parametrize("ps", [40, 64])
-def test_coop_nonfinite_input(ps):
+@pytest.mark.parametrize("ps,tpp", [(40, 16), (64, 16), (40, 8), (64, 8)])
+def test_coop_nonfinite_input(ps, tpp):
     """inf/NaN in x reach the same rows as in the reference (forward: bitwise,
-    NaN positions included; backward/symmetric: the same non-finite pattern)."""
+    NaN positions included; backward/symmetric: the same non-finite pattern).
+    900 rows: the last partition is short, so padding rows meet the inf."""
     A = W.poisson2d_matrix(30, eps=0.5)
     x = np.random.default_rng(5).uniform(-1, 1, A.shape[0])
     x[ps + 10] = np.inf
     x[3] = np.nan
+    x[A.shape[0] - 2] = -np.inf
     for sweep in ("forward", "backward", "symmetric"):
         ref = O.OracleL1GS(A, ps, isSymA=True, sweep=sweep, cache="packed").ldiv(x)
         got = gpu_apply(hsb200.L1GSPrecBuilder(hsb200.CUDABackend(), threads=256, blocks=20)(
-            A, ps, isSymA=True, sweep=SWEEPS[sweep], threads_per_part=16), x)
+            A, ps, isSymA=True, sweep=SWEEPS[sweep], threads_per_part=tpp), x)
         np.testing.assert_array_equal(np.isnan(got), np.isnan(ref))
         np.testing.assert_array_equal(np.isinf(got), np.isinf(ref))
         fin = np.isfinite(ref)
@@ -162,7 +167,9 @@ def test_coop_rejects_unsupported():
     with pytest.raises(NotImplementedError, match="not provided"):
         b(A, 100, isSymA=True, threads_per_part=4)    # 25 rows per lane: not instantiated
     with pytest.raises(NotImplementedError, match="not provided"):
-        b(A, 40, isSymA=True, threads_per_part=8)     # 4 and 8 lanes: exact fits only
+        b(A, 36, isSymA=True, threads_per_part=8)     # 8 lanes: partsizes that are multiples of 8
+    with pytest.raises(NotImplementedError, match="not provided"):
+        b(A, 36, isSymA=True, threads_per_part=4)     # 4 lanes: exact fits only
     with pytest.raises(ValueError, match="threads per partition"):
         b(A, 16, isSymA=True, threads_per_part=3)
     # a view cache always runs one thread per partition
@@ -229,3 +236,19 @@ def test_reference_order_is_default_and_bitwise():
     with pytest.raises(ValueError, match="reference summation order"):
         hsb200.L1GSPrecBuilder(hsb200.CUDABackend(), threads=256, blocks=148)(
             A, 64, isSymA=True, order="reference", threads_per_part=8)
+
+
+@pytest.mark.parametrize("ps", [32, 64, 256])
+def test_blocked_forward_keeps_reference_order(ps):
+    """The blocked kernel's forward sweep adds every row's terms in the
+    reference's order: with order="reference" the library runs it (8 lanes
+    per partition) and the result is bitwise; without options a forward
+    sweep at these partsizes runs it too and reports the reference order."""
+    A = W.poisson3d_7pt(30)
+    x = W.rhs_uniform(A.shape[0])
+    ref = O.OracleL1GS(A, ps, isSymA=True, sweep="forward", cache="packed").ldiv(x)
+    b = hsb200.L1GSPrecBuilder(hsb200.CUDABackend(), threads=256, blocks=148)
+    for kw in (dict(order="reference", threads_per_part=8), dict(order="reference"), {}):
+        P = b(A, ps, isSymA=True, sweep=hsb200.ForwardSweep(), **kw)
+        assert P.threads_per_part == 8 and P.order == "reference", kw
+        np.testing.assert_array_equal(gpu_apply(P, x), ref)
