@@ -341,6 +341,13 @@ def headline_pcg(A, b, repeats):
             "oracle_solve_s": round(oracle_s, 1), "oracle_threads": O.omp_threads()}
 
 
+def pcg_iteration_bytes(n, nnz, ps=16, tv=8):
+    """Algorithmic bytes of one single-system PCG iteration (FP64 CSR SpMV +
+    p.q, x/r update + r.r, the L1GS symmetric packed apply, r.z, p update)."""
+    spmv = nnz * 12 + (n + 1) * 4 + 3 * 8 * n
+    return spmv + 6 * 8 * n + algorithmic_bytes(n, nnz, ps, "symmetric", "packed", tv) + 2 * 8 * n + 3 * 8 * n
+
+
 def headline_serving(count):
     """Cut-down serving stream (the first `count` requests of the seeded
     stream): served, batched FP32-smoother PCG against the plain FP64 drop-in
@@ -357,6 +364,12 @@ def headline_serving(count):
     seq = serving.solve_sequential(reqs, partsize=16)
     tuner = OnlineTuner()
     closed = serving.serve([(0.0, A, b) for _, A, b in reqs], max_slots=64, iters_per_step=8, tuner=tuner)
+    fixed = serving.serve([(0.0, A, b) for _, A, b in reqs], max_slots=64, iters_per_step=8, partsize_of=lambda A: 8)
+    # algorithmic bytes both paths moved: at equal bandwidth, served/plain cannot exceed their ratio
+    from hsb200.autotune import batch_bytes_per_iteration
+    plain_bytes = sum(it * pcg_iteration_bytes(A.shape[0], A.nnz) for it, (_, A, _) in zip(seq["iterations"], reqs))
+    served_bytes = sum(closed["iterations"][i] * batch_bytes_per_iteration(A.shape[0], A.nnz, tuner.history[i])
+                       for i, (_, A, _) in enumerate(reqs))
     rate = 0.8 * closed["solves_per_s"]
     rng = np.random.default_rng(1)
     t = np.cumsum(rng.exponential(1.0 / rate, size=len(reqs)))
@@ -378,6 +391,15 @@ def headline_serving(count):
                                             "solves_per_s": round(opened["solves_per_s"], 3),
                                             "p50_ms": round(opened["p50_s"] * 1e3, 2),
                                             "p99_ms": round(opened["p99_s"] * 1e3, 2)},
+            "served_fp32_batched_fixed_ps8": {"solves_per_s": round(fixed["solves_per_s"], 3),
+                                              "p50_ms": round(fixed["p50_s"] * 1e3, 2),
+                                              "p99_ms": round(fixed["p99_s"] * 1e3, 2)},
+            "bytes": {"plain_GB": round(plain_bytes / 1e9, 1), "served_GB": round(served_bytes / 1e9, 1),
+                      "plain_over_served": round(plain_bytes / served_bytes, 3),
+                      "plain_iterations": int(sum(seq["iterations"])),
+                      "served_iterations": int(sum(closed["iterations"].values())),
+                      "plain_GBps": round(plain_bytes / seq["wall_s"] / 1e9, 1),
+                      "served_GBps": round(served_bytes / (len(reqs) / closed["solves_per_s"]) / 1e9, 1)},
             "served_vs_plain_closed_loop": round(closed["solves_per_s"] / seq["solves_per_s"], 3),
             "served_vs_plain_poisson": round(opened["solves_per_s"] / seq["solves_per_s"], 3)}
 

@@ -46,12 +46,8 @@ __global__ void __launch_bounds__(kRT)
         if (UPDATE) return sub_rn(__ldg(x + j), __ldg(z + j));
         return __ldg(x + j);
     };
-    const int64_t stride = (int64_t)gridDim.x * kRT;
-    const int64_t first = ((int64_t)blockIdx.x * (kRT / 32) + warp) * 32;
-    hsdev::RowPtrs rpp = hsdev::load_rowptrs(n, rp, first);   // one chunk ahead
-    for (int64_t row0 = first; row0 < n; row0 += stride) {
-        const T acc = hsdev::csr_warp_fold_next(wbuf[warp], n, rp, ci, v, row0, stride, rpp, T(0), xin,
-                                                hsdev::AddOp<T>());
+    for (int64_t row0 = ((int64_t)blockIdx.x * (kRT / 32) + warp) * 32; row0 < n; row0 += (int64_t)gridDim.x * kRT) {
+        const T acc = hsdev::csr_warp_fold(wbuf[warp], n, rp, ci, v, row0, T(0), xin, hsdev::AddOp<T>());
         const int64_t i = row0 + (threadIdx.x & 31);
         if (i < n) {
             r[i] = sub_rn(acc, b[i]);

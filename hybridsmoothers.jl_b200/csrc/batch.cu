@@ -96,13 +96,11 @@ __global__ void __launch_bounds__(kT, 5) seg_spmv_dot(const BlockMap* __restrict
     if (!m.s->done) {   // uniform over the CTA (one slot per CTA)
         const int warp = threadIdx.x >> 5;
         auto fp = [&](int32_t j) { return __ldg(m.p + j); };
-        const int64_t stride = kT;   // rows between the warp's consecutive chunks
-        hsdev::RowPtrs rpp = hsdev::load_rowptrs(m.n, m.rp, (int64_t)m.row0 + warp * 32);   // one chunk ahead
         for (int k = 0; k < kRPC / kT; ++k) {   // the warp's 32-row chunks of this CTA
             const int64_t row0 = (int64_t)m.row0 + (k * (kT / 32) + warp) * 32;
             if (row0 >= m.n) break;   // uniform over the warp
-            const double acc = hsdev::csr_warp_fold_next(wbuf[warp], m.n, m.rp, m.ci, m.v, row0, stride, rpp, 0.0,
-                                                         fp, hsdev::AddOp<double>());
+            const double acc =
+                hsdev::csr_warp_fold(wbuf[warp], m.n, m.rp, m.ci, m.v, row0, 0.0, fp, hsdev::AddOp<double>());
             const int64_t r = row0 + (threadIdx.x & 31);
             if (r < m.n) {
                 m.q[r] = acc;

@@ -145,12 +145,9 @@ constexpr int kWarpMinBlocks = 5;
 #define HS_WARP_SHARED(T) __shared__ T wbuf[kThreads / 32][hsdev::kWarpCap]
 #define HS_WARP_ROWS_LOOP                                                                                   \
     const int warp_ = threadIdx.x >> 5;                                                                       \
-    const int64_t rstride_ = (int64_t)gridDim.x * kThreads;                                                   \
-    hsdev::RowPtrs rpp_ = hsdev::load_rowptrs(n, rp, ((int64_t)blockIdx.x * (kThreads / 32) + warp_) * 32);   \
-    for (int64_t row0 = ((int64_t)blockIdx.x * (kThreads / 32) + warp_) * 32; row0 < n; row0 += rstride_)
-// Once per iteration of HS_WARP_ROWS_LOOP: folds the chunk and requests the next chunk's row pointers.
-#define HS_WARP_FOLD(acc0, f, op) \
-    hsdev::csr_warp_fold_next(wbuf[warp_], n, rp, ci, v, row0, rstride_, rpp_, acc0, f, op)
+    for (int64_t row0 = ((int64_t)blockIdx.x * (kThreads / 32) + warp_) * 32; row0 < n;                       \
+         row0 += (int64_t)gridDim.x * kThreads)
+#define HS_WARP_FOLD(acc0, f, op) hsdev::csr_warp_fold(wbuf[warp_], n, rp, ci, v, row0, acc0, f, op)
 
 // MODE 0: y = A x; MODE 1: y = y - A x (term by term); MODE 2: y = beta y + sum (a x) alpha.
 template <typename T, int MODE>

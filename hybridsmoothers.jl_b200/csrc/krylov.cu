@@ -159,12 +159,9 @@ __global__ void __launch_bounds__(kT, 5) pcg_spmv_dot(int32_t n, const int32_t* 
     if (!s->done) {
         const int warp = threadIdx.x >> 5;
         auto fp = [&](int32_t j) { return __ldg(p + j); };
-        const int64_t stride = (int64_t)gridDim.x * kT;
-        const int64_t first = ((int64_t)blockIdx.x * (kT / 32) + warp) * 32;
-        hsdev::RowPtrs rpp = hsdev::load_rowptrs(n, rp, first);   // one chunk ahead
-        for (int64_t row0 = first; row0 < n; row0 += stride) {
-            const double acc =
-                hsdev::csr_warp_fold_next(wbuf[warp], n, rp, ci, v, row0, stride, rpp, 0.0, fp, hsdev::AddOp<double>());
+        for (int64_t row0 = ((int64_t)blockIdx.x * (kT / 32) + warp) * 32; row0 < n;
+             row0 += (int64_t)gridDim.x * kT) {
+            const double acc = hsdev::csr_warp_fold(wbuf[warp], n, rp, ci, v, row0, 0.0, fp, hsdev::AddOp<double>());
             const int64_t r = row0 + (threadIdx.x & 31);
             if (r < n) {
                 q[r] = acc;

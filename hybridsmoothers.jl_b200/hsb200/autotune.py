@@ -159,6 +159,7 @@ class OnlineTuner:
         self.assigned = {}   # class -> candidates handed out so far
         self.obs = {}        # class -> {ps: [bytes to convergence per row, ...]}
         self.tags = {}       # tag -> (class, ps, n, nnz)
+        self.history = {}    # tag -> partsize it ran with (admitted requests)
 
     def partsize_for(self, A, tag):
         key = matrix_class(A)
@@ -173,11 +174,13 @@ class OnlineTuner:
         else:
             ps = self.default   # candidates still running: the default meanwhile
         self.tags[tag] = (key, ps, A.shape[0], A.nnz)
+        self.history[tag] = ps
         return ps
 
     def cancel(self, tag):
         """The request `tag` was not admitted: forget its assignment."""
         key, ps, _, _ = self.tags.pop(tag)
+        self.history.pop(tag, None)
         tried = self.assigned.get(key, [])
         if ps in tried and ps not in self.obs.get(key, {}):
             tried.remove(ps)
