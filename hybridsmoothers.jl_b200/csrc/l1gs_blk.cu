@@ -14,10 +14,14 @@
 // a_{row, c} * y_c.  Only the eight steps of a diagonal tile form a serial
 // chain; the off-diagonal tiles, all but 8/ps of the entries, are plain
 // independent multiply-adds.  Multiply and add are rounded separately, as
-// in the reference.  The streams pass through a per-warp ring of 2 KiB
-// chunks filled by 1D bulk copies (cp.async.bulk, no multicast) as in the
-// column-block kernel, tail stages repeating the first ones so every tile is
-// one linear run.
+// in the reference.
+//
+// A warp's group stream is one contiguous run read front to back, so the
+// lanes load each tile straight from global memory (16-byte loads, 512
+// contiguous bytes per warp instruction), one tile ahead of the arithmetic in
+// registers, while lane 0 keeps the next 16 KiB of the stream on its way into
+// L2 (cp.async.bulk.prefetch.L2, no multicast).  Shared memory holds only y
+// of the group.
 #include "l1gs_coop.cuh"
 
 namespace hscoop {
@@ -25,6 +29,8 @@ namespace {
 
 constexpr int kBlkWarps = 4;   // warps per block; every warp streams its own groups
 constexpr unsigned FULL = 0xffffffffu;
+constexpr uint32_t kPfStep = 4096;    // bytes per L2 prefetch
+constexpr uint32_t kPfAhead = 16384;  // bytes kept prefetched ahead of the reads
 
 template <typename T>
 struct Vec;
@@ -34,6 +40,13 @@ struct Vec<double> {
     static __device__ __forceinline__ double dot(double acc, const double2& a, const double2& y) {
         acc = add_rn(acc, mul_rn(a.x, y.x));
         return add_rn(acc, mul_rn(a.y, y.y));
+    }
+    static __device__ __forceinline__ double get(const double2& v, int c) { return c == 0 ? v.x : v.y; }
+    static __device__ __forceinline__ void set(double2& v, int c, double t) {
+        if (c == 0)
+            v.x = t;
+        else
+            v.y = t;
     }
 };
 template <>
@@ -45,228 +58,203 @@ struct Vec<float> {
         acc = add_rn(acc, mul_rn(a.z, y.z));
         return add_rn(acc, mul_rn(a.w, y.w));
     }
+    static __device__ __forceinline__ float get(const float4& v, int c) {
+        return c == 0 ? v.x : c == 1 ? v.y : c == 2 ? v.z : v.w;
+    }
+    static __device__ __forceinline__ void set(float4& v, int c, float t) {
+        if (c == 0)
+            v.x = t;
+        else if (c == 1)
+            v.y = t;
+        else if (c == 2)
+            v.z = t;
+        else
+            v.w = t;
+    }
 };
+
+__device__ __forceinline__ void prefetch_l2(const void* src, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(reinterpret_cast<uint64_t>(src)), "r"(bytes)
+                 : "memory");
+}
 
 // SWEEP: 0 forward, 1 backward, 2 symmetric.
 template <typename T, typename IO, int SWEEP>
 __global__ void __launch_bounds__(kBlkWarps * 32, 1) l1gs_blk_kernel(const Params p) {
-    constexpr int B = kBlkB, G = 32 / B, V = 16 / (int)sizeof(T);
-    constexpr uint32_t TILE = 32 * B;                 // entries of an off-diagonal warp tile
-    constexpr uint32_t DG = G * B * (B - 1) / 2;      // entries of a diagonal warp tile
+    constexpr int B = kBlkB, G = 32 / B, V = 16 / (int)sizeof(T), NV = B / V;
+    constexpr uint32_t TILE = 32 * B;              // entries of an off-diagonal warp tile
+    constexpr uint32_t DG = G * B * (B - 1) / 2;   // entries of a diagonal warp tile
+    static_assert(B - 1 <= NV * V, "a diagonal tile's entries fit the item buffer");
     using VT = typename Vec<T>::type;
+    using VO = Vec<T>;
     extern __shared__ __align__(128) unsigned char smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const Geometry geo = p.geo;
-    const uint32_t l2 = geo.che_log2, che = 1u << l2, nst = geo.nst, ntail = geo.ntail;
-    const int32_t nchg = (int32_t)(((uint32_t)p.Lg + che - 1) >> l2);   // chunks per group stream
-    const int wpb = blockDim.x >> 5;
-    const int32_t qstride = gridDim.x * wpb;
-    unsigned char* wbase = smem + (size_t)warp * geo.warp_bytes;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(wbase + geo.bars_off);
-    const int32_t q0 = p.gbeg + blockIdx.x * wpb + warp;
-    const int32_t my_groups = q0 < p.gend ? (p.gend - 1 - q0) / qstride + 1 : 0;
-    const int32_t total = my_groups * nchg;
-    const T* __restrict__ SC = static_cast<const T*>(p.SC);
-
-    // Producer state (lane 0): the next chunk to fetch and its source.
-    int32_t issued = 0, pc = 0, pg = 0;
-    const T* src = SC + (int64_t)q0 * p.Lgp;
-    auto issue_next = [&]() {
-        const uint32_t s = (uint32_t)issued & (nst - 1u);
-        uint32_t bytes = che * (uint32_t)sizeof(T);
-        if (pc == nchg - 1) bytes = (((uint32_t)p.Lg - ((uint32_t)pc << l2)) * (uint32_t)sizeof(T) + 15u) & ~15u;
-        const bool dup = s < ntail;
-        T* ringw = reinterpret_cast<T*>(wbase);
-        hsdev::mbar_arrive_expect_tx(bars + s, dup ? 2 * bytes : bytes);
-        hsdev::bulk_load(ringw + (size_t)s * che, src, bytes, bars + s);
-        if (dup) hsdev::bulk_load(ringw + (size_t)(nst + s) * che, src, bytes, bars + s);
-        ++issued;
-        if (++pc == nchg) {
-            pc = 0;
-            ++pg;
-            src = SC + ((int64_t)q0 + (int64_t)pg * qstride) * p.Lgp;
-        } else {
-            src += che;
-        }
-    };
-    if (lane == 0) {
-        for (uint32_t s = 0; s < nst; ++s) hsdev::mbar_init(bars + s, 1);
-        hsdev::fence_barrier_init();
-        while (issued < total && issued < (int32_t)nst) issue_next();
-    }
-    __syncwarp();
-
     const int g = lane / B, r = lane % B;
     const int ps = p.ps, nb = ps / B;
-    const uint32_t rmask = (che * nst) - 1u;
-    const T* ring = reinterpret_cast<const T*>(wbase);
-    T* ys = reinterpret_cast<T*>(wbase + geo.ys_off);   // y of the group's rows, natural order ([partition][row])
+    const int wpb = blockDim.x >> 5;
+    const int32_t qstride = gridDim.x * wpb;
+    const int32_t q0 = p.gbeg + blockIdx.x * wpb + warp;
+    T* ys = reinterpret_cast<T*>(smem + (size_t)warp * p.geo.warp_bytes);   // y of the group, natural row order
+    const T* __restrict__ SC = static_cast<const T*>(p.SC);
     const T* __restrict__ D = static_cast<const T*>(p.D);
     const IO* __restrict__ x = static_cast<const IO*>(p.x);
     IO* __restrict__ y = static_cast<IO*>(p.y);
+    const uint32_t lg_bytes = (uint32_t)p.Lg * (uint32_t)sizeof(T);
 
-    int32_t ready = 0;   // chunks known to have landed
-    int32_t freed = 0;   // chunks handed back to the producer
-    bool ok = true;
-    auto wait_upto = [&](int32_t last) -> bool {   // bounded
-        while (ready <= last) {
-            const bool got = hsdev::mbar_wait_bounded(bars + ((uint32_t)ready & (nst - 1u)),
-                                                      ((uint32_t)ready / nst) & 1u);
-            if (!__all_sync(FULL, got)) return false;
-            ++ready;
-        }
-        return true;
-    };
-    auto release = [&](int32_t upto) {   // chunks below `upto` are consumed: refill their stages
-        freed = upto;
-        __syncwarp();
-        if (lane == 0) {
-            hsdev::fence_proxy_async_smem();
-            while (issued < total && issued < freed + (int32_t)nst) issue_next();
-        }
-    };
-
-    for (int32_t gi = 0; gi < my_groups && ok; ++gi) {
-        const int64_t q = q0 + (int64_t)gi * qstride;
-        const int32_t c0 = gi * nchg;                  // first chunk of this group
-        const uint32_t vg = (uint32_t)c0 << l2;        // ring position of the group's entry 0 (mod 2^32)
-        const int64_t rowbase = q * G * (int64_t)ps;   // the group's rows are contiguous
-        const int64_t prow = rowbase + (int64_t)g * ps + r;   // this lane's row of block 0
-        T* yg = ys + g * ps;                           // this lane's partition
-        uint32_t pos = 0;                              // group-stream position
-        // the run [pos, pos + len) has landed (bounded wait)
-        auto have = [&](uint32_t len) -> bool {
-            const int32_t need = c0 + (int32_t)((pos + len - 1) >> l2);
-            return need < ready || wait_upto(need);
+    for (int32_t q = q0; q < p.gend; q += qstride) {
+        const T* gs = SC + (int64_t)q * p.Lgp;                 // the group stream
+        const int64_t rowbase = (int64_t)q * G * ps;           // the group's rows are contiguous
+        const int64_t prow = rowbase + (int64_t)g * ps + r;    // this lane's row of block 0
+        T* yg = ys + g * ps;                                   // this lane's partition
+        uint32_t pf = 0;                                       // stream bytes requested into L2 (lane 0)
+        auto prefetch_to = [&](uint32_t upto) {
+            if (lane == 0) {
+                while (pf < upto && pf < lg_bytes) {
+                    const uint32_t nbytes = min(kPfStep, (lg_bytes - pf + 15u) & ~15u);
+                    prefetch_l2(reinterpret_cast<const unsigned char*>(gs) + pf, nbytes);
+                    pf += nbytes;
+                }
+            }
         };
-        auto consumed = [&]() {
-            const int32_t done = c0 + (int32_t)(pos >> l2);
-            if (done > freed) release(done);
-        };
-        // sum over the off-diagonal tile at pos with y of block J
-        auto tile = [&](T acc, int J) -> T {
-            const T* tp = ring + ((vg + pos) & rmask) + lane * V;
-            const T* yp = yg + J * B;
+        // this lane's entries of the off-diagonal tile at `pos` (columns in order)
+        auto load_tile = [&](VT* buf, uint32_t pos) {
+            const VT* src = reinterpret_cast<const VT*>(gs + pos) + lane;
 #pragma unroll
-            for (int pv = 0; pv < B / V; ++pv)
-                acc = Vec<T>::dot(acc, *reinterpret_cast<const VT*>(tp + pv * 32 * V),
-                                  *reinterpret_cast<const VT*>(yp + pv * V));
+            for (int v = 0; v < NV; ++v) buf[v] = __ldg(src + v * 32);
+        };
+        // this lane's entries of the diagonal tile at `pos`: slot c holds column c
+        // (lower, rows below it) or column c + 1 (upper, rows above it)
+        auto load_diag = [&](VT* buf, uint32_t pos, bool lower) {
+            const T* dp = gs + pos;
+#pragma unroll
+            for (int c = 0; c < B - 1; ++c) {
+                T val = T(0);
+                if (lower) {
+                    if (r > c) val = __ldg(dp + G * (c * (B - 1) - c * (c - 1) / 2) + g * (B - 1 - c) + (r - c - 1));
+                } else {
+                    const int cu = c + 1;
+                    if (r < cu) val = __ldg(dp + G * (B * (B - 1) / 2 - cu * (cu + 1) / 2) + g * cu + r);
+                }
+                VO::set(buf[c / V], c % V, val);
+            }
+        };
+        auto tile = [&](T acc, const VT* buf, int J) -> T {
+            const VT* yp = reinterpret_cast<const VT*>(yg + J * B);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) acc = VO::dot(acc, buf[v], yp[v]);
             return acc;
         };
 
         if (SWEEP != 1) {   // forward: row blocks 0 .. nb-1
+            prefetch_to(kPfAhead);
             int64_t row = prow;
-            T xn = row < p.n ? (T)x[row] : T(0), dn = row < p.n ? D[row] : T(1);
-            for (int I = 0; I < nb; ++I) {
-                const bool valid = row < p.n;
-                const T xr = xn, dr = dn;
-                if (I + 1 < nb) {   // next block's x and D_Dl1, one block ahead
-                    const int64_t rn = row + B;
-                    xn = rn < p.n ? (T)x[rn] : T(0);
-                    dn = rn < p.n ? D[rn] : T(1);
+            T xr = row < p.n ? (T)x[row] : T(0), dr = row < p.n ? D[row] : T(1);
+            VT cur[NV], nxt[NV];
+            int I = 0, J = 0;   // the item: tile (I, J) while J < I, then the diagonal tile of I
+            uint32_t pos = 0;
+            load_diag(cur, 0, true);
+            T acc = T(0);
+            while (true) {
+                const bool is_tile = J < I;
+                const uint32_t npos = pos + (is_tile ? TILE : DG);
+                const int In = is_tile ? I : I + 1;
+                const int Jn = is_tile ? J + 1 : 0;
+                const bool more = In < nb;
+                if (more) {   // the next item's entries, one item ahead
+                    if (Jn < In)
+                        load_tile(nxt, npos);
+                    else
+                        load_diag(nxt, npos, true);
                 }
-                T acc = T(0);
-                for (int J = 0; J < I; ++J) {
-                    if (!have(TILE)) {
-                        ok = false;
-                        break;
+                prefetch_to(npos * (uint32_t)sizeof(T) + kPfAhead);
+                if (is_tile) {
+                    acc = tile(acc, cur, J);
+                } else {
+                    T yown = T(0);
+#pragma unroll
+                    for (int c = 0; c < B; ++c) {
+                        const T v = div_rn(sub_rn(xr, acc), dr);
+                        const T yc = __shfl_sync(FULL, v, c, B);
+                        if (r == c) yown = v;
+                        if (c < B - 1 && r > c) acc = add_rn(acc, mul_rn(VO::get(cur[c / V], c % V), yc));
                     }
-                    acc = tile(acc, J);
-                    pos += TILE;
-                    consumed();
+                    // rows past n (a short last partition, padding partitions) stay 0
+                    yg[I * B + r] = row < p.n ? yown : T(0);
+                    __syncwarp();
+                    acc = T(0);
+                    row += B;
+                    if (more) {
+                        xr = row < p.n ? (T)x[row] : T(0);
+                        dr = row < p.n ? D[row] : T(1);
+                    }
                 }
-                if (!ok) break;
-                if (!have(DG)) {
-                    ok = false;
-                    break;
-                }
-                const T* dp = ring + ((vg + pos) & rmask);
-                T aj[B - 1];
+                if (!more) break;
 #pragma unroll
-                for (int c = 0; c < B - 1; ++c)
-                    aj[c] = r > c ? dp[G * (c * (B - 1) - c * (c - 1) / 2) + g * (B - 1 - c) + (r - c - 1)] : T(0);
-                T yown = T(0);
-#pragma unroll
-                for (int c = 0; c < B; ++c) {
-                    const T v = div_rn(sub_rn(xr, acc), dr);
-                    const T yc = __shfl_sync(FULL, v, c, B);
-                    if (r == c) yown = v;
-                    if (c < B - 1 && r > c) acc = add_rn(acc, mul_rn(aj[c], yc));
-                }
-                // rows past n (a short last partition, padding partitions) stay 0
-                yg[I * B + r] = valid ? yown : T(0);
-                __syncwarp();
-                pos += DG;
-                consumed();
-                row += B;
+                for (int v = 0; v < NV; ++v) cur[v] = nxt[v];
+                I = In;
+                J = Jn;
+                pos = npos;
             }
         }
-        if (!ok) break;
         if (SWEEP != 0) {   // backward: row blocks nb-1 .. 0
+            const uint32_t base = SWEEP == 2 ? (uint32_t)p.Lg / 2 : 0u;
+            prefetch_to(base * (uint32_t)sizeof(T) + kPfAhead);
             int64_t row = prow + (int64_t)(nb - 1) * B;
-            T xn = (SWEEP == 1 && row < p.n) ? (T)x[row] : T(0), dn = row < p.n ? D[row] : T(1);
-            for (int I = nb - 1; I >= 0; --I) {
-                const bool valid = row < p.n;
-                const T dr = dn;
-                // symmetric: y .= D_Dl1 .* y (:897) for the block's rows, then the backward solve
-                const T xr = SWEEP == 2 ? mul_rn(dr, yg[I * B + r]) : xn;
-                if (I > 0) {
-                    const int64_t rn = row - B;
-                    if (SWEEP == 1) xn = rn < p.n ? (T)x[rn] : T(0);
-                    dn = rn < p.n ? D[rn] : T(1);
+            T xn = (SWEEP == 1 && row < p.n) ? (T)x[row] : T(0), dr = row < p.n ? D[row] : T(1);
+            VT cur[NV], nxt[NV];
+            int I = nb - 1, J = nb;   // the item: tile (I, J) while J < nb, then the diagonal tile of I
+            uint32_t pos = base;
+            load_diag(cur, pos, false);
+            T acc = T(0);
+            while (true) {
+                const bool is_tile = J < nb;
+                const uint32_t npos = pos + (is_tile ? TILE : DG);
+                const int In = is_tile ? I : I - 1;
+                const int Jn = is_tile ? J + 1 : I;   // block I-1 starts with its tile J = I
+                const bool more = In >= 0;
+                if (more) {
+                    if (Jn < nb)
+                        load_tile(nxt, npos);
+                    else
+                        load_diag(nxt, npos, false);
                 }
-                T acc = T(0);
-                for (int J = I + 1; J < nb; ++J) {
-                    if (!have(TILE)) {
-                        ok = false;
-                        break;
+                prefetch_to(npos * (uint32_t)sizeof(T) + kPfAhead);
+                if (is_tile) {
+                    acc = tile(acc, cur, J);
+                } else {
+                    // symmetric: y .= D_Dl1 .* y (:897) for the block's rows, then the backward solve
+                    const T xr = SWEEP == 2 ? mul_rn(dr, yg[I * B + r]) : xn;
+                    T yown = T(0);
+#pragma unroll
+                    for (int c = B - 1; c >= 0; --c) {
+                        const T v = div_rn(sub_rn(xr, acc), dr);
+                        const T yc = __shfl_sync(FULL, v, c, B);
+                        if (r == c) yown = v;
+                        if (c > 0 && r < c) acc = add_rn(acc, mul_rn(VO::get(cur[(c - 1) / V], (c - 1) % V), yc));
                     }
-                    acc = tile(acc, J);
-                    pos += TILE;
-                    consumed();
+                    yg[I * B + r] = row < p.n ? yown : T(0);
+                    __syncwarp();
+                    acc = T(0);
+                    row -= B;
+                    if (more) {
+                        if (SWEEP == 1) xn = row < p.n ? (T)x[row] : T(0);
+                        dr = row < p.n ? D[row] : T(1);
+                    }
                 }
-                if (!ok) break;
-                if (!have(DG)) {
-                    ok = false;
-                    break;
-                }
-                const T* dp = ring + ((vg + pos) & rmask);
-                T au[B];
+                if (!more) break;
 #pragma unroll
-                for (int c = 1; c < B; ++c)
-                    au[c] = r < c ? dp[G * (B * (B - 1) / 2 - c * (c + 1) / 2) + g * c + r] : T(0);
-                T yown = T(0);
-#pragma unroll
-                for (int c = B - 1; c >= 0; --c) {
-                    const T v = div_rn(sub_rn(xr, acc), dr);
-                    const T yc = __shfl_sync(FULL, v, c, B);
-                    if (r == c) yown = v;
-                    if (c > 0 && r < c) acc = add_rn(acc, mul_rn(au[c], yc));
-                }
-                __syncwarp();   // every lane has read yg[I * B + r] above
-                yg[I * B + r] = valid ? yown : T(0);
-                __syncwarp();
-                pos += DG;
-                consumed();
-                row -= B;
+                for (int v = 0; v < NV; ++v) cur[v] = nxt[v];
+                I = In;
+                J = Jn;
+                pos = npos;
             }
         }
-        if (!ok) break;
-        if (c0 + nchg > freed) release(c0 + nchg);   // the group's last, partly used chunk
         __syncwarp();
         for (int t = lane; t < G * ps; t += 32) {
             const int64_t rr = rowbase + t;
             if (rr < p.n) y[rr] = (IO)ys[t];
         }
         __syncwarp();
-    }
-    if (!ok) {
-        // A bounded wait ran out: record it, let the copies in flight land
-        // (bounded), and return.
-        if (lane == 0) hsdev::report_error(p.err, hsdev::kErrWaitTimeout);
-        const int32_t end = __shfl_sync(FULL, issued, 0);
-        for (int32_t c = ready; c < end; ++c)
-            (void)hsdev::mbar_wait_bounded(bars + ((uint32_t)c & (nst - 1u)), ((uint32_t)c / nst) & 1u);
     }
 }
 

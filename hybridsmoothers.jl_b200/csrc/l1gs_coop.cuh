@@ -132,6 +132,11 @@ struct Geometry {
 
 inline Geometry make_geometry(const Layout& L, size_t es) {
     Geometry g;
+    if (L.blk) {   // the blocked kernel reads its streams directly: y of the group only
+        g.ys_off = 0;
+        g.warp_bytes = (uint32_t)(((size_t)L.G * L.ps * es + 127) / 128 * 128);
+        return g;
+    }
     // Tuning overrides: HSB200_COOP_CHUNK = chunk bytes (1024, 2048 or 4096),
     // HSB200_COOP_AHEAD = chunks kept in flight beyond a column block (1..8).
     uint32_t chunk_bytes = 2048, ahead = 2;
@@ -145,8 +150,7 @@ inline Geometry make_geometry(const Layout& L, size_t es) {
     }
     const uint32_t che = (uint32_t)(chunk_bytes / es);
     while ((1u << g.che_log2) < che) ++g.che_log2;
-    // entries of the longest linear run: a column block, or a blocked off-diagonal warp tile
-    const int64_t maxcol = L.blk ? 32 * kBlkB : (int64_t)L.G * (L.ps - 1);
+    const int64_t maxcol = (int64_t)L.G * (L.ps - 1);        // entries of the longest column block
     g.ntail = (uint32_t)std::max<int64_t>(1, (maxcol + che - 1) / che);
     // A column block spans at most ntail + 1 chunks; keep `ahead` more in flight.
     g.nst = 4;
@@ -156,8 +160,7 @@ inline Geometry make_geometry(const Layout& L, size_t es) {
     g.ys_off = (uint32_t)((ring + 8 * g.nst + 15) / 16 * 16);
     const size_t rows = (size_t)L.G * L.ps * es;
     g.ds_off = (uint32_t)(g.ys_off + (rows + 15) / 16 * 16);
-    // the blocked kernel keeps D_Dl1 in registers: y only
-    g.warp_bytes = (uint32_t)((g.ds_off + (L.blk ? 0 : rows) + 127) / 128 * 128);
+    g.warp_bytes = (uint32_t)((g.ds_off + rows + 127) / 128 * 128);
     return g;
 }
 

@@ -4,6 +4,7 @@
 #include <vector>
 
 #include "l1gs_seg.cuh"
+#include "l1gs_seg_ring.cuh"
 
 namespace {
 
@@ -122,122 +123,51 @@ int dalloc(hsseg::View* view, T** out, size_t bytes) {
 // ---------------------------------------------------------------------------
 // Apply: warp per group of 32 partitions, lane = partition.
 // ---------------------------------------------------------------------------
-constexpr int kTab = 32;   // (group, direction) pairs whose stream position a warp keeps in shared memory
+using hsseg::kTab;
+using hsseg::TabEnt;
 
-struct TabEnt {
-    int64_t base;   // first slot
-    int32_t tot;    // slots
-    int32_t pad;
-};
+// Slots per chunk: 4 (FP64, 1280 bytes) or 6 (FP32, 1152 bytes).
+template <typename T>
+constexpr int seg_k() {
+    return sizeof(T) == 8 ? 4 : 6;
+}
 
+// Runtime partsize (2..128): y and D_Dl1 of the group in shared memory.
 template <typename T, typename IO, int SWEEP>
 __global__ void __launch_bounds__(kSegWarps * 32, 1) l1gs_seg_kernel(const hsseg::Params p) {
     constexpr int S = 33;
-    constexpr uint32_t SB = 32 * (sizeof(T) + 2);                 // bytes per slot
-    constexpr int K = hsseg::kSlotsPerChunk(sizeof(T));           // slots per chunk
-    constexpr uint32_t CHB = K * SB;                              // bytes per chunk
+    constexpr uint32_t SB = 32 * (sizeof(T) + 2);   // bytes per slot
+    constexpr int K = seg_k<T>();
     constexpr int NDIR = SWEEP == 2 ? 2 : 1;
     extern __shared__ __align__(128) unsigned char smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ps = p.ps, psq = (ps + 3) & ~3;
-    const uint32_t nst = p.nst;
     unsigned char* wbase = smem + (size_t)warp * p.warp_bytes;
-    unsigned char* ring = wbase + p.ring_off;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(wbase + p.bars_off);
-    TabEnt* tab = reinterpret_cast<TabEnt*>(wbase + p.tab_off);
     T* ys = reinterpret_cast<T*>(wbase + p.ys_off);   // y of row li, lane's partition: ys[li * S + lane]; row ps: +0
     T* ds = reinterpret_cast<T*>(wbase + p.ds_off);
     const T* __restrict__ D = static_cast<const T*>(p.D);
     const IO* __restrict__ x = static_cast<const IO*>(p.x);
     IO* __restrict__ y = static_cast<IO*>(p.y);
     const int wpb = blockDim.x >> 5;
-    const int32_t q0 = p.gbeg + blockIdx.x * wpb + warp, qstride = gridDim.x * wpb;
-    const int32_t my_groups = q0 < p.gend ? (p.gend - 1 - q0) / qstride + 1 : 0;
-    const int32_t npairs = my_groups * NDIR;   // (group, direction) pairs, in sweep order
-    auto dir_of = [&](int d) -> const hsseg::Dir& { return (SWEEP == 1 || d == 1) ? p.up : p.lo; };
-
-    // Stream positions of this warp's pairs (the first kTab into the table)
-    // and the number of chunks of all of them.
-    int32_t nch_lane = 0;
-    for (int32_t pi = lane; pi < npairs; pi += 32) {
-        const int64_t g = q0 + (int64_t)(pi / NDIR) * qstride;
-        const hsseg::Dir& dd = dir_of(pi % NDIR);
-        const int32_t tot = dd.total[g];
-        if (pi < kTab) {
-            tab[pi].base = dd.base[g];
-            tab[pi].tot = tot;
-        }
-        nch_lane += (tot + K - 1) / K;
-    }
-    const int32_t total = (int32_t)__reduce_add_sync(FULL, (unsigned)nch_lane);
+    hsseg::SegStream<SB, K, NDIR, SWEEP> rs;
+    rs.ring = wbase + p.ring_off;
+    rs.bars = reinterpret_cast<uint64_t*>(wbase + p.bars_off);
+    rs.tab = reinterpret_cast<TabEnt*>(wbase + p.tab_off);
+    rs.nst = p.nst;
+    rs.q0 = p.gbeg + blockIdx.x * wpb + warp;
+    rs.qstride = gridDim.x * wpb;
+    rs.lo = p.lo;
+    rs.up = p.up;
+    const int32_t my_groups = rs.q0 < p.gend ? (p.gend - 1 - rs.q0) / rs.qstride + 1 : 0;
     ys[ps * S + lane] = T(0);
-    __syncwarp();
-
-    // Producer (lane 0): walks the pairs' chunks in order.
-    int32_t issued = 0, ppi = 0, pc = 0, pnch = -1, ptot = 0;
-    const unsigned char* psrc = nullptr;
-    auto advance = [&]() -> bool {   // position on the next chunk; false at the end
-        while (ppi < npairs) {
-            if (pnch < 0) {
-                const hsseg::Dir& dd = dir_of(ppi % NDIR);
-                int64_t b;
-                if (ppi < kTab) {
-                    b = tab[ppi].base;
-                    ptot = tab[ppi].tot;
-                } else {
-                    const int64_t g = q0 + (int64_t)(ppi / NDIR) * qstride;
-                    b = dd.base[g];
-                    ptot = dd.total[g];
-                }
-                pnch = (ptot + K - 1) / K;
-                psrc = dd.stream + b * SB;
-                pc = 0;
-            }
-            if (pc < pnch) return true;
-            pnch = -1;
-            ++ppi;
-        }
-        return false;
-    };
-    auto issue_next = [&]() {
-        if (!advance()) return;
-        const uint32_t s = (uint32_t)issued & (nst - 1u);
-        const uint32_t bytes = (uint32_t)min(K, ptot - pc * K) * SB;
-        hsdev::mbar_arrive_expect_tx(bars + s, bytes);
-        hsdev::bulk_load(ring + (size_t)s * CHB, psrc + (size_t)pc * CHB, bytes, bars + s);
-        ++issued;
-        ++pc;
-    };
-    if (lane == 0) {
-        for (uint32_t s = 0; s < nst; ++s) hsdev::mbar_init(bars + s, 1);
-        hsdev::fence_barrier_init();
-        while (issued < total && issued < (int32_t)nst) issue_next();
-    }
-    __syncwarp();
-    int32_t ready = 0, freed = 0;
+    rs.init(lane, my_groups);
     bool ok = true;
-    auto wait_upto = [&](int32_t last) -> bool {
-        while (ready <= last) {
-            const bool got = hsdev::mbar_wait_bounded(bars + ((uint32_t)ready & (nst - 1u)), ((uint32_t)ready / nst) & 1u);
-            if (!__all_sync(FULL, got)) return false;
-            ++ready;
-        }
-        return true;
-    };
-    auto release = [&](int32_t upto) {   // chunks below `upto` are consumed: refill their stages
-        freed = upto;
-        __syncwarp();
-        if (lane == 0) {
-            hsdev::fence_proxy_async_smem();
-            while (issued < total && issued < freed + (int32_t)nst) issue_next();
-        }
-    };
 
     // (partition, row) of this lane's t-th element of a group, t = lane + 32 u
     const int dq = 32 / ps, dr = 32 - dq * ps;
     int32_t ch = 0;   // chunk of the next slot
     for (int32_t gi = 0; gi < my_groups && ok; ++gi) {
-        const int64_t g = q0 + (int64_t)gi * qstride;
+        const int64_t g = rs.q0 + (int64_t)gi * rs.qstride;
         const int64_t rowbase = g * 32 * (int64_t)ps;
         const int32_t nrows = (int32_t)min((int64_t)32 * ps, (int64_t)p.n - rowbase);
         // x and D_Dl1 of the group's rows -> [li][partition], all loads in flight at once
@@ -293,7 +223,7 @@ __global__ void __launch_bounds__(kSegWarps * 32, 1) l1gs_seg_kernel(const hsseg
         uint32_t mw[NDIR];
 #pragma unroll
         for (int d = 0; d < NDIR; ++d)
-            mw[d] = 4 * lane < psq ? *reinterpret_cast<const uint32_t*>(dir_of(d).maxc + g * psq + 4 * lane) : 0u;
+            mw[d] = 4 * lane < psq ? *reinterpret_cast<const uint32_t*>(rs.dir(d).maxc + g * psq + 4 * lane) : 0u;
         hsdev::cp_async_wait_all();
         __syncwarp();
         T* yk = ys + lane;
@@ -310,11 +240,11 @@ __global__ void __launch_bounds__(kSegWarps * 32, 1) l1gs_seg_kernel(const hsseg
                 T yi = yk[li * S];
                 T acc = T(0);
                 for (int k = 0; k < m; ++k) {
-                    if (ch >= ready && !wait_upto(ch)) {
+                    if (ch >= rs.ready && !rs.wait_upto(ch)) {
                         ok = false;
                         break;
                     }
-                    const unsigned char* sp = ring + (size_t)((uint32_t)ch & (nst - 1u)) * CHB + (size_t)wi * SB;
+                    const unsigned char* sp = rs.slot(ch, wi);
                     const T a = reinterpret_cast<const T*>(sp)[lane];
                     const int col = reinterpret_cast<const uint16_t*>(sp + 32 * sizeof(T))[lane];
                     acc = add_rn(acc, mul_rn(a, yk[col * S]));
@@ -322,7 +252,7 @@ __global__ void __launch_bounds__(kSegWarps * 32, 1) l1gs_seg_kernel(const hsseg
                     if (++wi == K) {
                         wi = 0;
                         ++ch;
-                        release(ch);
+                        rs.release(ch, lane);
                     }
                 }
                 if (!ok) break;
@@ -332,7 +262,7 @@ __global__ void __launch_bounds__(kSegWarps * 32, 1) l1gs_seg_kernel(const hsseg
             if (!ok) break;
             if (wi > 0) {   // the pair's last, partly used chunk
                 ++ch;
-                release(ch);
+                rs.release(ch, lane);
             }
         }
         if (!ok) break;
@@ -352,27 +282,156 @@ __global__ void __launch_bounds__(kSegWarps * 32, 1) l1gs_seg_kernel(const hsseg
         __syncwarp();
     }
     if (!ok) {
-        // A bounded wait ran out: record it, let the copies in flight land
-        // (bounded), and return.
+        // A bounded wait ran out: record it, let the copies in flight land, and return.
         hsdev::cp_async_wait_all();
         if (lane == 0) hsdev::report_error(p.err, hsdev::kErrWaitTimeout);
-        const int32_t end = __shfl_sync(FULL, issued, 0);
-        for (int32_t c = ready; c < end; ++c)
-            (void)hsdev::mbar_wait_bounded(bars + ((uint32_t)c & (nst - 1u)), ((uint32_t)c / nst) & 1u);
+        rs.drain();
     }
 }
 
-template <typename T, typename IO, int SWEEP>
-int launch_t(const hsseg::View& view, hsseg::Params& p, cudaStream_t st) {
-    constexpr uint32_t CHB = hsseg::kSlotsPerChunk(sizeof(T)) * 32 * (sizeof(T) + 2);
+// Partsize PS known at compile time (8, 16, 32): the row loop is unrolled, a
+// lane's D_Dl1 stays in registers, x and y move as 16-byte vectors of the
+// lane's own partition (rows contiguous), the row lists come in as broadcast
+// words, and a lane only ever touches its own column of y in shared memory.
+template <typename T, typename IO, int SWEEP, int PS>
+__global__ void __launch_bounds__(kSegWarps * 32, 1) l1gs_seg_ps_kernel(const hsseg::Params p) {
+    constexpr int S = 32;
+    constexpr uint32_t SB = 32 * (sizeof(T) + 2);
+    constexpr int K = seg_k<T>();
+    constexpr int NDIR = SWEEP == 2 ? 2 : 1;
+    constexpr int PSQ = (PS + 3) & ~3;   // bytes of a group's row list
+    constexpr int NW = PSQ / 4;
+    constexpr int VX = 16 / (int)sizeof(IO), VD = 16 / (int)sizeof(T);
+    static_assert(PS % VX == 0 && PS % VD == 0, "whole vectors per partition");
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned char* wbase = smem + (size_t)warp * p.warp_bytes;
+    T* yk = reinterpret_cast<T*>(wbase + p.ys_off) + lane;   // y of row li of the lane's partition: yk[li * S]; row PS: +0
+    const T* __restrict__ D = static_cast<const T*>(p.D);
+    const IO* __restrict__ x = static_cast<const IO*>(p.x);
+    IO* __restrict__ y = static_cast<IO*>(p.y);
+    const int wpb = blockDim.x >> 5;
+    hsseg::SegStream<SB, K, NDIR, SWEEP> rs;
+    rs.ring = wbase + p.ring_off;
+    rs.bars = reinterpret_cast<uint64_t*>(wbase + p.bars_off);
+    rs.tab = reinterpret_cast<TabEnt*>(wbase + p.tab_off);
+    rs.nst = p.nst;
+    rs.q0 = p.gbeg + blockIdx.x * wpb + warp;
+    rs.qstride = gridDim.x * wpb;
+    rs.lo = p.lo;
+    rs.up = p.up;
+    const int32_t my_groups = rs.q0 < p.gend ? (p.gend - 1 - rs.q0) / rs.qstride + 1 : 0;
+    yk[PS * S] = T(0);
+    rs.init(lane, my_groups);
+    bool ok = true;
+    int32_t ch = 0;   // chunk of the next slot
+    for (int32_t gi = 0; gi < my_groups && ok; ++gi) {
+        const int64_t g = rs.q0 + (int64_t)gi * rs.qstride;
+        const int64_t prow = (g * 32 + lane) * (int64_t)PS;   // first row of the lane's partition
+        const bool whole = p.vec_io && prow + PS <= p.n;
+        T dreg[PS];
+        if (whole) {
+#pragma unroll
+            for (int v = 0; v < PS / VX; ++v) {
+                const uint4 w = *reinterpret_cast<const uint4*>(x + prow + v * VX);
+                const IO* e = reinterpret_cast<const IO*>(&w);
+#pragma unroll
+                for (int c = 0; c < VX; ++c) yk[(v * VX + c) * S] = (T)e[c];
+            }
+#pragma unroll
+            for (int v = 0; v < PS / VD; ++v) {
+                const uint4 w = *reinterpret_cast<const uint4*>(D + prow + v * VD);
+                const T* e = reinterpret_cast<const T*>(&w);
+#pragma unroll
+                for (int c = 0; c < VD; ++c) dreg[v * VD + c] = e[c];
+            }
+        } else {   // the short last partition, padding partitions, or unaligned vectors
+#pragma unroll
+            for (int li = 0; li < PS; ++li) {
+                const bool valid = prow + li < p.n;
+                yk[li * S] = valid ? (T)x[prow + li] : T(0);
+                dreg[li] = valid ? D[prow + li] : T(1);
+            }
+        }
+        // slots per row of each direction (the same words for every lane)
+        uint32_t mw[NDIR][NW];
+#pragma unroll
+        for (int d = 0; d < NDIR; ++d)
+#pragma unroll
+            for (int w = 0; w < NW; ++w) mw[d][w] = reinterpret_cast<const uint32_t*>(rs.dir(d).maxc + g * PSQ)[w];
+#pragma unroll
+        for (int d = 0; d < NDIR; ++d) {
+            const bool lowerdir = SWEEP == 0 || (SWEEP == 2 && d == 0);
+            int wi = 0;   // slot of the next entry inside chunk ch
+#pragma unroll
+            for (int t = 0; t < PS; ++t) {
+                const int li = lowerdir ? t : PS - 1 - t;
+                const int m = (int)((mw[d][li >> 2] >> ((li & 3) * 8)) & 0xffu);
+                T acc = T(0);
+                for (int k = 0; k < m; ++k) {
+                    if (ch >= rs.ready && !rs.wait_upto(ch)) {
+                        ok = false;
+                        break;
+                    }
+                    const unsigned char* sp = rs.slot(ch, wi);
+                    const T a = reinterpret_cast<const T*>(sp)[lane];
+                    const int col = reinterpret_cast<const uint16_t*>(sp + 32 * sizeof(T))[lane];
+                    acc = add_rn(acc, mul_rn(a, yk[col * S]));
+                    if (++wi == K) {   // a finished chunk goes back at once
+                        wi = 0;
+                        ++ch;
+                        rs.release(ch, lane);
+                    }
+                }
+                if (!ok) break;
+                T yi = yk[li * S];
+                if (SWEEP == 2 && !lowerdir) yi = mul_rn(dreg[li], yi);   // y .= D_Dl1 .* y (:897)
+                yk[li * S] = div_rn(sub_rn(yi, acc), dreg[li]);
+            }
+            if (!ok) break;
+            if (wi > 0) {   // the pair's last, partly used chunk
+                ++ch;
+                rs.release(ch, lane);
+            }
+        }
+        if (!ok) break;
+        if (whole) {
+#pragma unroll
+            for (int v = 0; v < PS / VX; ++v) {
+                uint4 w;
+                IO* e = reinterpret_cast<IO*>(&w);
+#pragma unroll
+                for (int c = 0; c < VX; ++c) e[c] = (IO)yk[(v * VX + c) * S];
+                *reinterpret_cast<uint4*>(y + prow + v * VX) = w;
+            }
+        } else {
+#pragma unroll
+            for (int li = 0; li < PS; ++li)
+                if (prow + li < p.n) y[prow + li] = (IO)yk[li * S];
+        }
+    }
+    if (!ok) {
+        if (lane == 0) hsdev::report_error(p.err, hsdev::kErrWaitTimeout);
+        rs.drain();
+    }
+}
+
+// Shared-memory slice of a warp: ring, barriers, table, y (+ D_Dl1 for the
+// runtime-partsize kernel).
+template <typename T>
+void seg_geometry(hsseg::Params& p, int S, bool with_d) {
+    constexpr uint32_t CHB = seg_k<T>() * 32 * (sizeof(T) + 2);
     p.nst = 4;
     p.ring_off = 0;
     p.bars_off = p.nst * CHB;
     p.tab_off = (p.bars_off + 8 * p.nst + 15) / 16 * 16;
     p.ys_off = p.tab_off + kTab * (uint32_t)sizeof(TabEnt);
-    p.ds_off = (p.ys_off + (uint32_t)(33 * (p.ps + 1) * sizeof(T)) + 15) / 16 * 16;
-    p.warp_bytes = (p.ds_off + (uint32_t)(33 * p.ps * sizeof(T)) + 127) / 128 * 128;
-    auto kern = l1gs_seg_kernel<T, IO, SWEEP>;
+    p.ds_off = (p.ys_off + (uint32_t)(S * (p.ps + 1) * sizeof(T)) + 15) / 16 * 16;
+    p.warp_bytes = (p.ds_off + (with_d ? (uint32_t)(S * p.ps * sizeof(T)) : 0u) + 127) / 128 * 128;
+}
+
+template <typename K>
+int launch_kernel(K kern, hsseg::Params& p, cudaStream_t st) {
     int best_w = 0, best_warps = 0, best_per_sm = 0;
     for (int w = kSegWarps; w >= 1; w >>= 1) {
         const size_t smem = (size_t)w * p.warp_bytes;
@@ -393,8 +452,18 @@ int launch_t(const hsseg::View& view, hsseg::Params& p, cudaStream_t st) {
     const int64_t grid = std::max<int64_t>(1, (ngr + rounds * best_w - 1) / (rounds * best_w));
     kern<<<(int)grid, best_w * 32, (size_t)best_w * p.warp_bytes, st>>>(p);
     HS_LAUNCH_CHECK("l1gs_seg_kernel");
-    (void)view;
     return HS_OK;
+}
+
+template <typename T, typename IO, int SWEEP>
+int launch_t(const hsseg::View& view, hsseg::Params& p, cudaStream_t st) {
+    (void)view;
+    switch (p.ps) {
+        case 8: seg_geometry<T>(p, 32, false); return launch_kernel(l1gs_seg_ps_kernel<T, IO, SWEEP, 8>, p, st);
+        case 16: seg_geometry<T>(p, 32, false); return launch_kernel(l1gs_seg_ps_kernel<T, IO, SWEEP, 16>, p, st);
+        case 32: seg_geometry<T>(p, 32, false); return launch_kernel(l1gs_seg_ps_kernel<T, IO, SWEEP, 32>, p, st);
+        default: seg_geometry<T>(p, 33, true); return launch_kernel(l1gs_seg_kernel<T, IO, SWEEP>, p, st);
+    }
 }
 
 template <typename T, typename IO>
@@ -498,6 +567,7 @@ int launch(int sdt, int io, int sweep, const View& view, int32_t n, int32_t ps, 
     p.x = x;
     p.y = y;
     p.err = err;
+    p.vec_io = ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y) | reinterpret_cast<uintptr_t>(D)) & 15u) == 0;
     if (sdt == HS_F64 && io == HS_F64) return launch_io<double, double>(sweep, view, p, st);
     if (sdt == HS_F32 && io == HS_F32) return launch_io<float, float>(sweep, view, p, st);
     if (sdt == HS_F32 && io == HS_F64) return launch_io<float, double>(sweep, view, p, st);

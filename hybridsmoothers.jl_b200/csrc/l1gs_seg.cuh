@@ -29,7 +29,6 @@
 
 namespace hsseg {
 
-constexpr int kSlotsPerChunk(int es) { return es == 8 ? 6 : 10; }   // chunks of 1920 bytes, whole slots
 constexpr int kMaxPartsize = 128;                                    // y and D_Dl1 slices in shared memory
 
 // Device arrays of a segment-list view (one direction).
@@ -62,6 +61,7 @@ struct Params {
     const void* x;
     void* y;
     int32_t* err;
+    int32_t vec_io;   // x, y and D_Dl1 are 16-byte aligned
     uint32_t warp_bytes, ring_off, bars_off, tab_off, ys_off, ds_off, nst;
 };
 

@@ -1,14 +1,15 @@
-"""CPU check of the blocked cooperative sweep's layout, ring protocol and order
-of operations (csrc/l1gs_coop.cuh "blocked variant", csrc/l1gs_blk.cu),
-before any GPU run.
+"""CPU check of the blocked cooperative sweep's layout and order of operations
+(csrc/l1gs_coop.cuh "blocked variant", csrc/l1gs_blk.cu), before any GPU
+run.
 
 The stream is built with the layout's index formulas (restated below from
 hscoop::lower_idx / upper_idx), checked to be a bijection onto each group's
-stream, and read back the way the kernel reads it: per row block, the
-off-diagonal warp tiles as 16-byte vectors from the ring's linear address
-(`(vg + pos) & rmask` plus the lane's offset), then the diagonal tile's
-columns; every ring read asserts that its chunk has landed, has not been
-released and holds the intended stream entry.  The arithmetic is the
+stream, and read back the way the kernel reads it: item by item (per row
+block the off-diagonal warp tiles, then the diagonal tile), the next item's
+position and kind from the kernel's state machine, each off-diagonal tile as
+the lane's 16-byte vectors at `pos + lane * V + v * 32 * V`, each diagonal
+entry at the kernel's offset; every read asserts that it stays inside the
+group's stream and returns the intended entry.  The arithmetic is the
 kernel's: dense products in column order for the off-diagonal tiles, the
 diagonal solve with the solved value broadcast, separately rounded multiply
 and add, rows past n held at 0.  Forward sweeps must equal the oracle bit for
@@ -21,7 +22,6 @@ import pytest
 
 from hsb200 import workloads as W
 from oracle import hs_oracle as O
-from test_coop_layout_cpu import Ring
 
 B = 8
 G = 4
@@ -63,17 +63,6 @@ def upper_idx(L, k, li, lj):
     return q * L["Lgp"] + L["upper_off"] + off
 
 
-def ring_geometry(es):
-    """hscoop::make_geometry for the blocked layout: 2 KiB chunks, the
-    longest linear run one off-diagonal warp tile."""
-    che = 2048 // es
-    ntail = max(1, -(-TILE // che))
-    st = 4
-    while st < ntail + 3:
-        st *= 2
-    return che, st, ntail
-
-
 def build_stream(A, ps, sweep, dtype):
     R = A.tocsr()
     n = A.shape[0]
@@ -96,112 +85,116 @@ def build_stream(A, ps, sweep, dtype):
     return L, SC, ngroups
 
 
-def emulate(A, ps, sweep, D, x, dtype, warps=3):
+def emulate(A, ps, sweep, D, x, dtype):
     T = np.dtype(dtype).type
     es = np.dtype(dtype).itemsize
     n = A.shape[0]
     L, SC, ngroups = build_stream(A, ps, sweep, dtype)
-    che, st, ntail = ring_geometry(es)
+    owner = {}   # stream position -> (partition, row, column): what the read must return
+    for k in range(ngroups * G):
+        for li in range(ps):
+            for lj in range(ps):
+                if lj < li and sweep != "backward":
+                    owner[lower_idx(L, k, li, lj)] = (k, li, lj)
+                elif lj > li and sweep != "forward":
+                    owner[upper_idx(L, k, li, lj)] = (k, li, lj)
     V = L["V"]
     nb = ps // B
     y = np.zeros(n, dtype=dtype)
-    for w in range(warps):
-        groups = list(range(w, ngroups, warps))
-        ring = Ring(SC, L, groups, che, st, ntail, es)
-        nchg = ring.nchg
-        for gi, q in enumerate(groups):
-            c0 = gi * nchg
-            vg = c0 * che
-            base = q * L["Lgp"]
-            rowbase = q * G * ps
-            ys = np.zeros(G * ps, dtype=dtype)
-            pos = 0
+    for q in range(ngroups):
+        base = q * L["Lgp"]
+        rowbase = q * G * ps
+        ys = np.zeros(G * ps, dtype=dtype)
 
-            def have(length):
-                ring.wait_upto(c0 + (pos + length - 1) // che)
+        def rd(pos, off, k, li, lj):
+            assert 0 <= pos + off < L["Lg"], "read outside the group's stream"
+            assert pos % V == 0, "vector read not 16-byte aligned"
+            assert owner[base + pos + off] == (k, li, lj), "read of the wrong entry"
+            return SC[base + pos + off]
 
-            def consumed():
-                ring.release(c0 + pos // che)
+        def tile(acc, pos, I, J):
+            for lane in range(32):
+                g, r = divmod(lane, B)
+                for v in range(B // V):
+                    for c in range(V):
+                        col = v * V + c
+                        a = rd(pos, v * 32 * V + lane * V + c, q * G + g, I * B + r, J * B + col)
+                        acc[lane] = T(acc[lane] + T(a * ys[g * ps + J * B + col]))
+            return acc
 
-            def rd(off):   # ring read at group-stream position pos + off
-                return ring.read(vg + pos, off, base + pos + off)
-
-            def tile(acc, J):
-                for lane in range(32):
-                    g, r = divmod(lane, B)
-                    for pv in range(B // V):
-                        for c in range(V):
-                            a = rd(pv * 32 * V + lane * V + c)
-                            acc[lane] = T(acc[lane] + T(a * ys[g * ps + J * B + pv * V + c]))
-                return acc
-
-            rows = [[rowbase + g * ps + I * B + r for g, r in (divmod(l, B) for l in range(32))] for I in range(nb)]
-            with np.errstate(all="ignore"):
-                if sweep != "backward":
-                    for I in range(nb):
+        rows = [[rowbase + g * ps + I * B + r for g, r in (divmod(l, B) for l in range(32))] for I in range(nb)]
+        with np.errstate(all="ignore"):
+            if sweep != "backward":
+                I, J, pos = 0, 0, 0
+                acc = [T(0)] * 32
+                while True:
+                    is_tile = J < I
+                    npos = pos + (TILE if is_tile else DG)
+                    In, Jn = (I, J + 1) if is_tile else (I + 1, 0)
+                    if is_tile:
+                        acc = tile(acc, pos, I, J)
+                    else:
                         valid = [rr < n for rr in rows[I]]
                         xr = [T(x[rr]) if v else T(0) for rr, v in zip(rows[I], valid)]
                         dr = [D[rr] if v else T(1) for rr, v in zip(rows[I], valid)]
-                        acc = [T(0)] * 32
-                        for J in range(I):
-                            have(TILE)
-                            acc = tile(acc, J)
-                            pos += TILE
-                            consumed()
-                        have(DG)
                         yown = [T(0)] * 32
                         for c in range(B):
                             v = [T((xr[l] - acc[l]) / dr[l]) for l in range(32)]
                             for lane in range(32):
                                 g, r = divmod(lane, B)
-                                yc = v[g * B + c]
                                 if r == c:
                                     yown[lane] = v[lane]
                                 if c < B - 1 and r > c:
-                                    a = rd(G * (c * (B - 1) - c * (c - 1) // 2) + g * (B - 1 - c) + (r - c - 1))
-                                    acc[lane] = T(acc[lane] + T(a * yc))
+                                    off = G * (c * (B - 1) - c * (c - 1) // 2) + g * (B - 1 - c) + (r - c - 1)
+                                    a = rd(pos, off, q * G + g, I * B + r, I * B + c)
+                                    acc[lane] = T(acc[lane] + T(a * v[g * B + c]))
                         for lane in range(32):
                             g, r = divmod(lane, B)
                             ys[g * ps + I * B + r] = yown[lane] if valid[lane] else T(0)
-                        pos += DG
-                        consumed()
-                if sweep != "forward":
-                    for I in range(nb - 1, -1, -1):
+                        acc = [T(0)] * 32
+                    if In >= nb:
+                        assert npos == L["Ld"]
+                        break
+                    I, J, pos = In, Jn, npos
+            if sweep != "forward":
+                pos = L["Lg"] // 2 if sweep == "symmetric" else 0
+                I, J = nb - 1, nb
+                acc = [T(0)] * 32
+                while True:
+                    is_tile = J < nb
+                    npos = pos + (TILE if is_tile else DG)
+                    In, Jn = (I, J + 1) if is_tile else (I - 1, I)
+                    if is_tile:
+                        acc = tile(acc, pos, I, J)
+                    else:
                         valid = [rr < n for rr in rows[I]]
                         dr = [D[rr] if v else T(1) for rr, v in zip(rows[I], valid)]
                         if sweep == "symmetric":
                             xr = [T(dr[l] * ys[(l // B) * ps + I * B + l % B]) for l in range(32)]
                         else:
                             xr = [T(x[rr]) if v else T(0) for rr, v in zip(rows[I], valid)]
-                        acc = [T(0)] * 32
-                        for J in range(I + 1, nb):
-                            have(TILE)
-                            acc = tile(acc, J)
-                            pos += TILE
-                            consumed()
-                        have(DG)
                         yown = [T(0)] * 32
                         for c in range(B - 1, -1, -1):
                             v = [T((xr[l] - acc[l]) / dr[l]) for l in range(32)]
                             for lane in range(32):
                                 g, r = divmod(lane, B)
-                                yc = v[g * B + c]
                                 if r == c:
                                     yown[lane] = v[lane]
                                 if c > 0 and r < c:
-                                    a = rd(G * (B * (B - 1) // 2 - c * (c + 1) // 2) + g * c + r)
-                                    acc[lane] = T(acc[lane] + T(a * yc))
+                                    off = G * (B * (B - 1) // 2 - c * (c + 1) // 2) + g * c + r
+                                    a = rd(pos, off, q * G + g, I * B + r, I * B + c)
+                                    acc[lane] = T(acc[lane] + T(a * v[g * B + c]))
                         for lane in range(32):
                             g, r = divmod(lane, B)
                             ys[g * ps + I * B + r] = yown[lane] if valid[lane] else T(0)
-                        pos += DG
-                        consumed()
-            assert pos == L["Lg"]
-            ring.release(c0 + nchg)
-            for t in range(G * ps):
-                if rowbase + t < n:
-                    y[rowbase + t] = ys[t]
-        assert ring.ready == ring.issued == ring.total
+                        acc = [T(0)] * 32
+                    if In < 0:
+                        assert npos == L["Lg"]
+                        break
+                    I, J, pos = In, Jn, npos
+        for t in range(G * ps):
+            if rowbase + t < n:
+                y[rowbase + t] = ys[t]
     return y
 
 

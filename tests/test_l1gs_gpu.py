@@ -168,8 +168,8 @@ def random_matrix(n, density, seed, sym=False):
     return W._canon(A.tocsc())
 
 
-CASES = [(1, 37), (2, 40), (3, 100), (5, 101), (12, 1234), (16, 1000), (17, 999), (24, 2000), (31, 700),
-         (32, 2048), (33, 1111), (64, 3000), (100, 2345), (256, 4000)]
+CASES = [(1, 37), (2, 40), (3, 100), (5, 101), (8, 777), (12, 1234), (16, 1000), (17, 999), (24, 2000), (31, 700),
+         (32, 2048), (32, 1999), (33, 1111), (64, 3000), (100, 2345), (256, 4000)]
 
 
 @pytest.mark.parametrize("ps,n", CASES)
@@ -191,7 +191,7 @@ def test_random_bitwise_fp64(ps, n, sweep, cache):
             np.testing.assert_array_equal(P.SUbuffer, ref.SU)
 
 
-@pytest.mark.parametrize("ps", [2, 16, 33, 64, 130])
+@pytest.mark.parametrize("ps", [2, 8, 16, 32, 33, 64, 130])
 @pytest.mark.parametrize("sweep", ["forward", "symmetric"])
 @pytest.mark.parametrize("cache", ["packed", "view"])
 def test_fp32_and_mixed_bitwise(ps, sweep, cache):
@@ -214,6 +214,26 @@ def test_fp32_and_mixed_bitwise(ps, sweep, cache):
     refm = O.OracleL1GS(A, ps, isSymA=True, sweep=sweep, cache=cache, dtype=np.float32)
     refm.D = D64.astype(np.float32)
     np.testing.assert_array_equal(y, refm.ldiv(x.astype(np.float32)).astype(np.float64))
+
+
+@pytest.mark.parametrize("ps", [8, 16, 32])
+@pytest.mark.parametrize("sweep", ["forward", "backward", "symmetric"])
+def test_view_unaligned_vectors(ps, sweep):
+    """x and y that start one element past a 16-byte boundary: the view
+    kernels' vector loads and stores give way to element accesses."""
+    A = W.poisson3d_7pt(14)
+    n = A.shape[0]
+    x = np.random.default_rng(ps).uniform(-1, 1, n)
+    ref = O.OracleL1GS(A, ps, isSymA=True, sweep=sweep, cache="view").ldiv(x)
+    P = hsb200.L1GSPrecBuilder(hsb200.CUDABackend(), threads=64, blocks=8)(
+        A, ps, isSymA=True, sweep=SWEEPS[sweep], cache_strategy=hsb200.MatrixViewCache())
+    for dtype, want in ((torch.float64, ref),):
+        xb = torch.zeros(n + 1, dtype=dtype, device="cuda")
+        yb = torch.zeros(n + 1, dtype=dtype, device="cuda")
+        xb[1:] = dev(x, dtype)
+        hsb200.ldiv_(yb[1:], P, xb[1:])
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(yb[1:].cpu().numpy(), want)
 
 
 def test_in_place_apply():

@@ -114,8 +114,10 @@ class Ring:
         assert self.owner[c % self.nst] == c and self.freed <= c < self.ready
 
 
-def emulate(A_rows, ps, sweep, D, x, dtype, warps=2, K=6):
+def emulate(A_rows, ps, sweep, D, x, dtype, warps=2, K=None):
     T = np.dtype(dtype).type
+    if K is None:   # slots per chunk of the kernels: 4 (FP64), 6 (FP32)
+        K = 4 if np.dtype(dtype).itemsize == 8 else 6
     dirs, ngroups = build(A_rows, ps, dtype)
     n = A_rows.shape[0]
     order = {"forward": ["lo"], "backward": ["up"], "symmetric": ["lo", "up"]}[sweep]
