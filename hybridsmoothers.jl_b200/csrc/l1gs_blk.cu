@@ -16,12 +16,13 @@
 // independent multiply-adds.  Multiply and add are rounded separately, as
 // in the reference.
 //
-// A warp's group stream is one contiguous run read front to back, so the
-// lanes load each tile straight from global memory (16-byte loads, 512
-// contiguous bytes per warp instruction), one tile ahead of the arithmetic in
-// registers, while lane 0 keeps the next 16 KiB of the stream on its way into
-// L2 (cp.async.bulk.prefetch.L2, no multicast).  Shared memory holds only y
-// of the group.
+// A warp walks its groups' streams item by item (an item: one off-diagonal
+// warp tile, 2 KiB in FP64, or one diagonal warp tile) in the order the
+// sweep uses them.  Each item is copied into a per-warp ring of kRing slots
+// in shared memory by 16-byte cp.async copies of all 32 lanes, kRing - 1
+// items ahead of the arithmetic; cp.async.wait_group counts the items that
+// have landed, so no barrier or flag is waited on.  Shared memory holds the
+// ring and y of the group.
 #include "l1gs_coop.cuh"
 
 namespace hscoop {
@@ -29,8 +30,7 @@ namespace {
 
 constexpr int kBlkWarps = 4;   // warps per block; every warp streams its own groups
 constexpr unsigned FULL = 0xffffffffu;
-constexpr uint32_t kPfStep = 4096;    // bytes per L2 prefetch
-constexpr uint32_t kPfAhead = 16384;  // bytes kept prefetched ahead of the reads
+constexpr int kRing = 4;   // item slots per warp: kRing - 1 items in flight
 
 template <typename T>
 struct Vec;
@@ -73,18 +73,71 @@ struct Vec<float> {
     }
 };
 
-__device__ __forceinline__ void prefetch_l2(const void* src, uint32_t bytes) {
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(reinterpret_cast<uint64_t>(src)), "r"(bytes)
-                 : "memory");
-}
+// Position in a warp's item sequence: for each of its groups, the forward
+// items (row blocks 0..nb-1: tiles J = 0..I-1, then the diagonal tile), then
+// the backward items (row blocks nb-1..0: tiles J = I+1..nb-1, then the
+// diagonal tile), as the sweep has them.
+template <int SWEEP>
+struct ItemCursor {
+    int32_t q;      // group
+    int32_t dir;    // 0 forward (lower stream), 1 backward (upper stream)
+    int32_t I, J;   // row block; tile column block (J == I forward, J == nb backward: the diagonal tile)
+    uint32_t pos;   // entry position inside the group stream
+    bool valid;
+
+    __device__ __forceinline__ void start_group(int32_t q_, int32_t gend, int nb) {
+        q = q_;
+        valid = q < gend;
+        if (SWEEP == 1) {
+            dir = 1;
+            I = nb - 1;
+            J = nb;
+        } else {
+            dir = 0;
+            I = 0;
+            J = 0;
+        }
+        pos = 0;
+    }
+    __device__ __forceinline__ bool is_tile(int nb) const { return dir == 0 ? J < I : J < nb; }
+    __device__ __forceinline__ void advance(int nb, uint32_t Lg, int32_t qstride, int32_t gend, uint32_t tile,
+                                            uint32_t dg) {
+        const bool t = is_tile(nb);
+        pos += t ? tile : dg;
+        if (dir == 0) {
+            if (t) {
+                ++J;
+            } else if (++I, J = 0, I == nb) {
+                if (SWEEP == 2) {   // the upper stream follows in the same group
+                    dir = 1;
+                    I = nb - 1;
+                    J = nb;
+                    pos = Lg / 2;
+                } else {
+                    start_group(q + qstride, gend, nb);
+                }
+            }
+        } else {
+            if (t) {
+                ++J;
+            } else if (--I < 0) {
+                start_group(q + qstride, gend, nb);
+            } else {
+                J = I + 1;
+            }
+        }
+    }
+};
 
 // SWEEP: 0 forward, 1 backward, 2 symmetric.
 template <typename T, typename IO, int SWEEP>
-__global__ void __launch_bounds__(kBlkWarps * 32, 1) l1gs_blk_kernel(const Params p) {
+__global__ void __launch_bounds__(kBlkWarps * 32) l1gs_blk_kernel(const Params p) {
     constexpr int B = kBlkB, G = 32 / B, V = 16 / (int)sizeof(T), NV = B / V;
     constexpr uint32_t TILE = 32 * B;              // entries of an off-diagonal warp tile
     constexpr uint32_t DG = G * B * (B - 1) / 2;   // entries of a diagonal warp tile
-    static_assert(B - 1 <= NV * V, "a diagonal tile's entries fit the item buffer");
+    constexpr uint32_t SLOT = TILE;                // entries of a ring slot (the larger item)
+    constexpr int CH_TILE = TILE * sizeof(T) / 16, CH_DG = DG * sizeof(T) / 16;   // 16-byte chunks
+    static_assert(CH_TILE % 32 == 0, "whole copies per lane");
     using VT = typename Vec<T>::type;
     using VO = Vec<T>;
     extern __shared__ __align__(128) unsigned char smem[];
@@ -94,168 +147,119 @@ __global__ void __launch_bounds__(kBlkWarps * 32, 1) l1gs_blk_kernel(const Param
     const int wpb = blockDim.x >> 5;
     const int32_t qstride = gridDim.x * wpb;
     const int32_t q0 = p.gbeg + blockIdx.x * wpb + warp;
-    T* ys = reinterpret_cast<T*>(smem + (size_t)warp * p.geo.warp_bytes);   // y of the group, natural row order
+    T* ring = reinterpret_cast<T*>(smem + (size_t)warp * p.geo.warp_bytes);   // kRing slots
+    T* ys = ring + kRing * SLOT;                                              // y of the group, natural row order
     const T* __restrict__ SC = static_cast<const T*>(p.SC);
     const T* __restrict__ D = static_cast<const T*>(p.D);
     const IO* __restrict__ x = static_cast<const IO*>(p.x);
     IO* __restrict__ y = static_cast<IO*>(p.y);
-    const uint32_t lg_bytes = (uint32_t)p.Lg * (uint32_t)sizeof(T);
+
+    // Copies run kRing - 1 items ahead; one commit group per item (empty past the end).
+    ItemCursor<SWEEP> ic;
+    ic.start_group(q0, p.gend, nb);
+    auto issue = [&](int slot) {
+        if (ic.valid) {
+            const int nch = ic.is_tile(nb) ? CH_TILE : CH_DG;
+            const unsigned char* src = reinterpret_cast<const unsigned char*>(SC + (int64_t)ic.q * p.Lgp + ic.pos);
+            unsigned char* dst = reinterpret_cast<unsigned char*>(ring + slot * SLOT);
+#pragma unroll
+            for (int c = 0; c < CH_TILE / 32; ++c) {
+                const int k = lane + 32 * c;
+                if (k < nch) hsdev::cp_async_cg16(dst + 16 * k, src + 16 * k);
+            }
+            ic.advance(nb, (uint32_t)p.Lg, qstride, p.gend, TILE, DG);
+        }
+        hsdev::cp_async_commit();
+    };
+#pragma unroll
+    for (int s = 0; s < kRing - 1; ++s) issue(s);
+    int32_t k = 0;   // items consumed
+    auto next_item = [&]() -> const T* {
+        hsdev::cp_async_wait<kRing - 2>();   // item k has landed (this lane's copies) ...
+        __syncwarp();                        // ... and every lane's; slot (k - 1) is free
+        issue((k + kRing - 1) & (kRing - 1));
+        const T* slot = ring + (k & (kRing - 1)) * SLOT;
+        ++k;
+        return slot;
+    };
 
     for (int32_t q = q0; q < p.gend; q += qstride) {
-        const T* gs = SC + (int64_t)q * p.Lgp;                 // the group stream
         const int64_t rowbase = (int64_t)q * G * ps;           // the group's rows are contiguous
         const int64_t prow = rowbase + (int64_t)g * ps + r;    // this lane's row of block 0
         T* yg = ys + g * ps;                                   // this lane's partition
-        uint32_t pf = 0;                                       // stream bytes requested into L2 (lane 0)
-        auto prefetch_to = [&](uint32_t upto) {
-            if (lane == 0) {
-                while (pf < upto && pf < lg_bytes) {
-                    const uint32_t nbytes = min(kPfStep, (lg_bytes - pf + 15u) & ~15u);
-                    prefetch_l2(reinterpret_cast<const unsigned char*>(gs) + pf, nbytes);
-                    pf += nbytes;
-                }
-            }
-        };
-        // this lane's entries of the off-diagonal tile at `pos` (columns in order)
-        auto load_tile = [&](VT* buf, uint32_t pos) {
-            const VT* src = reinterpret_cast<const VT*>(gs + pos) + lane;
-#pragma unroll
-            for (int v = 0; v < NV; ++v) buf[v] = __ldg(src + v * 32);
-        };
-        // this lane's entries of the diagonal tile at `pos`: slot c holds column c
-        // (lower, rows below it) or column c + 1 (upper, rows above it)
-        auto load_diag = [&](VT* buf, uint32_t pos, bool lower) {
-            const T* dp = gs + pos;
-#pragma unroll
-            for (int c = 0; c < B - 1; ++c) {
-                T val = T(0);
-                if (lower) {
-                    if (r > c) val = __ldg(dp + G * (c * (B - 1) - c * (c - 1) / 2) + g * (B - 1 - c) + (r - c - 1));
-                } else {
-                    const int cu = c + 1;
-                    if (r < cu) val = __ldg(dp + G * (B * (B - 1) / 2 - cu * (cu + 1) / 2) + g * cu + r);
-                }
-                VO::set(buf[c / V], c % V, val);
-            }
-        };
-        auto tile = [&](T acc, const VT* buf, int J) -> T {
+        auto tile = [&](T acc, const T* tp, int J) -> T {
+            const VT* ap = reinterpret_cast<const VT*>(tp) + lane;
             const VT* yp = reinterpret_cast<const VT*>(yg + J * B);
 #pragma unroll
-            for (int v = 0; v < NV; ++v) acc = VO::dot(acc, buf[v], yp[v]);
+            for (int v = 0; v < NV; ++v) acc = VO::dot(acc, ap[v * 32], yp[v]);
             return acc;
         };
-
         if (SWEEP != 1) {   // forward: row blocks 0 .. nb-1
-            prefetch_to(kPfAhead);
             int64_t row = prow;
             T xr = row < p.n ? (T)x[row] : T(0), dr = row < p.n ? D[row] : T(1);
-            VT cur[NV], nxt[NV];
-            int I = 0, J = 0;   // the item: tile (I, J) while J < I, then the diagonal tile of I
-            uint32_t pos = 0;
-            load_diag(cur, 0, true);
-            T acc = T(0);
-            while (true) {
-                const bool is_tile = J < I;
-                const uint32_t npos = pos + (is_tile ? TILE : DG);
-                const int In = is_tile ? I : I + 1;
-                const int Jn = is_tile ? J + 1 : 0;
-                const bool more = In < nb;
-                if (more) {   // the next item's entries, one item ahead
-                    if (Jn < In)
-                        load_tile(nxt, npos);
-                    else
-                        load_diag(nxt, npos, true);
-                }
-                prefetch_to(npos * (uint32_t)sizeof(T) + kPfAhead);
-                if (is_tile) {
-                    acc = tile(acc, cur, J);
-                } else {
-                    T yown = T(0);
+            for (int I = 0; I < nb; ++I) {
+                T acc = T(0);
+                for (int J = 0; J < I; ++J) acc = tile(acc, next_item(), J);
+                const T* dp = next_item();
+                T aj[B - 1];
 #pragma unroll
-                    for (int c = 0; c < B; ++c) {
-                        const T v = div_rn(sub_rn(xr, acc), dr);
-                        const T yc = __shfl_sync(FULL, v, c, B);
-                        if (r == c) yown = v;
-                        if (c < B - 1 && r > c) acc = add_rn(acc, mul_rn(VO::get(cur[c / V], c % V), yc));
-                    }
-                    // rows past n (a short last partition, padding partitions) stay 0
-                    yg[I * B + r] = row < p.n ? yown : T(0);
-                    __syncwarp();
-                    acc = T(0);
-                    row += B;
-                    if (more) {
-                        xr = row < p.n ? (T)x[row] : T(0);
-                        dr = row < p.n ? D[row] : T(1);
-                    }
-                }
-                if (!more) break;
+                for (int c = 0; c < B - 1; ++c)
+                    aj[c] = r > c ? dp[G * (c * (B - 1) - c * (c - 1) / 2) + g * (B - 1 - c) + (r - c - 1)] : T(0);
+                T yown = T(0);
 #pragma unroll
-                for (int v = 0; v < NV; ++v) cur[v] = nxt[v];
-                I = In;
-                J = Jn;
-                pos = npos;
+                for (int c = 0; c < B; ++c) {
+                    const T v = div_rn(sub_rn(xr, acc), dr);
+                    const T yc = __shfl_sync(FULL, v, c, B);
+                    if (r == c) yown = v;
+                    if (c < B - 1 && r > c) acc = add_rn(acc, mul_rn(aj[c], yc));
+                }
+                // rows past n (a short last partition, padding partitions) stay 0
+                yg[I * B + r] = row < p.n ? yown : T(0);
+                __syncwarp();
+                row += B;
+                if (I + 1 < nb) {   // the next block's x and D_Dl1
+                    xr = row < p.n ? (T)x[row] : T(0);
+                    dr = row < p.n ? D[row] : T(1);
+                }
             }
         }
         if (SWEEP != 0) {   // backward: row blocks nb-1 .. 0
-            const uint32_t base = SWEEP == 2 ? (uint32_t)p.Lg / 2 : 0u;
-            prefetch_to(base * (uint32_t)sizeof(T) + kPfAhead);
             int64_t row = prow + (int64_t)(nb - 1) * B;
             T xn = (SWEEP == 1 && row < p.n) ? (T)x[row] : T(0), dr = row < p.n ? D[row] : T(1);
-            VT cur[NV], nxt[NV];
-            int I = nb - 1, J = nb;   // the item: tile (I, J) while J < nb, then the diagonal tile of I
-            uint32_t pos = base;
-            load_diag(cur, pos, false);
-            T acc = T(0);
-            while (true) {
-                const bool is_tile = J < nb;
-                const uint32_t npos = pos + (is_tile ? TILE : DG);
-                const int In = is_tile ? I : I - 1;
-                const int Jn = is_tile ? J + 1 : I;   // block I-1 starts with its tile J = I
-                const bool more = In >= 0;
-                if (more) {
-                    if (Jn < nb)
-                        load_tile(nxt, npos);
-                    else
-                        load_diag(nxt, npos, false);
-                }
-                prefetch_to(npos * (uint32_t)sizeof(T) + kPfAhead);
-                if (is_tile) {
-                    acc = tile(acc, cur, J);
-                } else {
-                    // symmetric: y .= D_Dl1 .* y (:897) for the block's rows, then the backward solve
-                    const T xr = SWEEP == 2 ? mul_rn(dr, yg[I * B + r]) : xn;
-                    T yown = T(0);
+            for (int I = nb - 1; I >= 0; --I) {
+                T acc = T(0);
+                for (int J = I + 1; J < nb; ++J) acc = tile(acc, next_item(), J);
+                const T* dp = next_item();
+                T au[B];
 #pragma unroll
-                    for (int c = B - 1; c >= 0; --c) {
-                        const T v = div_rn(sub_rn(xr, acc), dr);
-                        const T yc = __shfl_sync(FULL, v, c, B);
-                        if (r == c) yown = v;
-                        if (c > 0 && r < c) acc = add_rn(acc, mul_rn(VO::get(cur[(c - 1) / V], (c - 1) % V), yc));
-                    }
-                    yg[I * B + r] = row < p.n ? yown : T(0);
-                    __syncwarp();
-                    acc = T(0);
-                    row -= B;
-                    if (more) {
-                        if (SWEEP == 1) xn = row < p.n ? (T)x[row] : T(0);
-                        dr = row < p.n ? D[row] : T(1);
-                    }
-                }
-                if (!more) break;
+                for (int c = 1; c < B; ++c)
+                    au[c] = r < c ? dp[G * (B * (B - 1) / 2 - c * (c + 1) / 2) + g * c + r] : T(0);
+                // symmetric: y .= D_Dl1 .* y (:897) for the block's rows, then the backward solve
+                const T xr = SWEEP == 2 ? mul_rn(dr, yg[I * B + r]) : xn;
+                T yown = T(0);
 #pragma unroll
-                for (int v = 0; v < NV; ++v) cur[v] = nxt[v];
-                I = In;
-                J = Jn;
-                pos = npos;
+                for (int c = B - 1; c >= 0; --c) {
+                    const T v = div_rn(sub_rn(xr, acc), dr);
+                    const T yc = __shfl_sync(FULL, v, c, B);
+                    if (r == c) yown = v;
+                    if (c > 0 && r < c) acc = add_rn(acc, mul_rn(au[c], yc));
+                }
+                yg[I * B + r] = row < p.n ? yown : T(0);
+                __syncwarp();
+                row -= B;
+                if (I > 0) {
+                    if (SWEEP == 1) xn = row < p.n ? (T)x[row] : T(0);
+                    dr = row < p.n ? D[row] : T(1);
+                }
             }
         }
-        __syncwarp();
         for (int t = lane; t < G * ps; t += 32) {
             const int64_t rr = rowbase + t;
             if (rr < p.n) y[rr] = (IO)ys[t];
         }
         __syncwarp();
     }
+    hsdev::cp_async_wait<0>();   // nothing left in flight (the tail commits are empty)
 }
 
 template <typename T, typename IO, int SWEEP>

@@ -132,9 +132,9 @@ struct Geometry {
 
 inline Geometry make_geometry(const Layout& L, size_t es) {
     Geometry g;
-    if (L.blk) {   // the blocked kernel reads its streams directly: y of the group only
-        g.ys_off = 0;
-        g.warp_bytes = (uint32_t)(((size_t)L.G * L.ps * es + 127) / 128 * 128);
+    if (L.blk) {   // the blocked kernel: a ring of 4 item slots (32 x 8 entries each), then y of the group
+        g.ys_off = (uint32_t)(4 * 32 * kBlkB * es);
+        g.warp_bytes = (uint32_t)((g.ys_off + (size_t)L.G * L.ps * es + 127) / 128 * 128);
         return g;
     }
     // Tuning overrides: HSB200_COOP_CHUNK = chunk bytes (1024, 2048 or 4096),

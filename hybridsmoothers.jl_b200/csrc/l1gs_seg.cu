@@ -289,7 +289,7 @@ __global__ void __launch_bounds__(kSegWarps * 32, 1) l1gs_seg_kernel(const hsseg
     }
 }
 
-// Partsize PS known at compile time (8, 16, 32): the row loop is unrolled, a
+// Partsize PS known at compile time (8, 16): the row loop is unrolled, a
 // lane's D_Dl1 stays in registers, x and y move as 16-byte vectors of the
 // lane's own partition (rows contiguous), the row lists come in as broadcast
 // words, and a lane only ever touches its own column of y in shared memory.
@@ -461,7 +461,6 @@ int launch_t(const hsseg::View& view, hsseg::Params& p, cudaStream_t st) {
     switch (p.ps) {
         case 8: seg_geometry<T>(p, 32, false); return launch_kernel(l1gs_seg_ps_kernel<T, IO, SWEEP, 8>, p, st);
         case 16: seg_geometry<T>(p, 32, false); return launch_kernel(l1gs_seg_ps_kernel<T, IO, SWEEP, 16>, p, st);
-        case 32: seg_geometry<T>(p, 32, false); return launch_kernel(l1gs_seg_ps_kernel<T, IO, SWEEP, 32>, p, st);
         default: seg_geometry<T>(p, 33, true); return launch_kernel(l1gs_seg_kernel<T, IO, SWEEP>, p, st);
     }
 }

@@ -21,10 +21,14 @@ cached per matrix class (stencil width and size bucket) together with the
 trial cost.
 
 ``OnlineTuner`` serves the batched engine, which offers partsizes 8/16/32 of
-the packed FP32 smoother: it spends no trial work, but gives the first
-requests of a class the candidates in turn and, once each has finished,
-keeps the one with the fewest modelled bytes to convergence (iterations x
-bytes streamed per iteration; the batched kernels are bandwidth-bound).
+the packed FP32 smoother: it spends no trial work, but gives small requests
+of a class the candidates in turn and, once each has finished, keeps the one
+with the fewest modelled bytes to convergence (iterations x bytes streamed
+per iteration; the batched kernels are bandwidth-bound).  Classes are coarse
+(stencil width buckets), and iteration counts are compared per n^(1/d) (d = 2
+for widths up to 5, else 3: PCG iterations of a stencil operator grow like
+h^-1), so requests of different sizes inform one choice; large requests never
+explore.
 """
 from __future__ import annotations
 
@@ -147,51 +151,67 @@ def batch_bytes_per_iteration(n, nnz, ps):
     return 12 * nnz + 4 * (n + 1) + 4 * (2 * S + 3 * n) + 8 * 12 * n
 
 
+def serving_class(A):
+    """(width bucket, dimension) of the online tuner: widths up to 5, 6-9,
+    10-19, 20 and more."""
+    width = A.nnz / max(A.shape[0], 1)
+    bucket = 0 if width <= 5.5 else 1 if width <= 9.5 else 2 if width <= 19.5 else 3
+    return (bucket, 2 if bucket == 0 else 3)
+
+
 class OnlineTuner:
     """Partsize of the batched engine's FP32 smoother, learnt from the solves
-    themselves: per matrix class, each candidate is tried on a request; the
-    finished solves' iteration counts pick the partsize with the fewest
-    modelled bytes to convergence."""
+    themselves: per class, each candidate is tried on a small request (n at
+    most `explore_max_n`); the finished solves' iteration counts, scaled by
+    n^(1/d), pick the partsize with the fewest modelled bytes to
+    convergence.  Until then (and for large requests) the default runs."""
 
-    def __init__(self, candidates=(8, 16, 32), default=16):
+    def __init__(self, candidates=(8, 16, 32), default=8, explore_max_n=1 << 17):
         self.candidates = tuple(candidates)
         self.default = default
-        self.assigned = {}   # class -> candidates handed out so far
-        self.obs = {}        # class -> {ps: [bytes to convergence per row, ...]}
-        self.tags = {}       # tag -> (class, ps, n, nnz)
+        self.explore_max_n = explore_max_n
+        self.assigned = {}   # class -> candidates handed out for exploration so far
+        self.obs = {}        # class -> {ps: [normalised bytes to convergence per row, ...]}
+        self.tags = {}       # tag -> (class, ps, n, nnz, exploring)
         self.history = {}    # tag -> partsize it ran with (admitted requests)
 
     def partsize_for(self, A, tag):
-        key = matrix_class(A)
+        key = serving_class(A)
+        n = A.shape[0]
         done = self.obs.get(key, {})
         tried = self.assigned.setdefault(key, [])
         untried = [c for c in self.candidates if c not in tried]
-        if untried:
+        exploring = False
+        if all(c in done for c in self.candidates):
+            ps = min(self.candidates, key=lambda c: float(np.mean(done[c])))
+        elif untried and n <= self.explore_max_n:
             ps = untried[0]
             tried.append(ps)
-        elif all(c in done for c in self.candidates):
-            ps = min(self.candidates, key=lambda c: float(np.mean(done[c])))
+            exploring = True
         else:
-            ps = self.default   # candidates still running: the default meanwhile
-        self.tags[tag] = (key, ps, A.shape[0], A.nnz)
+            ps = self.default   # candidates still running, or a large request: the default
+        self.tags[tag] = (key, ps, n, A.nnz, exploring)
         self.history[tag] = ps
         return ps
 
     def cancel(self, tag):
         """The request `tag` was not admitted: forget its assignment."""
-        key, ps, _, _ = self.tags.pop(tag)
+        key, ps, _, _, exploring = self.tags.pop(tag)
         self.history.pop(tag, None)
         tried = self.assigned.get(key, [])
-        if ps in tried and ps not in self.obs.get(key, {}):
+        if exploring and ps in tried:
             tried.remove(ps)
 
     def observe(self, tag, iterations):
-        key, ps, n, nnz = self.tags.pop(tag)
-        cost = iterations * batch_bytes_per_iteration(n, nnz, ps) / max(n, 1)
+        key, ps, n, nnz, _ = self.tags.pop(tag)
+        n = max(n, 1)
+        cost = iterations / n ** (1.0 / key[1]) * batch_bytes_per_iteration(n, nnz, ps) / n
         self.obs.setdefault(key, {}).setdefault(ps, []).append(cost)
+        if ps not in self.assigned.setdefault(key, []):
+            self.assigned[key].append(ps)   # a default run counts as that candidate's trial
 
     def choice(self, A):
-        key = matrix_class(A)
+        key = serving_class(A)
         done = self.obs.get(key, {})
         if not done:
             return None

@@ -256,3 +256,104 @@ def test_blk_emulation_fp32_and_nonfinite():
             fin = np.isfinite(want)
             np.testing.assert_array_equal(np.isfinite(got), fin)
             np.testing.assert_allclose(got[fin], want[fin], rtol=1e-5, atol=1e-5 * np.abs(want[fin]).max())
+
+
+class ItemCursor:
+    """hscoop::ItemCursor (csrc/l1gs_blk.cu): the copy side's walk over a
+    warp's items, run ahead of the arithmetic."""
+
+    def __init__(self, sweep, q0, qstride, gend, nb, Lg):
+        self.sweep, self.qstride, self.gend, self.nb, self.Lg = sweep, qstride, gend, nb, Lg
+        self.start_group(q0)
+
+    def start_group(self, q):
+        self.q, self.valid = q, q < self.gend
+        if self.sweep == "backward":
+            self.dir, self.I, self.J = 1, self.nb - 1, self.nb
+        else:
+            self.dir, self.I, self.J = 0, 0, 0
+        self.pos = 0
+
+    def is_tile(self):
+        return self.J < self.I if self.dir == 0 else self.J < self.nb
+
+    def advance(self):
+        t = self.is_tile()
+        self.pos += TILE if t else DG
+        if self.dir == 0:
+            if t:
+                self.J += 1
+            else:
+                self.I, self.J = self.I + 1, 0
+                if self.I == self.nb:
+                    if self.sweep == "symmetric":
+                        self.dir, self.I, self.J, self.pos = 1, self.nb - 1, self.nb, self.Lg // 2
+                    else:
+                        self.start_group(self.q + self.qstride)
+        else:
+            if t:
+                self.J += 1
+            else:
+                self.I -= 1
+                if self.I < 0:
+                    self.start_group(self.q + self.qstride)
+                else:
+                    self.J = self.I + 1
+
+
+def consumer_items(sweep, q0, qstride, gend, nb, Lg):
+    """The arithmetic side's item order: (group, position, is tile, J)."""
+    out = []
+    for q in range(q0, gend, qstride):
+        if sweep != "backward":
+            pos = 0
+            for I in range(nb):
+                for J in range(I):
+                    out.append((q, pos, True, J))
+                    pos += TILE
+                out.append((q, pos, False, I))
+                pos += DG
+            assert pos == (Lg // 2 if sweep == "symmetric" else Lg)
+        if sweep != "forward":
+            pos = Lg // 2 if sweep == "symmetric" else 0
+            for I in range(nb - 1, -1, -1):
+                for J in range(I + 1, nb):
+                    out.append((q, pos, True, J))
+                    pos += TILE
+                out.append((q, pos, False, I))
+                pos += DG
+            assert pos == Lg
+    return out
+
+
+@pytest.mark.parametrize("ps", [8, 16, 64])
+@pytest.mark.parametrize("sweep", ["forward", "backward", "symmetric"])
+def test_blk_copy_cursor_matches_arithmetic(ps, sweep):
+    """The copies (kRing - 1 items ahead, one commit group per item, empty
+    groups past the end) land every item the arithmetic reads, in its order,
+    into the slot it reads, and never overwrite a slot still to be read."""
+    kring = 4
+    nb = ps // B
+    L = make_layout(ps, sweep != "backward", sweep != "forward", 8)
+    for q0, qstride, gend in ((0, 3, 7), (2, 3, 3), (5, 3, 4)):
+        want = consumer_items(sweep, q0, qstride, gend, nb, L["Lg"])
+        ic = ItemCursor(sweep, q0, qstride, gend, nb, L["Lg"])
+        groups = []   # commit groups in order: the item each copied, or None (empty)
+        slots = {}
+
+        def issue(slot):
+            if ic.valid:
+                groups.append((ic.q, ic.pos, ic.is_tile()))
+                slots[slot] = len(groups) - 1
+                ic.advance()
+            else:
+                groups.append(None)
+        for s in range(kring - 1):
+            issue(s)
+        for k, (q, pos, is_tile, _) in enumerate(want):
+            # wait_group(kring - 2): groups 0..k have completed
+            assert len(groups) == k + kring - 1
+            issue((k + kring - 1) % kring)
+            assert slots[k % kring] == k, "slot overwritten before it was read"
+            assert groups[k] == (q, pos, is_tile)
+        assert not ic.valid and all(gr is None for gr in groups[len(want):])
