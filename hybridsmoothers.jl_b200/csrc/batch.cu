@@ -38,6 +38,7 @@ constexpr int kRPB = 256;     // rows per CSR-stream pass (= threads per CTA)
 constexpr int kSub = 4;       // passes per CTA
 constexpr int kRPC = kRPB * kSub;   // rows per CTA of the segmented kernels
 constexpr int kT = 256;
+constexpr int kBatchE = 16;   // stream rows per tile of the batched smoother
 
 struct Scalars {
     double bb, rr, rz, pq, alpha, beta, rtol;
@@ -74,8 +75,7 @@ struct BlockMap {
 // One work item of the batched L1GS apply: 32 partitions (a group) of a slot,
 // with its stream bases, D_Dl1 and vectors already offset to the group.
 struct PrecItem {
-    const float* SL;
-    const float* SU;
+    const float* ST;   // the group's tile stream: lower tiles, then upper tiles (E x 32 floats each)
     const float* Di;
     const double* x;   // r of the group's first row
     double* y;         // z likewise
@@ -89,18 +89,25 @@ struct PrecItem {
 // Same arithmetic as the single-system driver: compensated (Dot2) dots,
 // separately rounded updates, storage-order SpMV rows.  The streaming kernels
 // load kSub elements per thread before using any.
-__global__ void __launch_bounds__(kT, 5) seg_spmv_dot(const BlockMap* __restrict__ map, double* __restrict__ partials) {
+__global__ void __launch_bounds__(kT, 4) seg_spmv_dot(const BlockMap* __restrict__ map, double* __restrict__ partials) {
     __shared__ double wbuf[kT / 32][hsdev::kWarpCap];
     const BlockMap m = map[blockIdx.x];
     DD part{0.0, 0.0};
+    const int warp = threadIdx.x >> 5;
+    // The row pointers of all the warp's chunks, requested before the slot's
+    // flag is known (one round trip instead of one per chunk).
+    hsdev::RowPtrs rpp[kRPC / kT];
+#pragma unroll
+    for (int k = 0; k < kRPC / kT; ++k)
+        rpp[k] = hsdev::load_rowptrs(m.n, m.rp, (int64_t)m.row0 + (k * (kT / 32) + warp) * 32);
     if (!m.s->done) {   // uniform over the CTA (one slot per CTA)
-        const int warp = threadIdx.x >> 5;
         auto fp = [&](int32_t j) { return __ldg(m.p + j); };
+#pragma unroll
         for (int k = 0; k < kRPC / kT; ++k) {   // the warp's 32-row chunks of this CTA
             const int64_t row0 = (int64_t)m.row0 + (k * (kT / 32) + warp) * 32;
             if (row0 >= m.n) break;   // uniform over the warp
-            const double acc =
-                hsdev::csr_warp_fold(wbuf[warp], m.n, m.rp, m.ci, m.v, row0, 0.0, fp, hsdev::AddOp<double>());
+            const double acc = hsdev::csr_warp_fold_rp(wbuf[warp], m.n, rpp[k], m.ci, m.v, row0, 0.0, fp,
+                                                       hsdev::AddOp<double>());
             const int64_t r = row0 + (threadIdx.x & 31);
             if (r < m.n) {
                 m.q[r] = acc;
@@ -266,13 +273,34 @@ __global__ void init_scalars(const double* __restrict__ pbb, const double* __res
 }
 
 // ---- batched L1GS symmetric apply (FP32 smoother, FP64 vectors) -----------
-// Work item -> 32 partitions (a group) of one slot, one lane each.  The packed
-// streams of the group are read tile by tile with 1D bulk copies (one per
-// stream row, 128 bytes) into a per-warp ring; y and D_Dl1 live in registers,
-// exactly like the single-system partsize<=32 kernel.  The elected lane keeps
-// the stream bases of the item it is issuing for in registers, so a refill is
-// one instruction sequence with no dependent loads.  Tiles of converged slots
-// are still fetched and applied until they leave the tables at the next rebuild.
+// Work item -> 32 partitions (a group) of one slot, one lane each.  At
+// admission the slot's packed triangles are regrouped so that each group's
+// tiles (E stream rows x 32 partitions, lower then upper, the last tile of
+// each triangle padded with zeros) are contiguous: a tile is one 1D bulk copy
+// of E x 128 bytes into the per-warp ring.  y and D_Dl1 live in registers,
+// exactly like the single-system partsize<=32 kernel; the sums read only the
+// triangle's entries, so the padding is never added.  The elected lane keeps
+// the tile stream of the item it is issuing for in a register.  Tiles of
+// converged slots are still fetched and applied until they leave the tables
+// at the next rebuild.
+template <int E>
+__global__ void batch_tiles_kernel(int64_t ngroups, int32_t tlen, int32_t nt, int64_t npad,
+                                   const float* __restrict__ SLi, const float* __restrict__ SUi,
+                                   float* __restrict__ tiles) {
+    const int64_t per_group = (int64_t)2 * nt * E * 32;
+    const int64_t total = ngroups * per_group;
+    for (int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; o < total;
+         o += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t g = o / per_group;
+        const int64_t w = o - g * per_group;
+        const int64_t t = w / (E * 32), rem = w - t * (E * 32);
+        const int64_t row = rem / 32, lane = rem - row * 32;
+        const bool upper = t >= nt;
+        const int64_t e = (upper ? t - nt : t) * E + row;
+        tiles[o] = e < tlen ? (upper ? SUi : SLi)[e * npad + g * 32 + lane] : 0.0f;
+    }
+}
+
 template <int PS, int E, int STAGES>
 __global__ void __launch_bounds__(128, 3)
     l1gs_batched_kernel(const PrecItem* __restrict__ items, int32_t nitems, double* __restrict__ rz_part,
@@ -296,39 +324,22 @@ __global__ void __launch_bounds__(128, 3)
     const int32_t my_items = w0 < nitems ? (nitems - 1 - w0) / wstride + 1 : 0;
     const int32_t total = my_items * NTPG;
 
-    // Tile refills: lane 0 posts the byte count on the stage's barrier and
-    // lanes 0..rows-1 each copy one 128-byte stream row, so a refill is one
-    // round of parallel bulk copies.  Every lane keeps the stream bases of the
-    // item it issues for (one broadcast load per item).
+    // Tile refills: lane 0 copies the tile (E x 128 contiguous bytes) with one
+    // bulk copy onto the stage's barrier.  It keeps the tile stream of the
+    // item it issues for (one load per item).
     int32_t cache_ii = -1;
-    const float* cSL = nullptr;
-    const float* cSU = nullptr;
-    int64_t cnpad = 0;
-    auto issue = [&](int32_t c) {   // called by the whole warp
+    const float* cST = nullptr;
+    auto issue = [&](int32_t c) {   // called by lane 0
         const int32_t ii = c / NTPG;
         if (ii != cache_ii) {
-            const PrecItem& it = items[w0 + ii * wstride];
-            cSL = it.SL;
-            cSU = it.SU;
-            cnpad = it.npad;
+            cST = items[w0 + ii * wstride].ST;
             cache_ii = ii;
         }
-        int32_t ti = c - ii * NTPG;
-        const float* base = ti < NT ? cSL : cSU;
-        if (ti >= NT) ti -= NT;
+        const int32_t ti = c - ii * NTPG;
         const int stage = c & (STAGES - 1);
-        const int rows = min(E, TLEN - ti * E);
         uint64_t* bar = bars + stage;
-        if (lane == 0) hsdev::mbar_arrive_expect_tx(bar, (uint32_t)(rows * 128));
-        if (lane < rows) {
-            const float* src = base + (int64_t)(ti * E + lane) * cnpad;
-            float* dst = ring + stage * (E * 32) + lane * 32;
-            asm volatile(
-                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], 128, [%2];" ::"r"(
-                    hsdev::smem_u32(dst)),
-                "l"(src), "r"(hsdev::smem_u32(bar))
-                : "memory");
-        }
+        hsdev::mbar_arrive_expect_tx(bar, (uint32_t)(E * 32 * 4));
+        hsdev::bulk_load(ring + stage * (E * 32), cST + (int64_t)ti * E * 32, (uint32_t)(E * 32 * 4), bar);
     };
     int32_t last_wait = 0;   // the tile of the latest wait (a timeout drains from here)
     auto wait = [&](int32_t c) -> bool {
@@ -338,7 +349,7 @@ __global__ void __launch_bounds__(128, 3)
     };
     auto release = [&](int32_t c) {
         __syncwarp();
-        if (c + STAGES < total) {
+        if (lane == 0 && c + STAGES < total) {
             hsdev::fence_proxy_async_smem();
             issue(c + STAGES);
         }
@@ -348,14 +359,18 @@ __global__ void __launch_bounds__(128, 3)
         hsdev::fence_barrier_init();
     }
     __syncwarp();
-    for (int32_t c = 0; c < min(total, STAGES); ++c) issue(c);
+    if (lane == 0)
+        for (int32_t c = 0; c < min(total, STAGES); ++c) issue(c);
     __syncwarp();
 
     int32_t c = 0;
+    PrecItem nit{};   // the next item, loaded one item ahead
+    if (my_items > 0) nit = items[w0];
     for (int32_t ii = 0; ii < my_items; ++ii) {
         // A converged slot's z is computed too (harmless: the dot and p kernels
         // skip it, its r is frozen) -- no dependent load of its flag here.
-        const PrecItem it = items[w0 + ii * wstride];
+        const PrecItem it = nit;
+        if (ii + 1 < my_items) nit = items[w0 + (ii + 1) * wstride];
         float d[PS];
 #pragma unroll
         for (int li = 0; li < PS; ++li) d[li] = it.Di[(int64_t)li * it.npad + lane];
@@ -453,6 +468,7 @@ struct hs_batch_slot {
     hs_l1gs* P = nullptr;
     int32_t n = 0, ps = 0;
     double* vec = nullptr;   // x r z p q b (6n doubles)
+    float* tiles = nullptr;  // per group: the smoother's tiles, contiguous (batch_tiles_kernel)
     double* x_out = nullptr; // host destination
     int64_t bytes = 0;
     int32_t blk0 = 0, nblk = 0;
@@ -498,7 +514,8 @@ int64_t slot_estimate(int32_t n, int64_t nnz, int ps) {
     const int64_t nparts = (n + ps - 1) / ps;
     const int64_t npad = (nparts + 31) / 32 * 32;
     const int64_t tlen = (int64_t)ps * (ps - 1) / 2;
-    const int64_t prec = 4 * (2 * tlen * npad + (int64_t)ps * npad + n);
+    const int64_t ntile = (tlen + kBatchE - 1) / kBatchE;
+    const int64_t prec = 4 * (2 * tlen * npad + (int64_t)ps * npad + n) + 4 * 2 * ntile * kBatchE * npad;
     const int64_t mat = 4 * (n + 1) + 12 * nnz;
     return prec + mat + 6 * 8 * (int64_t)n + 64 * 1024;
 }
@@ -508,7 +525,7 @@ int launch_batched(hs_batch* B, const hs_batch_s::Cls& cl, cudaStream_t st) {
     constexpr uint32_t wb = batched_warp_bytes<PS>();
     const int wpb = 4;
     const size_t smem = (size_t)wb * wpb;
-    auto kern = l1gs_batched_kernel<PS, 16, 4>;
+    auto kern = l1gs_batched_kernel<PS, kBatchE, 4>;
     if (int rc = hs::ensure_dynamic_smem((const void*)kern, (int)smem)) return rc;
     int per_sm = 0;
     HS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, wpb * 32, smem));
@@ -547,8 +564,7 @@ int rebuild(hs_batch* B) {
             double* z = sl.vec + 2 * (size_t)sl.n;
             for (int32_t g = 0; g < lv.ngroups; ++g) {
                 PrecItem it{};
-                it.SL = static_cast<const float*>(lv.SLi) + (int64_t)g * 32;
-                it.SU = static_cast<const float*>(lv.SUi) + (int64_t)g * 32;
+                it.ST = sl.tiles + (int64_t)g * 2 * ((lv.tlen + kBatchE - 1) / kBatchE) * kBatchE * 32;
                 it.Di = static_cast<const float*>(lv.Di) + (int64_t)g * 32;
                 const int64_t row0 = (int64_t)g * 32 * ps;
                 it.x = r + row0;
@@ -648,6 +664,7 @@ void free_slot(hs_batch* B, hs_batch_slot& sl) {
     if (sl.P) hs::l1gs_destroy_async(sl.P, B->solve);
     if (sl.A) hs::matrix_destroy_async(sl.A, B->solve);
     if (sl.vec) cudaFreeAsync(sl.vec, B->solve);
+    if (sl.tiles) cudaFreeAsync(sl.tiles, B->solve);
     B->used -= sl.bytes;
     sl = hs_batch_slot();
 }
@@ -736,11 +753,29 @@ int hs_batch_submit(hs_batch* B, const hs_sparse* A, const double* b_host, doubl
         cudaError_t e = cudaMallocAsync(&sl.vec, sizeof(double) * 6 * (size_t)A->n, B->setup);
         if (e) rc = hs::cuda_error(e, "cudaMallocAsync (slot vectors)");
     }
+    if (!rc) {   // the smoother's tiles, regrouped for the batched kernel
+        hs::L1gsView lv;
+        hs::l1gs_view_of(sl.P, &lv);
+        const int32_t nt = (int32_t)((lv.tlen + kBatchE - 1) / kBatchE);
+        const int64_t count = (int64_t)lv.ngroups * 2 * nt * kBatchE * 32;
+        cudaError_t e = cudaMallocAsync(&sl.tiles, sizeof(float) * (size_t)std::max<int64_t>(count, 32), B->setup);
+        if (e) {
+            rc = hs::cuda_error(e, "cudaMallocAsync (slot tiles)");
+        } else if (count > 0) {
+            const int grid = (int)std::min<int64_t>((count + kT - 1) / kT, 8192);
+            batch_tiles_kernel<kBatchE><<<grid, kT, 0, B->setup>>>(lv.ngroups, (int32_t)lv.tlen, nt, lv.npad,
+                                                                    static_cast<const float*>(lv.SLi),
+                                                                    static_cast<const float*>(lv.SUi), sl.tiles);
+            hs::count_launch();
+            if ((e = cudaGetLastError()) != cudaSuccess) rc = hs::cuda_error(e, "batch_tiles_kernel");
+        }
+    }
     // Every failure from here on releases what the slot holds (in stream
     // order on the setup stream, after the work already queued there).
     auto fail = [&](int code) {
         cudaStreamSynchronize(B->setup);
         if (sl.vec) cudaFreeAsync(sl.vec, B->setup);
+        if (sl.tiles) cudaFreeAsync(sl.tiles, B->setup);
         if (sl.P) hs::l1gs_destroy_async(sl.P, B->setup);
         if (sl.A) hs::matrix_destroy_async(sl.A, B->setup);
         return code;

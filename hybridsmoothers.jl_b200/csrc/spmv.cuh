@@ -32,19 +32,42 @@ struct SubOp {
 constexpr int kWarpCap = 256;   // products per window (2 KB of FP64 per warp)
 constexpr int kWarpKU = 4;      // entries per lane per load round
 
+// The row pointers of a lane's row in the 32-row chunk at row0 (0, 0 past n).
+struct RowPtrs {
+    int32_t ra, rb;
+};
+__device__ __forceinline__ RowPtrs load_rowptrs(int32_t n, const int32_t* __restrict__ rp, int64_t row0) {
+    const int64_t r = row0 + (threadIdx.x & 31);
+    RowPtrs p{0, 0};
+    if (r < n) {
+        p.ra = __ldg(rp + r);
+        p.rb = __ldg(rp + r + 1);
+    }
+    return p;
+}
+
+template <typename T, typename F, typename Op>
+__device__ __forceinline__ T csr_warp_fold_rp(T* __restrict__ wbuf, int32_t n, RowPtrs rpp,
+                                              const int32_t* __restrict__ ci, const T* __restrict__ v, int64_t row0,
+                                              T acc0, F f, Op op);
+
 template <typename T, typename F, typename Op>
 __device__ __forceinline__ T csr_warp_fold(T* __restrict__ wbuf, int32_t n, const int32_t* __restrict__ rp,
                                            const int32_t* __restrict__ ci, const T* __restrict__ v, int64_t row0,
                                            T acc0, F f, Op op) {
+    return csr_warp_fold_rp(wbuf, n, load_rowptrs(n, rp, row0), ci, v, row0, acc0, f, op);
+}
+
+// csr_warp_fold with the chunk's row pointers already loaded (load_rowptrs).
+template <typename T, typename F, typename Op>
+__device__ __forceinline__ T csr_warp_fold_rp(T* __restrict__ wbuf, int32_t n, RowPtrs rpp,
+                                              const int32_t* __restrict__ ci, const T* __restrict__ v, int64_t row0,
+                                              T acc0, F f, Op op) {
     const int lane = threadIdx.x & 31;
     const int64_t r = row0 + lane;
     const bool valid = r < n;
     const int nrows = (int)min((int64_t)32, (int64_t)n - row0);
-    int32_t ra = 0, rb = 0;
-    if (valid) {
-        ra = __ldg(rp + r);
-        rb = __ldg(rp + r + 1);
-    }
+    const int32_t ra = rpp.ra, rb = rpp.rb;
     const int32_t q0 = __shfl_sync(0xffffffffu, ra, 0);
     const int32_t q1 = __shfl_sync(0xffffffffu, rb, nrows - 1);
     T acc = acc0;
