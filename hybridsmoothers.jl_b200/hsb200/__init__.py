@@ -228,8 +228,10 @@ class L1GSPrecBuilder:
         precision: None (the matrix type) or np.float32 for an FP32 smoother
         built from an FP64 matrix.
         threads_per_part: 0 (the library chooses), 1 (one thread per
-        partition: every row summed in the reference's order, bit-identical)
-        or 4/8/16/32 lanes sharing a partition (forward sweeps stay
+        partition: every row summed in the reference's order, bit-identical),
+        8 with a partsize that is a multiple of 8 (the blocked sweep over 8x8
+        tiles, the library's choice from partsize 32), or 4/16/32 lanes
+        sharing a partition column by column (forward sweeps stay
         bit-identical; backward/symmetric agree to rounding).  Packed caches
         only; a matrix-view cache always uses 1.
         order: None (the library chooses), "reference" (every row summed in

@@ -80,17 +80,19 @@ typedef struct {
 /* Build options beyond the reference's arguments. */
 typedef struct {
     /* Threads that share one partition of a packed sweep.  0: chosen by the
-     * library; 1: one thread per partition, which sums every row in the
-     * reference's order (bit-identical results); 4, 8, 16 or 32: lanes of a
-     * warp share a partition (for large partsizes, where partitions are too
-     * few to keep the GPU busy one thread each).  With several lanes, forward
-     * sweeps stay bit-identical; backward and symmetric sweeps add a row's
-     * terms in descending column order and agree with the reference's
-     * ascending order to rounding.  Matrix-view caches always use 1. */
+     * library (8 for partsizes from 32 that are multiples of 8, else 1 while
+     * the partitions keep the GPU busy); 1: one thread per partition, which
+     * sums every row in the reference's order (bit-identical results); 8 with
+     * a partsize that is a multiple of 8: the blocked sweep (8 x 8 tiles);
+     * 4, 16 or 32: lanes of a warp share a partition, column by column.  With
+     * several lanes, forward sweeps stay bit-identical; backward and
+     * symmetric sweeps agree with the reference's ascending order to
+     * rounding.  Matrix-view caches always use 1. */
     int32_t threads_per_part;
     /* Summation order of each row's terms.  0: chosen by the library; 1: the
      * reference's ascending order everywhere (bit-identical to the reference;
-     * requires threads_per_part 0 or 1); 2: the library may reorder (partial
+     * requires threads_per_part 0 or 1, or 8 for a forward sweep with a
+     * partsize that is a multiple of 8); 2: the library may reorder (partial
      * sums combined at the end of the row), agreeing with the reference to
      * rounding: relative 1e-12 in FP64. */
     int32_t order;
