@@ -97,7 +97,7 @@ def test_same_result_alone_and_in_mix():
 
 def test_budget_admission():
     reqs = small_stream(4, seed=5, lo=20000, hi=30000)
-    eng = serving.BatchEngine(max_slots=8, hbm_budget=7_000_000)   # one ~20-30k-row system at a time
+    eng = serving.BatchEngine(max_slots=8, hbm_budget=8_500_000)   # one ~20-30k-row system at a time
     admitted = [eng.submit(A, b, i, 16) for i, (_, A, b) in enumerate(reqs)]
     assert admitted[0] and not all(admitted)
     done = set()
@@ -132,10 +132,10 @@ def test_serve_stream_reports_latency():
 def test_autotuner_picks_a_candidate():
     from hsb200.autotune import Autotuner
     A = W.variable_diffusion((24, 24, 24), np.random.default_rng(1))
-    tuner = Autotuner(trial_iters=10)
-    ps, cache = tuner.choose(A)
-    assert ps in (8, 16, 32) and cache == "packed"
-    assert tuner.choose(A) == (ps, cache)   # cached by matrix class
+    tuner = Autotuner(partsizes=(8, 16, 32), trial_iters=10)
+    ps, cache, tpp = tuner.choose(A)
+    assert ps in (8, 16, 32) and cache in ("packed", "view") and tpp in (0, 1)
+    assert tuner.choose(A) == (ps, cache, tpp)   # cached by matrix class
 
 
 def test_admission_during_launch_reuses_slot():
