@@ -143,7 +143,7 @@ __global__ void __launch_bounds__(kBlkWarps * 32) l1gs_blk_kernel(const Params p
     extern __shared__ __align__(128) unsigned char smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane / B, r = lane % B;
-    const int ps = p.ps, nb = ps / B;
+    const int ps = p.ps, psb = (ps + B - 1) / B * B, nb = psb / B;   // rows past ps: zero padding
     const int wpb = blockDim.x >> 5;
     const int32_t qstride = gridDim.x * wpb;
     const int32_t q0 = p.gbeg + blockIdx.x * wpb + warp;
@@ -186,7 +186,9 @@ __global__ void __launch_bounds__(kBlkWarps * 32) l1gs_blk_kernel(const Params p
     for (int32_t q = q0; q < p.gend; q += qstride) {
         const int64_t rowbase = (int64_t)q * G * ps;           // the group's rows are contiguous
         const int64_t prow = rowbase + (int64_t)g * ps + r;    // this lane's row of block 0
-        T* yg = ys + g * ps;                                   // this lane's partition
+        T* yg = ys + g * psb;                                  // this lane's partition (padded)
+        // row li of this lane's partition holds a real row: li < ps and inside the matrix
+        auto real = [&](int li, int64_t row) { return li < ps && row < p.n; };
         auto tile = [&](T acc, const T* tp, int J) -> T {
             const VT* ap = reinterpret_cast<const VT*>(tp) + lane;
             const VT* yp = reinterpret_cast<const VT*>(yg + J * B);
@@ -196,7 +198,7 @@ __global__ void __launch_bounds__(kBlkWarps * 32) l1gs_blk_kernel(const Params p
         };
         if (SWEEP != 1) {   // forward: row blocks 0 .. nb-1
             int64_t row = prow;
-            T xr = row < p.n ? (T)x[row] : T(0), dr = row < p.n ? D[row] : T(1);
+            T xr = real(r, row) ? (T)x[row] : T(0), dr = real(r, row) ? D[row] : T(1);
             for (int I = 0; I < nb; ++I) {
                 T acc = T(0);
                 for (int J = 0; J < I; ++J) acc = tile(acc, next_item(), J);
@@ -214,18 +216,20 @@ __global__ void __launch_bounds__(kBlkWarps * 32) l1gs_blk_kernel(const Params p
                     if (c < B - 1 && r > c) acc = add_rn(acc, mul_rn(aj[c], yc));
                 }
                 // rows past n (a short last partition, padding partitions) stay 0
-                yg[I * B + r] = row < p.n ? yown : T(0);
+                yg[I * B + r] = real(I * B + r, row) ? yown : T(0);
                 __syncwarp();
                 row += B;
                 if (I + 1 < nb) {   // the next block's x and D_Dl1
-                    xr = row < p.n ? (T)x[row] : T(0);
-                    dr = row < p.n ? D[row] : T(1);
+                    const bool v = real((I + 1) * B + r, row);
+                    xr = v ? (T)x[row] : T(0);
+                    dr = v ? D[row] : T(1);
                 }
             }
         }
         if (SWEEP != 0) {   // backward: row blocks nb-1 .. 0
             int64_t row = prow + (int64_t)(nb - 1) * B;
-            T xn = (SWEEP == 1 && row < p.n) ? (T)x[row] : T(0), dr = row < p.n ? D[row] : T(1);
+            const bool v0 = real((nb - 1) * B + r, row);
+            T xn = (SWEEP == 1 && v0) ? (T)x[row] : T(0), dr = v0 ? D[row] : T(1);
             for (int I = nb - 1; I >= 0; --I) {
                 T acc = T(0);
                 for (int J = I + 1; J < nb; ++J) acc = tile(acc, next_item(), J);
@@ -244,17 +248,20 @@ __global__ void __launch_bounds__(kBlkWarps * 32) l1gs_blk_kernel(const Params p
                     if (r == c) yown = v;
                     if (c > 0 && r < c) acc = add_rn(acc, mul_rn(au[c], yc));
                 }
-                yg[I * B + r] = row < p.n ? yown : T(0);
+                yg[I * B + r] = real(I * B + r, row) ? yown : T(0);
                 __syncwarp();
                 row -= B;
                 if (I > 0) {
-                    if (SWEEP == 1) xn = row < p.n ? (T)x[row] : T(0);
-                    dr = row < p.n ? D[row] : T(1);
+                    const bool v = real((I - 1) * B + r, row);
+                    if (SWEEP == 1) xn = v ? (T)x[row] : T(0);
+                    dr = v ? D[row] : T(1);
                 }
             }
         }
-        for (int t = lane; t < G * ps; t += 32) {
-            const int64_t rr = rowbase + t;
+        for (int t = lane; t < G * psb; t += 32) {
+            const int pp = t / psb, li = t - pp * psb;
+            if (li >= ps) continue;
+            const int64_t rr = rowbase + (int64_t)pp * ps + li;
             if (rr < p.n) y[rr] = (IO)ys[t];
         }
         __syncwarp();
@@ -308,7 +315,6 @@ int launch_sweep(int sweep, const Params& p, LaunchCache* lc, cudaStream_t st) {
 }  // namespace
 
 int launch_blk(int sdt, int io, int sweep, const Params& p, LaunchCache* lc, cudaStream_t st) {
-    if (p.ps % kBlkB != 0) return hs::set_error(HS_ERR_UNSUPPORTED, "blocked sweep needs a partsize that is a multiple of 8");
     if (sdt == HS_F64 && io == HS_F64) return launch_sweep<double, double>(sweep, p, lc, st);
     if (sdt == HS_F32 && io == HS_F32) return launch_sweep<float, float>(sweep, p, lc, st);
     if (sdt == HS_F32 && io == HS_F64) return launch_sweep<float, double>(sweep, p, lc, st);

@@ -37,8 +37,9 @@
 
 namespace hscoop {
 
-// Blocked variant ("blk", partsizes that are multiples of 8): B = 8 lanes per
-// partition, G = 4 partitions per warp, the partition cut into 8 x 8 tiles.
+// Blocked variant ("blk"): B = 8 lanes per partition, G = 4 partitions per
+// warp, the partition (padded to psb, a multiple of 8, with zero rows and
+// columns) cut into 8 x 8 tiles.
 // The sweep is left-looking by row block: row block I first adds the
 // off-diagonal tiles (I, J) of the blocks solved before it -- a dense
 // product with y of those blocks, lanes = rows, no dependence between
@@ -65,21 +66,29 @@ __host__ __device__ __forceinline__ int64_t colbase(int64_t ps, int64_t G, int64
 struct Layout {
     int32_t ps = 0, G = 0;
     int32_t blk = 0, V = 0;  // blocked variant; elements per 16 bytes
+    int32_t psb = 0;         // blocked: ps rounded up to a multiple of 8 (rows past ps are padding)
     int64_t Ld = 0;          // entries per direction per group: G*ps*(ps-1)/2
     int64_t Lg = 0;          // entries of one group stream (Ld, or 2*Ld for both directions)
     int64_t Lgp = 0;         // group stride in the buffer: Lg rounded up to 128 bytes
     int64_t upper_off = 0;   // first upper entry inside a group stream (0, or Ld)
 };
 
-inline bool blk_ok(int ps, int tpp) { return tpp == kBlkB && ps >= kBlkB && ps % kBlkB == 0; }
+inline bool blk_ok(int ps, int tpp) { return tpp == kBlkB && ps >= kBlkB; }
+inline int blk_psb(int ps) { return (ps + kBlkB - 1) / kBlkB * kBlkB; }
+// Stream bytes of the padded blocked layout over the reference's triangles.
+inline double blk_padding(int ps) {
+    const double b = blk_psb(ps);
+    return ps > 1 ? b * (b - 1) / ((double)ps * (ps - 1)) : 1e9;
+}
 
 inline Layout make_layout(int ps, int tpp, bool lower, bool upper, size_t es) {
     Layout L;
     L.ps = ps;
     L.G = 32 / tpp;
     L.blk = blk_ok(ps, tpp) ? 1 : 0;
+    L.psb = L.blk ? blk_psb(ps) : ps;
     L.V = (int32_t)(16 / es);
-    L.Ld = (int64_t)L.G * ps * (ps - 1) / 2;
+    L.Ld = (int64_t)L.G * L.psb * (L.psb - 1) / 2;
     L.Lg = (lower && upper) ? 2 * L.Ld : L.Ld;
     const int64_t q = 128 / (int64_t)es;
     L.Lgp = (L.Lg + q - 1) / q * q;
@@ -108,7 +117,7 @@ __host__ __device__ __forceinline__ int64_t upper_idx(const Layout& L, int64_t k
         constexpr int64_t B = kBlkB, TILE = 32 * B;
         const int64_t G = L.G, V = L.V, DG = G * B * (B - 1) / 2;
         const int64_t I = li / B, ii = li - I * B, J = lj / B, jj = lj - J * B;
-        const int64_t m = L.ps / B - 1 - I;                     // row blocks after I (consumed before it)
+        const int64_t m = L.psb / B - 1 - I;                    // row blocks after I (consumed before it)
         const int64_t rs = TILE * (m * (m - 1) / 2) + m * DG;
         const int64_t off = J > I ? rs + (J - I - 1) * TILE + (jj / V) * 32 * V + (g * B + ii) * V + jj % V
                                   : rs + m * TILE + G * (B * (B - 1) / 2 - jj * (jj + 1) / 2) + g * jj + ii;
@@ -134,7 +143,7 @@ inline Geometry make_geometry(const Layout& L, size_t es) {
     Geometry g;
     if (L.blk) {   // the blocked kernel: a ring of 4 item slots (32 x 8 entries each), then y of the group
         g.ys_off = (uint32_t)(4 * 32 * kBlkB * es);
-        g.warp_bytes = (uint32_t)((g.ys_off + (size_t)L.G * L.ps * es + 127) / 128 * 128);
+        g.warp_bytes = (uint32_t)((g.ys_off + (size_t)L.G * L.psb * es + 127) / 128 * 128);
         return g;
     }
     // Tuning overrides: HSB200_COOP_CHUNK = chunk bytes (1024, 2048 or 4096),

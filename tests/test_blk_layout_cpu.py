@@ -30,10 +30,11 @@ DG = G * B * (B - 1) // 2
 
 
 def make_layout(ps, lower, upper, es):
-    Ld = G * ps * (ps - 1) // 2
+    psb = -(-ps // B) * B   # padded to a multiple of 8 (zero rows and columns)
+    Ld = G * psb * (psb - 1) // 2
     Lg = 2 * Ld if (lower and upper) else Ld
     q = 128 // es
-    return dict(ps=ps, G=G, V=16 // es, Ld=Ld, Lg=Lg, Lgp=(Lg + q - 1) // q * q, upper_off=Ld if lower else 0)
+    return dict(ps=ps, psb=psb, G=G, V=16 // es, Ld=Ld, Lg=Lg, Lgp=(Lg + q - 1) // q * q, upper_off=Ld if lower else 0)
 
 
 def lower_idx(L, k, li, lj):
@@ -54,7 +55,7 @@ def upper_idx(L, k, li, lj):
     V = L["V"]
     I, ii = divmod(li, B)
     J, jj = divmod(lj, B)
-    m = L["ps"] // B - 1 - I
+    m = L["psb"] // B - 1 - I
     rs = TILE * (m * (m - 1) // 2) + m * DG
     if J > I:
         off = rs + (J - I - 1) * TILE + (jj // V) * 32 * V + (g * B + ii) * V + jj % V
@@ -91,20 +92,21 @@ def emulate(A, ps, sweep, D, x, dtype):
     n = A.shape[0]
     L, SC, ngroups = build_stream(A, ps, sweep, dtype)
     owner = {}   # stream position -> (partition, row, column): what the read must return
-    for k in range(ngroups * G):
-        for li in range(ps):
-            for lj in range(ps):
+    for k in range(ngroups * G):   # padded rows and columns too: they hold zeros
+        for li in range(L["psb"]):
+            for lj in range(L["psb"]):
                 if lj < li and sweep != "backward":
                     owner[lower_idx(L, k, li, lj)] = (k, li, lj)
                 elif lj > li and sweep != "forward":
                     owner[upper_idx(L, k, li, lj)] = (k, li, lj)
     V = L["V"]
-    nb = ps // B
+    psb = L["psb"]
+    nb = psb // B
     y = np.zeros(n, dtype=dtype)
     for q in range(ngroups):
         base = q * L["Lgp"]
         rowbase = q * G * ps
-        ys = np.zeros(G * ps, dtype=dtype)
+        ys = np.zeros(G * psb, dtype=dtype)
 
         def rd(pos, off, k, li, lj):
             assert 0 <= pos + off < L["Lg"], "read outside the group's stream"
@@ -119,10 +121,11 @@ def emulate(A, ps, sweep, D, x, dtype):
                     for c in range(V):
                         col = v * V + c
                         a = rd(pos, v * 32 * V + lane * V + c, q * G + g, I * B + r, J * B + col)
-                        acc[lane] = T(acc[lane] + T(a * ys[g * ps + J * B + col]))
+                        acc[lane] = T(acc[lane] + T(a * ys[g * psb + J * B + col]))
             return acc
 
         rows = [[rowbase + g * ps + I * B + r for g, r in (divmod(l, B) for l in range(32))] for I in range(nb)]
+        real = [[(I * B + l % B) < ps and rows[I][l] < n for l in range(32)] for I in range(nb)]
         with np.errstate(all="ignore"):
             if sweep != "backward":
                 I, J, pos = 0, 0, 0
@@ -134,7 +137,7 @@ def emulate(A, ps, sweep, D, x, dtype):
                     if is_tile:
                         acc = tile(acc, pos, I, J)
                     else:
-                        valid = [rr < n for rr in rows[I]]
+                        valid = real[I]
                         xr = [T(x[rr]) if v else T(0) for rr, v in zip(rows[I], valid)]
                         dr = [D[rr] if v else T(1) for rr, v in zip(rows[I], valid)]
                         yown = [T(0)] * 32
@@ -150,7 +153,7 @@ def emulate(A, ps, sweep, D, x, dtype):
                                     acc[lane] = T(acc[lane] + T(a * v[g * B + c]))
                         for lane in range(32):
                             g, r = divmod(lane, B)
-                            ys[g * ps + I * B + r] = yown[lane] if valid[lane] else T(0)
+                            ys[g * psb + I * B + r] = yown[lane] if valid[lane] else T(0)
                         acc = [T(0)] * 32
                     if In >= nb:
                         assert npos == L["Ld"]
@@ -167,10 +170,10 @@ def emulate(A, ps, sweep, D, x, dtype):
                     if is_tile:
                         acc = tile(acc, pos, I, J)
                     else:
-                        valid = [rr < n for rr in rows[I]]
+                        valid = real[I]
                         dr = [D[rr] if v else T(1) for rr, v in zip(rows[I], valid)]
                         if sweep == "symmetric":
-                            xr = [T(dr[l] * ys[(l // B) * ps + I * B + l % B]) for l in range(32)]
+                            xr = [T(dr[l] * ys[(l // B) * psb + I * B + l % B]) for l in range(32)]
                         else:
                             xr = [T(x[rr]) if v else T(0) for rr, v in zip(rows[I], valid)]
                         yown = [T(0)] * 32
@@ -186,19 +189,20 @@ def emulate(A, ps, sweep, D, x, dtype):
                                     acc[lane] = T(acc[lane] + T(a * v[g * B + c]))
                         for lane in range(32):
                             g, r = divmod(lane, B)
-                            ys[g * ps + I * B + r] = yown[lane] if valid[lane] else T(0)
+                            ys[g * psb + I * B + r] = yown[lane] if valid[lane] else T(0)
                         acc = [T(0)] * 32
                     if In < 0:
                         assert npos == L["Lg"]
                         break
                     I, J, pos = In, Jn, npos
-        for t in range(G * ps):
-            if rowbase + t < n:
-                y[rowbase + t] = ys[t]
+        for t in range(G * psb):
+            pp, li = divmod(t, psb)
+            if li < ps and rowbase + pp * ps + li < n:
+                y[rowbase + pp * ps + li] = ys[t]
     return y
 
 
-@pytest.mark.parametrize("ps", [8, 16, 32, 64])
+@pytest.mark.parametrize("ps", [8, 16, 31, 32, 64])
 def test_blk_layout_is_a_bijection(ps):
     """Every strict-triangle slot of every partition maps to a distinct entry
     of its group's stream, and the stream has no holes."""
@@ -207,8 +211,8 @@ def test_blk_layout_is_a_bijection(ps):
             L = make_layout(ps, lower, upper, es)
             seen = set()
             for k in range(2 * G):
-                for li in range(ps):
-                    for lj in range(ps):
+                for li in range(L["psb"]):
+                    for lj in range(L["psb"]):
                         if lj < li and lower:
                             p = lower_idx(L, k, li, lj)
                         elif lj > li and upper:
@@ -222,7 +226,8 @@ def test_blk_layout_is_a_bijection(ps):
             assert len(seen) == 2 * L["Lg"]
 
 
-@pytest.mark.parametrize("ps,n", [(8, 77), (16, 150), (24, 333), (32, 300), (40, 257), (64, 500), (128, 700)])
+@pytest.mark.parametrize("ps,n", [(8, 77), (16, 150), (24, 333), (32, 300), (40, 257), (64, 500), (128, 700),
+                                  (12, 200), (31, 500), (33, 400), (100, 1000)])
 @pytest.mark.parametrize("sweep", ["forward", "backward", "symmetric"])
 def test_blk_emulation_matches_oracle(ps, n, sweep):
     A = W.poisson2d_matrix(int(math.ceil(math.sqrt(n))), eps=0.3)

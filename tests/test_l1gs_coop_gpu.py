@@ -70,9 +70,11 @@ def random_matrix(n, density, seed):
 # (partsize, lanes per partition, n): ragged last partitions, groups with
 # padding partitions, every instantiated (lanes, rows-per-lane) pair -- exact
 # fits for 4 lanes, exact and other partsizes for 16 and 32; 8 lanes: the
-# blocked kernel at one to 64 row blocks per partition
+# blocked kernel at one to 64 row blocks per partition, partsizes that are
+# multiples of 8 and padded ones
 COOP_CASES = [(16, 4, 1000), (32, 4, 999), (64, 4, 3000), (32, 8, 2048), (64, 8, 3000), (128, 8, 4000),
               (8, 8, 777), (24, 8, 1001), (40, 8, 999), (56, 8, 3001), (256, 8, 5000), (512, 8, 4100),
+              (12, 8, 999), (31, 8, 2000), (33, 8, 1500), (100, 8, 2345), (300, 8, 2500),
               (5, 16, 301), (17, 16, 500), (33, 16, 1111), (64, 16, 4000), (100, 16, 2345), (256, 16, 4000),
               (2, 32, 50), (20, 32, 700), (128, 32, 3001), (256, 32, 4000), (300, 32, 2500), (512, 32, 3000)]
 
@@ -96,7 +98,7 @@ def test_coop_random_fp64(ps, tpp, n, sweep):
             np.testing.assert_array_equal(P.SUbuffer, ref.SU)
 
 
-@pytest.mark.parametrize("ps,tpp", [(16, 4), (33, 16), (64, 16), (130, 32), (32, 8), (72, 8), (256, 8)])
+@pytest.mark.parametrize("ps,tpp", [(16, 4), (33, 16), (64, 16), (130, 32), (32, 8), (72, 8), (256, 8), (31, 8), (100, 8)])
 @pytest.mark.parametrize("sweep", ["forward", "symmetric"])
 def test_coop_fp32_and_mixed(ps, tpp, sweep):
     A = W.poisson2d_matrix(40, eps=0.3)
@@ -167,7 +169,7 @@ def test_coop_rejects_unsupported():
     with pytest.raises(NotImplementedError, match="not provided"):
         b(A, 100, isSymA=True, threads_per_part=4)    # 25 rows per lane: not instantiated
     with pytest.raises(NotImplementedError, match="not provided"):
-        b(A, 36, isSymA=True, threads_per_part=8)     # 8 lanes: partsizes that are multiples of 8
+        b(A, 5, isSymA=True, threads_per_part=8)      # 8 lanes: partsizes from 8 (padded to multiples of 8)
     with pytest.raises(NotImplementedError, match="not provided"):
         b(A, 36, isSymA=True, threads_per_part=4)     # 4 lanes: exact fits only
     with pytest.raises(ValueError, match="threads per partition"):
@@ -238,7 +240,7 @@ def test_reference_order_is_default_and_bitwise():
             A, 64, isSymA=True, order="reference", threads_per_part=8)
 
 
-@pytest.mark.parametrize("ps", [32, 64, 256])
+@pytest.mark.parametrize("ps", [31, 32, 64, 100, 256])
 def test_blocked_forward_keeps_reference_order(ps):
     """The blocked kernel's forward sweep adds every row's terms in the
     reference's order: with order="reference" the library runs it (8 lanes
