@@ -1804,18 +1804,18 @@ int l1gs_view_of(const hs_l1gs* P, L1gsView* v) {
 // ---------------------------------------------------------------------------
 namespace {
 // Threads per partition when the caller leaves it open (0).  Partsizes from
-// 32 take the blocked kernel (8 lanes per partition, off-diagonal 8 x 8 tiles
+// 30 take the blocked kernel (8 lanes per partition, off-diagonal 8 x 8 tiles
 // as dense products) when padding the partition to a multiple of 8 adds at
 // most 15 % to its triangle (every partsize from 32 but a few just above a
 // multiple of 8 below 100, e.g. 33-37, 41-44).  Otherwise one thread per
 // partition (the reference's order) while the partitions give every SM about
 // six warps of 32 partitions; below that (large partsizes, small matrices)
 // the column-block kernel's lanes share a partition, eight rows per lane
-// where the partsize allows it.  Partsizes below 32 always keep one thread per
-// partition.
+// where the partsize allows it.  Other partsizes below 32 keep one thread per
+// partition (y and D_Dl1 of the partition in registers).
 int auto_threads_per_part(int32_t ps, int64_t nparts) {
+    if (ps >= 30 && hscoop::blk_padding(ps) <= 1.15) return hscoop::kBlkB;   // 30 and 31 pad to 32
     if (ps < 32) return 1;
-    if (hscoop::blk_padding(ps) <= 1.15) return hscoop::kBlkB;
     if (nparts / 32 >= 6 * (int64_t)hs::num_sms()) return 1;
     int tpp = 4;
     while (tpp < 32 && tpp * 8 < ps) tpp *= 2;
