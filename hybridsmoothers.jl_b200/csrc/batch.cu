@@ -709,6 +709,20 @@ int hs_batch_create(const hs_batch_config* cfg, void* stream, hs_batch** out) {
         return hs::cuda_error(e, "hs_batch_create");
     }
     cudaMemset(B->d_scal, 0, sizeof(Scalars) * cfg->max_slots);
+    // Reserve the budget (at most 90 % of the free memory) in the stream-ordered
+    // pool the slots allocate from, so admissions take memory the pool holds
+    // instead of mapping new memory while systems are being solved.
+    hs::keep_pool_reserve();
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+        const size_t want = (size_t)std::min<int64_t>(cfg->hbm_budget, (int64_t)(0.9 * (double)free_b));
+        void* p = nullptr;
+        if (want > 0 && cudaMallocAsync(&p, want, B->setup) == cudaSuccess) {
+            cudaFreeAsync(p, B->setup);
+            cudaStreamSynchronize(B->setup);
+        }
+        cudaGetLastError();   // a reserve that could not be made is not an error
+    }
     B->err = hs::device_error_word();
     *out = B;
     return HS_OK;

@@ -15,6 +15,8 @@ int cheb_apply(hs_cheb* S, const void* r, void* z, int io, cudaStream_t st);
 // input, a non-null `diag` (n entries) receives DiagonalIndices and *bad
 // (initialised by the caller to n) the smallest column whose diagonal is
 // missing or zero.
+// The device's default stream-ordered pool keeps what it has reserved.
+void keep_pool_reserve();
 int csr_from_host(const hs_sparse* A, int32_t dtype, int32_t* rp, int32_t* ci, void* v, cudaStream_t st,
                   int32_t* diag = nullptr, int32_t* bad = nullptr);
 

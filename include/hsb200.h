@@ -298,6 +298,8 @@ typedef struct {
     int64_t hbm_used, hbm_budget, iterations_run;
 } hs_batch_info;
 
+/* The engine reserves its HBM budget (at most 90 % of the free device memory)
+ * in the device's stream-ordered pool at creation; slots are carved from it. */
 int hs_batch_create(const hs_batch_config* cfg, void* stream, hs_batch** out);
 /* Admit one system (host matrix, host b); x_host receives the solution when
  * it converges.  partsize 0 = the batch default.  A must be symmetric (the
