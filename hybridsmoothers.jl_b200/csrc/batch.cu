@@ -65,12 +65,40 @@ struct SlotDev {
 // pointer it needs, so a CTA starts after one load of its entry.
 struct BlockMap {
     int32_t n, row0;
-    const int32_t* rp;
-    const int32_t* ci;
-    const double* v;
+    const int64_t* soff;   // the slot's 32-row slices: first entry of each (slice_fill_kernel)
+    const int32_t* scol;
+    const double* sval;
     double *x, *r, *z, *p, *q;
     const Scalars* s;
 };
+
+// ---- the slot's matrix in 32-row slices -------------------------------------
+// The batched SpMV reads each slot's matrix as 32-row slices (an own copy made
+// at admission): a slice holds w entries per row, w its longest row, stored
+// column by column ([k][row]), so lane r reads entry k of its row at
+// off + 32 k + r -- coalesced, with no row pointers and no window in shared
+// memory.  A row's entries keep their storage order and its padding entries
+// (value 0, column = the row) follow them, so the sum is the CSR sequence
+// followed by +-0 terms: the same value bit for bit (an accumulator that
+// starts at +0 is never -0).
+__global__ void slice_fill_kernel(int32_t n, int64_t nslices, const int32_t* __restrict__ rp,
+                                  const int32_t* __restrict__ ci, const double* __restrict__ v,
+                                  const int64_t* __restrict__ off, int32_t* __restrict__ scol,
+                                  double* __restrict__ sval) {
+    const int lane = threadIdx.x & 31;
+    for (int64_t sl = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; sl < nslices;
+         sl += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        const int64_t o = off[sl];
+        const int32_t w = (int32_t)((off[sl + 1] - o) / 32);
+        const int64_t row = sl * 32 + lane;
+        const int32_t q0 = row < n ? rp[row] : 0, len = row < n ? rp[row + 1] - q0 : 0;
+        for (int32_t k = 0; k < w; ++k) {
+            const bool real = k < len;
+            scol[o + 32 * (int64_t)k + lane] = real ? ci[q0 + k] : (row < n ? (int32_t)row : 0);
+            sval[o + 32 * (int64_t)k + lane] = real ? v[q0 + k] : 0.0;
+        }
+    }
+}
 
 // One work item of the batched L1GS apply: 32 partitions (a group) of a slot,
 // with its stream bases, D_Dl1 and vectors already offset to the group.
@@ -90,25 +118,45 @@ struct PrecItem {
 // separately rounded updates, storage-order SpMV rows.  The streaming kernels
 // load kSub elements per thread before using any.
 __global__ void __launch_bounds__(kT, 4) seg_spmv_dot(const BlockMap* __restrict__ map, double* __restrict__ partials) {
-    __shared__ double wbuf[kT / 32][hsdev::kWarpCap];
+    constexpr int KU = 8;   // entries of a row loaded before any is used
     const BlockMap m = map[blockIdx.x];
     DD part{0.0, 0.0};
-    const int warp = threadIdx.x >> 5;
-    // The row pointers of all the warp's chunks, requested before the slot's
-    // flag is known (one round trip instead of one per chunk).
-    hsdev::RowPtrs rpp[kRPC / kT];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // The slice bounds of all the warp's slices, requested before the slot's
+    // flag is known.
+    constexpr int NS = kRPC / kT;
+    int64_t o0[NS], o1[NS];
+    const int64_t nsl = ((int64_t)m.n + 31) / 32;
 #pragma unroll
-    for (int k = 0; k < kRPC / kT; ++k)
-        rpp[k] = hsdev::load_rowptrs(m.n, m.rp, (int64_t)m.row0 + (k * (kT / 32) + warp) * 32);
+    for (int k = 0; k < NS; ++k) {
+        const int64_t sl = ((int64_t)m.row0 >> 5) + k * (kT / 32) + warp;
+        o0[k] = sl < nsl ? m.soff[sl] : 0;
+        o1[k] = sl < nsl ? m.soff[sl + 1] : 0;
+    }
     if (!m.s->done) {   // uniform over the CTA (one slot per CTA)
-        auto fp = [&](int32_t j) { return __ldg(m.p + j); };
 #pragma unroll
-        for (int k = 0; k < kRPC / kT; ++k) {   // the warp's 32-row chunks of this CTA
+        for (int k = 0; k < NS; ++k) {   // the warp's 32-row slices of this CTA
             const int64_t row0 = (int64_t)m.row0 + (k * (kT / 32) + warp) * 32;
             if (row0 >= m.n) break;   // uniform over the warp
-            const double acc = hsdev::csr_warp_fold_rp(wbuf[warp], m.n, rpp[k], m.ci, m.v, row0, 0.0, fp,
-                                                       hsdev::AddOp<double>());
-            const int64_t r = row0 + (threadIdx.x & 31);
+            const int32_t w = (int32_t)((o1[k] - o0[k]) / 32);
+            const int32_t* __restrict__ cp = m.scol + o0[k] + lane;
+            const double* __restrict__ vp = m.sval + o0[k] + lane;
+            double acc = 0.0;
+            for (int32_t j = 0; j < w; j += KU) {
+                int32_t c[KU];
+                double a[KU], b[KU];
+#pragma unroll
+                for (int u = 0; u < KU; ++u) {
+                    c[u] = j + u < w ? __ldg(cp + 32 * (j + u)) : 0;
+                    a[u] = j + u < w ? __ldg(vp + 32 * (j + u)) : 0.0;
+                }
+#pragma unroll
+                for (int u = 0; u < KU; ++u) b[u] = j + u < w ? __ldg(m.p + c[u]) : 0.0;
+#pragma unroll
+                for (int u = 0; u < KU; ++u)
+                    if (j + u < w) acc = __dadd_rn(acc, __dmul_rn(a[u], b[u]));
+            }
+            const int64_t r = row0 + lane;
             if (r < m.n) {
                 m.q[r] = acc;
                 hsdev::dd_add_prod(part, m.p[r], acc);
@@ -469,6 +517,9 @@ struct hs_batch_slot {
     int32_t n = 0, ps = 0;
     double* vec = nullptr;   // x r z p q b (6n doubles)
     float* tiles = nullptr;  // per group: the smoother's tiles, contiguous (batch_tiles_kernel)
+    int64_t* soff = nullptr; // the matrix in 32-row slices (slice_fill_kernel)
+    int32_t* scol = nullptr;
+    double* sval = nullptr;
     double* x_out = nullptr; // host destination
     int64_t bytes = 0;
     int32_t blk0 = 0, nblk = 0;
@@ -510,13 +561,49 @@ struct hs_batch_s {
 
 namespace {
 
+// The slot's matrix in 32-row slices: widths and offsets from the host row
+// pointers, entries gathered from the slot's device CSR on the admission
+// stream (stream-ordered allocations, no host wait).
+int build_slices(hs_batch_slot& sl, int32_t n, const int32_t* rp_host, cudaStream_t st) {
+    const int32_t* rp = nullptr;
+    const int32_t* ci = nullptr;
+    const void* mv = nullptr;
+    int mdt = 0;
+    hs::matrix_arrays(sl.A, &rp, &ci, &mv, &mdt);
+    const int64_t nsl = ((int64_t)n + 31) / 32;
+    std::vector<int64_t> off((size_t)nsl + 1);
+    int64_t total = 0;
+    for (int64_t k = 0; k < nsl; ++k) {
+        off[(size_t)k] = total;
+        int32_t w = 0;
+        const int64_t r1 = std::min<int64_t>((k + 1) * 32, n);
+        for (int64_t r = k * 32; r < r1; ++r) w = std::max(w, rp_host[r + 1] - rp_host[r]);
+        total += 32 * (int64_t)w;
+    }
+    off[(size_t)nsl] = total;
+    cudaError_t e;
+    if ((e = cudaMallocAsync(&sl.soff, sizeof(int64_t) * (size_t)(nsl + 1), st)) ||
+        (e = cudaMallocAsync(&sl.scol, sizeof(int32_t) * (size_t)std::max<int64_t>(total, 32), st)) ||
+        (e = cudaMallocAsync(&sl.sval, sizeof(double) * (size_t)std::max<int64_t>(total, 32), st)))
+        return hs::cuda_error(e, "cudaMallocAsync (slices)");
+    // (pageable source: the call returns once the bytes are staged)
+    if ((e = cudaMemcpyAsync(sl.soff, off.data(), sizeof(int64_t) * off.size(), cudaMemcpyHostToDevice, st)))
+        return hs::cuda_error(e, "slice offsets");
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((32 * nsl + kT - 1) / kT, 8192));
+    slice_fill_kernel<<<grid, kT, 0, st>>>(n, nsl, rp, ci, static_cast<const double*>(mv), sl.soff, sl.scol, sl.sval);
+    hs::count_launch();
+    if ((e = cudaGetLastError()) != cudaSuccess) return hs::cuda_error(e, "slice_fill_kernel");
+    return HS_OK;
+}
+
 int64_t slot_estimate(int32_t n, int64_t nnz, int ps) {
     const int64_t nparts = (n + ps - 1) / ps;
     const int64_t npad = (nparts + 31) / 32 * 32;
     const int64_t tlen = (int64_t)ps * (ps - 1) / 2;
     const int64_t ntile = (tlen + kBatchE - 1) / kBatchE;
     const int64_t prec = 4 * (2 * tlen * npad + (int64_t)ps * npad + n) + 4 * 2 * ntile * kBatchE * npad;
-    const int64_t mat = 4 * (n + 1) + 12 * nnz;
+    const int64_t nsl = ((int64_t)n + 31) / 32;
+    const int64_t mat = 4 * (n + 1) + 12 * nnz + 8 * (nsl + 1) + 12 * (nnz + 2 * (int64_t)n);   // CSR + slices
     return prec + mat + 6 * 8 * (int64_t)n + 64 * 1024;
 }
 
@@ -587,11 +674,10 @@ int rebuild(hs_batch* B) {
         active.push_back((int32_t)s);
         sl.blk0 = (int32_t)map.size();
         sl.nblk = (sl.n + kRPC - 1) / kRPC;
-        const void* mv = nullptr;
-        int mdt = 0;
         BlockMap m{};
-        hs::matrix_arrays(sl.A, &m.rp, &m.ci, &mv, &mdt);
-        m.v = static_cast<const double*>(mv);
+        m.soff = sl.soff;
+        m.scol = sl.scol;
+        m.sval = sl.sval;
         m.n = sl.n;
         m.x = sl.vec;
         m.r = sl.vec + sl.n;
@@ -665,6 +751,9 @@ void free_slot(hs_batch* B, hs_batch_slot& sl) {
     if (sl.A) hs::matrix_destroy_async(sl.A, B->solve);
     if (sl.vec) cudaFreeAsync(sl.vec, B->solve);
     if (sl.tiles) cudaFreeAsync(sl.tiles, B->solve);
+    if (sl.soff) cudaFreeAsync(sl.soff, B->solve);
+    if (sl.scol) cudaFreeAsync(sl.scol, B->solve);
+    if (sl.sval) cudaFreeAsync(sl.sval, B->solve);
     B->used -= sl.bytes;
     sl = hs_batch_slot();
 }
@@ -767,6 +856,7 @@ int hs_batch_submit(hs_batch* B, const hs_sparse* A, const double* b_host, doubl
         cudaError_t e = cudaMallocAsync(&sl.vec, sizeof(double) * 6 * (size_t)A->n, B->setup);
         if (e) rc = hs::cuda_error(e, "cudaMallocAsync (slot vectors)");
     }
+    if (!rc) rc = build_slices(sl, A->n, A->ptr, B->setup);
     if (!rc) {   // the smoother's tiles, regrouped for the batched kernel
         hs::L1gsView lv;
         hs::l1gs_view_of(sl.P, &lv);
@@ -790,6 +880,9 @@ int hs_batch_submit(hs_batch* B, const hs_sparse* A, const double* b_host, doubl
         cudaStreamSynchronize(B->setup);
         if (sl.vec) cudaFreeAsync(sl.vec, B->setup);
         if (sl.tiles) cudaFreeAsync(sl.tiles, B->setup);
+        if (sl.soff) cudaFreeAsync(sl.soff, B->setup);
+        if (sl.scol) cudaFreeAsync(sl.scol, B->setup);
+        if (sl.sval) cudaFreeAsync(sl.sval, B->setup);
         if (sl.P) hs::l1gs_destroy_async(sl.P, B->setup);
         if (sl.A) hs::matrix_destroy_async(sl.A, B->setup);
         return code;

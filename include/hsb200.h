@@ -80,10 +80,11 @@ typedef struct {
 /* Build options beyond the reference's arguments. */
 typedef struct {
     /* Threads that share one partition of a packed sweep.  0: chosen by the
-     * library (8 for partsizes from 32 that are multiples of 8, else 1 while
-     * the partitions keep the GPU busy); 1: one thread per partition, which
-     * sums every row in the reference's order (bit-identical results); 8 with
-     * a partsize that is a multiple of 8: the blocked sweep (8 x 8 tiles);
+     * library (8 from partsize 30 where padding the partition to a multiple
+     * of 8 adds at most 15 % to its triangle, else 1 while the partitions keep
+     * the GPU busy); 1: one thread per partition, which sums every row in the
+     * reference's order (bit-identical results); 8 with a partsize from 8: the
+     * blocked sweep (8 x 8 tiles, the partition padded to a multiple of 8);
      * 4, 16 or 32: lanes of a warp share a partition, column by column.  With
      * several lanes, forward sweeps stay bit-identical; backward and
      * symmetric sweeps agree with the reference's ascending order to
@@ -91,8 +92,8 @@ typedef struct {
     int32_t threads_per_part;
     /* Summation order of each row's terms.  0: chosen by the library; 1: the
      * reference's ascending order everywhere (bit-identical to the reference;
-     * requires threads_per_part 0 or 1, or 8 for a forward sweep with a
-     * partsize that is a multiple of 8); 2: the library may reorder (partial
+     * requires threads_per_part 0 or 1, or 8 for a forward sweep); 2: the
+     * library may reorder (partial
      * sums combined at the end of the row), agreeing with the reference to
      * rounding: relative 1e-12 in FP64. */
     int32_t order;
