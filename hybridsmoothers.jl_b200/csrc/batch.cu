@@ -603,7 +603,7 @@ int64_t slot_estimate(int32_t n, int64_t nnz, int ps) {
     const int64_t ntile = (tlen + kBatchE - 1) / kBatchE;
     const int64_t prec = 4 * (2 * tlen * npad + (int64_t)ps * npad + n) + 4 * 2 * ntile * kBatchE * npad;
     const int64_t nsl = ((int64_t)n + 31) / 32;
-    const int64_t mat = 4 * (n + 1) + 12 * nnz + 8 * (nsl + 1) + 12 * (nnz + 2 * (int64_t)n);   // CSR + slices
+    const int64_t mat = 4 * (n + 1) + 12 * nnz + 8 * (nsl + 1) + 12 * (nnz + (int64_t)n);   // CSR + slices
     return prec + mat + 6 * 8 * (int64_t)n + 64 * 1024;
 }
 

@@ -97,7 +97,16 @@ def test_same_result_alone_and_in_mix():
 
 def test_budget_admission():
     reqs = small_stream(4, seed=5, lo=20000, hi=30000)
-    eng = serving.BatchEngine(max_slots=8, hbm_budget=8_500_000)   # one ~20-30k-row system at a time
+    # each system's own budget figure, from an engine with room for it
+    need = []
+    for _, A, b in reqs:
+        probe = serving.BatchEngine(max_slots=1, hbm_budget=1 << 30)
+        assert probe.submit(A, b, 0, 16)
+        need.append(probe.info().hbm_used)
+        probe.close()
+    budget = int(1.2 * max(need))
+    assert budget < 2 * min(need)   # room for one of these systems at a time
+    eng = serving.BatchEngine(max_slots=8, hbm_budget=budget)
     admitted = [eng.submit(A, b, i, 16) for i, (_, A, b) in enumerate(reqs)]
     assert admitted[0] and not all(admitted)
     done = set()
