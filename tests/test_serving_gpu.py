@@ -104,8 +104,9 @@ def test_budget_admission():
         assert probe.submit(A, b, 0, 16)
         need.append(probe.info().hbm_used)
         probe.close()
-    budget = int(1.2 * max(need))
-    assert budget < 2 * min(need)   # room for one of these systems at a time
+    budget = max(need)
+    two = sorted(need)[:2]
+    assert budget < two[0] + two[1]   # room for one of these systems at a time
     eng = serving.BatchEngine(max_slots=8, hbm_budget=budget)
     admitted = [eng.submit(A, b, i, 16) for i, (_, A, b) in enumerate(reqs)]
     assert admitted[0] and not all(admitted)
