@@ -65,40 +65,12 @@ struct SlotDev {
 // pointer it needs, so a CTA starts after one load of its entry.
 struct BlockMap {
     int32_t n, row0;
-    const int64_t* soff;   // the slot's 32-row slices: first entry of each (slice_fill_kernel)
+    const int64_t* soff;   // the slot's matrix in 32-row slices (spmv.cuh): first entry of each
     const int32_t* scol;
     const double* sval;
     double *x, *r, *z, *p, *q;
     const Scalars* s;
 };
-
-// ---- the slot's matrix in 32-row slices -------------------------------------
-// The batched SpMV reads each slot's matrix as 32-row slices (an own copy made
-// at admission): a slice holds w entries per row, w its longest row, stored
-// column by column ([k][row]), so lane r reads entry k of its row at
-// off + 32 k + r -- coalesced, with no row pointers and no window in shared
-// memory.  A row's entries keep their storage order and its padding entries
-// (value 0, column = the row) follow them, so the sum is the CSR sequence
-// followed by +-0 terms: the same value bit for bit (an accumulator that
-// starts at +0 is never -0).
-__global__ void slice_fill_kernel(int32_t n, int64_t nslices, const int32_t* __restrict__ rp,
-                                  const int32_t* __restrict__ ci, const double* __restrict__ v,
-                                  const int64_t* __restrict__ off, int32_t* __restrict__ scol,
-                                  double* __restrict__ sval) {
-    const int lane = threadIdx.x & 31;
-    for (int64_t sl = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; sl < nslices;
-         sl += ((int64_t)gridDim.x * blockDim.x) >> 5) {
-        const int64_t o = off[sl];
-        const int32_t w = (int32_t)((off[sl + 1] - o) / 32);
-        const int64_t row = sl * 32 + lane;
-        const int32_t q0 = row < n ? rp[row] : 0, len = row < n ? rp[row + 1] - q0 : 0;
-        for (int32_t k = 0; k < w; ++k) {
-            const bool real = k < len;
-            scol[o + 32 * (int64_t)k + lane] = real ? ci[q0 + k] : (row < n ? (int32_t)row : 0);
-            sval[o + 32 * (int64_t)k + lane] = real ? v[q0 + k] : 0.0;
-        }
-    }
-}
 
 // One work item of the batched L1GS apply: 32 partitions (a group) of a slot,
 // with its stream bases, D_Dl1 and vectors already offset to the group.
@@ -118,7 +90,6 @@ struct PrecItem {
 // separately rounded updates, storage-order SpMV rows.  The streaming kernels
 // load kSub elements per thread before using any.
 __global__ void __launch_bounds__(kT, 4) seg_spmv_dot(const BlockMap* __restrict__ map, double* __restrict__ partials) {
-    constexpr int KU = 8;   // entries of a row loaded before any is used
     const BlockMap m = map[blockIdx.x];
     DD part{0.0, 0.0};
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -134,28 +105,12 @@ __global__ void __launch_bounds__(kT, 4) seg_spmv_dot(const BlockMap* __restrict
         o1[k] = sl < nsl ? m.soff[sl + 1] : 0;
     }
     if (!m.s->done) {   // uniform over the CTA (one slot per CTA)
+        auto fp = [&](int32_t j) { return __ldg(m.p + j); };
 #pragma unroll
         for (int k = 0; k < NS; ++k) {   // the warp's 32-row slices of this CTA
             const int64_t row0 = (int64_t)m.row0 + (k * (kT / 32) + warp) * 32;
             if (row0 >= m.n) break;   // uniform over the warp
-            const int32_t w = (int32_t)((o1[k] - o0[k]) / 32);
-            const int32_t* __restrict__ cp = m.scol + o0[k] + lane;
-            const double* __restrict__ vp = m.sval + o0[k] + lane;
-            double acc = 0.0;
-            for (int32_t j = 0; j < w; j += KU) {
-                int32_t c[KU];
-                double a[KU], b[KU];
-#pragma unroll
-                for (int u = 0; u < KU; ++u) {
-                    c[u] = j + u < w ? __ldg(cp + 32 * (j + u)) : 0;
-                    a[u] = j + u < w ? __ldg(vp + 32 * (j + u)) : 0.0;
-                }
-#pragma unroll
-                for (int u = 0; u < KU; ++u) b[u] = j + u < w ? __ldg(m.p + c[u]) : 0.0;
-#pragma unroll
-                for (int u = 0; u < KU; ++u)
-                    if (j + u < w) acc = __dadd_rn(acc, __dmul_rn(a[u], b[u]));
-            }
+            const double acc = hsdev::slice_row_sum(o0[k], o1[k], m.scol, m.sval, fp);
             const int64_t r = row0 + lane;
             if (r < m.n) {
                 m.q[r] = acc;
@@ -590,7 +545,7 @@ int build_slices(hs_batch_slot& sl, int32_t n, const int32_t* rp_host, cudaStrea
     if ((e = cudaMemcpyAsync(sl.soff, off.data(), sizeof(int64_t) * off.size(), cudaMemcpyHostToDevice, st)))
         return hs::cuda_error(e, "slice offsets");
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((32 * nsl + kT - 1) / kT, 8192));
-    slice_fill_kernel<<<grid, kT, 0, st>>>(n, nsl, rp, ci, static_cast<const double*>(mv), sl.soff, sl.scol, sl.sval);
+    hsdev::slice_fill_kernel<<<grid, kT, 0, st>>>(n, nsl, rp, ci, static_cast<const double*>(mv), sl.soff, sl.scol, sl.sval);
     hs::count_launch();
     if ((e = cudaGetLastError()) != cudaSuccess) return hs::cuda_error(e, "slice_fill_kernel");
     return HS_OK;

@@ -24,6 +24,8 @@
 #include <cstring>
 #include <vector>
 
+#include <cub/device/device_scan.cuh>
+
 #include "internal.cuh"
 #include "reduce.cuh"
 #include "spmv.cuh"
@@ -41,6 +43,10 @@ struct hs_matrix_s {
     int32_t* rp = nullptr;
     int32_t* ci = nullptr;
     void* v = nullptr;
+    // FP64 copy in 32-row slices (spmv.cuh), built at the first PCG solve
+    int64_t* soff = nullptr;
+    int32_t* scol = nullptr;
+    double* sval = nullptr;
     int64_t bytes = 0;
     bool stream_ordered = false;   // buffers from cudaMallocAsync
     cudaStream_t alloc_stream = nullptr;
@@ -426,6 +432,72 @@ int matrix_spmv(const hs_matrix* M, const void* x, void* y, double alpha, double
     return M->dtype == HS_F64 ? hsm::spmv_t<double>(M, x, y, alpha, beta, st)
                               : hsm::spmv_t<float>(M, x, y, alpha, beta, st);
 }
+// The FP64 matrix in 32-row slices, built once (on stream st; one wait for
+// the entry count) and kept with the matrix.
+int matrix_slices(hs_matrix* M, cudaStream_t st, const int64_t** soff, const int32_t** scol, const double** sval) {
+    if (M->dtype != HS_F64) return hs::set_error(HS_ERR_UNSUPPORTED, "sliced copy of an FP32 matrix");
+    if (!M->soff) {
+        const int32_t n = M->n;
+        const int64_t nsl = ((int64_t)n + 31) / 32;
+        const bool so = M->stream_ordered;
+        auto alloc = [&](void** p, size_t bytes) -> cudaError_t {
+            return so ? cudaMallocAsync(p, bytes ? bytes : 16, st) : cudaMalloc(p, bytes ? bytes : 16);
+        };
+        auto release = [&](void* p) {
+            if (!p) return;
+            if (so)
+                cudaFreeAsync(p, st);
+            else
+                cudaFree(p);
+        };
+        int64_t* ent = nullptr;
+        int64_t* off = nullptr;
+        void* tmp = nullptr;
+        size_t tbytes = 0;
+        int64_t total = 0;
+        cudaError_t e;
+        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((32 * (nsl + 1) + 255) / 256, 8192));
+        if ((e = alloc((void**)&ent, sizeof(int64_t) * (size_t)(nsl + 1))) ||
+            (e = alloc((void**)&off, sizeof(int64_t) * (size_t)(nsl + 1))))
+            goto fail;
+        hsdev::slice_width_kernel<<<grid, 256, 0, st>>>(n, nsl, M->rp, ent);
+        hs::count_launch();
+        if ((e = cub::DeviceScan::ExclusiveSum(nullptr, tbytes, ent, off, nsl + 1, st)) ||
+            (e = alloc(&tmp, tbytes)) || (e = cub::DeviceScan::ExclusiveSum(tmp, tbytes, ent, off, nsl + 1, st)) ||
+            (e = cudaMemcpyAsync(&total, off + nsl, sizeof(int64_t), cudaMemcpyDeviceToHost, st)) ||
+            (e = cudaStreamSynchronize(st)))
+            goto fail;
+        release(tmp);
+        tmp = nullptr;
+        release(ent);
+        ent = nullptr;
+        if ((e = alloc((void**)&M->scol, sizeof(int32_t) * (size_t)total)) ||
+            (e = alloc((void**)&M->sval, sizeof(double) * (size_t)total)))
+            goto fail;
+        hsdev::slice_fill_kernel<<<grid, 256, 0, st>>>(n, nsl, M->rp, M->ci, static_cast<const double*>(M->v), off,
+                                                       M->scol, M->sval);
+        hs::count_launch();
+        if ((e = cudaGetLastError()) != cudaSuccess) goto fail;
+        M->soff = off;
+        M->bytes += (int64_t)(8 * (nsl + 1) + 12 * total);
+        goto done;
+    fail:
+        release(tmp);
+        release(ent);
+        release(off);
+        release(M->scol);
+        release(M->sval);
+        M->scol = nullptr;
+        M->sval = nullptr;
+        return hs::cuda_error(e, "sliced matrix copy");
+    done:;
+    }
+    *soff = M->soff;
+    *scol = M->scol;
+    *sval = M->sval;
+    return HS_OK;
+}
+
 int matrix_n(const hs_matrix* M) { return M->n; }
 int64_t matrix_nnz(const hs_matrix* M) { return M->nnz; }
 void matrix_arrays(const hs_matrix* M, const int32_t** rp, const int32_t** ci, const void** v, int* dtype) {
@@ -452,7 +524,7 @@ namespace hsm {
 
 void destroy_matrix(hs_matrix* M, cudaStream_t free_stream = nullptr) {
     if (!M) return;
-    void* ptrs[] = {M->rp, M->ci, M->v};
+    void* ptrs[] = {M->rp, M->ci, M->v, M->soff, M->scol, M->sval};
     for (void* q : ptrs) {
         if (!q) continue;
         if (M->stream_ordered)
@@ -926,3 +998,38 @@ extern "C" int hs_cheb_smooth_noalloc(int32_t n, int64_t nnz, const int32_t* rp,
     for (int i = 0; i < 4; ++i) S.w[i] = nullptr;
     return rc;
 }
+
+namespace hsdev {
+
+__global__ void slice_width_kernel(int32_t n, int64_t nslices, const int32_t* __restrict__ rp,
+                                   int64_t* __restrict__ ent) {
+    const int lane = threadIdx.x & 31;
+    for (int64_t sl = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; sl <= nslices;
+         sl += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        const int64_t row = sl * 32 + lane;
+        const int32_t len = (sl < nslices && row < n) ? rp[row + 1] - rp[row] : 0;
+        const int32_t w = (int32_t)__reduce_max_sync(0xffffffffu, (unsigned)len);
+        if (lane == 0) ent[sl] = 32 * (int64_t)w;
+    }
+}
+
+__global__ void slice_fill_kernel(int32_t n, int64_t nslices, const int32_t* __restrict__ rp,
+                                  const int32_t* __restrict__ ci, const double* __restrict__ v,
+                                  const int64_t* __restrict__ soff, int32_t* __restrict__ scol,
+                                  double* __restrict__ sval) {
+    const int lane = threadIdx.x & 31;
+    for (int64_t sl = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; sl < nslices;
+         sl += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        const int64_t o = soff[sl];
+        const int32_t w = (int32_t)((soff[sl + 1] - o) / 32);
+        const int64_t row = sl * 32 + lane;
+        const int32_t q0 = row < n ? rp[row] : 0, len = row < n ? rp[row + 1] - q0 : 0;
+        for (int32_t k = 0; k < w; ++k) {
+            const bool real = k < len;
+            scol[o + 32 * (int64_t)k + lane] = real ? ci[q0 + k] : (row < n ? (int32_t)row : 0);
+            sval[o + 32 * (int64_t)k + lane] = real ? v[q0 + k] : 0.0;
+        }
+    }
+}
+
+}  // namespace hsdev

@@ -150,6 +150,39 @@ __global__ void kjl_check(const double* __restrict__ partials, int nb, PcgScalar
 
 // q = A p (storage-order rows, bitwise mul!) and compensated partials of p.q.
 // A warp owns 32 rows at a time (warp CSR-stream), warps stride over the matrix.
+// q = A p with the p.q partials over the matrix's 32-row slices (spmv.cuh):
+// the same row sums bit for bit as the CSR kernel below, with each lane's
+// row entries loaded eight at a time.  Each warp takes every (grid x 8)-th
+// slice; the next slice's bounds are loaded one slice ahead.
+__global__ void __launch_bounds__(kT, 4) pcg_spmv_dot_sliced(int32_t n, const int64_t* __restrict__ soff,
+                                                         const int32_t* __restrict__ scol,
+                                                         const double* __restrict__ sval,
+                                                         const double* __restrict__ p, double* __restrict__ q,
+                                                         const PcgScalars* __restrict__ s,
+                                                         double* __restrict__ partials) {
+    DD part{0.0, 0.0};
+    const int64_t nsl = ((int64_t)n + 31) / 32;
+    const int64_t stride = (int64_t)gridDim.x * (kT / 32);
+    int64_t sl = (int64_t)blockIdx.x * (kT / 32) + (threadIdx.x >> 5);
+    int64_t o0 = sl < nsl ? soff[sl] : 0, o1 = sl < nsl ? soff[sl + 1] : 0;
+    if (!s->done) {
+        auto fp = [&](int32_t j) { return __ldg(p + j); };
+        for (; sl < nsl; sl += stride) {
+            const int64_t nx = sl + stride;
+            const int64_t n0 = nx < nsl ? soff[nx] : 0, n1 = nx < nsl ? soff[nx + 1] : 0;
+            const double acc = hsdev::slice_row_sum(o0, o1, scol, sval, fp);
+            const int64_t r = sl * 32 + (threadIdx.x & 31);
+            if (r < n) {
+                q[r] = acc;
+                hsdev::dd_add_prod(part, p[r], acc);
+            }
+            o0 = n0;
+            o1 = n1;
+        }
+    }
+    store_dd(partials, part);
+}
+
 __global__ void __launch_bounds__(kT, 5) pcg_spmv_dot(int32_t n, const int32_t* __restrict__ rp,
                                                   const int32_t* __restrict__ ci, const double* __restrict__ v,
                                                   const double* __restrict__ p, double* __restrict__ q,
@@ -593,12 +626,16 @@ int pcg_impl(hs_matrix* A, int32_t prec_type, void* prec, const double* b, doubl
     const void* Av = nullptr;
     int Adt = 0;
     hs::matrix_arrays(A, &Arp, &Aci, &Av, &Adt);
+    const int64_t* Asoff = nullptr;
+    const int32_t* Ascol = nullptr;
+    const double* Asval = nullptr;
+    if (Adt == HS_F64 && (rc = hs::matrix_slices(A, st, &Asoff, &Ascol, &Asval))) return rc;
     const int nq = (int)std::max<int64_t>(1, std::min<int64_t>((n + kT - 1) / kT, (int64_t)hsdev::kRedMaxBlocks));
     auto iteration = [&](cudaStream_t cs) -> int {
         int r2;
         int npq = nb;
         if (Adt == HS_F64) {
-            pcg_spmv_dot<<<nq, kT, 0, cs>>>((int32_t)n, Arp, Aci, (const double*)Av, p, q, s, pa);
+            pcg_spmv_dot_sliced<<<nq, kT, 0, cs>>>((int32_t)n, Asoff, Ascol, Asval, p, q, s, pa);
             npq = nq;
         } else {
             if ((r2 = hs::matrix_spmv(A, p, q, 1.0, 0.0, cs))) return r2;
