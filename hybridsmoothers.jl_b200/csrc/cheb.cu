@@ -180,6 +180,36 @@ __global__ void __launch_bounds__(kThreads, kWarpMinBlocks) spmv_kernel(int32_t 
     }
 }
 
+// The same three forms over the matrix's 32-row slices (FP64): the folds of
+// spmv_kernel, operation for operation.
+template <int MODE>
+__global__ void __launch_bounds__(kThreads, 4) spmv_sliced_kernel(int32_t n, const int64_t* __restrict__ soff,
+                                                              const int32_t* __restrict__ scol,
+                                                              const double* __restrict__ sval,
+                                                              const double* __restrict__ x, double* __restrict__ y,
+                                                              double alpha, double beta) {
+    auto fx = [&](int32_t j) { return __ldg(x + j); };
+    const int64_t nsl = ((int64_t)n + 31) / 32;
+    const int64_t stride = (int64_t)gridDim.x * (kThreads / 32);
+    for (int64_t sl = (int64_t)blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5); sl < nsl; sl += stride) {
+        const int64_t r = sl * 32 + (threadIdx.x & 31);
+        const bool valid = r < n;
+        const int64_t o0 = soff[sl], o1 = soff[sl + 1];
+        double acc;
+        if (MODE == 0) {
+            acc = hsdev::slice_row_fold(o0, o1, scol, sval, 0.0, fx, AddOp<double>());
+        } else if (MODE == 1) {
+            acc = hsdev::slice_row_fold(o0, o1, scol, sval, valid ? y[r] : 0.0, fx, SubOp<double>());
+        } else {
+            double a0 = 0.0;
+            if (valid && beta != 0.0) a0 = (beta == 1.0) ? y[r] : __dmul_rn(y[r], beta);
+            auto op = [alpha](double a, double p) { return __dadd_rn(a, __dmul_rn(p, alpha)); };
+            acc = hsdev::slice_row_fold(o0, o1, scol, sval, a0, fx, op);
+        }
+        if (valid) y[r] = acc;
+    }
+}
+
 // l1inv[i] = 1 / sum_j |a_ij| (storage order), FP64: _l1_rowsum (chebyshev.jl:27-36)
 __global__ void l1inv_kernel(int32_t n, const int32_t* __restrict__ rp, const double* __restrict__ v,
                              double* __restrict__ l1inv) {
@@ -410,6 +440,29 @@ inline int grid_elems(int64_t n) {
 template <typename T>
 int spmv_t(const hs_matrix* M, const void* x, void* y, double alpha, double beta, cudaStream_t st) {
     const int g = grid_rows(M->n);
+    if (sizeof(T) == 8) {
+        // FP64: the sliced copy (built here unless the stream is being captured)
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        cudaStreamIsCapturing(st, &cs);
+        const int64_t* so = M->soff;
+        const int32_t* sc = M->scol;
+        const double* sv = M->sval;
+        if (!so && cs == cudaStreamCaptureStatusNone) {
+            if (int rc = hs::matrix_slices(const_cast<hs_matrix*>(M), st, &so, &sc, &sv)) return rc;
+        }
+        if (so) {
+            const double* xx = static_cast<const double*>(x);
+            double* yy = static_cast<double*>(y);
+            if (alpha == 1.0 && beta == 0.0)
+                spmv_sliced_kernel<0><<<g, kThreads, 0, st>>>(M->n, so, sc, sv, xx, yy, 1.0, 0.0);
+            else if (alpha == -1.0 && beta == 1.0)
+                spmv_sliced_kernel<1><<<g, kThreads, 0, st>>>(M->n, so, sc, sv, xx, yy, -1.0, 1.0);
+            else
+                spmv_sliced_kernel<2><<<g, kThreads, 0, st>>>(M->n, so, sc, sv, xx, yy, alpha, beta);
+            HS_LAUNCH_CHECK("spmv_sliced_kernel");
+            return HS_OK;
+        }
+    }
     const T* v = static_cast<const T*>(M->v);
     const T* xx = static_cast<const T*>(x);
     T* yy = static_cast<T*>(y);
@@ -1026,7 +1079,7 @@ __global__ void slice_fill_kernel(int32_t n, int64_t nslices, const int32_t* __r
         const int32_t q0 = row < n ? rp[row] : 0, len = row < n ? rp[row + 1] - q0 : 0;
         for (int32_t k = 0; k < w; ++k) {
             const bool real = k < len;
-            scol[o + 32 * (int64_t)k + lane] = real ? ci[q0 + k] : (row < n ? (int32_t)row : 0);
+            scol[o + 32 * (int64_t)k + lane] = real ? ci[q0 + k] : -1;   // padding: skipped
             sval[o + 32 * (int64_t)k + lane] = real ? v[q0 + k] : 0.0;
         }
     }

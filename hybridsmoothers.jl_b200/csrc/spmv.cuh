@@ -108,9 +108,8 @@ __device__ __forceinline__ T csr_warp_fold_rp(T* __restrict__ wbuf, int32_t n, R
 // longest row) stored column by column ([k][row]) from soff[s], so lane r
 // reads entry k of its row at soff[s] + 32 k + r -- coalesced, with no row
 // pointers and no window in shared memory.  A row's entries keep their
-// storage order and its padding entries (value 0, column = the row) follow
-// them, so the sum is the CSR sequence followed by +-0 terms: the same value
-// bit for bit for a finite x (an accumulator that starts at +0 is never -0).
+// storage order and its padding entries (column -1) follow them and are
+// skipped, so every fold is the CSR fold's sequence of operations exactly.
 
 // ent[s] = 32 * w_s for s < nslices, ent[nslices] = 0 (exclusive-scan input).
 __global__ void slice_width_kernel(int32_t n, int64_t nslices, const int32_t* __restrict__ rp,
@@ -122,32 +121,39 @@ __global__ void slice_fill_kernel(int32_t n, int64_t nslices, const int32_t* __r
                                   const int64_t* __restrict__ soff, int32_t* __restrict__ scol,
                                   double* __restrict__ sval);
 
-// Row (32 s + lane) of A times x for the slice with entries [o0, o1): the
-// storage-order sum, eight entries of the row in flight at a time.
-template <typename F>
-__device__ __forceinline__ double slice_row_sum(int64_t o0, int64_t o1, const int32_t* __restrict__ scol,
-                                                const double* __restrict__ sval, F fx) {
+// Fold of row (32 s + lane) for the slice with entries [o0, o1):
+// acc = op(acc, v_k * fx(c_k)) over the row's entries in storage order, as
+// csr_warp_fold does; eight entries of the row in flight at a time.
+template <typename F, typename Op>
+__device__ __forceinline__ double slice_row_fold(int64_t o0, int64_t o1, const int32_t* __restrict__ scol,
+                                                 const double* __restrict__ sval, double acc, F fx, Op op) {
     constexpr int KU = 8;
     const int lane = threadIdx.x & 31;
     const int32_t w = (int32_t)((o1 - o0) / 32);
     const int32_t* __restrict__ cp = scol + o0 + lane;
     const double* __restrict__ vp = sval + o0 + lane;
-    double acc = 0.0;
     for (int32_t j = 0; j < w; j += KU) {
         int32_t c[KU];
         double a[KU], b[KU];
 #pragma unroll
         for (int u = 0; u < KU; ++u) {
-            c[u] = j + u < w ? __ldg(cp + 32 * (j + u)) : 0;
+            c[u] = j + u < w ? __ldg(cp + 32 * (j + u)) : -1;
             a[u] = j + u < w ? __ldg(vp + 32 * (j + u)) : 0.0;
         }
 #pragma unroll
-        for (int u = 0; u < KU; ++u) b[u] = j + u < w ? fx(c[u]) : 0.0;
+        for (int u = 0; u < KU; ++u) b[u] = c[u] >= 0 ? fx(c[u]) : 0.0;
 #pragma unroll
         for (int u = 0; u < KU; ++u)
-            if (j + u < w) acc = __dadd_rn(acc, __dmul_rn(a[u], b[u]));
+            if (c[u] >= 0) acc = op(acc, __dmul_rn(a[u], b[u]));
     }
     return acc;
+}
+
+// Row (32 s + lane) of A times x: the storage-order sum from +0.
+template <typename F>
+__device__ __forceinline__ double slice_row_sum(int64_t o0, int64_t o1, const int32_t* __restrict__ scol,
+                                                const double* __restrict__ sval, F fx) {
+    return slice_row_fold(o0, o1, scol, sval, 0.0, fx, AddOp<double>());
 }
 
 }  // namespace hsdev
