@@ -14,7 +14,10 @@
 // a_{row, c} * y_c.  Only the eight steps of a diagonal tile form a serial
 // chain; the off-diagonal tiles, all but 8/ps of the entries, are plain
 // independent multiply-adds.  Multiply and add are rounded separately, as
-// in the reference.
+// in the reference.  Forward sweeps divide by D_Dl1 at every step (the
+// reference's operations: bit-identical); backward and symmetric sweeps,
+// which agree with the reference to rounding anyway, multiply by 1/D_Dl1
+// (one division per row instead of eight).
 //
 // A warp walks its groups' streams item by item (an item: one off-diagonal
 // warp tile, 2 KiB in FP64, or one diagonal warp tile) in the order the
@@ -208,9 +211,13 @@ __global__ void __launch_bounds__(kBlkWarps * 32) l1gs_blk_kernel(const Params p
                 for (int c = 0; c < B - 1; ++c)
                     aj[c] = r > c ? dp[G * (c * (B - 1) - c * (c - 1) / 2) + g * (B - 1 - c) + (r - c - 1)] : T(0);
                 T yown = T(0);
+                // Backward and symmetric sweeps agree with the reference to rounding
+                // anyway: there each lane divides once (1/D_Dl1) and the eight steps
+                // multiply.  Forward sweeps divide at every step (bit-identical).
+                const T rinv = SWEEP == 0 ? T(0) : div_rn(T(1), dr);
 #pragma unroll
                 for (int c = 0; c < B; ++c) {
-                    const T v = div_rn(sub_rn(xr, acc), dr);
+                    const T v = SWEEP == 0 ? div_rn(sub_rn(xr, acc), dr) : mul_rn(sub_rn(xr, acc), rinv);
                     const T yc = __shfl_sync(FULL, v, c, B);
                     if (r == c) yown = v;
                     if (c < B - 1 && r > c) acc = add_rn(acc, mul_rn(aj[c], yc));
@@ -240,10 +247,11 @@ __global__ void __launch_bounds__(kBlkWarps * 32) l1gs_blk_kernel(const Params p
                     au[c] = r < c ? dp[G * (B * (B - 1) / 2 - c * (c + 1) / 2) + g * c + r] : T(0);
                 // symmetric: y .= D_Dl1 .* y (:897) for the block's rows, then the backward solve
                 const T xr = SWEEP == 2 ? mul_rn(dr, yg[I * B + r]) : xn;
+                const T rinv = div_rn(T(1), dr);
                 T yown = T(0);
 #pragma unroll
                 for (int c = B - 1; c >= 0; --c) {
-                    const T v = div_rn(sub_rn(xr, acc), dr);
+                    const T v = mul_rn(sub_rn(xr, acc), rinv);
                     const T yc = __shfl_sync(FULL, v, c, B);
                     if (r == c) yown = v;
                     if (c > 0 && r < c) acc = add_rn(acc, mul_rn(au[c], yc));

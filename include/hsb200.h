@@ -93,9 +93,9 @@ typedef struct {
     /* Summation order of each row's terms.  0: chosen by the library; 1: the
      * reference's ascending order everywhere (bit-identical to the reference;
      * requires threads_per_part 0 or 1, or 8 for a forward sweep); 2: the
-     * library may reorder (partial
-     * sums combined at the end of the row), agreeing with the reference to
-     * rounding: relative 1e-12 in FP64. */
+     * library may reorder a row's sum (partial sums combined at the end of
+     * the row) or multiply by 1/D_Dl1 instead of dividing, agreeing with the
+     * reference to rounding: relative 1e-12 in FP64. */
     int32_t order;
 } hs_l1gs_options;
 

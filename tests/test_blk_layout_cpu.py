@@ -11,8 +11,9 @@ the lane's 16-byte vectors at `pos + lane * V + v * 32 * V`, each diagonal
 entry at the kernel's offset; every read asserts that it stays inside the
 group's stream and returns the intended entry.  The arithmetic is the
 kernel's: dense products in column order for the off-diagonal tiles, the
-diagonal solve with the solved value broadcast, separately rounded multiply
-and add, rows past n held at 0.  Forward sweeps must equal the oracle bit for
+diagonal solve with the solved value broadcast (forward: divided by D_Dl1 at
+every step; backward and symmetric: multiplied by 1/D_Dl1), separately rounded
+multiply and add, rows past n held at 0.  Forward sweeps must equal the oracle bit for
 bit, backward and symmetric sweeps within 1e-12.
 """
 import math
@@ -141,8 +142,12 @@ def emulate(A, ps, sweep, D, x, dtype):
                         xr = [T(x[rr]) if v else T(0) for rr, v in zip(rows[I], valid)]
                         dr = [D[rr] if v else T(1) for rr, v in zip(rows[I], valid)]
                         yown = [T(0)] * 32
+                        rinv = [T(T(1) / dr[l]) for l in range(32)]
                         for c in range(B):
-                            v = [T((xr[l] - acc[l]) / dr[l]) for l in range(32)]
+                            if sweep == "forward":   # a division at every step: bit-identical
+                                v = [T((xr[l] - acc[l]) / dr[l]) for l in range(32)]
+                            else:                    # symmetric: multiply by 1/D_Dl1
+                                v = [T(T(xr[l] - acc[l]) * rinv[l]) for l in range(32)]
                             for lane in range(32):
                                 g, r = divmod(lane, B)
                                 if r == c:
@@ -177,8 +182,9 @@ def emulate(A, ps, sweep, D, x, dtype):
                         else:
                             xr = [T(x[rr]) if v else T(0) for rr, v in zip(rows[I], valid)]
                         yown = [T(0)] * 32
+                        rinv = [T(T(1) / dr[l]) for l in range(32)]
                         for c in range(B - 1, -1, -1):
-                            v = [T((xr[l] - acc[l]) / dr[l]) for l in range(32)]
+                            v = [T(T(xr[l] - acc[l]) * rinv[l]) for l in range(32)]
                             for lane in range(32):
                                 g, r = divmod(lane, B)
                                 if r == c:
