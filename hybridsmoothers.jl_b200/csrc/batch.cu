@@ -545,7 +545,7 @@ int build_slices(hs_batch_slot& sl, int32_t n, const int32_t* rp_host, cudaStrea
     if ((e = cudaMemcpyAsync(sl.soff, off.data(), sizeof(int64_t) * off.size(), cudaMemcpyHostToDevice, st)))
         return hs::cuda_error(e, "slice offsets");
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((32 * nsl + kT - 1) / kT, 8192));
-    hsdev::slice_fill_kernel<<<grid, kT, 0, st>>>(n, nsl, rp, ci, static_cast<const double*>(mv), sl.soff, sl.scol, sl.sval);
+    hsdev::slice_fill_kernel<double><<<grid, kT, 0, st>>>(n, nsl, rp, ci, static_cast<const double*>(mv), sl.soff, sl.scol, sl.sval);
     hs::count_launch();
     if ((e = cudaGetLastError()) != cudaSuccess) return hs::cuda_error(e, "slice_fill_kernel");
     return HS_OK;

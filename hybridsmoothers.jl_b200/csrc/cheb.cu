@@ -46,7 +46,7 @@ struct hs_matrix_s {
     // FP64 copy in 32-row slices (spmv.cuh), built at the first PCG solve
     int64_t* soff = nullptr;
     int32_t* scol = nullptr;
-    double* sval = nullptr;
+    void* sval = nullptr;      // values in the matrix type
     int64_t bytes = 0;
     bool stream_ordered = false;   // buffers from cudaMallocAsync
     cudaStream_t alloc_stream = nullptr;
@@ -154,6 +154,13 @@ constexpr int kWarpMinBlocks = 5;
     for (int64_t row0 = ((int64_t)blockIdx.x * (kThreads / 32) + warp_) * 32; row0 < n;                       \
          row0 += (int64_t)gridDim.x * kThreads)
 #define HS_WARP_FOLD(acc0, f, op) hsdev::csr_warp_fold(wbuf[warp_], n, rp, ci, v, row0, acc0, f, op)
+// The same fold over the matrix's 32-row slices when the kernel has them
+// (soff non-null): the same operations in the same order.
+#define HS_ROW_FOLD(acc0, f, op)                                                                        \
+    (soff ? hsdev::slice_row_fold(soff[row0 >> 5], soff[(row0 >> 5) + 1], scol, sval, acc0, f, op) \
+          : HS_WARP_FOLD(acc0, f, op))
+#define HS_SLICE_PARAMS(T) \
+    const int64_t *__restrict__ soff, const int32_t *__restrict__ scol, const T *__restrict__ sval
 
 // MODE 0: y = A x; MODE 1: y = y - A x (term by term); MODE 2: y = beta y + sum (a x) alpha.
 template <typename T, int MODE>
@@ -316,13 +323,13 @@ __global__ void sqrt_kernel(int32_t n, const double* __restrict__ a, double* __r
 template <typename T>
 __global__ void __launch_bounds__(kThreads) cheb4_init_kernel(int32_t n, const int32_t* __restrict__ rp,
                                                               const int32_t* __restrict__ ci, const T* __restrict__ v,
-                                                              const T* __restrict__ x, const T* __restrict__ b,
+                                                              HS_SLICE_PARAMS(T), const T* __restrict__ x, const T* __restrict__ b,
                                                               T* __restrict__ r, T* __restrict__ z) {
     HS_WARP_SHARED(T);
     auto fx = [&](int32_t j) { return __ldg(x + j); };
     HS_WARP_ROWS_LOOP {
         const int64_t i = row0 + (threadIdx.x & 31);
-        const T ax = HS_WARP_FOLD(T(0), fx, AddOp<T>());
+        const T ax = HS_ROW_FOLD(T(0), fx, AddOp<T>());
         if (i < n) {
             r[i] = sub_rn(b[i], ax);
             z[i] = T(0);
@@ -345,7 +352,7 @@ __global__ void cheb4_init_zero_kernel(int32_t n, const IO* __restrict__ b, T* _
 template <typename T>
 __global__ void __launch_bounds__(kThreads) cheb4_step_kernel(int32_t n, const int32_t* __restrict__ rp,
                                                               const int32_t* __restrict__ ci, const T* __restrict__ v,
-                                                              const T* __restrict__ l1inv, T ak, T bk,
+                                                              HS_SLICE_PARAMS(T), const T* __restrict__ l1inv, T ak, T bk,
                                                               const T* __restrict__ z_old, const T* __restrict__ r_old,
                                                               T* __restrict__ z_new, T* __restrict__ r_new,
                                                               T* __restrict__ x) {
@@ -356,7 +363,7 @@ __global__ void __launch_bounds__(kThreads) cheb4_step_kernel(int32_t n, const i
     HS_WARP_ROWS_LOOP {
         const int64_t i = row0 + (threadIdx.x & 31);
         const bool valid = i < n;
-        const T acc = HS_WARP_FOLD(valid ? r_old[i] : T(0), zk, SubOp<T>());
+        const T acc = HS_ROW_FOLD(valid ? r_old[i] : T(0), zk, SubOp<T>());
         if (valid) {
             const T zi = zk((int32_t)i);
             z_new[i] = zi;
@@ -371,14 +378,14 @@ __global__ void __launch_bounds__(kThreads) cheb4_step_kernel(int32_t n, const i
 template <typename T>
 __global__ void __launch_bounds__(kThreads) cheb1_init_kernel(int32_t n, const int32_t* __restrict__ rp,
                                                               const int32_t* __restrict__ ci, const T* __restrict__ v,
-                                                              const T* __restrict__ x, const T* __restrict__ b,
+                                                              HS_SLICE_PARAMS(T), const T* __restrict__ x, const T* __restrict__ b,
                                                               const T* __restrict__ l1inv, T inv_rho, T c0,
                                                               T* __restrict__ r, T* __restrict__ z) {
     HS_WARP_SHARED(T);
     auto fx = [&](int32_t j) { return __ldg(x + j); };
     HS_WARP_ROWS_LOOP {
         const int64_t i = row0 + (threadIdx.x & 31);
-        const T tmp = HS_WARP_FOLD(T(0), fx, AddOp<T>());
+        const T tmp = HS_ROW_FOLD(T(0), fx, AddOp<T>());
         if (i < n) {
             const T ri = mul_rn(mul_rn(l1inv[i], sub_rn(b[i], tmp)), inv_rho);
             r[i] = ri;
@@ -402,14 +409,14 @@ __global__ void cheb1_init_zero_kernel(int32_t n, const IO* __restrict__ b, cons
 template <typename T>
 __global__ void __launch_bounds__(kThreads) cheb1_step_kernel(int32_t n, const int32_t* __restrict__ rp,
                                                               const int32_t* __restrict__ ci, const T* __restrict__ v,
-                                                              const T* __restrict__ l1inv, T inv_rho, T c1, T c2,
+                                                              HS_SLICE_PARAMS(T), const T* __restrict__ l1inv, T inv_rho, T c1, T c2,
                                                               const T* __restrict__ z_old, T* __restrict__ z_new,
                                                               T* __restrict__ r, T* __restrict__ x) {
     HS_WARP_SHARED(T);
     auto fz = [&](int32_t j) { return __ldg(z_old + j); };
     HS_WARP_ROWS_LOOP {
         const int64_t i = row0 + (threadIdx.x & 31);
-        const T tmp = HS_WARP_FOLD(T(0), fz, AddOp<T>());
+        const T tmp = HS_ROW_FOLD(T(0), fz, AddOp<T>());
         if (i < n) {
             const T zo = z_old[i];
             x[i] = add_rn(x[i], zo);
@@ -446,10 +453,11 @@ int spmv_t(const hs_matrix* M, const void* x, void* y, double alpha, double beta
         cudaStreamIsCapturing(st, &cs);
         const int64_t* so = M->soff;
         const int32_t* sc = M->scol;
-        const double* sv = M->sval;
+        const void* svv = M->sval;
         if (!so && cs == cudaStreamCaptureStatusNone) {
-            if (int rc = hs::matrix_slices(const_cast<hs_matrix*>(M), st, &so, &sc, &sv)) return rc;
+            if (int rc = hs::matrix_slices(const_cast<hs_matrix*>(M), st, &so, &sc, &svv)) return rc;
         }
+        const double* sv = static_cast<const double*>(svv);
         if (so) {
             const double* xx = static_cast<const double*>(x);
             double* yy = static_cast<double*>(y);
@@ -487,9 +495,9 @@ int matrix_spmv(const hs_matrix* M, const void* x, void* y, double alpha, double
 }
 // The FP64 matrix in 32-row slices, built once (on stream st; one wait for
 // the entry count) and kept with the matrix.
-int matrix_slices(hs_matrix* M, cudaStream_t st, const int64_t** soff, const int32_t** scol, const double** sval) {
-    if (M->dtype != HS_F64) return hs::set_error(HS_ERR_UNSUPPORTED, "sliced copy of an FP32 matrix");
+int matrix_slices(hs_matrix* M, cudaStream_t st, const int64_t** soff, const int32_t** scol, const void** sval) {
     if (!M->soff) {
+        const size_t es = M->dtype == HS_F64 ? 8 : 4;
         const int32_t n = M->n;
         const int64_t nsl = ((int64_t)n + 31) / 32;
         const bool so = M->stream_ordered;
@@ -525,14 +533,18 @@ int matrix_slices(hs_matrix* M, cudaStream_t st, const int64_t** soff, const int
         release(ent);
         ent = nullptr;
         if ((e = alloc((void**)&M->scol, sizeof(int32_t) * (size_t)total)) ||
-            (e = alloc((void**)&M->sval, sizeof(double) * (size_t)total)))
+            (e = alloc((void**)&M->sval, es * (size_t)total)))
             goto fail;
-        hsdev::slice_fill_kernel<<<grid, 256, 0, st>>>(n, nsl, M->rp, M->ci, static_cast<const double*>(M->v), off,
-                                                       M->scol, M->sval);
+        if (M->dtype == HS_F64)
+            hsdev::slice_fill_kernel<double><<<grid, 256, 0, st>>>(n, nsl, M->rp, M->ci, static_cast<const double*>(M->v),
+                                                                   off, M->scol, static_cast<double*>(M->sval));
+        else
+            hsdev::slice_fill_kernel<float><<<grid, 256, 0, st>>>(n, nsl, M->rp, M->ci, static_cast<const float*>(M->v),
+                                                                  off, M->scol, static_cast<float*>(M->sval));
         hs::count_launch();
         if ((e = cudaGetLastError()) != cudaSuccess) goto fail;
         M->soff = off;
-        M->bytes += (int64_t)(8 * (nsl + 1) + 12 * total);
+        M->bytes += (int64_t)(8 * (nsl + 1) + (4 + (int64_t)es) * total);
         goto done;
     fail:
         release(tmp);
@@ -646,6 +658,9 @@ int cheb_smooth_t(hs_cheb* S, T* x, const void* b, int io, bool x_is_zero, cudaS
     const int32_t n = S->n;
     const hs_matrix* M = S->A;
     const T* v = static_cast<const T*>(M->v);
+    const int64_t* so = M->soff;   // the sliced copy (built with the smoother)
+    const int32_t* sc = M->scol;
+    const T* sv = static_cast<const T*>(M->sval);
     const T* l1 = static_cast<const T*>(S->l1inv);
     T* r[2] = {static_cast<T*>(S->w[0]), static_cast<T*>(S->w[1])};
     T* z[2] = {static_cast<T*>(S->w[2]), static_cast<T*>(S->w[3])};
@@ -659,7 +674,7 @@ int cheb_smooth_t(hs_cheb* S, T* x, const void* b, int io, bool x_is_zero, cudaS
             HS_LAUNCH_CHECK("cheb4_init_zero_kernel");
         } else {
             cheb4_init_kernel<T><<<g, kThreads, 0, st>>>(
-                                        n, M->rp, M->ci, v, x, static_cast<const T*>(b), r[0], z[0]);
+                                        n, M->rp, M->ci, v, so, sc, sv, x, static_cast<const T*>(b), r[0], z[0]);
             HS_LAUNCH_CHECK("cheb4_init_kernel");
         }
         int cur = 0;
@@ -667,7 +682,7 @@ int cheb_smooth_t(hs_cheb* S, T* x, const void* b, int io, bool x_is_zero, cudaS
             const T ak = (T)((double)(2 * k - 3) / (double)(2 * k + 1));
             const T bk = (T)((double)(8 * k - 4) / ((double)(2 * k + 1) * S->rho));
             cheb4_step_kernel<T><<<g, kThreads, 0, st>>>(
-                                        n, M->rp, M->ci, v, l1, ak, bk, z[cur], r[cur], z[cur ^ 1], r[cur ^ 1], x);
+                                        n, M->rp, M->ci, v, so, sc, sv, l1, ak, bk, z[cur], r[cur], z[cur ^ 1], r[cur ^ 1], x);
             HS_LAUNCH_CHECK("cheb4_step_kernel");
             cur ^= 1;
         }
@@ -687,7 +702,7 @@ int cheb_smooth_t(hs_cheb* S, T* x, const void* b, int io, bool x_is_zero, cudaS
         HS_LAUNCH_CHECK("cheb1_init_zero_kernel");
     } else {
         cheb1_init_kernel<T><<<g, kThreads, 0, st>>>(
-                                    n, M->rp, M->ci, v, x, static_cast<const T*>(b), l1, inv_rho, c0, r[0], z[0]);
+                                    n, M->rp, M->ci, v, so, sc, sv, x, static_cast<const T*>(b), l1, inv_rho, c0, r[0], z[0]);
         HS_LAUNCH_CHECK("cheb1_init_kernel");
     }
     double rho_s = (1.0 - a) / (1.0 + a);
@@ -698,7 +713,7 @@ int cheb_smooth_t(hs_cheb* S, T* x, const void* b, int io, bool x_is_zero, cudaS
             const T c1 = (T)(rho_new * rho_s);
             const T c2 = (T)(4.0 * rho_new / (1.0 - a));
             cheb1_step_kernel<T><<<g, kThreads, 0, st>>>(
-                                        n, M->rp, M->ci, v, l1, inv_rho, c1, c2, z[cur], z[cur ^ 1], r[0], x);
+                                        n, M->rp, M->ci, v, so, sc, sv, l1, inv_rho, c1, c2, z[cur], z[cur ^ 1], r[0], x);
             HS_LAUNCH_CHECK("cheb1_step_kernel");
             cur ^= 1;
             rho_s = rho_new;
@@ -901,6 +916,12 @@ int hs_cheb_create(const hs_sparse* A, int32_t kind, int32_t degree, int32_t eig
         hs::count_launch();
         S->l1inv = l32;
     }
+    {   // the smoother's matrix in 32-row slices, for its steps
+        const int64_t* so = nullptr;
+        const int32_t* scl = nullptr;
+        const void* sv = nullptr;
+        if ((rc = hs::matrix_slices(S->A, st, &so, &scl, &sv))) return fail(rc);
+    }
     const size_t es = hsm::dsize(smoother_dtype);
     for (int i = 0; i < 6; ++i)
         if ((e = cudaMalloc(&S->w[i], es * (size_t)n))) return fail(hs::cuda_error(e, "cudaMalloc (work)"));
@@ -1063,25 +1084,6 @@ __global__ void slice_width_kernel(int32_t n, int64_t nslices, const int32_t* __
         const int32_t len = (sl < nslices && row < n) ? rp[row + 1] - rp[row] : 0;
         const int32_t w = (int32_t)__reduce_max_sync(0xffffffffu, (unsigned)len);
         if (lane == 0) ent[sl] = 32 * (int64_t)w;
-    }
-}
-
-__global__ void slice_fill_kernel(int32_t n, int64_t nslices, const int32_t* __restrict__ rp,
-                                  const int32_t* __restrict__ ci, const double* __restrict__ v,
-                                  const int64_t* __restrict__ soff, int32_t* __restrict__ scol,
-                                  double* __restrict__ sval) {
-    const int lane = threadIdx.x & 31;
-    for (int64_t sl = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; sl < nslices;
-         sl += ((int64_t)gridDim.x * blockDim.x) >> 5) {
-        const int64_t o = soff[sl];
-        const int32_t w = (int32_t)((soff[sl + 1] - o) / 32);
-        const int64_t row = sl * 32 + lane;
-        const int32_t q0 = row < n ? rp[row] : 0, len = row < n ? rp[row + 1] - q0 : 0;
-        for (int32_t k = 0; k < w; ++k) {
-            const bool real = k < len;
-            scol[o + 32 * (int64_t)k + lane] = real ? ci[q0 + k] : -1;   // padding: skipped
-            sval[o + 32 * (int64_t)k + lane] = real ? v[q0 + k] : 0.0;
-        }
     }
 }
 

@@ -9,9 +9,9 @@ int matrix_spmv(const hs_matrix* M, const void* x, void* y, double alpha, double
 int matrix_n(const hs_matrix* M);
 int64_t matrix_nnz(const hs_matrix* M);
 void matrix_arrays(const hs_matrix* M, const int32_t** rp, const int32_t** ci, const void** v, int* dtype);
-// The FP64 matrix in 32-row slices (spmv.cuh), built at the first call and
-// kept with the matrix.
-int matrix_slices(hs_matrix* M, cudaStream_t st, const int64_t** soff, const int32_t** scol, const double** sval);
+// The matrix in 32-row slices (spmv.cuh; values in the matrix type), built
+// at the first call and kept with the matrix.
+int matrix_slices(hs_matrix* M, cudaStream_t st, const int64_t** soff, const int32_t** scol, const void** sval);
 int cheb_apply(hs_cheb* S, const void* r, void* z, int io, cudaStream_t st);
 // Uploads a validated host matrix as device CSR in `dtype` (a CSC input is
 // transposed on the device); rp has n+1 entries, ci and v nnz.  For a CSC

@@ -628,8 +628,9 @@ int pcg_impl(hs_matrix* A, int32_t prec_type, void* prec, const double* b, doubl
     hs::matrix_arrays(A, &Arp, &Aci, &Av, &Adt);
     const int64_t* Asoff = nullptr;
     const int32_t* Ascol = nullptr;
-    const double* Asval = nullptr;
-    if (Adt == HS_F64 && (rc = hs::matrix_slices(A, st, &Asoff, &Ascol, &Asval))) return rc;
+    const void* Asv = nullptr;
+    if (Adt == HS_F64 && (rc = hs::matrix_slices(A, st, &Asoff, &Ascol, &Asv))) return rc;
+    const double* Asval = static_cast<const double*>(Asv);
     const int nq = (int)std::max<int64_t>(1, std::min<int64_t>((n + kT - 1) / kT, (int64_t)hsdev::kRedMaxBlocks));
     auto iteration = [&](cudaStream_t cs) -> int {
         int r2;

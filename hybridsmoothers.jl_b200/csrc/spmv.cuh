@@ -115,36 +115,52 @@ __device__ __forceinline__ T csr_warp_fold_rp(T* __restrict__ wbuf, int32_t n, R
 __global__ void slice_width_kernel(int32_t n, int64_t nslices, const int32_t* __restrict__ rp,
                                    int64_t* __restrict__ ent);
 
-// The entries of each slice (soff: the exclusive scan of slice_width_kernel).
+// The entries of each slice (soff: the exclusive scan of slice_width_kernel);
+// padding entries get column -1.
+template <typename T>
 __global__ void slice_fill_kernel(int32_t n, int64_t nslices, const int32_t* __restrict__ rp,
-                                  const int32_t* __restrict__ ci, const double* __restrict__ v,
+                                  const int32_t* __restrict__ ci, const T* __restrict__ v,
                                   const int64_t* __restrict__ soff, int32_t* __restrict__ scol,
-                                  double* __restrict__ sval);
+                                  T* __restrict__ sval) {
+    const int lane = threadIdx.x & 31;
+    for (int64_t sl = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; sl < nslices;
+         sl += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        const int64_t o = soff[sl];
+        const int32_t w = (int32_t)((soff[sl + 1] - o) / 32);
+        const int64_t row = sl * 32 + lane;
+        const int32_t q0 = row < n ? rp[row] : 0, len = row < n ? rp[row + 1] - q0 : 0;
+        for (int32_t k = 0; k < w; ++k) {
+            const bool real = k < len;
+            scol[o + 32 * (int64_t)k + lane] = real ? ci[q0 + k] : -1;
+            sval[o + 32 * (int64_t)k + lane] = real ? v[q0 + k] : T(0);
+        }
+    }
+}
 
 // Fold of row (32 s + lane) for the slice with entries [o0, o1):
 // acc = op(acc, v_k * fx(c_k)) over the row's entries in storage order, as
 // csr_warp_fold does; eight entries of the row in flight at a time.
-template <typename F, typename Op>
-__device__ __forceinline__ double slice_row_fold(int64_t o0, int64_t o1, const int32_t* __restrict__ scol,
-                                                 const double* __restrict__ sval, double acc, F fx, Op op) {
+template <typename T, typename F, typename Op>
+__device__ __forceinline__ T slice_row_fold(int64_t o0, int64_t o1, const int32_t* __restrict__ scol,
+                                            const T* __restrict__ sval, T acc, F fx, Op op) {
     constexpr int KU = 8;
     const int lane = threadIdx.x & 31;
     const int32_t w = (int32_t)((o1 - o0) / 32);
     const int32_t* __restrict__ cp = scol + o0 + lane;
-    const double* __restrict__ vp = sval + o0 + lane;
+    const T* __restrict__ vp = sval + o0 + lane;
     for (int32_t j = 0; j < w; j += KU) {
         int32_t c[KU];
-        double a[KU], b[KU];
+        T a[KU], b[KU];
 #pragma unroll
         for (int u = 0; u < KU; ++u) {
             c[u] = j + u < w ? __ldg(cp + 32 * (j + u)) : -1;
-            a[u] = j + u < w ? __ldg(vp + 32 * (j + u)) : 0.0;
+            a[u] = j + u < w ? __ldg(vp + 32 * (j + u)) : T(0);
         }
 #pragma unroll
-        for (int u = 0; u < KU; ++u) b[u] = c[u] >= 0 ? fx(c[u]) : 0.0;
+        for (int u = 0; u < KU; ++u) b[u] = c[u] >= 0 ? fx(c[u]) : T(0);
 #pragma unroll
         for (int u = 0; u < KU; ++u)
-            if (c[u] >= 0) acc = op(acc, __dmul_rn(a[u], b[u]));
+            if (c[u] >= 0) acc = op(acc, mul_rn(a[u], b[u]));
     }
     return acc;
 }
