@@ -27,18 +27,24 @@ struct hs_richardson_s {
     void* residual = nullptr;
     void* correction = nullptr;
     void* xbuf[2] = {nullptr, nullptr};
+    const int64_t* soff = nullptr;   // the matrix's 32-row slices (owned by the matrix)
+    const int32_t* scol = nullptr;
+    const void* sval = nullptr;
 };
 
 namespace {
 
 // residual = A xin - b, where xin_j = x_j (first sweep) or x_j - z_j (later
-// sweeps, also stored into xout for the rows of this warp).  Warp CSR-stream.
+// sweeps, also stored into xout for the rows of this warp).  Over the matrix's
+// 32-row slices (spmv.cuh) when soff is given, else warp CSR-stream: the same
+// fold either way.
 constexpr int kRT = 256;
 
 template <typename T, bool UPDATE>
 __global__ void __launch_bounds__(kRT)
     richardson_residual(int32_t n, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
-                        const T* __restrict__ v, const T* __restrict__ x, const T* __restrict__ z,
+                        const T* __restrict__ v, const int64_t* __restrict__ soff, const int32_t* __restrict__ scol,
+                        const T* __restrict__ sval, const T* __restrict__ x, const T* __restrict__ z,
                         const T* __restrict__ b, T* __restrict__ r, T* __restrict__ xout) {
     __shared__ T wbuf[kRT / 32][hsdev::kWarpCap];
     const int warp = threadIdx.x >> 5;
@@ -47,7 +53,9 @@ __global__ void __launch_bounds__(kRT)
         return __ldg(x + j);
     };
     for (int64_t row0 = ((int64_t)blockIdx.x * (kRT / 32) + warp) * 32; row0 < n; row0 += (int64_t)gridDim.x * kRT) {
-        const T acc = hsdev::csr_warp_fold(wbuf[warp], n, rp, ci, v, row0, T(0), xin, hsdev::AddOp<T>());
+        const T acc = soff ? hsdev::slice_row_fold(soff[row0 >> 5], soff[(row0 >> 5) + 1], scol, sval, T(0), xin,
+                                                   hsdev::AddOp<T>())
+                           : hsdev::csr_warp_fold(wbuf[warp], n, rp, ci, v, row0, T(0), xin, hsdev::AddOp<T>());
         const int64_t i = row0 + (threadIdx.x & 31);
         if (i < n) {
             r[i] = sub_rn(acc, b[i]);
@@ -70,6 +78,9 @@ int smooth_t(hs_richardson* S, T* x, const T* b, int sweeps, cudaStream_t st) {
     int dt = 0;
     hs::matrix_arrays(S->A, &rp, &ci, &vv, &dt);
     const T* v = static_cast<const T*>(vv);
+    const int64_t* so = S->soff;
+    const int32_t* sc = S->scol;
+    const T* sv = static_cast<const T*>(S->sval);
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((n + kRT - 1) / kRT, INT32_MAX));
     T* r = static_cast<T*>(S->residual);
     T* z = static_cast<T*>(S->correction);
@@ -79,9 +90,9 @@ int smooth_t(hs_richardson* S, T* x, const T* b, int sweeps, cudaStream_t st) {
     for (int k = 0; k < sweeps; ++k) {
         T* xnext = static_cast<T*>(S->xbuf[nb]);
         if (k == 0) {
-            richardson_residual<T, false><<<grid, kRT, 0, st>>>(n, rp, ci, v, xcur, z, b, r, nullptr);
+            richardson_residual<T, false><<<grid, kRT, 0, st>>>(n, rp, ci, v, so, sc, sv, xcur, z, b, r, nullptr);
         } else {
-            richardson_residual<T, true><<<grid, kRT, 0, st>>>(n, rp, ci, v, xcur, z, b, r, xnext);
+            richardson_residual<T, true><<<grid, kRT, 0, st>>>(n, rp, ci, v, so, sc, sv, xcur, z, b, r, xnext);
             xcur = xnext;
             nb ^= 1;
         }
@@ -117,6 +128,11 @@ int hs_richardson_create(const hs_matrix* A, hs_l1gs* P, hs_richardson** out) {
     S->P = P;
     S->n = n;
     S->dtype = dt;
+    // the matrix in 32-row slices (kept with the matrix; built once)
+    if ((rc = hs::matrix_slices(const_cast<hs_matrix*>(A), nullptr, &S->soff, &S->scol, &S->sval))) {
+        delete S;
+        return rc;
+    }
     const size_t bytes = (dt == HS_F64 ? 8 : 4) * (size_t)n;
     cudaError_t e;
     if ((e = cudaMalloc(&S->residual, bytes)) || (e = cudaMalloc(&S->correction, bytes)) ||
