@@ -1371,6 +1371,8 @@ int setup_device(hs_l1gs* P, const int32_t* rp_h, const int32_t* ci_h, const TM*
         if ((rc = hsseg::build<TM, TS>(n, P->ps, P->nparts, rp_d, ci_d, v_d, lower, upper, &P->seg, st))) return rc;
         P->bytes += P->seg.bytes;
         P->use_seg = true;
+        P->io_groups = P->seg.ngroups;   // groups of seg.G partitions
+        P->io_group_parts = P->seg.G;
         HS_CUDA(cudaStreamSynchronize(st));
         if (!on_device) {
             cudaFree(rp_d);
@@ -1732,7 +1734,7 @@ int launch_apply(hs_l1gs* P, const void* x, void* y, cudaStream_t st) {
     if (P->cache == HS_CACHE_VIEW && P->use_seg) {
         if (!P->err_word) P->err_word = hs::device_error_word();
         return hsseg::launch(P->sdt, dtype_of<IO>::value, P->sweep, P->seg, P->n, P->ps, P->rng_beg,
-                             P->rng_end < 0 ? P->ngroups : P->rng_end, P->D, x, y, P->err_word, st);
+                             P->rng_end < 0 ? P->seg.ngroups : P->rng_end, P->D, x, y, P->err_word, st);
     }
     if (P->cache == HS_CACHE_PACKED) {
         switch (P->sweep) {

@@ -37,15 +37,15 @@ __global__ void seg_count_kernel(int32_t n, int32_t ps, const int32_t* __restric
     }
 }
 
-// One warp per (group, row): the largest count of the 32 partitions' rows.
-__global__ void seg_max_kernel(int32_t n, int32_t ps, int32_t psq, int32_t nparts, int64_t items,
+// One warp per (group, row): the largest count of the G partitions' rows.
+__global__ void seg_max_kernel(int32_t n, int32_t ps, int32_t psq, int32_t G, int32_t nparts, int64_t items,
                                const int32_t* __restrict__ cnt, uint8_t* __restrict__ maxc) {
     const int lane = threadIdx.x & 31;
     for (int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; w < items;
          w += ((int64_t)gridDim.x * blockDim.x) >> 5) {
         const int64_t g = w / ps, li = w - g * ps;
-        const int64_t k = g * 32 + lane, row = k * ps + li;
-        const int32_t c = (k < nparts && row < n) ? cnt[row] : 0;
+        const int64_t k = g * G + lane, row = k * ps + li;
+        const int32_t c = (lane < G && k < nparts && row < n) ? cnt[row] : 0;
         const unsigned m = __reduce_max_sync(FULL, (unsigned)c);
         if (lane == 0) maxc[g * psq + li] = (uint8_t)m;
     }
@@ -69,29 +69,29 @@ __global__ void seg_off_kernel(int32_t ngroups, int32_t ps, int32_t psq, const u
 // Every slot's columns start as `ps` (the zero row); the scatter then writes
 // the real entries over them.
 template <typename TS>
-__global__ void seg_pad_kernel(int64_t slots, int32_t ps, unsigned char* __restrict__ stream) {
-    constexpr int64_t SB = 32 * (sizeof(TS) + 2);
-    const int64_t m = slots * 32;
+__global__ void seg_pad_kernel(int64_t slots, int32_t ps, int32_t G, unsigned char* __restrict__ stream) {
+    const int64_t SB = G * (int64_t)(sizeof(TS) + 2);
+    const int64_t m = slots * G;
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < m; e += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t slot = e >> 5, lane = e & 31;
-        reinterpret_cast<uint16_t*>(stream + slot * SB + 32 * sizeof(TS))[lane] = (uint16_t)ps;
+        const int64_t slot = e / G, lane = e - slot * G;
+        reinterpret_cast<uint16_t*>(stream + slot * SB + G * sizeof(TS))[lane] = (uint16_t)ps;
     }
 }
 
 template <typename TM, typename TS>
-__global__ void seg_scatter_kernel(int32_t n, int32_t ps, const int32_t* __restrict__ ci, const TM* __restrict__ v,
-                                   const int32_t* __restrict__ cnt, const int32_t* __restrict__ q0,
-                                   const uint16_t* __restrict__ off, const int64_t* __restrict__ base,
-                                   unsigned char* __restrict__ stream) {
-    constexpr int64_t SB = 32 * (sizeof(TS) + 2);
+__global__ void seg_scatter_kernel(int32_t n, int32_t ps, int32_t G, const int32_t* __restrict__ ci,
+                                   const TM* __restrict__ v, const int32_t* __restrict__ cnt,
+                                   const int32_t* __restrict__ q0, const uint16_t* __restrict__ off,
+                                   const int64_t* __restrict__ base, unsigned char* __restrict__ stream) {
+    const int64_t SB = G * (int64_t)(sizeof(TS) + 2);
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t k = i / ps, li = i - k * ps, g = k / 32, lane = k - g * 32, s = k * ps;
+        const int64_t k = i / ps, li = i - k * ps, g = k / G, lane = k - g * G, s = k * ps;
         const int64_t slot0 = base[g] + off[g * ps + li];
         for (int32_t t = 0; t < cnt[i]; ++t) {
             const int32_t q = q0[i] + t;
             unsigned char* sp = stream + (slot0 + t) * SB;
             reinterpret_cast<TS*>(sp)[lane] = (TS)v[q];
-            reinterpret_cast<uint16_t*>(sp + 32 * sizeof(TS))[lane] = (uint16_t)(ci[q] - s);
+            reinterpret_cast<uint16_t*>(sp + G * sizeof(TS))[lane] = (uint16_t)(ci[q] - s);
         }
     }
 }
@@ -132,19 +132,22 @@ constexpr int seg_k() {
     return sizeof(T) == 8 ? 4 : 6;
 }
 
-// Runtime partsize (2..128): y and D_Dl1 of the group in shared memory.
-template <typename T, typename IO, int SWEEP>
+// Runtime partsize (2..512): y and D_Dl1 of the group in shared memory.  G
+// partitions per group; lanes G..31 repeat lanes 0..G-1 (same loads, same
+// values written), so no lane needs a guard.
+template <typename T, typename IO, int SWEEP, int G>
 __global__ void __launch_bounds__(kSegWarps * 32, 1) l1gs_seg_kernel(const hsseg::Params p) {
-    constexpr int S = 33;
-    constexpr uint32_t SB = 32 * (sizeof(T) + 2);   // bytes per slot
-    constexpr int K = seg_k<T>();
+    constexpr int S = G + 1;
+    constexpr uint32_t SB = G * (sizeof(T) + 2);           // bytes per slot
+    constexpr int K = seg_k<T>() * (32 / G);               // slots per chunk
     constexpr int NDIR = SWEEP == 2 ? 2 : 1;
     extern __shared__ __align__(128) unsigned char smem[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, pl = lane & (G - 1);
     const int ps = p.ps, psq = (ps + 3) & ~3;
     unsigned char* wbase = smem + (size_t)warp * p.warp_bytes;
-    T* ys = reinterpret_cast<T*>(wbase + p.ys_off);   // y of row li, lane's partition: ys[li * S + lane]; row ps: +0
+    T* ys = reinterpret_cast<T*>(wbase + p.ys_off);   // y of row li, partition pl: ys[li * S + pl]; row ps: +0
     T* ds = reinterpret_cast<T*>(wbase + p.ds_off);
+    uint8_t* mxs = wbase + p.mx_off;                   // the group's slots per row, per direction (psq bytes each)
     const T* __restrict__ D = static_cast<const T*>(p.D);
     const IO* __restrict__ x = static_cast<const IO*>(p.x);
     IO* __restrict__ y = static_cast<IO*>(p.y);
@@ -159,7 +162,7 @@ __global__ void __launch_bounds__(kSegWarps * 32, 1) l1gs_seg_kernel(const hsseg
     rs.lo = p.lo;
     rs.up = p.up;
     const int32_t my_groups = rs.q0 < p.gend ? (p.gend - 1 - rs.q0) / rs.qstride + 1 : 0;
-    ys[ps * S + lane] = T(0);
+    ys[ps * S + pl] = T(0);
     rs.init(lane, my_groups);
     bool ok = true;
 
@@ -168,12 +171,12 @@ __global__ void __launch_bounds__(kSegWarps * 32, 1) l1gs_seg_kernel(const hsseg
     int32_t ch = 0;   // chunk of the next slot
     for (int32_t gi = 0; gi < my_groups && ok; ++gi) {
         const int64_t g = rs.q0 + (int64_t)gi * rs.qstride;
-        const int64_t rowbase = g * 32 * (int64_t)ps;
-        const int32_t nrows = (int32_t)min((int64_t)32 * ps, (int64_t)p.n - rowbase);
+        const int64_t rowbase = g * G * (int64_t)ps;
+        const int32_t nrows = (int32_t)min((int64_t)G * ps, (int64_t)p.n - rowbase);
         // x and D_Dl1 of the group's rows -> [li][partition], all loads in flight at once
         if constexpr (sizeof(IO) == sizeof(T)) {
             int pp = lane / ps, li = lane - pp * ps;
-            for (int t = lane; t < 32 * ps; t += 32) {
+            for (int t = lane; t < G * ps; t += 32) {
                 T* yd = ys + li * S + pp;
                 T* dd = ds + li * S + pp;
                 if (t < nrows) {
@@ -192,7 +195,7 @@ __global__ void __launch_bounds__(kSegWarps * 32, 1) l1gs_seg_kernel(const hsseg
             }
         } else {   // FP64 vectors, FP32 smoother: x converted on the way in
             int pp = lane / ps, li = lane - pp * ps;
-            for (int t0 = lane; t0 < 32 * ps; t0 += 32 * 8) {
+            for (int t0 = lane; t0 < G * ps; t0 += 32 * 8) {
                 IO xv[8];
 #pragma unroll
                 for (int u = 0; u < 8; ++u) {
@@ -202,7 +205,7 @@ __global__ void __launch_bounds__(kSegWarps * 32, 1) l1gs_seg_kernel(const hsseg
 #pragma unroll
                 for (int u = 0; u < 8; ++u) {
                     const int t = t0 + 32 * u;
-                    if (t < 32 * ps) {
+                    if (t < G * ps) {
                         T* dd = ds + li * S + pp;
                         ys[li * S + pp] = (T)xv[u];
                         if (t < nrows)
@@ -219,23 +222,25 @@ __global__ void __launch_bounds__(kSegWarps * 32, 1) l1gs_seg_kernel(const hsseg
                 }
             }
         }
-        // slots per row of each direction: bytes [4 lane, 4 lane + 4) of the group's row list
-        uint32_t mw[NDIR];
+        // slots per row of each direction, staged as words
 #pragma unroll
         for (int d = 0; d < NDIR; ++d)
-            mw[d] = 4 * lane < psq ? *reinterpret_cast<const uint32_t*>(rs.dir(d).maxc + g * psq + 4 * lane) : 0u;
+            for (int w = lane; w < psq / 4; w += 32)
+                reinterpret_cast<uint32_t*>(mxs + d * psq)[w] =
+                    reinterpret_cast<const uint32_t*>(rs.dir(d).maxc + g * psq)[w];
         hsdev::cp_async_wait_all();
         __syncwarp();
-        T* yk = ys + lane;
-        const T* dk = ds + lane;
+        T* yk = ys + pl;
+        const T* dk = ds + pl;
 #pragma unroll
         for (int d = 0; d < NDIR; ++d) {
             if (!ok) break;
             const bool lowerdir = SWEEP == 0 || (SWEEP == 2 && d == 0);
+            const uint8_t* mx = mxs + d * psq;
             int wi = 0;   // slot of the next entry inside chunk ch
             for (int t = 0; t < ps; ++t) {
                 const int li = lowerdir ? t : ps - 1 - t;
-                const int m = (int)((__shfl_sync(FULL, mw[d], li >> 2) >> ((li & 3) * 8)) & 0xffu);
+                const int m = mx[li];
                 const T dv = dk[li * S];
                 T yi = yk[li * S];
                 T acc = T(0);
@@ -245,8 +250,8 @@ __global__ void __launch_bounds__(kSegWarps * 32, 1) l1gs_seg_kernel(const hsseg
                         break;
                     }
                     const unsigned char* sp = rs.slot(ch, wi);
-                    const T a = reinterpret_cast<const T*>(sp)[lane];
-                    const int col = reinterpret_cast<const uint16_t*>(sp + 32 * sizeof(T))[lane];
+                    const T a = reinterpret_cast<const T*>(sp)[pl];
+                    const int col = reinterpret_cast<const uint16_t*>(sp + G * sizeof(T))[pl];
                     acc = add_rn(acc, mul_rn(a, yk[col * S]));
                     // a finished chunk goes back at once: a row may span more chunks than the ring holds
                     if (++wi == K) {
@@ -416,18 +421,21 @@ __global__ void __launch_bounds__(kSegWarps * 32, 1) l1gs_seg_ps_kernel(const hs
     }
 }
 
-// Shared-memory slice of a warp: ring, barriers, table, y (+ D_Dl1 for the
-// runtime-partsize kernel).
+// Shared-memory slice of a warp: ring, barriers, table, y (+ D_Dl1 and the
+// staged row counts for the runtime-partsize kernel).
 template <typename T>
-void seg_geometry(hsseg::Params& p, int S, bool with_d) {
-    constexpr uint32_t CHB = seg_k<T>() * 32 * (sizeof(T) + 2);
+void seg_geometry(hsseg::Params& p, int G, bool with_d) {
+    const uint32_t CHB = (uint32_t)(seg_k<T>() * (32 / G) * G * (sizeof(T) + 2));
+    const uint32_t S = with_d ? G + 1 : 32;
     p.nst = 4;
     p.ring_off = 0;
     p.bars_off = p.nst * CHB;
     p.tab_off = (p.bars_off + 8 * p.nst + 15) / 16 * 16;
     p.ys_off = p.tab_off + kTab * (uint32_t)sizeof(TabEnt);
     p.ds_off = (p.ys_off + (uint32_t)(S * (p.ps + 1) * sizeof(T)) + 15) / 16 * 16;
-    p.warp_bytes = (p.ds_off + (with_d ? (uint32_t)(S * p.ps * sizeof(T)) : 0u) + 127) / 128 * 128;
+    p.mx_off = (p.ds_off + (with_d ? (uint32_t)(S * p.ps * sizeof(T)) : 0u) + 15) / 16 * 16;
+    const uint32_t psq = (uint32_t)((p.ps + 3) & ~3);
+    p.warp_bytes = (p.mx_off + (with_d ? 2 * psq : 0u) + 127) / 128 * 128;
 }
 
 template <typename K>
@@ -459,9 +467,26 @@ template <typename T, typename IO, int SWEEP>
 int launch_t(const hsseg::View& view, hsseg::Params& p, cudaStream_t st) {
     (void)view;
     switch (p.ps) {
-        case 8: seg_geometry<T>(p, 32, false); return launch_kernel(l1gs_seg_ps_kernel<T, IO, SWEEP, 8>, p, st);
-        case 16: seg_geometry<T>(p, 32, false); return launch_kernel(l1gs_seg_ps_kernel<T, IO, SWEEP, 16>, p, st);
-        default: seg_geometry<T>(p, 33, true); return launch_kernel(l1gs_seg_kernel<T, IO, SWEEP>, p, st);
+        case 8:
+            if (p.G == 32) {
+                seg_geometry<T>(p, 32, false);
+                return launch_kernel(l1gs_seg_ps_kernel<T, IO, SWEEP, 8>, p, st);
+            }
+            break;
+        case 16:
+            if (p.G == 32) {
+                seg_geometry<T>(p, 32, false);
+                return launch_kernel(l1gs_seg_ps_kernel<T, IO, SWEEP, 16>, p, st);
+            }
+            break;
+        default: break;
+    }
+    seg_geometry<T>(p, p.G, true);
+    switch (p.G) {
+        case 32: return launch_kernel(l1gs_seg_kernel<T, IO, SWEEP, 32>, p, st);
+        case 16: return launch_kernel(l1gs_seg_kernel<T, IO, SWEEP, 16>, p, st);
+        case 8: return launch_kernel(l1gs_seg_kernel<T, IO, SWEEP, 8>, p, st);
+        default: return launch_kernel(l1gs_seg_kernel<T, IO, SWEEP, 4>, p, st);
     }
 }
 
@@ -482,8 +507,10 @@ template <typename TM, typename TS>
 int build(int32_t n, int32_t ps, int32_t nparts, const int32_t* rp, const int32_t* ci, const TM* v, bool lower,
           bool upper, View* view, cudaStream_t st) {
     if (ps > kMaxPartsize) return hs::set_error(HS_ERR_UNSUPPORTED, "segment lists need partsize <= %d", kMaxPartsize);
-    const int32_t ngroups = (int32_t)(((int64_t)nparts + 31) / 32);
+    const int32_t G = pick_group(ps, sizeof(TS));
+    const int32_t ngroups = (int32_t)(((int64_t)nparts + G - 1) / G);
     const int32_t psq = (ps + 3) & ~3;
+    view->G = G;
     view->ngroups = ngroups;
     const int64_t items = (int64_t)ngroups * ps;
     Tmp tmp;
@@ -496,7 +523,7 @@ int build(int32_t n, int32_t ps, int32_t nparts, const int32_t* rp, const int32_
         return rc;
     seg_count_kernel<<<grid_of(n), 256, 0, st>>>(n, ps, rp, ci, cntL, qL, cntU, qU);
     HS_LAUNCH_CHECK("seg_count_kernel");
-    constexpr int64_t SB = 32 * (sizeof(TS) + 2);
+    const int64_t SB = G * (int64_t)(sizeof(TS) + 2);
     for (int d = 0; d < 2; ++d) {
         if ((d == 0 && !lower) || (d == 1 && !upper)) continue;
         Dir& dd = d == 0 ? view->lo : view->up;
@@ -506,7 +533,7 @@ int build(int32_t n, int32_t ps, int32_t nparts, const int32_t* rp, const int32_
             (rc = dalloc(view, &dd.base, 8 * (size_t)ngroups)))
             return rc;
         HS_CUDA(cudaMemsetAsync(dd.maxc, 0, (size_t)ngroups * psq, st));
-        seg_max_kernel<<<grid_of(items * 32), 256, 0, st>>>(n, ps, psq, nparts, items, cnt, dd.maxc);
+        seg_max_kernel<<<grid_of(items * 32), 256, 0, st>>>(n, ps, psq, G, nparts, items, cnt, dd.maxc);
         HS_LAUNCH_CHECK("seg_max_kernel");
         seg_off_kernel<<<grid_of(ngroups), 256, 0, st>>>(ngroups, ps, psq, dd.maxc, off, dd.total, d == 1);
         HS_LAUNCH_CHECK("seg_off_kernel");
@@ -524,10 +551,10 @@ int build(int32_t n, int32_t ps, int32_t nparts, const int32_t* rp, const int32_
         if ((rc = dalloc(view, &dd.stream, (size_t)(acc * SB)))) return rc;
         HS_CUDA(cudaMemsetAsync(dd.stream, 0, (size_t)(acc * SB), st));
         if (acc > 0) {
-            seg_pad_kernel<TS><<<grid_of(acc * 32), 256, 0, st>>>(acc, ps, dd.stream);
+            seg_pad_kernel<TS><<<grid_of(acc * G), 256, 0, st>>>(acc, ps, G, dd.stream);
             HS_LAUNCH_CHECK("seg_pad_kernel");
         }
-        seg_scatter_kernel<TM, TS><<<grid_of(n), 256, 0, st>>>(n, ps, ci, v, cnt, q0, off, dd.base, dd.stream);
+        seg_scatter_kernel<TM, TS><<<grid_of(n), 256, 0, st>>>(n, ps, G, ci, v, cnt, q0, off, dd.base, dd.stream);
         HS_LAUNCH_CHECK("seg_scatter_kernel");
         HS_CUDA(cudaStreamSynchronize(st));   // the host base vector and the scratch go out of scope
     }
@@ -566,6 +593,7 @@ int launch(int sdt, int io, int sweep, const View& view, int32_t n, int32_t ps, 
     p.x = x;
     p.y = y;
     p.err = err;
+    p.G = view.G;
     p.vec_io = ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y) | reinterpret_cast<uintptr_t>(D)) & 15u) == 0;
     if (sdt == HS_F64 && io == HS_F64) return launch_io<double, double>(sweep, view, p, st);
     if (sdt == HS_F32 && io == HS_F32) return launch_io<float, float>(sweep, view, p, st);

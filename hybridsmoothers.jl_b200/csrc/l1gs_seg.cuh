@@ -29,7 +29,16 @@
 
 namespace hsseg {
 
-constexpr int kMaxPartsize = 128;                                    // y and D_Dl1 slices in shared memory
+constexpr int kMaxPartsize = 512;   // y and D_Dl1 of a group in shared memory
+
+// Partitions per group (and per warp): the largest of 32, 16, 8, 4 whose y
+// and D_Dl1 slices ((2 ps + 1) rows of G + 1 values) take at most 24 KiB, so
+// several warps stay resident per SM.
+inline int pick_group(int ps, size_t es) {
+    int G = 32;
+    while (G > 4 && (size_t)(2 * ps + 1) * (G + 1) * es > 24 * 1024) G /= 2;
+    return G;
+}
 
 // Device arrays of a segment-list view (one direction).
 struct Dir {
@@ -42,6 +51,7 @@ struct Dir {
 
 struct View {
     Dir lo, up;
+    int32_t G = 32;        // partitions per group (lanes that carry a partition)
     int32_t ngroups = 0;
     int64_t bytes = 0;   // device memory held
 };
@@ -62,7 +72,8 @@ struct Params {
     void* y;
     int32_t* err;
     int32_t vec_io;   // x, y and D_Dl1 are 16-byte aligned
-    uint32_t warp_bytes, ring_off, bars_off, tab_off, ys_off, ds_off, nst;
+    int32_t G;        // partitions per group
+    uint32_t warp_bytes, ring_off, bars_off, tab_off, ys_off, ds_off, mx_off, nst;
 };
 
 int launch(int sdt, int io, int sweep, const View& view, int32_t n, int32_t ps, int32_t gbeg, int32_t gend,

@@ -19,11 +19,11 @@ from hsb200 import workloads as W
 from oracle import hs_oracle as O
 
 
-def build(A_rows, ps, dtype):
+def build(A_rows, ps, dtype, G=32):
     R = A_rows
     n = R.shape[0]
     nparts = -(-n // ps)
-    ngroups = -(-nparts // 32)
+    ngroups = -(-nparts // G)
     cntL = np.zeros(n, int)
     qL = np.zeros(n, int)
     cntU = np.zeros(n, int)
@@ -48,12 +48,12 @@ def build(A_rows, ps, dtype):
     dirs = {}
     for name, cnt, q0, desc in (("lo", cntL, qL, False), ("up", cntU, qU, True)):
         maxc = np.zeros((ngroups, ps), int)
-        cnti = np.zeros((ngroups, ps, 32), int)
+        cnti = np.zeros((ngroups, ps, G), int)
         for g in range(ngroups):
             for li in range(ps):
                 vals = []
-                for lane in range(32):
-                    k = g * 32 + lane
+                for lane in range(G):
+                    k = g * G + lane
                     row = k * ps + li
                     c = cnt[row] if (k < nparts and row < n) else 0
                     cnti[g, li, lane] = c
@@ -70,11 +70,11 @@ def build(A_rows, ps, dtype):
             total[g] = acc
         base = np.concatenate([[0], np.cumsum(total)[:-1]]).astype(int)
         slots = int(total.sum())
-        vals = np.zeros((slots, 32), dtype=dtype)
-        cols = np.full((slots, 32), ps, dtype=np.int64)
+        vals = np.zeros((slots, G), dtype=dtype)
+        cols = np.full((slots, G), ps, dtype=np.int64)
         for i in range(n):
             k, li = divmod(i, ps)
-            g, lane = divmod(k, 32)
+            g, lane = divmod(k, G)
             s = k * ps
             for t in range(cnt[i]):
                 q = q0[i] + t
@@ -114,11 +114,11 @@ class Ring:
         assert self.owner[c % self.nst] == c and self.freed <= c < self.ready
 
 
-def emulate(A_rows, ps, sweep, D, x, dtype, warps=2, K=None):
+def emulate(A_rows, ps, sweep, D, x, dtype, warps=2, K=None, G=32):
     T = np.dtype(dtype).type
-    if K is None:   # slots per chunk of the kernels: 4 (FP64), 6 (FP32)
-        K = 4 if np.dtype(dtype).itemsize == 8 else 6
-    dirs, ngroups = build(A_rows, ps, dtype)
+    if K is None:   # slots per chunk of the kernels: 4 (FP64), 6 (FP32), times 32 / G
+        K = (4 if np.dtype(dtype).itemsize == 8 else 6) * (32 // G)
+    dirs, ngroups = build(A_rows, ps, dtype, G)
     n = A_rows.shape[0]
     order = {"forward": ["lo"], "backward": ["up"], "symmetric": ["lo", "up"]}[sweep]
     y = np.zeros(n, dtype=dtype)
@@ -132,11 +132,11 @@ def emulate(A_rows, ps, sweep, D, x, dtype, warps=2, K=None):
         ring = Ring(chunks)
         ch = 0
         for g in groups:
-            ys = np.zeros((ps + 1, 32), dtype=dtype)   # row ps: the padding slots' target, +0
-            ds = np.ones((ps, 32), dtype=dtype)
-            for lane in range(32):
+            ys = np.zeros((ps + 1, G), dtype=dtype)   # row ps: the padding slots' target, +0
+            ds = np.ones((ps, G), dtype=dtype)
+            for lane in range(G):
                 for li in range(ps):
-                    row = (g * 32 + lane) * ps + li
+                    row = (g * G + lane) * ps + li
                     if row < n:
                         ys[li, lane] = T(x[row])
                         ds[li, lane] = D[row]
@@ -150,14 +150,14 @@ def emulate(A_rows, ps, sweep, D, x, dtype, warps=2, K=None):
                     for li in rows:
                         m = dd["maxc"][g, li]
                         assert dd["off"][g, li] == o
-                        acc = np.zeros(32, dtype=dtype)
+                        acc = np.zeros(G, dtype=dtype)
                         for k in range(m):
                             assert (ch - start) * K + wi == o + k
                             ring.wait_upto(ch)
                             ring.check(ch)
                             a = dd["vals"][dd["base"][g] + o + k]
                             col = dd["cols"][dd["base"][g] + o + k]
-                            acc = acc + a * ys[col, np.arange(32)]
+                            acc = acc + a * ys[col, np.arange(G)]
                             wi += 1
                             if wi == K:
                                 wi = 0
@@ -172,9 +172,9 @@ def emulate(A_rows, ps, sweep, D, x, dtype, warps=2, K=None):
                     ch += 1
                     ring.release(ch)
                 assert ch - start == -(-int(dd["total"][g]) // K)
-            for lane in range(32):
+            for lane in range(G):
                 for li in range(ps):
-                    row = (g * 32 + lane) * ps + li
+                    row = (g * G + lane) * ps + li
                     if row < n:
                         y[row] = ys[li, lane]
         assert ring.ready == ring.issued == len(chunks)
@@ -231,3 +231,26 @@ def test_seg_emulation_nonfinite(sweep):
         want = ref.ldiv(x)
     got = emulate(rows_of(A, True), ps, sweep, ref.D, x, np.float64)
     np.testing.assert_array_equal(got, want)
+
+
+def pick_group(ps, es):
+    """hsseg::pick_group: the largest of 32, 16, 8, 4 with y and D_Dl1 of a
+    group in at most 24 KiB."""
+    G = 32
+    while G > 4 and (2 * ps + 1) * (G + 1) * es > 24 * 1024:
+        G //= 2
+    return G
+
+
+@pytest.mark.parametrize("ps,n", [(64, 3000), (128, 3000), (256, 5000), (300, 4000), (512, 6000)])
+@pytest.mark.parametrize("sweep", ["forward", "symmetric"])
+def test_seg_emulation_small_groups(ps, n, sweep):
+    """Groups of fewer than 32 partitions (large partsizes)."""
+    G = pick_group(ps, 8)
+    assert G < 32
+    A = W.poisson2d_matrix(int(np.ceil(np.sqrt(n))), eps=0.3)
+    A = W._canon(A[:n, :n].tocsc())
+    x = np.random.default_rng(ps).uniform(-1, 1, n)
+    ref = O.OracleL1GS(A, ps, isSymA=True, sweep=sweep, cache="view")
+    got = emulate(rows_of(A, True), ps, sweep, ref.D, x, np.float64, G=G)
+    np.testing.assert_array_equal(got, ref.ldiv(x))
