@@ -88,7 +88,7 @@ def packed_len(n, ps):
     return ps * (ps - 1) * (nparts - 1) // 2 + lps * (lps - 1) // 2
 
 
-SEG_MAX_PARTSIZE = 128   # views up to this partsize run the segment-list kernel
+SEG_MAX_PARTSIZE = 512   # views up to this partsize run the segment-list kernel
 
 
 def inblock_entries(A, ps):
@@ -101,7 +101,7 @@ def inblock_entries(A, ps):
 
 def algorithmic_bytes(n, nnz, ps, sweep, cache, tv, nonsym=False, inblock=None):
     """Per-apply bytes: packed Tv*(S + 3N) per direction, symmetric fused
-    Tv*(2S + 3N).  View up to partsize 128 (segment lists): the in-block
+    Tv*(2S + 3N).  View up to partsize 512 (segment lists): the in-block
     entries each direction reads, E_d*(Tv + 2) (value and 2-byte local
     column), plus 3*Tv*N; larger partsizes scan the rows:
     nnz*(Ti+Tv) + (N+1)*Ti + 3*Tv*N (+ N*Ti for the non-symmetric
