@@ -70,7 +70,7 @@ __global__ void seg_off_kernel(int32_t ngroups, int32_t ps, int32_t psq, const u
 // the real entries over them.
 template <typename TS>
 __global__ void seg_pad_kernel(int64_t slots, int32_t ps, int32_t G, unsigned char* __restrict__ stream) {
-    const int64_t SB = G * (int64_t)(sizeof(TS) + 2);
+    const int64_t SB = hsseg::slot_bytes(G, sizeof(TS));
     const int64_t m = slots * G;
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < m; e += (int64_t)gridDim.x * blockDim.x) {
         const int64_t slot = e / G, lane = e - slot * G;
@@ -83,7 +83,7 @@ __global__ void seg_scatter_kernel(int32_t n, int32_t ps, int32_t G, const int32
                                    const TM* __restrict__ v, const int32_t* __restrict__ cnt,
                                    const int32_t* __restrict__ q0, const uint16_t* __restrict__ off,
                                    const int64_t* __restrict__ base, unsigned char* __restrict__ stream) {
-    const int64_t SB = G * (int64_t)(sizeof(TS) + 2);
+    const int64_t SB = hsseg::slot_bytes(G, sizeof(TS));
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const int64_t k = i / ps, li = i - k * ps, g = k / G, lane = k - g * G, s = k * ps;
         const int64_t slot0 = base[g] + off[g * ps + li];
@@ -138,7 +138,7 @@ constexpr int seg_k() {
 template <typename T, typename IO, int SWEEP, int G>
 __global__ void __launch_bounds__(kSegWarps * 32, 1) l1gs_seg_kernel(const hsseg::Params p) {
     constexpr int S = G + 1;
-    constexpr uint32_t SB = G * (sizeof(T) + 2);           // bytes per slot
+    constexpr uint32_t SB = hsseg::slot_bytes(G, sizeof(T));   // bytes per slot
     constexpr int K = seg_k<T>() * (32 / G);               // slots per chunk
     constexpr int NDIR = SWEEP == 2 ? 2 : 1;
     extern __shared__ __align__(128) unsigned char smem[];
@@ -301,7 +301,7 @@ __global__ void __launch_bounds__(kSegWarps * 32, 1) l1gs_seg_kernel(const hsseg
 template <typename T, typename IO, int SWEEP, int PS>
 __global__ void __launch_bounds__(kSegWarps * 32, 1) l1gs_seg_ps_kernel(const hsseg::Params p) {
     constexpr int S = 32;
-    constexpr uint32_t SB = 32 * (sizeof(T) + 2);
+    constexpr uint32_t SB = hsseg::slot_bytes(32, sizeof(T));
     constexpr int K = seg_k<T>();
     constexpr int NDIR = SWEEP == 2 ? 2 : 1;
     constexpr int PSQ = (PS + 3) & ~3;   // bytes of a group's row list
@@ -425,7 +425,7 @@ __global__ void __launch_bounds__(kSegWarps * 32, 1) l1gs_seg_ps_kernel(const hs
 // staged row counts for the runtime-partsize kernel).
 template <typename T>
 void seg_geometry(hsseg::Params& p, int G, bool with_d) {
-    const uint32_t CHB = (uint32_t)(seg_k<T>() * (32 / G) * G * (sizeof(T) + 2));
+    const uint32_t CHB = (uint32_t)(seg_k<T>() * (32 / G) * hsseg::slot_bytes(G, sizeof(T)));
     const uint32_t S = with_d ? G + 1 : 32;
     p.nst = 4;
     p.ring_off = 0;
@@ -523,7 +523,7 @@ int build(int32_t n, int32_t ps, int32_t nparts, const int32_t* rp, const int32_
         return rc;
     seg_count_kernel<<<grid_of(n), 256, 0, st>>>(n, ps, rp, ci, cntL, qL, cntU, qU);
     HS_LAUNCH_CHECK("seg_count_kernel");
-    const int64_t SB = G * (int64_t)(sizeof(TS) + 2);
+    const int64_t SB = hsseg::slot_bytes(G, sizeof(TS));
     for (int d = 0; d < 2; ++d) {
         if ((d == 0 && !lower) || (d == 1 && !upper)) continue;
         Dir& dd = d == 0 ? view->lo : view->up;

@@ -10,7 +10,7 @@
 // them, a number of slots equal to the largest count of any of the 32
 // partitions' rows there; slot k of row li holds, for every lane, the value
 // and the local column (j - start) of that partition's k-th in-block entry
-// ([value x 32][column x 32] per slot).  A lane's slots past its own count
+// ([value x 32][column x 32] per slot, padded to 16 bytes).  A lane's slots past its own count
 // hold the value 0 and the column `ps`, a row of y that is always +0: adding
 // 0 * 0 leaves an accumulator unchanged bit for bit (an accumulator that
 // starts at +0 is never -0), so every lane runs the same slots without a
@@ -30,6 +30,12 @@
 namespace hsseg {
 
 constexpr int kMaxPartsize = 512;   // y and D_Dl1 of a group in shared memory
+
+// Bytes of a slot of G partitions: [G values][G uint16 columns], padded to 16
+// bytes so every slot, and every chunk of slots, is a legal 1D bulk copy.
+__host__ __device__ constexpr uint32_t slot_bytes(int G, size_t es) {
+    return (uint32_t)((G * (es + 2) + 15) / 16 * 16);
+}
 
 // Partitions per group (and per warp): the largest of 32, 16, 8, 4 whose y
 // and D_Dl1 slices ((2 ps + 1) rows of G + 1 values) take at most 24 KiB, so

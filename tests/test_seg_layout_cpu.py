@@ -254,3 +254,27 @@ def test_seg_emulation_small_groups(ps, n, sweep):
     ref = O.OracleL1GS(A, ps, isSymA=True, sweep=sweep, cache="view")
     got = emulate(rows_of(A, True), ps, sweep, ref.D, x, np.float64, G=G)
     np.testing.assert_array_equal(got, ref.ldiv(x))
+
+
+def slot_bytes(G, es):
+    """hsseg::slot_bytes: [G values][G uint16 columns], padded to 16 bytes."""
+    return -(-(G * (es + 2)) // 16) * 16
+
+
+def test_seg_copies_are_legal_bulk_copies():
+    """Every slot, chunk and ring stage of the segment-list kernels starts on
+    a 16-byte boundary and is a multiple of 16 bytes long, for every
+    partsize the kernels take and both value types (a 1D bulk copy needs
+    both)."""
+    for es in (8, 4):
+        K0 = 4 if es == 8 else 6
+        for ps in range(2, 513):
+            G = pick_group(ps, es)
+            assert G in (32, 16, 8, 4)
+            SB = slot_bytes(G, es)
+            assert SB % 16 == 0 and SB >= G * (es + 2)
+            K = K0 * (32 // G)
+            CHB = K * SB
+            assert CHB % 16 == 0
+            for slots in range(1, K + 1):   # the last, partial chunk of a pair
+                assert (slots * SB) % 16 == 0
