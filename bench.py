@@ -589,21 +589,23 @@ def suite_batchiter(args):
     from hsb200 import serving
     from hsb200 import workloads as W
     reqs = W.serving_stream(count=48, lo=1e3, hi=2e6)
-    eng = serving.BatchEngine(max_slots=64)
-    for i, (_, A, b) in enumerate(reqs):
-        eng.submit(A, b, i, 8)
-    eng.step(1)
-    torch.cuda.synchronize()
-    steps = args.batch_steps
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        eng.step(8)
-    dt = time.perf_counter() - t0
-    info = eng.info()
-    eng.close()
     rows = sum(A.shape[0] for _, A, _ in reqs)
-    return {"suite": "batchiter", "workload": "48 serving-stream systems, batched FP32-L1GS ps8 PCG",
-            "rows": rows, "active_after": info.active, "us_per_batched_iteration": dt / steps / 8 * 1e6}
+    out = {"suite": "batchiter", "workload": "48 serving-stream systems, batched FP32-L1GS ps8 PCG", "rows": rows}
+    for sched in ("persistent", "segmented"):
+        eng = serving.BatchEngine(max_slots=64, schedule=sched)
+        for i, (_, A, b) in enumerate(reqs):
+            eng.submit(A, b, i, 8)
+        eng.step(8)   # admission, tables, capture
+        torch.cuda.synchronize()
+        steps = args.batch_steps
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            eng.step(8)
+        dt = time.perf_counter() - t0
+        info = eng.info()
+        eng.close()
+        out[sched] = {"active_after": info.active, "us_per_batched_iteration": round(dt / steps / 8 * 1e6, 1)}
+    return out
 
 
 SUITES = {"pcg1d": suite_pcg1d, "pcg128": suite_pcg128, "gmres96": suite_gmres96, "mixed160": suite_mixed160,

@@ -57,7 +57,7 @@ __device__ __forceinline__ void store_dd(double* partials, DD v) {
 
 // Per slot: its CTA range (for the per-slot reductions) and scalars.
 struct SlotDev {
-    int32_t n, blk0, nblk, item0, nitems, pad;
+    int32_t n, blk0, nblk, item0, nitems, ps;
     Scalars* s;
 };
 
@@ -459,6 +459,551 @@ constexpr uint32_t batched_warp_bytes() {
     return ((16 * 32 * 4 * 4) + 8 * 4 + 32 * (PS + 1) * 4 + 127) / 128 * 128;
 }
 
+// ---- persistent schedule: every iteration of every slot in one launch -----
+// The work of a batched iteration is cut into CTA-sized items, ordered by
+// (iteration, phase, slot, chunk), with the phases
+//   0  q = A p and p.q partials            one item per kPairs chunks of kRPC rows
+//   1  x += alpha p, r -= alpha q, r.r     likewise
+//   2  z = M^-1 r and r.z partials         one item per kPW * kGPW groups
+//   3  p = z + beta p                      one item per kPairs chunks
+// CTAs take kTake consecutive items per ticket from one counter.  The first
+// item of a slot's phase (its closer) waits until the slot's previous phase is
+// open and every item of it has been counted, computes that phase's scalar (alpha before
+// phase 1, the convergence test before 2, beta before 3) with the segmented
+// kernels' fixed-order reductions -- the iterates are bitwise those of the
+// segmented schedule -- and publishes the slot's stage, which the phase's
+// other items wait for.  Every wait is for items earlier in the order, taken
+// by running CTAs that never wait for a later item, so a launch cannot
+// deadlock however many CTAs are resident.  A finished item is counted with a
+// fire-and-forget atomic.  Waits poll for at most kStageWaitNs; one that runs
+// out sets the abort word and the launch ends with HS_ERR_TIMEOUT.
+// One kernel holds the registers and shared memory of its largest phase for
+// all phases (2 CTAs of 256 threads per SM), so an item carries two chunks
+// (phase 2: two groups per warp) whose loads are interleaved: the
+// latency-bound SpMV gets its memory parallelism per warp instead of from
+// more warps.  The phase bodies are separate (non-inlined) functions, each
+// with the kernel's 128 registers to itself (inlined together they spilled).
+constexpr int kPW = kT / 32;   // warps per CTA
+constexpr int kPairs = 2;      // chunks per item (phases 0, 1, 3)
+constexpr int kGPW = 2;        // groups per warp per item (phase 2)
+constexpr int kTake = 4;       // items per ticket
+constexpr int32_t kStageDone = 1 << 30;
+constexpr uint64_t kStageWaitNs = 2000000000ull;
+constexpr uint32_t kPWarpBytes = batched_warp_bytes<32>();   // per-warp ring + staging, largest partsize
+
+struct Work {
+    int32_t slot;     // slot index (SlotDev, Scalars, stage words)
+    int16_t phase;    // 0..3 as above
+    int16_t closer;   // the slot's first item of this phase
+    int32_t first;    // phases 0, 1, 3: first BlockMap entry; phase 2: first PrecItem
+    int32_t count;    // chunks (phases 0, 1, 3) or groups (phase 2) in the item
+};
+
+// Control words: [0] ticket, [1] CTAs that left, [2] abort, [3] unused, then
+// per slot s: [4 + 2 s] stage (4 t + phase that may run, or kStageDone),
+// [5 + 2 s] items of the current phase finished.
+constexpr int kCtl = 4;
+
+__device__ __forceinline__ int32_t phase_items(const SlotDev& sd, int ph) {
+    return ph == 2 ? (sd.nitems + kPW * kGPW - 1) / (kPW * kGPW) : (sd.nblk + kPairs - 1) / kPairs;
+}
+
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Thread 0, bounded poll.  Other items: until the stage reaches `need`.
+// Closer: until the previous phase is open (stage need - 1: the counter holds
+// that phase's items, not the phase before it) and its `nprev` items are
+// counted.  Returns 0 (go), 1 (the slot has finished: skip) or 2 (abort).
+// The fence after the observed words orders the CTA's later loads (after the
+// caller's __syncthreads) behind the writes of the CTAs that published them.
+__device__ __forceinline__ int wait_slot(const int32_t* stw, bool closer, int32_t need, int32_t nprev,
+                                         int32_t* abortw, int32_t* err) {
+    const volatile int32_t* vst = stw;
+    const volatile int32_t* vfin = stw + 1;
+    const volatile int32_t* vab = abortw;
+    uint64_t t0 = 0;
+    for (uint32_t k = 0;; ++k) {
+        const int32_t v = *vst;
+        if (v >= kStageDone) {
+            __threadfence();
+            return 1;
+        }
+        if (closer ? (v >= need - 1 && *vfin >= nprev) : v >= need) {
+            __threadfence();
+            return 0;
+        }
+        if (*vab) return 2;
+        if (k == 0) t0 = globaltimer_ns();
+        if ((k & 15) == 15 && globaltimer_ns() - t0 > kStageWaitNs) {
+            atomicExch(abortw, 1);
+            hsdev::report_error(err, hsdev::kErrWaitTimeout);
+            return 2;
+        }
+        __nanosleep(64);
+    }
+}
+
+__device__ __forceinline__ void store_dd_at(double* partials, int32_t idx, DD v) {
+    v = hsdev::block_dd(v);
+    if (threadIdx.x == 0) {
+        partials[2 * idx] = v.s;
+        partials[2 * idx + 1] = v.c;
+    }
+}
+
+// range_sum over partials written in this launch: L2 loads (no stale L1 or
+// read-only-cache copies), same order as range_sum.
+__device__ __noinline__ double range_sum_l2(const double* partials, int32_t first, int32_t count) {
+    DD v{0.0, 0.0};
+    const double2* p2 = reinterpret_cast<const double2*>(partials) + first;
+    for (int base = threadIdx.x; base < count; base += 8 * blockDim.x) {
+        double2 w[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            if (base + k * (int)blockDim.x < count) w[k] = __ldcg(p2 + base + k * blockDim.x);
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            if (base + k * (int)blockDim.x < count) v = hsdev::dd_add(v, DD{w[k].x, w[k].y});
+    }
+    return hsdev::dd_value(hsdev::block_dd(v));
+}
+
+// Phase 0 over `count` chunks of one slot (seg_spmv_dot's arithmetic per
+// chunk): the two chunks' 32-row slices are folded side by side, so a warp
+// keeps two dependent load chains in flight.
+__device__ __noinline__ void pers_spmv(const BlockMap* __restrict__ mm, int count, double* partials, int32_t idx) {
+    constexpr int NS = kRPC / kT;
+    constexpr int KU = 8;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const BlockMap ma = mm[0];
+    const BlockMap mb = mm[count > 1 ? 1 : 0];
+    const int64_t nsl = ((int64_t)ma.n + 31) / 32;
+    int64_t oa0[NS], oa1[NS], ob0[NS], ob1[NS];
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+        const int64_t sa = ((int64_t)ma.row0 >> 5) + k * kPW + warp;
+        const int64_t sb = ((int64_t)mb.row0 >> 5) + k * kPW + warp;
+        oa0[k] = sa < nsl ? __ldg(ma.soff + sa) : 0;
+        oa1[k] = sa < nsl ? __ldg(ma.soff + sa + 1) : 0;
+        ob0[k] = count > 1 && sb < nsl ? __ldg(mb.soff + sb) : 0;
+        ob1[k] = count > 1 && sb < nsl ? __ldg(mb.soff + sb + 1) : 0;
+    }
+    const double* p = ma.p;   // written in this launch: plain loads
+    DD pa{0.0, 0.0}, pb{0.0, 0.0};
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+        const int64_t ra0 = (int64_t)ma.row0 + (k * kPW + warp) * 32;
+        const int64_t rb0 = (int64_t)mb.row0 + (k * kPW + warp) * 32;
+        const bool va = ra0 < ma.n, vb = count > 1 && rb0 < mb.n;
+        if (!va && !vb) break;   // uniform over the warp
+        const int32_t wa = va ? (int32_t)((oa1[k] - oa0[k]) / 32) : 0;
+        const int32_t wb = vb ? (int32_t)((ob1[k] - ob0[k]) / 32) : 0;
+        const int32_t* __restrict__ cpa = ma.scol + oa0[k] + lane;
+        const double* __restrict__ vpa = ma.sval + oa0[k] + lane;
+        const int32_t* __restrict__ cpb = mb.scol + ob0[k] + lane;
+        const double* __restrict__ vpb = mb.sval + ob0[k] + lane;
+        double acca = 0.0, accb = 0.0;
+        const int32_t w = wa > wb ? wa : wb;
+        for (int32_t j = 0; j < w; j += KU) {   // slice_row_fold's order, per slice
+            int32_t ca[KU], cb[KU];
+            double aa[KU], ab[KU], xa[KU], xb[KU];
+#pragma unroll
+            for (int u = 0; u < KU; ++u) {
+                ca[u] = j + u < wa ? __ldg(cpa + 32 * (j + u)) : -1;
+                aa[u] = j + u < wa ? __ldg(vpa + 32 * (j + u)) : 0.0;
+                cb[u] = j + u < wb ? __ldg(cpb + 32 * (j + u)) : -1;
+                ab[u] = j + u < wb ? __ldg(vpb + 32 * (j + u)) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < KU; ++u) {
+                xa[u] = ca[u] >= 0 ? p[ca[u]] : 0.0;
+                xb[u] = cb[u] >= 0 ? p[cb[u]] : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < KU; ++u) {
+                if (ca[u] >= 0) acca = __dadd_rn(acca, __dmul_rn(aa[u], xa[u]));
+                if (cb[u] >= 0) accb = __dadd_rn(accb, __dmul_rn(ab[u], xb[u]));
+            }
+        }
+        const int64_t ra = ra0 + lane, rb = rb0 + lane;
+        if (va && ra < ma.n) {
+            ma.q[ra] = acca;
+            hsdev::dd_add_prod(pa, p[ra], acca);
+        }
+        if (vb && rb < mb.n) {
+            mb.q[rb] = accb;
+            hsdev::dd_add_prod(pb, p[rb], accb);
+        }
+    }
+    store_dd_at(partials, idx, pa);
+    if (count > 1) store_dd_at(partials, idx + 1, pb);
+}
+
+// Phase 1 over `count` chunks (seg_update's arithmetic per chunk).
+__device__ __noinline__ void pers_update(const BlockMap* __restrict__ mm, int count, double alpha, double* partials,
+                                         int32_t idx) {
+    BlockMap m[kPairs];
+    double xv[kPairs][kSub], pv[kPairs][kSub], rv[kPairs][kSub], qv[kPairs][kSub];
+#pragma unroll
+    for (int c = 0; c < kPairs; ++c) {
+        m[c] = mm[c < count ? c : 0];
+#pragma unroll
+        for (int k = 0; k < kSub; ++k) {
+            const int i = m[c].row0 + k * kRPB + threadIdx.x;
+            if (c < count && i < m[c].n) {
+                xv[c][k] = m[c].x[i];
+                pv[c][k] = m[c].p[i];
+                rv[c][k] = m[c].r[i];
+                qv[c][k] = m[c].q[i];
+            }
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < kPairs; ++c) {
+        if (c >= count) break;   // uniform
+        DD part{0.0, 0.0};
+#pragma unroll
+        for (int k = 0; k < kSub; ++k) {
+            const int i = m[c].row0 + k * kRPB + threadIdx.x;
+            if (i < m[c].n) {
+                m[c].x[i] = __dadd_rn(xv[c][k], __dmul_rn(alpha, pv[c][k]));
+                const double ri = __dsub_rn(rv[c][k], __dmul_rn(alpha, qv[c][k]));
+                m[c].r[i] = ri;
+                hsdev::dd_add_prod(part, ri, ri);
+            }
+        }
+        store_dd_at(partials, idx + c, part);
+    }
+}
+
+// Phase 3 over `count` chunks (seg_p's arithmetic).
+__device__ __noinline__ void pers_p(const BlockMap* __restrict__ mm, int count, double beta) {
+    BlockMap m[kPairs];
+    double zv[kPairs][kSub], pv[kPairs][kSub];
+#pragma unroll
+    for (int c = 0; c < kPairs; ++c) {
+        m[c] = mm[c < count ? c : 0];
+#pragma unroll
+        for (int k = 0; k < kSub; ++k) {
+            const int i = m[c].row0 + k * kRPB + threadIdx.x;
+            if (c < count && i < m[c].n) {
+                zv[c][k] = m[c].z[i];
+                pv[c][k] = m[c].p[i];
+            }
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < kPairs; ++c) {
+#pragma unroll
+        for (int k = 0; k < kSub; ++k) {
+            const int i = m[c].row0 + k * kRPB + threadIdx.x;
+            if (c < count && i < m[c].n) m[c].p[i] = __dadd_rn(zv[c][k], __dmul_rn(beta, pv[c][k]));
+        }
+    }
+}
+
+// Phase 2 for up to kGPW groups of one warp (l1gs_batched_kernel's
+// arithmetic per group), streamed through the warp's ring: the next group's
+// first tiles are in flight while the current one is solved.  The ring
+// position `c` runs on across items (stage c % 4, parity (c / 4) % 2), so
+// every tile is issued and waited for exactly once.  False after a bounded
+// wait ran out.
+template <int PS>
+__device__ __noinline__ bool pers_apply(const PrecItem* __restrict__ items, int64_t g0, int ng, unsigned char* wbase,
+                                        uint32_t& c, double* rz_part) {
+    constexpr int E = kBatchE;
+    constexpr int STAGES = 4;
+    constexpr int TLEN = PS * (PS - 1) / 2;
+    constexpr int NT = (TLEN + E - 1) / E;
+    constexpr uint32_t NTPG = 2 * NT;
+    constexpr int XS = PS + 1;
+    constexpr uint32_t kRing = E * 32 * 4 * STAGES;
+    static_assert(kRing + 8 * STAGES + 32 * XS * 4 <= kPWarpBytes, "per-warp shared memory");
+    const int lane = threadIdx.x & 31;
+    float* ring = reinterpret_cast<float*>(wbase);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(wbase + kRing);
+    float* xs = reinterpret_cast<float*>(wbase + kRing + 8 * STAGES);
+    const uint32_t c0 = c, end = c0 + (uint32_t)ng * NTPG;
+    const float* st0 = items[g0].ST;
+    const float* st1 = ng > 1 ? items[g0 + kPW].ST : st0;
+    auto issue = [&](uint32_t k) {   // lane 0
+        const uint32_t r = k - c0;
+        const uint32_t j = r / NTPG;
+        const float* src = (j == 0 ? st0 : st1) + (int64_t)(r - j * NTPG) * E * 32;
+        const uint32_t s = k & (STAGES - 1);
+        hsdev::mbar_arrive_expect_tx(bars + s, (uint32_t)(E * 32 * 4));
+        hsdev::bulk_load(ring + s * (E * 32), src, (uint32_t)(E * 32 * 4), bars + s);
+    };
+    uint32_t last_wait = c0;
+    auto wait = [&](uint32_t k) -> bool {
+        last_wait = k;
+        const bool ok = hsdev::mbar_wait_bounded(bars + (k & (STAGES - 1)), (k / STAGES) & 1u);
+        return __all_sync(0xffffffffu, ok);
+    };
+    auto release = [&](uint32_t k) {
+        __syncwarp();
+        if (lane == 0 && k + STAGES < end) {
+            hsdev::fence_proxy_async_smem();
+            issue(k + STAGES);
+        }
+    };
+    // The ring's stages were last read by this warp's previous item.
+    __syncwarp();
+    if (lane == 0) {
+        hsdev::fence_proxy_async_smem();
+        for (uint32_t k = c0; k < end && k < c0 + STAGES; ++k) issue(k);
+    }
+    for (int j = 0; j < ng; ++j) {
+        const int64_t gi = g0 + (int64_t)j * kPW;
+        const PrecItem it = items[gi];
+        const uint32_t cj = c0 + (uint32_t)j * NTPG;
+        // D_Dl1 in registers up to partsize 16; above, read at each use (L1)
+        constexpr bool kDReg = PS <= 16;
+        float d[kDReg ? PS : 1];
+        if (kDReg) {
+#pragma unroll
+            for (int li = 0; li < PS; ++li) d[kDReg ? li : 0] = __ldg(it.Di + (int64_t)li * it.npad + lane);
+        }
+        auto dl = [&](int li) { return kDReg ? d[kDReg ? li : 0] : __ldg(it.Di + (int64_t)li * it.npad + lane); };
+#pragma unroll
+        for (int m = 0; m < PS; ++m) {
+            const int t = lane + 32 * m;
+            xs[(t / PS) * XS + (t % PS)] = t < it.rows ? (float)it.x[t] : 0.0f;
+        }
+        __syncwarp();
+        float yv[PS];
+#pragma unroll
+        for (int li = 0; li < PS; ++li) yv[li] = xs[lane * XS + li];
+#pragma unroll
+        for (int li = 0; li < PS; ++li) {
+            float acc = 0.0f;
+#pragma unroll
+            for (int lj = 0; lj < li; ++lj) {
+                const int e = li * (li - 1) / 2 + lj;
+                const uint32_t k = cj + e / E;
+                if (e % E == 0 && !wait(k)) goto timeout;
+                acc = __fadd_rn(acc, __fmul_rn(ring[(k & (STAGES - 1)) * (E * 32) + (e % E) * 32 + lane], yv[lj]));
+                if (e % E == E - 1 || e == TLEN - 1) release(k);
+            }
+            yv[li] = __fdiv_rn(__fsub_rn(yv[li], acc), dl(li));
+        }
+#pragma unroll
+        for (int li = 0; li < PS; ++li) yv[li] = __fmul_rn(dl(li), yv[li]);
+#pragma unroll
+        for (int li = PS - 1; li >= 0; --li) {
+            float acc = 0.0f;
+#pragma unroll
+            for (int lj = li + 1; lj < PS; ++lj) {
+                const int q = PS - 1 - li;
+                const int e = q * (q - 1) / 2 + (lj - li - 1);
+                const uint32_t k = cj + NT + e / E;
+                if (e % E == 0 && !wait(k)) goto timeout;
+                acc = __fadd_rn(acc, __fmul_rn(ring[(k & (STAGES - 1)) * (E * 32) + (e % E) * 32 + lane], yv[lj]));
+                if (e % E == E - 1 || e == TLEN - 1) release(k);
+            }
+            yv[li] = __fdiv_rn(__fsub_rn(yv[li], acc), dl(li));
+        }
+        __syncwarp();
+#pragma unroll
+        for (int li = 0; li < PS; ++li) xs[lane * XS + li] = yv[li];
+        __syncwarp();
+        DD part{0.0, 0.0};   // this group's share of r.z
+#pragma unroll
+        for (int m = 0; m < PS; ++m) {
+            const int t = lane + 32 * m;
+            if (t < it.rows) {
+                const double z = (double)xs[(t / PS) * XS + (t % PS)];
+                it.y[t] = z;
+                hsdev::dd_add_prod(part, it.x[t], z);
+            }
+        }
+        part = hsdev::warp_dd(part);
+        if (lane == 0) {
+            rz_part[2 * gi] = part.s;
+            rz_part[2 * gi + 1] = part.c;
+        }
+        __syncwarp();
+    }
+    c = end;
+    return true;
+timeout:
+    // let the copies in flight land before the shared memory is left
+    for (uint32_t k = last_wait; k < end && k < last_wait + STAGES; ++k)
+        (void)hsdev::mbar_wait_bounded(bars + (k & (STAGES - 1)), (k / STAGES) & 1u);
+    c = end;
+    return false;
+}
+
+__device__ __forceinline__ void reset_stages(int32_t* ctl, const Scalars* scal, const int32_t* active, int32_t nactive,
+                                             int first, int stride) {
+    for (int32_t a = first; a < nactive; a += stride) {
+        const int32_t s = active[a];
+        const int done = *reinterpret_cast<const volatile int*>(&scal[s].done);
+        ctl[kCtl + 2 * s] = done ? kStageDone : 0;
+        ctl[kCtl + 2 * s + 1] = 0;
+    }
+}
+
+// Before the first launch over a new active set.
+__global__ void persist_reset(int32_t* ctl, const Scalars* scal, const int32_t* active, int32_t nactive) {
+    if (threadIdx.x == 0) {
+        ctl[0] = 0;
+        ctl[1] = 0;
+    }
+    reset_stages(ctl, scal, active, nactive, threadIdx.x, blockDim.x);
+}
+
+__global__ void __launch_bounds__(kT, 2)
+    batch_persistent_kernel(const Work* __restrict__ work, int32_t nwork, int32_t iters,
+                            const SlotDev* __restrict__ slots, const int32_t* __restrict__ active, int32_t nactive,
+                            const BlockMap* __restrict__ map, const PrecItem* __restrict__ items, double* partials,
+                            double* rz_part, Scalars* scal, int32_t* ctl, int32_t maxit, int32_t* err) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ int32_t sh_tk, sh_flag, sh_bad;
+    __shared__ double sh_val;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned char* wbase = smem + (size_t)warp * kPWarpBytes;
+    if (lane == 0) {
+        uint64_t* bars = reinterpret_cast<uint64_t*>(wbase + kBatchE * 32 * 4 * 4);
+        for (int s = 0; s < 4; ++s) hsdev::mbar_init(bars + s, 1);
+        hsdev::fence_barrier_init();
+    }
+    if (threadIdx.x == 0) sh_bad = 0;
+    __syncthreads();
+    uint32_t c = 0;   // this warp's ring position
+    int32_t* abortw = ctl + 2;
+    const int64_t total = (int64_t)nwork * iters;
+    bool stop = false;
+    while (!stop) {
+        if (threadIdx.x == 0) sh_tk = atomicAdd(ctl, 1);
+        __syncthreads();
+        const int64_t w0 = (int64_t)sh_tk * kTake;
+        if (w0 >= total) break;   // uniform
+        const int64_t w1 = w0 + kTake < total ? w0 + kTake : total;
+        for (int64_t wi = w0; wi < w1; ++wi) {
+            const int32_t t = (int32_t)(wi / nwork);
+            const Work wk = work[wi - (int64_t)t * nwork];
+            const int32_t need = 4 * t + wk.phase;
+            int32_t* stw = ctl + kCtl + 2 * wk.slot;
+            const SlotDev sd = slots[wk.slot];
+            // The closer of phase 0 at the launch's first iteration has no
+            // previous phase to close (the stage starts at 0).
+            const bool closing = wk.closer && !(t == 0 && wk.phase == 0);
+            if (threadIdx.x == 0) {
+                const int f = wait_slot(stw, closing, need, closing ? phase_items(sd, (wk.phase + 3) & 3) : 0,
+                                        abortw, err);
+                sh_flag = f;
+                if (f == 0 && !closing && (wk.phase == 1 || wk.phase == 3)) {
+                    const volatile Scalars* vs = sd.s;
+                    sh_val = wk.phase == 1 ? vs->alpha : vs->beta;
+                }
+            }
+            __syncthreads();
+            int flag = sh_flag;
+            __syncthreads();
+            if (flag == 2) {
+                stop = true;
+                break;
+            }
+            if (flag == 1) continue;   // the slot has finished
+            if (closing) {
+                // the previous phase's scalar, then the stage of this phase
+                double v = 0.0;
+                if (wk.phase == 1 || wk.phase == 2) v = range_sum_l2(partials, sd.blk0, sd.nblk);
+                else if (wk.phase == 3) v = range_sum_l2(rz_part, sd.item0, sd.nitems);
+                if (threadIdx.x == 0) {
+                    volatile Scalars* vs = sd.s;
+                    int32_t next = need;
+                    if (wk.phase == 1) {
+                        const double a = __ddiv_rn(vs->rz, v);
+                        vs->pq = v;
+                        vs->alpha = a;
+                        sh_val = a;
+                    } else if (wk.phase == 2) {
+                        const int32_t itn = vs->it + 1;
+                        vs->it = itn;
+                        vs->rr = v;
+                        if (sqrt(v) <= __dmul_rn(vs->rtol, sqrt(vs->bb))) {
+                            vs->done = 1;
+                            vs->conv_it = itn;
+                            next = kStageDone;
+                        } else if (itn >= maxit) {
+                            vs->done = 2;   // gave up
+                            vs->conv_it = itn;
+                            next = kStageDone;
+                        }
+                    } else if (wk.phase == 3) {
+                        const double bt = __ddiv_rn(v, vs->rz);
+                        vs->beta = bt;
+                        vs->rz = v;
+                        sh_val = bt;
+                    }
+                    *reinterpret_cast<volatile int32_t*>(stw + 1) = 0;
+                    __threadfence();
+                    *reinterpret_cast<volatile int32_t*>(stw) = next;
+                    sh_flag = next >= kStageDone ? 1 : 0;
+                }
+                __syncthreads();
+                flag = sh_flag;
+                __syncthreads();
+                if (flag) continue;   // converged (or stopped) at this check
+            }
+            const double val = sh_val;
+            switch (wk.phase) {
+                case 0: pers_spmv(map + wk.first, wk.count, partials, wk.first); break;
+                case 1: pers_update(map + wk.first, wk.count, val, partials, wk.first); break;
+                case 2:
+                    if (warp < wk.count) {
+                        const int ng = warp + kPW < wk.count ? 2 : 1;
+                        const int64_t g0 = (int64_t)wk.first + warp;
+                        bool ok = true;
+                        if (sd.ps == 8) ok = pers_apply<8>(items, g0, ng, wbase, c, rz_part);
+                        else if (sd.ps == 16) ok = pers_apply<16>(items, g0, ng, wbase, c, rz_part);
+                        else ok = pers_apply<32>(items, g0, ng, wbase, c, rz_part);
+                        if (!ok && lane == 0) {
+                            sh_bad = 1;
+                            atomicExch(abortw, 1);
+                        }
+                    }
+                    break;
+                default: pers_p(map + wk.first, wk.count, val); break;
+            }
+            // count the item (no wait for the result)
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                __threadfence();
+                atomicAdd(stw + 1, 1);
+            }
+            if (sh_bad) {   // written before the barrier above
+                stop = true;
+                break;
+            }
+        }
+        __syncthreads();   // sh_tk is rewritten by the next ticket
+    }
+    // The last CTA to leave resets the counters for the next launch.
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (sh_bad) {
+            atomicExch(abortw, 1);
+            hsdev::report_error(err, hsdev::kErrWaitTimeout);
+        }
+        __threadfence();
+        const int32_t prev = atomicAdd(ctl + 1, 1);
+        if (prev == (int32_t)gridDim.x - 1) {
+            __threadfence();
+            reset_stages(ctl, scal, active, nactive, 0, 1);
+            ctl[0] = 0;
+            ctl[1] = 0;
+            __threadfence();
+        }
+    }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -510,8 +1055,14 @@ struct hs_batch_s {
     bool dirty = true;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    int32_t exec_iters = 0;       // iterations in the captured persistent launch
     int32_t* err = nullptr;
     int64_t iterations_run = 0;
+    // persistent schedule (cfg.schedule == HS_BATCH_PERSISTENT)
+    Work* d_work = nullptr;
+    int32_t max_work = 0, nwork = 0, pers_grid = 0;
+    int32_t* d_ctl = nullptr;     // ticket, exits, abort, stage words
+    int32_t* h_ctl = nullptr;     // pinned copy of the abort word after a launch
 };
 
 namespace {
@@ -644,7 +1195,30 @@ int rebuild(hs_batch* B) {
             m.row0 = b * kRPC;
             map.push_back(m);
         }
-        sd[s] = SlotDev{sl.n, sl.blk0, sl.nblk, item0[s], nitem[s], 0, B->d_scal + s};
+        sd[s] = SlotDev{sl.n, sl.blk0, sl.nblk, item0[s], nitem[s], sl.ps, B->d_scal + s};
+    }
+    // Persistent schedule: one iteration's work items in (phase, slot, chunk) order.
+    std::vector<Work> work;
+    if (B->cfg.schedule == HS_BATCH_PERSISTENT) {
+        for (int32_t ph = 0; ph < 4; ++ph)
+            for (int32_t s : active) {
+                const hs_batch_slot& sl = B->slots[(size_t)s];
+                if (ph == 2) {
+                    for (int32_t g = 0; g < nitem[(size_t)s]; g += kPW * kGPW)
+                        work.push_back(Work{s, 2, (int16_t)(g == 0), item0[(size_t)s] + g,
+                                            std::min<int32_t>(kPW * kGPW, nitem[(size_t)s] - g)});
+                } else {
+                    for (int32_t b = 0; b < sl.nblk; b += kPairs)
+                        work.push_back(Work{s, (int16_t)ph, (int16_t)(b == 0), sl.blk0 + b,
+                                            std::min<int32_t>(kPairs, sl.nblk - b)});
+                }
+            }
+        if ((int32_t)work.size() > B->max_work) {
+            cudaFree(B->d_work);
+            B->d_work = nullptr;
+            B->max_work = std::max<int32_t>((int32_t)work.size() * 2, 4096);
+            HS_CUDA(cudaMalloc(&B->d_work, sizeof(Work) * B->max_work));
+        }
     }
     if ((int32_t)map.size() > B->max_blocks || (int32_t)items.size() > B->max_items) {
         cudaFree(B->d_map);
@@ -666,9 +1240,16 @@ int rebuild(hs_batch* B) {
         HS_CUDA(cudaMemcpyAsync(B->d_active, active.data(), sizeof(int32_t) * active.size(), cudaMemcpyHostToDevice, st));
     if (!items.empty())
         HS_CUDA(cudaMemcpyAsync(B->d_items, items.data(), sizeof(PrecItem) * items.size(), cudaMemcpyHostToDevice, st));
+    if (!work.empty()) {
+        HS_CUDA(cudaMemcpyAsync(B->d_work, work.data(), sizeof(Work) * work.size(), cudaMemcpyHostToDevice, st));
+        persist_reset<<<1, kT, 0, st>>>(B->d_ctl, B->d_scal, B->d_active, (int32_t)active.size());
+        hs::count_launch();
+        HS_CUDA(cudaGetLastError());
+    }
     HS_CUDA(cudaStreamSynchronize(st));   // host vectors above go out of scope
     B->nblocks = (int32_t)map.size();
     B->nactive = (int32_t)active.size();
+    B->nwork = (int32_t)work.size();
     if (B->exec) {
         cudaGraphExecDestroy(B->exec);
         B->exec = nullptr;
@@ -678,6 +1259,37 @@ int rebuild(hs_batch* B) {
         B->graph = nullptr;
     }
     B->dirty = false;
+    return HS_OK;
+}
+
+// The persistent kernel's shared memory and resident CTAs (before any capture).
+int prepare_persistent(hs_batch* B) {
+    const size_t smem = (size_t)kPW * kPWarpBytes;
+    if (int rc = hs::ensure_dynamic_smem((const void*)batch_persistent_kernel, (int)smem)) return rc;
+    if (!B->pers_grid) {
+        int per_sm = 0;
+        HS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_persistent_kernel, kT, smem));
+        B->pers_grid = std::max(1, per_sm) * hs::num_sms();
+    }
+    return HS_OK;
+}
+
+// `iters` iterations of every active slot: one persistent launch (several only
+// when the ticket count would pass 2^30).
+int enqueue_persistent(hs_batch* B, int32_t iters, cudaStream_t st) {
+    const size_t smem = (size_t)kPW * kPWarpBytes;
+    const int32_t kmax = (int32_t)std::max<int64_t>(1, ((int64_t)1 << 30) / std::max<int32_t>(B->nwork, 1));
+    for (int32_t done = 0; done < iters;) {
+        const int32_t k = std::min(iters - done, kmax);
+        const int64_t tickets = ((int64_t)B->nwork * k + kTake - 1) / kTake;
+        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(tickets, B->pers_grid));
+        batch_persistent_kernel<<<grid, kT, smem, st>>>(B->d_work, B->nwork, k, B->d_slots, B->d_active, B->nactive,
+                                                       B->d_map, B->d_items, B->d_partials, B->d_rzpart, B->d_scal,
+                                                       B->d_ctl, B->cfg.maxit, B->err);
+        hs::count_launch();
+        HS_LAUNCH_CHECK("batch_persistent_kernel");
+        done += k;
+    }
     return HS_OK;
 }
 
@@ -736,6 +1348,8 @@ int hs_batch_create(const hs_batch_config* cfg, void* stream, hs_batch** out) {
     if (cfg->max_slots < 1 || cfg->max_slots > 4096) return hs::set_error(HS_ERR_ARG, "max_slots out of range");
     if (cfg->hbm_budget <= 0) return hs::set_error(HS_ERR_ARG, "hbm_budget must be positive");
     if (cfg->maxit < 1) return hs::set_error(HS_ERR_ARG, "maxit must be positive");
+    if (cfg->schedule != HS_BATCH_PERSISTENT && cfg->schedule != HS_BATCH_SEGMENTED)
+        return hs::set_error(HS_ERR_ARG, "schedule must be HS_BATCH_PERSISTENT or HS_BATCH_SEGMENTED");
     hs_batch* B = new hs_batch();
     B->cfg = *cfg;
     B->slots.resize(cfg->max_slots);
@@ -748,10 +1362,14 @@ int hs_batch_create(const hs_batch_config* cfg, void* stream, hs_batch** out) {
         (e = cudaMalloc(&B->d_slots, sizeof(SlotDev) * cfg->max_slots)) ||
         (e = cudaMalloc(&B->d_scal, sizeof(Scalars) * cfg->max_slots)) ||
         (e = cudaMalloc(&B->d_active, sizeof(int32_t) * cfg->max_slots)) ||
-        (e = cudaMalloc(&B->d_init, sizeof(double) * 4 * hsdev::kRedMaxBlocks))) {
-        delete B;
+        (e = cudaMalloc(&B->d_init, sizeof(double) * 4 * hsdev::kRedMaxBlocks)) ||
+        (e = cudaMalloc(&B->d_ctl, sizeof(int32_t) * (kCtl + 2 * (size_t)cfg->max_slots))) ||
+        (e = cudaMallocHost(&B->h_ctl, sizeof(int32_t)))) {
+        hs_batch_destroy(B);
         return hs::cuda_error(e, "hs_batch_create");
     }
+    B->h_ctl[0] = 0;
+    cudaMemset(B->d_ctl, 0, sizeof(int32_t) * (kCtl + 2 * (size_t)cfg->max_slots));
     cudaMemset(B->d_scal, 0, sizeof(Scalars) * cfg->max_slots);
     // Reserve the budget (at most 90 % of the free memory) in the stream-ordered
     // pool the slots allocate from, so admissions take memory the pool holds
@@ -884,7 +1502,27 @@ int hs_batch_launch(hs_batch* B, int32_t iters) {
         B->pending_admission = false;
     }
     if (B->dirty && (rc = rebuild(B))) return rc;
-    if (B->nactive > 0) {
+    if (B->nactive > 0 && B->cfg.schedule == HS_BATCH_PERSISTENT) {
+        // one persistent launch for all `iters` iterations, captured once per
+        // active set and iteration count
+        if (!B->exec || B->exec_iters != iters) {
+            if (B->exec) cudaGraphExecDestroy(B->exec);
+            if (B->graph) cudaGraphDestroy(B->graph);
+            B->exec = nullptr;
+            B->graph = nullptr;
+            if ((rc = prepare_persistent(B))) return rc;
+            cudaStream_t st = B->solve;
+            HS_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            rc = enqueue_persistent(B, iters, st);
+            cudaError_t ce = cudaStreamEndCapture(st, &B->graph);
+            if (rc) return rc;
+            HS_CUDA(ce);
+            HS_CUDA(cudaGraphInstantiate(&B->exec, B->graph, 0));
+            B->exec_iters = iters;
+        }
+        HS_CUDA(cudaGraphLaunch(B->exec, B->solve));
+        B->iterations_run += iters;
+    } else if (B->nactive > 0) {
         if (!B->exec) {
             // warm launch (kernel attributes), then capture one iteration
             cudaStream_t st = B->solve;
@@ -906,6 +1544,7 @@ int hs_batch_launch(hs_batch* B, int32_t iters) {
     for (auto& sl : B->slots) sl.launched = sl.state == 1;
     HS_CUDA(cudaMemcpyAsync(B->h_scal, B->d_scal, sizeof(Scalars) * B->slots.size(), cudaMemcpyDeviceToHost,
                             B->solve));
+    HS_CUDA(cudaMemcpyAsync(B->h_ctl, B->d_ctl + 2, sizeof(int32_t), cudaMemcpyDeviceToHost, B->solve));
     HS_CUDA(cudaEventRecord(B->launched, B->solve));
     B->inflight = true;
     return HS_OK;
@@ -917,6 +1556,14 @@ int hs_batch_wait(hs_batch* B, int32_t* finished) {
     if (B->inflight) {
         B->inflight = false;
         HS_CUDA(cudaEventSynchronize(B->launched));
+        if (B->h_ctl[0]) {   // a bounded wait of the persistent launch ran out
+            B->h_ctl[0] = 0;
+            HS_CUDA(cudaMemsetAsync(B->d_ctl + 2, 0, sizeof(int32_t), B->solve));
+            HS_CUDA(cudaStreamSynchronize(B->solve));
+            B->dirty = true;
+            return hs::set_error(HS_ERR_TIMEOUT,
+                                 "batched launch: a device-side wait ran out; the active systems' iterates are undefined");
+        }
         for (size_t s = 0; s < B->slots.size(); ++s) {
             hs_batch_slot& sl = B->slots[s];
             if (sl.state == 1 && sl.launched && B->h_scal[s].done) {
@@ -980,13 +1627,15 @@ int hs_batch_destroy(hs_batch* B) {
     if (B->exec) cudaGraphExecDestroy(B->exec);
     if (B->graph) cudaGraphDestroy(B->graph);
     void* ptrs[] = {B->d_slots, B->d_scal, B->d_map, B->d_active, B->d_items, B->d_partials, B->d_rzpart,
-                    B->d_init};
-    for (void* p : ptrs) cudaFree(p);
-    cudaStreamDestroy(B->solve);
-    cudaStreamDestroy(B->setup);
+                    B->d_init, B->d_work, B->d_ctl};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (B->solve) cudaStreamDestroy(B->solve);
+    if (B->setup) cudaStreamDestroy(B->setup);
     if (B->launched) cudaEventDestroy(B->launched);
     if (B->admitted) cudaEventDestroy(B->admitted);
     if (B->h_scal) cudaFreeHost(B->h_scal);
+    if (B->h_ctl) cudaFreeHost(B->h_ctl);
     delete B;
     return HS_OK;
 }

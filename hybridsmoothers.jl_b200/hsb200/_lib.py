@@ -19,6 +19,7 @@ HS_SWEEP_FORWARD, HS_SWEEP_BACKWARD, HS_SWEEP_SYMMETRIC = 0, 1, 2
 HS_CACHE_PACKED, HS_CACHE_VIEW = 0, 1
 HS_EIG_POWER, HS_EIG_LANCZOS = 0, 1
 HS_PREC_NONE, HS_PREC_L1GS, HS_PREC_CHEB = 0, 1, 2
+HS_BATCH_PERSISTENT, HS_BATCH_SEGMENTED = 0, 1
 
 
 class HSError(RuntimeError):
@@ -65,7 +66,7 @@ class hs_solve_info(C.Structure):
 
 class hs_batch_config(C.Structure):
     _fields_ = [("max_slots", C.c_int32), ("hbm_budget", C.c_int64), ("partsize", C.c_int32), ("rtol", C.c_double),
-                ("maxit", C.c_int32)]
+                ("maxit", C.c_int32), ("schedule", C.c_int32)]
 
 
 class hs_batch_result(C.Structure):

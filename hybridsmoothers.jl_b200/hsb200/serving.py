@@ -3,8 +3,9 @@ reference, whose callers solve one system at a time through LinearSolve).
 
 * ``BatchEngine`` wraps the C engine (``hs_batch_*``): each admitted system
   keeps its FP64 matrix, an FP32 L1GS SymmetricSweep packed preconditioner and
-  its PCG state in HBM; one ``step`` advances every active system with one set
-  of graph-captured launches.  Admission is refused while no slot or not enough
+  its PCG state in HBM; one ``step`` advances every active system with one
+  graph-captured persistent launch (or, ``schedule="segmented"``, a graph of
+  separate launches per iteration).  Admission is refused while no slot or not enough
   of the HBM budget is free.
 * ``serve`` replays a timed request stream with continuous batching: requests
   that arrive while others are on the GPU are admitted as slots and memory free
@@ -29,11 +30,22 @@ from ._lib import check, lib
 from ._lib import hs_batch_config, hs_batch_info, hs_batch_result  # noqa: E402
 
 
+SCHEDULES = {"persistent": _L.HS_BATCH_PERSISTENT, "segmented": _L.HS_BATCH_SEGMENTED}
+
+
 class BatchEngine:
-    def __init__(self, max_slots=64, hbm_budget=64 << 30, partsize=16, rtol=1e-8, maxit=5000):
+    """schedule: "persistent" (one persistent kernel per launch runs all its
+    iterations of all systems, work items from a device queue) or "segmented"
+    (a replayed CUDA graph of separate launches per iteration); the iterates
+    are identical."""
+
+    def __init__(self, max_slots=64, hbm_budget=64 << 30, partsize=16, rtol=1e-8, maxit=5000,
+                 schedule="persistent"):
         import torch
         torch.cuda.init()
-        cfg = hs_batch_config(max_slots, int(hbm_budget), partsize, rtol, maxit)
+        if schedule not in SCHEDULES:
+            raise ValueError(f"schedule must be one of {sorted(SCHEDULES)}")
+        cfg = hs_batch_config(max_slots, int(hbm_budget), partsize, rtol, maxit, SCHEDULES[schedule])
         self._h = C.c_void_p()
         self._destroy = lib().hs_batch_destroy   # usable in __del__ at interpreter exit
         check(lib().hs_batch_create(C.byref(cfg), None, C.byref(self._h)))

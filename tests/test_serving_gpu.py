@@ -187,3 +187,65 @@ def test_admission_during_launch_reuses_slot():
     alone.close()
     assert res[2] == ref[1]
     np.testing.assert_array_equal(res[1], ref[0])
+
+
+def _finish_all(eng, count, iters, limit=3000):
+    res = {}
+    for _ in range(limit):
+        eng.step(iters)
+        for tag, x, it, ok, rel in eng.poll():
+            res[tag] = (x.copy(), it, ok, rel)
+        if len(res) == count:
+            break
+    return res
+
+
+@pytest.mark.parametrize("maxit", [5000, 7])
+def test_persistent_schedule_matches_segmented(maxit):
+    """The persistent launch (one kernel per launch, work items from a device
+    queue, each system's phases ordered by its own stage counter) and the
+    segmented graph run the same arithmetic: solutions, iteration counts and
+    flags are identical -- systems of all three partsizes, admitted in two
+    waves, and (maxit 7) an iteration cap that stops every system."""
+    reqs = small_stream(7, seed=31)
+    out = {}
+    for sched in ("persistent", "segmented"):
+        eng = serving.BatchEngine(max_slots=8, maxit=maxit, schedule=sched)
+        for i in range(4):
+            assert eng.submit(reqs[i][1], reqs[i][2], i, (8, 16, 32)[i % 3])
+        eng.step(3)
+        for i in range(4, 7):
+            assert eng.submit(reqs[i][1], reqs[i][2], i, (8, 16, 32)[i % 3])
+        out[sched] = _finish_all(eng, len(reqs), 6)
+        assert eng.info().active == 0
+        eng.close()
+    assert len(out["persistent"]) == len(reqs) == len(out["segmented"])
+    for i in range(len(reqs)):
+        xp, itp, okp, relp = out["persistent"][i]
+        xs, its, oks, rels = out["segmented"][i]
+        assert (itp, okp, relp) == (its, oks, rels)
+        np.testing.assert_array_equal(xp, xs)
+        if maxit == 7:
+            assert itp == 7 and not okp
+        else:
+            assert okp and relp <= 1e-8
+
+
+@pytest.mark.parametrize("schedule", ["persistent", "segmented"])
+def test_zero_rhs_finishes_at_admission(schedule):
+    """b = 0 is solved by x = 0 at admission (0 iterations) while another
+    system iterates beside it."""
+    (_, A, b), = small_stream(1, seed=2)
+    eng = serving.BatchEngine(max_slots=2, schedule=schedule)
+    assert eng.submit(A, np.zeros_like(b), 0, 8)
+    assert eng.submit(A, b, 1, 16)
+    res = _finish_all(eng, 2, 8)
+    eng.close()
+    x0, it0, ok0, rel0 = res[0]
+    assert it0 == 0 and ok0 and not np.any(x0)
+    assert res[1][2] and true_relres(A, res[1][0], b) <= 5e-8
+
+
+def test_schedule_argument_checked():
+    with pytest.raises(ValueError):
+        serving.BatchEngine(max_slots=1, schedule="fused")
