@@ -183,28 +183,6 @@ __global__ void __launch_bounds__(kT, 4) pcg_spmv_dot_sliced(int32_t n, const in
     store_dd(partials, part);
 }
 
-__global__ void __launch_bounds__(kT, 5) pcg_spmv_dot(int32_t n, const int32_t* __restrict__ rp,
-                                                  const int32_t* __restrict__ ci, const double* __restrict__ v,
-                                                  const double* __restrict__ p, double* __restrict__ q,
-                                                  const PcgScalars* __restrict__ s, double* __restrict__ partials) {
-    __shared__ double wbuf[kT / 32][hsdev::kWarpCap];
-    DD part{0.0, 0.0};
-    if (!s->done) {
-        const int warp = threadIdx.x >> 5;
-        auto fp = [&](int32_t j) { return __ldg(p + j); };
-        for (int64_t row0 = ((int64_t)blockIdx.x * (kT / 32) + warp) * 32; row0 < n;
-             row0 += (int64_t)gridDim.x * kT) {
-            const double acc = hsdev::csr_warp_fold(wbuf[warp], n, rp, ci, v, row0, 0.0, fp, hsdev::AddOp<double>());
-            const int64_t r = row0 + (threadIdx.x & 31);
-            if (r < n) {
-                q[r] = acc;
-                hsdev::dd_add_prod(part, p[r], acc);
-            }
-        }
-    }
-    store_dd(partials, part);
-}
-
 // alpha = r.z / p.q (every block sums the partials itself, in the same order,
 // so every block holds the same alpha); x += alpha p; r -= alpha q; partials
 // of r.r.  Skipped (r.r only) once converged.

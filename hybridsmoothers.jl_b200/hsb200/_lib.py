@@ -19,7 +19,7 @@ HS_SWEEP_FORWARD, HS_SWEEP_BACKWARD, HS_SWEEP_SYMMETRIC = 0, 1, 2
 HS_CACHE_PACKED, HS_CACHE_VIEW = 0, 1
 HS_EIG_POWER, HS_EIG_LANCZOS = 0, 1
 HS_PREC_NONE, HS_PREC_L1GS, HS_PREC_CHEB = 0, 1, 2
-HS_BATCH_PERSISTENT, HS_BATCH_SEGMENTED = 0, 1
+HS_BATCH_SEGMENTED, HS_BATCH_PERSISTENT = 0, 1
 
 
 class HSError(RuntimeError):

@@ -3,9 +3,9 @@ reference, whose callers solve one system at a time through LinearSolve).
 
 * ``BatchEngine`` wraps the C engine (``hs_batch_*``): each admitted system
   keeps its FP64 matrix, an FP32 L1GS SymmetricSweep packed preconditioner and
-  its PCG state in HBM; one ``step`` advances every active system with one
-  graph-captured persistent launch (or, ``schedule="segmented"``, a graph of
-  separate launches per iteration).  Admission is refused while no slot or not enough
+  its PCG state in HBM; one ``step`` advances every active system with a
+  replayed CUDA graph of per-phase launches (or, ``schedule="persistent"``,
+  one graph-captured persistent launch for all the step's iterations).  Admission is refused while no slot or not enough
   of the HBM budget is free.
 * ``serve`` replays a timed request stream with continuous batching: requests
   that arrive while others are on the GPU are admitted as slots and memory free
@@ -34,13 +34,13 @@ SCHEDULES = {"persistent": _L.HS_BATCH_PERSISTENT, "segmented": _L.HS_BATCH_SEGM
 
 
 class BatchEngine:
-    """schedule: "persistent" (one persistent kernel per launch runs all its
-    iterations of all systems, work items from a device queue) or "segmented"
-    (a replayed CUDA graph of separate launches per iteration); the iterates
-    are identical."""
+    """schedule: "segmented" (a replayed CUDA graph of separate launches per
+    iteration, each phase at its own occupancy; the faster) or "persistent"
+    (one persistent kernel per launch runs all its iterations of all systems,
+    work items from a device queue); the iterates are bitwise identical."""
 
     def __init__(self, max_slots=64, hbm_budget=64 << 30, partsize=16, rtol=1e-8, maxit=5000,
-                 schedule="persistent"):
+                 schedule="segmented"):
         import torch
         torch.cuda.init()
         if schedule not in SCHEDULES:

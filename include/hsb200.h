@@ -282,21 +282,23 @@ int hs_gmres_krylovjl(hs_matrix* A, int32_t prec_type, void* prec, int32_t memor
 /* enough of the HBM budget are free.                                      */
 /* ---------------------------------------------------------------------- */
 typedef struct hs_batch_s hs_batch;
-/* How a launch runs the iterations (identical iterates either way):        */
-/*   HS_BATCH_PERSISTENT  one persistent kernel runs every iteration of the  */
-/*                        launch for all systems; CTAs take work items from  */
-/*                        a device queue and a system's phases wait on its   */
-/*                        own stage counter (bounded waits: HS_ERR_TIMEOUT)  */
-/*   HS_BATCH_SEGMENTED   one CUDA graph of 7 + (partsize classes) launches  */
-/*                        per iteration, replayed                            */
-enum { HS_BATCH_PERSISTENT = 0, HS_BATCH_SEGMENTED = 1 };
+/* How a launch runs the iterations (bitwise identical iterates):           */
+/*   HS_BATCH_SEGMENTED   (default) one CUDA graph of 7 + (partsize classes) */
+/*                        launches per iteration, replayed; each phase runs  */
+/*                        at its own occupancy                               */
+/*   HS_BATCH_PERSISTENT  one persistent kernel (captured in a graph) runs   */
+/*                        every iteration of the launch for all systems;     */
+/*                        CTAs take work items from a device queue and a     */
+/*                        system's phases wait on its own stage word         */
+/*                        (bounded waits: HS_ERR_TIMEOUT)                    */
+enum { HS_BATCH_SEGMENTED = 0, HS_BATCH_PERSISTENT = 1 };
 typedef struct {
     int32_t max_slots;     /* systems resident at once */
     int64_t hbm_budget;    /* bytes the batch may hold on the device */
     int32_t partsize;      /* default partsize (8, 16 or 32) */
     double rtol;           /* ||r|| <= rtol ||b|| */
     int32_t maxit;         /* per-system iteration cap */
-    int32_t schedule;      /* HS_BATCH_PERSISTENT or HS_BATCH_SEGMENTED */
+    int32_t schedule;      /* HS_BATCH_SEGMENTED or HS_BATCH_PERSISTENT */
 } hs_batch_config;
 typedef struct {
     int64_t tag;

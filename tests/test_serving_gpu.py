@@ -61,11 +61,12 @@ def test_batch_solves_match_single(ps):
     eng.close()
 
 
-def test_same_result_alone_and_in_mix():
+@pytest.mark.parametrize("schedule", ["segmented", "persistent"])
+def test_same_result_alone_and_in_mix(schedule):
     reqs = small_stream(8, seed=11)
     target = reqs[3]
     # alone
-    eng = serving.BatchEngine(max_slots=8)
+    eng = serving.BatchEngine(max_slots=8, schedule=schedule)
     eng.submit(target[1], target[2], 0, 16)
     alone = None
     while alone is None:
@@ -74,7 +75,7 @@ def test_same_result_alone_and_in_mix():
             alone = (x.copy(), it)
     eng.close()
     # in a mix, admitted after others are already iterating
-    eng = serving.BatchEngine(max_slots=8)
+    eng = serving.BatchEngine(max_slots=8, schedule=schedule)
     for i in (0, 1, 2):
         eng.submit(reqs[i][1], reqs[i][2], 100 + i, (8, 16, 32)[i % 3])
     eng.step(3)
@@ -148,14 +149,15 @@ def test_autotuner_picks_a_candidate():
     assert tuner.choose(A) == (ps, cache, tpp)   # cached by matrix class
 
 
-def test_admission_during_launch_reuses_slot():
+@pytest.mark.parametrize("schedule", ["segmented", "persistent"])
+def test_admission_during_launch_reuses_slot(schedule):
     """A system submitted while a launch is in flight, into the slot a
     finished system just left, joins at the next launch: the in-flight copy
     of that slot's scalars (the previous occupant's, converged) must not mark
     it finished, and its result equals the alone result bitwise."""
     reqs = small_stream(2, seed=23)
     (_, A1, b1), (_, A2, b2) = reqs
-    eng = serving.BatchEngine(max_slots=1)
+    eng = serving.BatchEngine(max_slots=1, schedule=schedule)
     assert eng.submit(A1, b1, 1, 8)
     first = None
     while first is None:
@@ -177,7 +179,7 @@ def test_admission_during_launch_reuses_slot():
             break
     eng.close()
     assert res is not None and res[0] == 2 and res[3]
-    alone = serving.BatchEngine(max_slots=1)
+    alone = serving.BatchEngine(max_slots=1, schedule=schedule)
     alone.submit(A2, b2, 0, 8)
     ref = None
     while ref is None:
