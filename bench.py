@@ -44,6 +44,8 @@ def parse_args():
     ap.add_argument("--workload", default="poisson128-l1gs-sym-packed-ps16")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="time the K applies as K separate calls instead of one CUDA graph replay")
     ap.add_argument("--soak-s", type=float, default=1.0, help="untimed load before timing, for clock samples")
     ap.add_argument("--suite", default=None,
                     help="secondary measurements instead of the headline line: pcg1d, pcg128, gmres96, mixed160, "
@@ -716,20 +718,50 @@ def main():
             P.apply(xd, yd)
         torch.cuda.synchronize()
 
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    launches0 = hsb200.kernel_launches()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    for _ in range(args.steps):
-        P.apply(xd, yd)
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    launches = hsb200.kernel_launches() - launches0
-    ms = ev0.elapsed_time(ev1)
+    # The K timed applies are one CUDA graph (captured once, replayed once in
+    # the timed region): the same K kernels, without the host's per-call launch
+    # path between them.  The per-call loop is timed too and reported beside.
+    graph = None
+    if not args.no_graph:
+        graph = torch.cuda.CUDAGraph()
+        l0 = hsb200.kernel_launches()
+        with torch.cuda.graph(graph, capture_error_mode="thread_local"):
+            for _ in range(args.steps):
+                P.apply(xd, yd)
+        graph_launches = hsb200.kernel_launches() - l0
+        graph.replay()   # untimed
+        torch.cuda.synchronize()
+
+    def timed(use_graph):
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        l0 = hsb200.kernel_launches()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        if use_graph:
+            graph.replay()
+        else:
+            for _ in range(args.steps):
+                P.apply(xd, yd)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        nl = graph_launches if use_graph else hsb200.kernel_launches() - l0
+        return e0.elapsed_time(e1), nl
+
+    ms_calls, launches_calls = timed(False)
+    if graph is not None:
+        ms, launches = timed(True)
+    else:
+        ms, launches = ms_calls, launches_calls
     clocks.stop()
+    if world > 1:
+        t = torch.tensor([ms_calls], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_calls = float(t.item())
+    config["launch"] = ("one CUDA graph of the K applies" if graph is not None else "K separate calls")
+    config["ms_per_step_separate_calls"] = round(ms_calls / args.steps, 5)
     if world > 1:
         t = torch.tensor([ms], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
