@@ -33,11 +33,6 @@ struct L1gsView {
     int32_t sdt, sweep, cache;
 };
 int l1gs_view_of(const hs_l1gs* P, L1gsView* v);
-// hs_l1gs_apply on FP64 vectors that also leaves the compensated partial sums
-// of x.y, one pair per warp, in dotp when the launch supports it and its warps
-// fit in `cap` pairs; *nslots = the pairs written, or 0.
-int l1gs_apply_dot(hs_l1gs* P, const double* x, double* y, cudaStream_t st, double* dotp, int32_t cap,
-                   int32_t* nslots);
 // Symmetric packed-cache L1GS built from a device CSR matrix (read during the
 // call only; for a symmetric matrix its rows are the CSC columns isSymA reads).
 int l1gs_create_from_matrix(const hs_matrix* M, int32_t partsize, double eta, int32_t sweep, int32_t smoother_dtype,

@@ -111,11 +111,11 @@ __device__ __forceinline__ double sum_partials_all(const double* __restrict__ pa
 
 // kjl: Krylov.jl's stopping test (sqrt(r.z) <= atol + rtol sqrt(r0.z0)),
 // else ||r|| <= rtol ||b||.
-__global__ void pcg_init_scalars(const double* __restrict__ partials_bb, int nb, const double* __restrict__ partials_rz,
-                                 int nrz, PcgScalars* s, double rtol, double atol, int kjl) {
+__global__ void pcg_init_scalars(const double* __restrict__ partials_bb, const double* __restrict__ partials_rz,
+                                 int nb, PcgScalars* s, double rtol, double atol, int kjl) {
     const double bb = sum_partials(partials_bb, nb);
     __syncthreads();
-    const double rz = sum_partials(partials_rz, nrz);
+    const double rz = sum_partials(partials_rz, nb);
     if (threadIdx.x == 0) {
         s->bb = bb;
         s->rr = bb;
@@ -148,9 +148,11 @@ __global__ void kjl_check(const double* __restrict__ partials, int nb, PcgScalar
     }
 }
 
+// q = A p (storage-order rows, bitwise mul!) and compensated partials of p.q.
+// A warp owns 32 rows at a time (warp CSR-stream), warps stride over the matrix.
 // q = A p with the p.q partials over the matrix's 32-row slices (spmv.cuh):
-// the same row sums bit for bit as mul!'s storage-order CSR fold, with each
-// lane's row entries loaded eight at a time.  Each warp takes every (grid x 8)-th
+// the same row sums bit for bit as the CSR kernel below, with each lane's
+// row entries loaded eight at a time.  Each warp takes every (grid x 8)-th
 // slice; the next slice's bounds are loaded one slice ahead.
 __global__ void __launch_bounds__(kT, 4) pcg_spmv_dot_sliced(int32_t n, const int64_t* __restrict__ soff,
                                                          const int32_t* __restrict__ scol,
@@ -184,14 +186,11 @@ __global__ void __launch_bounds__(kT, 4) pcg_spmv_dot_sliced(int32_t n, const in
 // alpha = r.z / p.q (every block sums the partials itself, in the same order,
 // so every block holds the same alpha); x += alpha p; r -= alpha q; partials
 // of r.r.  Skipped (r.r only) once converged.
-// With `arrivals` (the convergence test of this library's PCG): the block
-// that finishes last sums the r.r partials -- in pcg_check's order -- and
-// applies the test, so no separate check launch follows.
 __global__ void __launch_bounds__(kT) pcg_update(int64_t n, PcgScalars* __restrict__ s, const double* __restrict__ ppq,
                                                  int npq, const double* __restrict__ prz, int nrz,
                                                  const double* __restrict__ p, const double* __restrict__ q,
                                                  double* __restrict__ x, double* __restrict__ r,
-                                                 double* __restrict__ partials, int32_t* arrivals) {
+                                                 double* __restrict__ partials) {
     const bool done = s->done;
     const double rz = sum_partials_all(prz, nrz);
     const double pq = sum_partials_all(ppq, npq);
@@ -230,30 +229,17 @@ __global__ void __launch_bounds__(kT) pcg_update(int64_t n, PcgScalars* __restri
         }
     }
     store_dd(partials, v);
-    if (!arrivals) return;
-    __shared__ int last;
+}
+
+__global__ void pcg_check(const double* __restrict__ partials, int nb, PcgScalars* s) {
+    const double rr = sum_partials(partials, nb);
     if (threadIdx.x == 0) {
-        __threadfence();   // this block's partial, before its arrival
-        last = atomicAdd(arrivals, 1) == (int)gridDim.x - 1;
-        __threadfence();
-    }
-    __syncthreads();
-    if (!last) return;
-    // partials written in this launch: L2 loads, pcg_check's order
-    DD w{0.0, 0.0};
-    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x)
-        w = hsdev::dd_add(w, DD{__ldcg(partials + 2 * i), __ldcg(partials + 2 * i + 1)});
-    const double rr = hsdev::dd_value(hsdev::block_dd(w));
-    if (threadIdx.x == 0) {
-        *arrivals = 0;   // for the next iteration
-        volatile PcgScalars* vs = s;
-        if (!vs->done) {
-            const int32_t it = vs->it + 1;
-            vs->it = it;
-            vs->rr = rr;
-            if (sqrt(rr) <= __dmul_rn(vs->rtol, sqrt(vs->bb))) {
-                vs->done = 1;
-                vs->conv_it = it;
+        if (!s->done) {
+            s->it += 1;
+            s->rr = rr;
+            if (sqrt(rr) <= __dmul_rn(s->rtol, sqrt(s->bb))) {
+                s->done = 1;
+                s->conv_it = s->it;
             }
         }
     }
@@ -561,10 +547,7 @@ int pcg_impl(hs_matrix* A, int32_t prec_type, void* prec, const double* b, doubl
         }
     } rejoin{own, caller, join};
     const int64_t n = hs::matrix_n(A);
-    // r z p q, three partial arrays, the preconditioner's r.z pairs (kDotCap),
-    // the arrivals counter of the fused check, the scalars
-    constexpr int32_t kDotCap = 4096;
-    const int64_t need = 4 * n + 6 * hsdev::kRedMaxBlocks + 2 * kDotCap + 2 + (int64_t)(sizeof(PcgScalars) / 8 + 1);
+    const int64_t need = 4 * n + 6 * hsdev::kRedMaxBlocks + 2 + (int64_t)(sizeof(PcgScalars) / 8 + 1);
     if (ws.cap < need) {
         if (ws.base) {
             HS_CUDA(cudaStreamSynchronize(own));   // earlier solves on this device may still read it
@@ -582,9 +565,7 @@ int pcg_impl(hs_matrix* A, int32_t prec_type, void* prec, const double* b, doubl
     double* pa = q + n;
     double* pb = pa + 2 * hsdev::kRedMaxBlocks;
     double* pc = pb + 2 * hsdev::kRedMaxBlocks;
-    double* pz = pc + 2 * hsdev::kRedMaxBlocks;
-    double* scal = pz + 2 * kDotCap;
-    int32_t* arrivals = reinterpret_cast<int32_t*>(scal + 1);
+    double* scal = pc + 2 * hsdev::kRedMaxBlocks;
     PcgScalars* s = reinterpret_cast<PcgScalars*>(scal + 2);
     int rc;
     const int ge = grid_elems(n), nb = tile_blocks(n);
@@ -608,22 +589,12 @@ int pcg_impl(hs_matrix* A, int32_t prec_type, void* prec, const double* b, doubl
     zero_kernel<<<ge, kT, 0, st>>>(n, x);
     copy_kernel<<<ge, kT, 0, st>>>(n, b, r);
     hs::count_launch(2);
-    HS_CUDA(cudaMemsetAsync(arrivals, 0, sizeof(int32_t), st));
-    // This library's PCG with an L1GS preconditioner: the apply leaves the
-    // r.z partials itself where its kernel can (one pair per warp, in pz),
-    // so no separate dot pass follows it.
-    const bool fuse_rz = !kjl && prec_type == HS_PREC_L1GS;
-    int32_t nz = 0;
-    if (fuse_rz) rc = hs::l1gs_apply_dot(static_cast<hs_l1gs*>(prec), r, z, st, pz, kDotCap, &nz);
-    else rc = prec_apply(prec_type, prec, r, z, n, st);
-    if (rc) return rc;
-    const double* prz = nz ? pz : pb;   // the r.z partials the update and the p kernel read
-    const int nrz = nz ? nz : nb;
+    if ((rc = prec_apply(prec_type, prec, r, z, n, st))) return rc;
     copy_kernel<<<ge, kT, 0, st>>>(n, z, p);
     dot_kernel<<<nb, kT, 0, st>>>(n, b, b, pa);
-    if (!nz) dot_kernel<<<nb, kT, 0, st>>>(n, r, z, pb);
-    pcg_init_scalars<<<1, kT, 0, st>>>(pa, nb, prz, nrz, s, rtol, atol, kjl ? 1 : 0);
-    hs::count_launch(nz ? 3 : 4);
+    dot_kernel<<<nb, kT, 0, st>>>(n, r, z, pb);
+    pcg_init_scalars<<<1, kT, 0, st>>>(pa, pb, nb, s, rtol, atol, kjl ? 1 : 0);
+    hs::count_launch(4);
     HS_LAUNCH_CHECK("pcg init");
 
     // One iteration as a graph: q = A p with the p.q partials (pa); alpha,
@@ -649,23 +620,14 @@ int pcg_impl(hs_matrix* A, int32_t prec_type, void* prec, const double* b, doubl
             if ((r2 = hs::matrix_spmv(A, p, q, 1.0, 0.0, cs))) return r2;
             dot_kernel<<<nb, kT, 0, cs>>>(n, p, q, pa);
         }
-        // the convergence test rides on the update's last block (this library's PCG)
-        pcg_update<<<nb, kT, 0, cs>>>(n, s, pa, npq, prz, nrz, p, q, x, r, pc, kjl ? nullptr : arrivals);
-        hs::count_launch(2);   // spmv (+dot), update
-        if (nz) {
-            int32_t nz2 = 0;
-            if ((r2 = hs::l1gs_apply_dot(static_cast<hs_l1gs*>(prec), r, z, cs, pz, kDotCap, &nz2))) return r2;
-            if (nz2 != nz) return hs::set_error(HS_ERR_CUDA, "preconditioner launch shape changed within a solve");
-        } else {
-            if ((r2 = prec_apply(prec_type, prec, r, z, n, cs))) return r2;
-            dot_kernel<<<nb, kT, 0, cs>>>(n, r, z, pb);
-            hs::count_launch(1);
-        }
-        if (kjl) {
-            kjl_check<<<1, kT, 0, cs>>>(prz, nrz, s);
-            hs::count_launch(1);
-        }
-        pcg_p<<<nb, kT, 0, cs>>>(n, s, prz, nrz, z, p);   // counted by the check below
+        pcg_update<<<nb, kT, 0, cs>>>(n, s, pa, npq, pb, nb, p, q, x, r, pc);
+        if (!kjl) pcg_check<<<1, kT, 0, cs>>>(pc, nb, s);
+        hs::count_launch(kjl ? 2 : 3);   // spmv (+dot), update, check
+        if ((r2 = prec_apply(prec_type, prec, r, z, n, cs))) return r2;
+        dot_kernel<<<nb, kT, 0, cs>>>(n, r, z, pb);
+        if (kjl) kjl_check<<<1, kT, 0, cs>>>(pb, nb, s);
+        pcg_p<<<nb, kT, 0, cs>>>(n, s, pb, nb, z, p);
+        hs::count_launch(kjl ? 2 : 1);   // dot (+ check); the check below counts pcg_p
         HS_LAUNCH_CHECK("pcg iteration");
         return HS_OK;
     };

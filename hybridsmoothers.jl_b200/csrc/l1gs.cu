@@ -30,7 +30,6 @@
 
 #include "internal.cuh"
 #include "l1gs_coop.cuh"
-#include "reduce.cuh"
 #include "l1gs_seg.cuh"
 
 namespace {
@@ -155,7 +154,6 @@ struct PackedParams {
     int32_t* err;
     uint32_t warp_bytes;
     uint32_t ring_bytes;
-    double* dotp = nullptr;   // if set (compile-time-partsize kernel): per warp, the compensated x.y pair
 };
 
 template <typename T, int E, int STAGES, int SWEEP>
@@ -217,8 +215,7 @@ struct TileRing {
 };
 
 // ---- compile-time partsize: y and D_Dl1 in registers, fully unrolled -------
-// DOT: also leave the warp's compensated x.y pair in p.dotp (Krylov r.z).
-template <typename T, typename IO, int SWEEP, int PS, int E, int STAGES, int MINB, bool DOT = false>
+template <typename T, typename IO, int SWEEP, int PS, int E, int STAGES, int MINB>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, MINB)
     l1gs_packed_small_kernel(const __grid_constant__ CUtensorMap tmL, const __grid_constant__ CUtensorMap tmU,
                              const PackedParams p) {
@@ -249,7 +246,6 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, MINB)
     if (NT > 0) ring.prologue();
 
     int32_t c = 0;  // first tile of the current direction
-    hsdev::DD dot{0.0, 0.0};
     for (int32_t gi = 0; gi < my_groups; ++gi) {
         const int64_t g = ring.g0 + (int64_t)gi * ring.gstride;
         const int64_t k = g * 32 + lane;
@@ -311,21 +307,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, MINB)
         for (int m = 0; m < PS; ++m) {
             const int t = lane + 32 * m;
             const int64_t row = rowbase + t;
-            if (row < p.n) {
-                const IO yo = (IO)xs[(t / PS) * XS + (t % PS)];
-                if (DOT) hsdev::dd_add_prod(dot, (double)x[row], (double)yo);   // x before y: x == y allowed
-                y[row] = yo;
-            }
+            if (row < p.n) y[row] = (IO)xs[(t / PS) * XS + (t % PS)];
         }
         __syncwarp();
-    }
-    if (DOT) {   // the warp's share of x.y (Krylov r.z), one compensated pair
-        dot = hsdev::warp_dd(dot);
-        if (lane == 0 && p.dotp) {
-            const int64_t w = (int64_t)blockIdx.x * wpb + warp;
-            p.dotp[2 * w] = dot.s;
-            p.dotp[2 * w + 1] = dot.c;
-        }
     }
     return;
 timeout:
@@ -1207,9 +1191,6 @@ struct hs_l1gs_s {
     alignas(64) CUtensorMap tmU;
     void* dev_x = nullptr;
     void* dev_y = nullptr;
-    // l1gs_apply_dot: where the launch leaves its x.y pairs (set for one call)
-    double* dot_out = nullptr;
-    int32_t dot_cap = 0, dot_slots = 0;
     // host-buffer apply: streams (copy in, copy out, then 4 apply streams) and
     // chunk events, made on first use
     cudaStream_t hstream[2 + 4] = {};
@@ -1511,7 +1492,7 @@ inline void pick_tile(int ps, int sdt, int* E, int* stages, int* minb) {
 
 template <typename KERN>
 int launch_packed_kernel(KERN kern, hs_l1gs* P, PackedParams& p, int stages, bool balanced, uint32_t extra_bytes,
-                         cudaStream_t st, bool dot_capable = false) {
+                         cudaStream_t st) {
     // per warp: the tile ring, one mbarrier per stage, then the kernel's slice
     p.warp_bytes = (p.ring_bytes + 8 * stages + extra_bytes + 127) / 128 * 128;
     const int wpb = (int)std::max<int64_t>(1, std::min<int64_t>(kWarpsPerBlock, (200 * 1024) / p.warp_bytes));
@@ -1542,12 +1523,6 @@ int launch_packed_kernel(KERN kern, hs_l1gs* P, PackedParams& p, int stages, boo
     }
     const int grid = (int)std::max<int64_t>(
         1, std::min<int64_t>(P->launch_grid, ((int64_t)p.ngroups - p.gbeg + wpb - 1) / wpb));
-    // x.y partials requested (l1gs_apply_dot): one pair per warp of this launch
-    p.dotp = nullptr;
-    if (dot_capable && P->dot_out && (int64_t)grid * wpb <= P->dot_cap) {
-        p.dotp = P->dot_out;
-        P->dot_slots = grid * wpb;
-    }
     kern<<<grid, wpb * 32, smem, st>>>(P->tmL, P->tmU, p);
     HS_LAUNCH_CHECK("l1gs_packed_kernel");
     return HS_OK;
@@ -1570,19 +1545,11 @@ int launch_packed_t(hs_l1gs* P, const void* x, void* y, cudaStream_t st) {
     if (!P->err_word) P->err_word = hs::device_error_word();
     p.err = P->err_word;
     p.ring_bytes = (uint32_t)(E * 32 * sizeof(T) * STAGES);
-    // The x.y variant (l1gs_apply_dot) for symmetric sweeps on FP64 vectors: CG's r.z.
-    constexpr bool kDotable = SWEEP == 2 && sizeof(IO) == 8;
-#define HS_SMALL(PSV, MB)                                                                                   \
-    {                                                                                                       \
-        constexpr int XS = (PSV % 2 == 0) ? PSV + 1 : PSV;                                                  \
-        if constexpr (kDotable) {                                                                           \
-            if (P->dot_out)                                                                                 \
-                return launch_packed_kernel(l1gs_packed_small_kernel<T, IO, SWEEP, PSV, E, STAGES, MB, true>, \
-                                            P, p, STAGES, sizeof(T) == 8, (uint32_t)(32 * XS * sizeof(T)), st, \
-                                            true);                                                          \
-        }                                                                                                   \
-        return launch_packed_kernel(l1gs_packed_small_kernel<T, IO, SWEEP, PSV, E, STAGES, MB>, P, p,       \
-                                    STAGES, sizeof(T) == 8, (uint32_t)(32 * XS * sizeof(T)), st);           \
+#define HS_SMALL(PSV, MB)                                                                                \
+    {                                                                                                    \
+        constexpr int XS = (PSV % 2 == 0) ? PSV + 1 : PSV;                                               \
+        return launch_packed_kernel(l1gs_packed_small_kernel<T, IO, SWEEP, PSV, E, STAGES, MB>, P, p,    \
+                                    STAGES, sizeof(T) == 8, (uint32_t)(32 * XS * sizeof(T)), st);        \
     }
     if constexpr (STAGES == 4) {
         switch (P->ps) {
@@ -2090,26 +2057,6 @@ int l1gs_create_from_matrix(const hs_matrix* M, int32_t partsize, double eta, in
 void l1gs_destroy_async(hs_l1gs* P, cudaStream_t st) { release(P, st); }
 }  // namespace hs
 
-namespace hs {
-// hs_l1gs_apply on FP64 vectors that also leaves the compensated partial sums
-// of x.y (one pair per warp) in dotp when the launch is the
-// compile-time-partsize packed kernel and its warps fit in `cap` pairs;
-// *nslots = the pairs written, or 0 (the caller computes x.y itself).
-int l1gs_apply_dot(hs_l1gs* P, const double* x, double* y, cudaStream_t st, double* dotp, int32_t cap,
-                   int32_t* nslots) {
-    if (!P || !nslots) return hs::set_error(HS_ERR_ARG, "l1gs_apply_dot: NULL argument");
-    P->dot_out = dotp;
-    P->dot_cap = cap;
-    P->dot_slots = 0;
-    const int rc = hs_l1gs_apply(P, x, y, HS_F64, st);
-    *nslots = rc ? 0 : P->dot_slots;
-    P->dot_out = nullptr;
-    P->dot_cap = 0;
-    P->dot_slots = 0;
-    return rc;
-}
-}  // namespace hs
-
 extern "C" {
 
 int hs_l1gs_create(const hs_sparse* A, int32_t partsize, int32_t is_sym, double eta, int32_t sweep, int32_t cache,
@@ -2132,7 +2079,6 @@ int hs_l1gs_apply(hs_l1gs* P, const void* x, void* y, int32_t io_dtype, void* st
     if (P->sdt == HS_F32 && io_dtype == HS_F64) return launch_apply<float, double>(P, x, y, st);
     return hs::set_error(HS_ERR_UNSUPPORTED, "FP64 smoother with FP32 vectors is not provided");
 }
-
 
 // Host-buffer apply.  Page-locked (mapped) host vectors are read and written
 // by the apply kernel itself over PCIe: every row of x is read once and every
