@@ -191,6 +191,33 @@ def test_random_bitwise_fp64(ps, n, sweep, cache):
             np.testing.assert_array_equal(P.SUbuffer, ref.SU)
 
 
+# One partition holding the whole matrix (partsize = N, the reference's plain
+# Gauss-Seidel check, test/test_preconditioners.jl:614-709), partsize > N (a
+# single short partition), and matrices of 1 to 7 rows.
+SMALL_CASES = [(50, 50), (50, 64), (1, 16), (2, 2), (3, 16), (33, 32), (7, 256)]
+
+
+@pytest.mark.parametrize("n,ps", SMALL_CASES)
+@pytest.mark.parametrize("sweep", ["forward", "backward", "symmetric"])
+@pytest.mark.parametrize("cache", ["packed", "view"])
+def test_single_partition_and_tiny_n(n, ps, sweep, cache):
+    A = W.poisson_test_matrix(n)
+    x = np.random.default_rng(n * 1000 + ps).uniform(-1, 1, n)
+    ref = O.OracleL1GS(A, ps, isSymA=True, sweep=sweep, cache=cache)
+    want = ref.ldiv(x)
+    # the reference's order (bitwise), then the library's own choice, which
+    # may reorder a row's sum (relative 1e-12, absolute floor 1e-12 max|y|)
+    for order in ("reference", None):
+        P = hsb200.L1GSPrecBuilder(hsb200.CUDABackend(), threads=256, blocks=148)(
+            A, ps, isSymA=True, sweep=SWEEPS[sweep], cache_strategy=CACHES[cache], order=order)
+        np.testing.assert_array_equal(P.D_DL1, ref.D)
+        got = gpu_apply(P, x)
+        if P.order == "reference":
+            np.testing.assert_array_equal(got, want)
+        else:
+            np.testing.assert_allclose(got, want, rtol=1e-12, atol=1e-12 * np.abs(want).max())
+
+
 @pytest.mark.parametrize("ps", [2, 8, 16, 32, 33, 64, 130])
 @pytest.mark.parametrize("sweep", ["forward", "symmetric"])
 @pytest.mark.parametrize("cache", ["packed", "view"])
